@@ -1,0 +1,204 @@
+/*
+ * picard_gpu.h -- C ABI of the B200 (sm_100a) implementation of Picard's
+ * per-timestep particle-in-cell loop.
+ *
+ * The reference (Guardiarch/Picard) is a set of Fortran 90 subroutines called
+ * in a fixed order by `program picard` (picard.f90:554-674).  Every routine on
+ * that path has one entry point here, with the reference subroutine it replaces
+ * cited beside it.  A Fortran host binds these through an `iso_c_binding`
+ * interface module (bind(C, name="...")); a C or C++ host calls them directly.
+ *
+ * State model.  The reference passes its state arrays (real_particles,
+ * int_particles, U, E, N, F, C, D) to every subroutine.  Here the state lives
+ * on the device inside a `picard_ctx`, created once from a `picard_params`
+ * block; the per-subroutine entry points take the context plus the scalars the
+ * reference passes that can change from call to call (dt, iteration, maxerr,
+ * maxit).  Host copies in the reference's own column-major layouts are moved
+ * with picard_gpu_set_particles / picard_gpu_get_particles and
+ * picard_gpu_set_field / picard_gpu_get_field.
+ *
+ * Errors.  The reference has no status reporting.  Every entry point returns a
+ * picard_status; picard_gpu_last_error() gives a message for the last failure
+ * on the calling thread.  No entry point aborts the process.
+ *
+ * Threading.  A context is bound to one CUDA stream; calls on one context must
+ * come from one host thread at a time.  Different contexts are independent.
+ */
+#ifndef PICARD_GPU_H
+#define PICARD_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PICARD_API __attribute__((visibility("default")))
+#else
+#define PICARD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PICARD_MAX_SPECIES 8
+
+typedef enum picard_status {
+  PICARD_OK = 0,
+  PICARD_ERR_BAD_ARG = 1,       /* argument out of range / inconsistent params   */
+  PICARD_ERR_CAPACITY = 2,      /* particle count would exceed max_per_proc       */
+  PICARD_ERR_NOT_CONVERGED = 3, /* Jacobi ran 2*maxit+1 sweeps without converging */
+  PICARD_ERR_TIMEOUT = 4,       /* a bounded device wait gave up                  */
+  PICARD_ERR_CUDA = 5,          /* CUDA runtime error (message has the details)   */
+  PICARD_ERR_STATE = 6          /* call made in the wrong state                   */
+} picard_status;
+
+/* Particle storage on the device.
+ * F64:    SoA FP64 positions and velocities, the reference's arithmetic.  Cell
+ *         indices and the removed/wrapped particle sets match the FP64 oracle
+ *         bit for bit.
+ * CELL32: packed int32 CIC base-node index + FP32 in-cell offset + FP32
+ *         velocity (28 B per particle + 1 B species).  The performance layout. */
+typedef enum picard_layout { PICARD_LAYOUT_F64 = 0, PICARD_LAYOUT_CELL32 = 1 } picard_layout;
+
+/* Jacobi arithmetic.
+ * F64:        every sweep in FP64 (24 B per node per sweep).
+ * F32_REFINE: the iterate is held as an FP64 anchor plus an FP32 increment; the
+ *             FP32 sweeps advance the increment and an FP64 pass folds it into
+ *             the anchor every few sweeps.  Same iterate sequence and stopping
+ *             rule as the FP64 sweeps (12 B per node per sweep). */
+typedef enum picard_solver { PICARD_SOLVER_F64 = 0, PICARD_SOLVER_F32_REFINE = 1 } picard_solver;
+
+/* Fields that can be copied in the reference's layouts (picard.f90:95-113). */
+typedef enum picard_field {
+  PICARD_FIELD_U = 0, /* U(Nx+2,Ny+2,Nz+2)            */
+  PICARD_FIELD_E = 1, /* E(3,Nx+2,Ny+2,Nz+2)          */
+  PICARD_FIELD_N = 2, /* N(species,Nx+2,Ny+2,Nz+2)    */
+  PICARD_FIELD_C = 3, /* C(Nx+2,Ny+2,Nz+2)            */
+  PICARD_FIELD_F = 4, /* F(species,3,Nx+2,Ny+2,Nz+2)  */
+  PICARD_FIELD_D = 5  /* D(2Nx+1,2Ny+1,2Nz+1)         */
+} picard_field;
+
+/* Run parameters.  The first block is what picard.f90:41-302 hard-codes, for a
+ * single domain (iprocs = jprocs = kprocs = 1, so Nx = Nx_local).  Species
+ * index s (0-based) is the reference's species s+1: 0 = electrons, 1 = H+.
+ * Two-index arrays keep the reference's memory order: v0[s][c] is v0(c+1,s+1).
+ * picard_params_derive() fills the second block from the first, following
+ * picard.f90:333-467; like the reference, it also rewrites density[] and ppc[]
+ * (inactive species get 0, electron density and ppc follow quasi-neutrality). */
+typedef struct picard_params {
+  /* ---- inputs ---- */
+  int32_t nx, ny, nz;          /* cells per axis (Nx_local, Ny_local, Nz_local)   */
+  int32_t species;             /* active species, 2..8                            */
+  int32_t max_per_proc;        /* particle capacity                               */
+  int32_t xflow, yflow, zflow; /* nonzero: open axis; zero: periodic axis         */
+  int32_t maxit;               /* Jacobi sweep cap (2*maxit+1 sweeps at most)     */
+  int32_t produce_dt_scaled;   /* 0: ParticlesProduce.f90:70 as written (a rate
+                                  per step); 1: rate multiplied by dt             */
+  int32_t gyration[8], fluid[8];
+  int32_t ppc[8];
+  double xmin, xmax, ymin, ymax, zmin, zmax;
+  double dt, maxerr;
+  double mass[8], charge[8], density[8], kelvin[8];
+  double v0[8][4];
+  double B0[4];
+  double vn[8], Qn[8], nu_i[8], nu_d[8], Ek[8];
+  uint64_t seed;               /* Philox key for every stochastic step            */
+  /* ---- derived (picard_params_derive) ---- */
+  double Lx_min, Lx_max, Ly_min, Ly_max, Lz_min, Lz_max;
+  double dxyz[3], dV;
+  int32_t ipp[8], epp[8], hpp[8];
+  double n2p[8], eta[8];
+  double ve[4], E0[4];
+  double tB[8][4], sB[8][4];
+  double u0;                   /* energy-log normalisation, picard.f90:476-480    */
+} picard_params;
+
+typedef struct picard_ctx picard_ctx;
+
+/* ---------------------------------------------------------------- params */
+
+/* Fill the inputs with the reference defaults of picard.f90:145-302 on one
+ * rank (Nx_local = Ny_local = Nz_local = 30, species = 3). */
+PICARD_API int picard_params_default(picard_params* p);
+
+/* picard.f90:333-467: domain extents, dxyz, dV, quasi-neutral electron density,
+ * ipp/epp/hpp/ppc, n2p, eta, mass-weighted bulk velocity ve, motional field
+ * E0 = -ve x B0, Boris factors tB and sB, energy normalisation u0. */
+PICARD_API int picard_params_derive(picard_params* p);
+
+/* ---------------------------------------------------------------- context */
+
+PICARD_API int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, picard_ctx** out);
+PICARD_API int picard_gpu_destroy(picard_ctx* ctx);
+PICARD_API int picard_gpu_synchronize(picard_ctx* ctx);
+PICARD_API const char* picard_gpu_last_error(void);
+/* Device bytes held by a context created with these arguments (for admission
+ * by memory budget); nothing is allocated. */
+PICARD_API int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver, uint64_t* bytes);
+
+/* Particles in the reference layout: real_particles(8, n) column-major
+ * (x, y, z, vx, vy, vz, tmp, tmp) and int_particles(n) holding the 1-based
+ * species number (picard.f90:74-92). */
+PICARD_API int picard_gpu_set_particles(picard_ctx* ctx, const double* real_particles,
+                             const int32_t* int_particles, int32_t num_local);
+PICARD_API int picard_gpu_get_particles(picard_ctx* ctx, double* real_particles, int32_t* int_particles,
+                             int32_t capacity, int32_t* num_local);
+PICARD_API int picard_gpu_get_num_local(picard_ctx* ctx, int32_t* num_local);
+
+/* Fields in the reference layout (see picard_field). */
+PICARD_API int picard_gpu_get_field(picard_ctx* ctx, int32_t which, double* out);
+PICARD_API int picard_gpu_set_field(picard_ctx* ctx, int32_t which, const double* in);
+
+/* ------------------------------------------- one entry per reference routine */
+
+PICARD_API int picard_gpu_calc_distance(picard_ctx* ctx);                       /* CalcDistance.f90:1-95        */
+PICARD_API int picard_gpu_particles_initialize(picard_ctx* ctx);                /* ParticlesInitialize.f90:2-125*/
+PICARD_API int picard_gpu_bc_inflow(picard_ctx* ctx, int32_t iteration);        /* BCinflow.f90:2-476           */
+PICARD_API int picard_gpu_advance_position(picard_ctx* ctx, double dt);         /* AdvancePosition.f90:4-19     */
+PICARD_API int picard_gpu_particles_produce(picard_ctx* ctx, int32_t iteration);/* ParticlesProduce.f90:1-113   */
+PICARD_API int picard_gpu_bc_outflow(picard_ctx* ctx);                          /* BCoutflow.f90:5-87           */
+PICARD_API int picard_gpu_particles_transfer(picard_ctx* ctx);                  /* ParticlesTransfer.f90:2-614  */
+PICARD_API int picard_gpu_particles_gridify(picard_ctx* ctx);                   /* ParticlesGridify.f90:1-296   */
+PICARD_API int picard_gpu_particles_gridify_all(picard_ctx* ctx);               /* ParticlesGridifyAll.f90:1-455*/
+PICARD_API int picard_gpu_bc_potentials(picard_ctx* ctx);                       /* BCpotentials.f90:1-145       */
+/* Returns PICARD_ERR_NOT_CONVERGED after 2*maxit+1 sweeps (the reference only
+ * prints "Maximum iteration reached!", CalcEpotential.f90:67-69); U holds the
+ * last iterate either way.  *sweeps receives the number of sweeps done. */
+PICARD_API int picard_gpu_calc_epotential(picard_ctx* ctx, double maxerr, int32_t maxit,
+                               int32_t* sweeps);                     /* CalcEpotential.f90:4-246     */
+PICARD_API int picard_gpu_calc_efield(picard_ctx* ctx);                         /* CalcEfield.f90:3-232         */
+PICARD_API int picard_gpu_bc_fields(picard_ctx* ctx);                           /* BCfields.f90:3-94            */
+PICARD_API int picard_gpu_advance_velocity(picard_ctx* ctx, double dt);         /* AdvanceVelocity.f90:6-125    */
+PICARD_API int picard_gpu_advance_velocity_exp(picard_ctx* ctx, double deltat,
+                                    double dt);                      /* AdvanceVelocity.f90:128-236  */
+PICARD_API int picard_gpu_advance_velocity_imp(picard_ctx* ctx, double deltat,
+                                    double dt);                      /* AdvanceVelocity.f90:239-347  */
+/* picard.f90:651-665: out[0] = uP, out[1] = uE, out[2] = uB (un-normalised,
+ * FP64), *num = num_local. */
+PICARD_API int picard_gpu_energy(picard_ctx* ctx, double out[3], int32_t* num);
+
+/* ----------------------------------------------------------- main loop */
+
+/* One line of the reference's energy log (picard.f90:667-671). */
+typedef void (*picard_log_fn)(int32_t iteration, double time, int32_t num_local,
+                              double uP_norm, double uE_norm, double uB_norm, void* user);
+
+/* picard.f90:554-674 call for call, iterations iter_start+1 .. iter_end, with
+ * the write-step branch off (writeFields = writeParticles = .false.).  log_fn
+ * (may be NULL) is called every log_interval iterations.  *sweeps_total
+ * (may be NULL) accumulates Jacobi sweeps. */
+PICARD_API int picard_gpu_run(picard_ctx* ctx, int32_t iter_start, int32_t iter_end, int32_t log_interval,
+                   picard_log_fn log_fn, void* user, int64_t* sweeps_total);
+
+/* The same iterations through the fused device path: one particle pass per
+ * step (velocity push of the previous step, position advance, outflow and
+ * periodic wrap, compaction), inflow candidates generated, advanced and
+ * filtered in one kernel, no host round trip inside a step.  Results equal
+ * picard_gpu_run's within the parity tolerances. */
+PICARD_API int picard_gpu_run_fused(picard_ctx* ctx, int32_t iter_start, int32_t iter_end,
+                         int64_t* sweeps_total);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PICARD_GPU_H */

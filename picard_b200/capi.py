@@ -1,0 +1,124 @@
+"""ctypes binding of libpicard_gpu.so (include/picard_gpu.h).
+
+The library is built in-tree (picard_b200/lib/libpicard_gpu.so, see build.py).
+There is no CPU fallback: if the library is missing or the machine has no CUDA
+device, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .params import PicardParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpicard_gpu.so")
+
+OK = 0
+ERR_BAD_ARG = 1
+ERR_CAPACITY = 2
+ERR_NOT_CONVERGED = 3
+ERR_TIMEOUT = 4
+ERR_CUDA = 5
+ERR_STATE = 6
+STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CAPACITY", 3: "NOT_CONVERGED", 4: "TIMEOUT", 5: "CUDA", 6: "STATE"}
+
+LAYOUT_F64 = 0
+LAYOUT_CELL32 = 1
+SOLVER_F64 = 0
+SOLVER_F32_REFINE = 1
+
+FIELD_U, FIELD_E, FIELD_N, FIELD_C, FIELD_F, FIELD_D = range(6)
+
+LOG_FN = C.CFUNCTYPE(None, C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_void_p)
+
+
+class PicardError(RuntimeError):
+    def __init__(self, code: int, where: str, message: str):
+        super().__init__(f"{where}: {STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libpicard_gpu.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `python -m picard_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER(PicardParams)
+    ctx = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int32)
+    sig = {
+        "picard_params_default": [P],
+        "picard_params_derive": [P],
+        "picard_gpu_create": [P, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)],
+        "picard_gpu_destroy": [ctx],
+        "picard_gpu_synchronize": [ctx],
+        "picard_gpu_footprint": [P, C.c_int32, C.c_int32, C.POINTER(C.c_uint64)],
+        "picard_gpu_set_particles": [ctx, dp, ip, C.c_int32],
+        "picard_gpu_get_particles": [ctx, dp, ip, C.c_int32, ip],
+        "picard_gpu_get_num_local": [ctx, ip],
+        "picard_gpu_get_field": [ctx, C.c_int32, dp],
+        "picard_gpu_set_field": [ctx, C.c_int32, dp],
+        "picard_gpu_calc_distance": [ctx],
+        "picard_gpu_particles_initialize": [ctx],
+        "picard_gpu_bc_inflow": [ctx, C.c_int32],
+        "picard_gpu_advance_position": [ctx, C.c_double],
+        "picard_gpu_particles_produce": [ctx, C.c_int32],
+        "picard_gpu_bc_outflow": [ctx],
+        "picard_gpu_particles_transfer": [ctx],
+        "picard_gpu_particles_gridify": [ctx],
+        "picard_gpu_particles_gridify_all": [ctx],
+        "picard_gpu_bc_potentials": [ctx],
+        "picard_gpu_calc_epotential": [ctx, C.c_double, C.c_int32, ip],
+        "picard_gpu_calc_efield": [ctx],
+        "picard_gpu_bc_fields": [ctx],
+        "picard_gpu_advance_velocity": [ctx, C.c_double],
+        "picard_gpu_advance_velocity_exp": [ctx, C.c_double, C.c_double],
+        "picard_gpu_advance_velocity_imp": [ctx, C.c_double, C.c_double],
+        "picard_gpu_energy": [ctx, dp, ip],
+        "picard_gpu_run": [ctx, C.c_int32, C.c_int32, C.c_int32, LOG_FN, C.c_void_p, C.POINTER(C.c_int64)],
+        "picard_gpu_run_fused": [ctx, C.c_int32, C.c_int32, C.POINTER(C.c_int64)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.picard_gpu_last_error.argtypes = []
+    L.picard_gpu_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().picard_gpu_last_error().decode(errors="replace")
+
+
+def check(rc: int, where: str, allow=(OK,)) -> int:
+    if rc not in allow:
+        raise PicardError(rc, where, last_error())
+    return rc
+
+
+def params_default() -> PicardParams:
+    p = PicardParams()
+    check(lib().picard_params_default(C.byref(p)), "picard_params_default")
+    return p
+
+
+def params_derive(p: PicardParams) -> PicardParams:
+    q = p.copy()
+    check(lib().picard_params_derive(C.byref(q)), "picard_params_derive")
+    return q
+
+
+def footprint(p: PicardParams, layout: int, solver: int) -> int:
+    b = C.c_uint64(0)
+    check(lib().picard_gpu_footprint(C.byref(p), layout, solver, C.byref(b)), "picard_gpu_footprint")
+    return int(b.value)

@@ -1,0 +1,91 @@
+// context.cuh -- the device state behind a picard_ctx.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "grid.cuh"
+#include "kernels.cuh"
+
+struct picard_ctx {
+  picard_params prm;
+  picard::KParams K;
+  int layout = 0, solver = 0;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  long long capacity = 0;
+
+  // particles: two buffers of each layout's arrays (compaction ping-pong)
+  picard::PartF64 f64[2] = {};
+  picard::PartC32 c32[2] = {};
+  int cur = 0;
+  int* d_count = nullptr;  // [2] live counts of the two buffers
+  int* d_err = nullptr;
+  long long num_local = 0;  // host mirror of d_count[cur]
+
+  // node arrays (plane-major, see common.cuh)
+  unsigned long long* Nacc = nullptr;  // [species][nodes] fixed point
+  unsigned long long* Facc = nullptr;  // [species*3][nodes], allocated on first gridify_all
+  double* N = nullptr;                 // [species][nodes]
+  double* F = nullptr;                 // [species*3][nodes]
+  double* C = nullptr;
+  double* U = nullptr;
+  double* E = nullptr;                 // [3][nodes]
+  float4* E32 = nullptr;               // CELL32 gather copy
+  double* D = nullptr;                 // (2Nx+1)(2Ny+1)(2Nz+1)
+
+  // Jacobi
+  double* b = nullptr;
+  double* U1 = nullptr;     // second FP64 iterate / anchor buffer
+  double* Usnap = nullptr;  // FP64 solver: iterate at the batch start
+  float* w[2] = {nullptr, nullptr};
+  float* r = nullptr;
+  double* partials = nullptr;  // [m_max + 1][nblocks]
+  double* r2 = nullptr;        // [m_max + 1]
+  picard::JacobiGeom G;
+  int m_max = 1024;
+  double last_residual = 0.0, last_bnorm = 0.0;
+  long long last_sweeps = 0;
+
+  // scratch
+  int* blk_counts = nullptr;
+  int* blk_offsets = nullptr;
+  int* cell_counts = nullptr;
+  int* cell_offsets = nullptr;
+  double* red_partial = nullptr;
+  double* red_result = nullptr;  // [8]
+  int red_blocks = 0;
+  double* h_pinned = nullptr;    // [m_max + 16] host staging
+  int* h_pinned_i = nullptr;     // [16]
+
+  // fused-path scratch
+  int* tile_state = nullptr;
+  int* tile_ticket = nullptr;
+  double* up_partial = nullptr;
+  long long tile_cap = 0;
+
+  picard::InflowTable inflow;
+  std::vector<void*> allocs;
+};
+
+namespace picard {
+int fail(int code, const std::string& msg);
+int check_cuda(cudaError_t e, const char* what);
+picard::KParams make_kparams(const picard_params& p);
+picard::InflowTable make_inflow_table(const picard_params& p);
+// Reads the device particle count into ctx->num_local after surfacing any
+// device-side capacity error.
+int sync_count_public(picard_ctx* c);
+}  // namespace picard
+
+#define PICARD_CUDA(expr)                                          \
+  do {                                                             \
+    int rc_ = ::picard::check_cuda((expr), #expr);                 \
+    if (rc_ != PICARD_OK) return rc_;                              \
+  } while (0)
+#define PICARD_TRY(expr)      \
+  do {                        \
+    int rc_ = (expr);         \
+    if (rc_ != PICARD_OK) return rc_; \
+  } while (0)

@@ -1,0 +1,628 @@
+// grid.cu -- node-array kernels: deposit finalisation, open-boundary
+// potentials, Jacobi sweeps, E-field, field energy.
+//
+// Jacobi.  CalcEpotential.f90:58-96 runs pure Jacobi from U = 0 (inside) and
+// stops at the top of sweep ss when ||b - L U_{ss-1}|| <= maxerr ||b||.  The
+// update is U_new = U - af (b - L U)... written as
+// U_new = ax(U+x + U-x) + ay(..) + az(..) - af b, so one read of the 7-point
+// stencil of U_{s-1} gives both U_s and the residual of U_{s-1}.  Each sweep
+// kernel therefore writes U_s and the block partial sums of |res(U_{s-1})|^2;
+// a check kernel after every batch of sweeps reduces the partials of each
+// sweep in a fixed order (deterministic) and finds the first iterate that
+// meets the reference's stopping test.  The batch starts from an anchor
+// (a snapshot of the iterate), so the iterate the test selects is rebuilt by
+// replaying the sweeps from the anchor.
+//
+// F32_REFINE keeps the iterate as U = V + sigma * w: V in FP64 (the anchor),
+// w in FP32.  The FP32 sweeps advance w with the scaled anchor residual
+// r = (b - L V) / sigma, which gives the same Jacobi iterate sequence because
+// the update is linear; the anchor pass folds w into V in FP64 and recomputes
+// r and its FP64 norm (the exact stopping test of the anchor iterate).
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "common.cuh"
+#include "grid.cuh"
+
+namespace picard {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int grid_for(long long n, int threads = kThreads) {
+  long long b = (n + threads - 1) / threads;
+  return b < 1 ? 1 : int(b);
+}
+
+// --------------------------------------------------------- deposit finish
+
+// Ghost node -> interior node whose deposit it mirrors (-1: open-face ghost,
+// which the reference folds and zeroes).
+__device__ inline int mirror(int i, int n, int open) {
+  if (i >= 1 && i <= n) return i;
+  if (open) return -1;
+  return i < 1 ? i + n : i - n;
+}
+
+// N_s = n2p_s * acc * 2^-36 at every node (ParticlesGridify.f90:98-121 with the
+// folds of 149-278), C = sum_s q_s N_s (288-293).
+__global__ void finish_deposit_kernel(KParams P, const unsigned long long* Nacc, double* N, double* Cout) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.nodes) return;
+  int i = int(g % P.nxp), j = int((g / P.nxp) % P.nyp), k = int(g / ((long long)P.nxp * P.nyp));
+  int mi = mirror(i, P.nx, P.xflow), mj = mirror(j, P.ny, P.yflow), mk = mirror(k, P.nz, P.zflow);
+  double c = 0.0;
+  for (int s = 0; s < P.species; ++s) {
+    double v = 0.0;
+    if (mi >= 0 && mj >= 0 && mk >= 0) {
+      long long acc = (long long)Nacc[(long long)s * P.nodes + node_index(P, mi, mj, mk)];
+      v = P.n2p[s] * ((double)acc * (1.0 / kDepositScale));
+    }
+    N[(long long)s * P.nodes + g] = v;
+    c = c + v * P.charge[s];
+  }
+  Cout[g] = c;
+}
+
+__global__ void finish_flux_kernel(KParams P, const unsigned long long* Facc, double* F) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.nodes) return;
+  int i = int(g % P.nxp), j = int((g / P.nxp) % P.nyp), k = int(g / ((long long)P.nxp * P.nyp));
+  int mi = mirror(i, P.nx, P.xflow), mj = mirror(j, P.ny, P.yflow), mk = mirror(k, P.nz, P.zflow);
+  for (int sc = 0; sc < 3 * P.species; ++sc) {
+    int s = sc / 3;
+    double v = 0.0;
+    if (mi >= 0 && mj >= 0 && mk >= 0) {
+      long long acc = (long long)Facc[(long long)sc * P.nodes + node_index(P, mi, mj, mk)];
+      v = P.n2p[s] * ((double)acc * (1.0 / kFluxScale));
+    }
+    F[(long long)sc * P.nodes + g] = v;
+  }
+}
+
+// ------------------------------------------------------ BCpotentials (a9)
+
+// BCpotentials.f90:51-139 on one rank.  One block computes a 16 x 16 tile of
+// face nodes (p1, p2) for both faces of one axis; it walks the interior cells
+// plane by plane along the face normal in 16 x 16 in-plane tiles, staging the
+// charge tile and the two 31 x 31 windows of the inverse-distance table D in
+// shared memory.
+constexpr int kBT = 16;
+
+struct FaceGeom {
+  int axis;         // normal axis
+  int n1, n2, nn;   // in-plane extents (p1 fastest) and normal extent
+};
+
+__device__ inline long long dindex(const KParams& P, int a, int b, int c) {
+  // 1-based D(a, b, c) of a (2Nx+1, 2Ny+1, 2Nz+1) array
+  long long DX = 2LL * P.nx + 1, DY = 2LL * P.ny + 1;
+  return (long long)(a - 1) + DX * ((long long)(b - 1) + DY * (long long)(c - 1));
+}
+
+__global__ void bc_potentials_kernel(KParams P, int axis, const double* __restrict__ C, const double* __restrict__ D,
+                                     double* U) {
+  __shared__ double cs[kBT][kBT];
+  __shared__ double d0[2 * kBT][2 * kBT + 1];
+  __shared__ double d1[2 * kBT][2 * kBT + 1];
+  const int Nx = P.nx, Ny = P.ny, Nz = P.nz;
+  // in-plane axes (a1 fastest), normal axis
+  int n1, n2, nn;
+  if (axis == 0) n1 = Ny, n2 = Nz, nn = Nx;
+  else if (axis == 1) n1 = Nx, n2 = Nz, nn = Ny;
+  else n1 = Nx, n2 = Ny, nn = Nz;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // tx along p1, ty along p2
+  const int p1 = blockIdx.x * kBT + tx + 1, p2 = blockIdx.y * kBT + ty + 1;  // 1-based face node
+  double acc0 = 0.0, acc1 = 0.0;
+  const int N1 = n1, N2 = n2;
+  for (int q = 1; q <= nn; ++q) {
+    for (int t2 = 0; t2 < (N2 + kBT - 1) / kBT; ++t2)
+      for (int t1 = 0; t1 < (N1 + kBT - 1) / kBT; ++t1) {
+        // charge tile: cells (q1, q2) = (t1*16 + tx + 1, t2*16 + ty + 1)
+        int q1 = t1 * kBT + tx + 1, q2 = t2 * kBT + ty + 1;
+        double cv = 0.0;
+        if (q1 <= N1 && q2 <= N2) {
+          int ci, cj, ck;
+          if (axis == 0) ci = q, cj = q1, ck = q2;
+          else if (axis == 1) ci = q1, cj = q, ck = q2;
+          else ci = q1, cj = q2, ck = q;
+          cv = C[node_index(P, ci, cj, ck)];
+        }
+        cs[ty][tx] = cv;
+        // D windows: offsets o1 = q1 - p1 in [t1*16 - b1*16 - 15, ... + 15]
+        int base1 = t1 * kBT - blockIdx.x * kBT - (kBT - 1);
+        int base2 = t2 * kBT - blockIdx.y * kBT - (kBT - 1);
+        // normal offsets of the two faces: face 0 at node 1 -> offset q;
+        // face 1 at node N+2 -> offset q - (N + 1)
+        int on0 = q, on1 = q - (nn + 1);
+        for (int e = ty * kBT + tx; e < (2 * kBT) * (2 * kBT); e += kBT * kBT) {
+          int w1 = e % (2 * kBT), w2 = e / (2 * kBT);
+          int o1 = base1 + w1, o2 = base2 + w2;
+          double v0 = 0.0, v1 = 0.0;
+          if (o1 >= -(N1 - 1) && o1 <= N1 - 1 && o2 >= -(N2 - 1) && o2 <= N2 - 1) {
+            int a0, b0, c0, a1, b1, c1;
+            if (axis == 0) {
+              a0 = Nx + 1 + on0; b0 = Ny + 1 + o1; c0 = Nz + 1 + o2;
+              a1 = Nx + 1 + on1; b1 = b0; c1 = c0;
+            } else if (axis == 1) {
+              a0 = Nx + 1 + o1; b0 = Ny + 1 + on0; c0 = Nz + 1 + o2;
+              a1 = a0; b1 = Ny + 1 + on1; c1 = c0;
+            } else {
+              a0 = Nx + 1 + o1; b0 = Ny + 1 + o2; c0 = Nz + 1 + on0;
+              a1 = a0; b1 = b0; c1 = Nz + 1 + on1;
+            }
+            v0 = D[dindex(P, a0, b0, c0)];
+            v1 = D[dindex(P, a1, b1, c1)];
+          }
+          d0[w2][w1] = v0;
+          d1[w2][w1] = v1;
+        }
+        __syncthreads();
+        // thread (tx, ty) owns face node (p1, p2): offset of cell (u1, u2) of
+        // the tile is (t1*16 + u1 + 1 - p1, ...) -> window index u1 - tx + 15
+#pragma unroll 4
+        for (int u2 = 0; u2 < kBT; ++u2)
+#pragma unroll
+          for (int u1 = 0; u1 < kBT; ++u1) {
+            double c = cs[u2][u1];
+            acc0 += c * d0[u2 - ty + kBT - 1][u1 - tx + kBT - 1];
+            acc1 += c * d1[u2 - ty + kBT - 1][u1 - tx + kBT - 1];
+          }
+        __syncthreads();
+      }
+  }
+  if (p1 <= N1 && p2 <= N2) {
+    const double scale = 1.0 / (2.0 * kTau * kEps0);
+    long long g0, g1;
+    if (axis == 0) {
+      g0 = node_index(P, 0, p1, p2);
+      g1 = node_index(P, Nx + 1, p1, p2);
+    } else if (axis == 1) {
+      g0 = node_index(P, p1, 0, p2);
+      g1 = node_index(P, p1, Ny + 1, p2);
+    } else {
+      g0 = node_index(P, p1, p2, 0);
+      g1 = node_index(P, p1, p2, Nz + 1);
+    }
+    U[g0] = acc0 * scale;
+    U[g1] = acc1 * scale;
+  }
+}
+
+// ------------------------------------------------------------- Jacobi
+
+struct Stencil {
+  int nx, ny, nz, nxp, nyp;
+  int px, py, pz;  // periodic axes
+  long long nodes;
+};
+
+__device__ inline void neighbours(const Stencil& S, int i, int j, int k, long long& xm, long long& xp, long long& ym,
+                                  long long& yp, long long& zm, long long& zp) {
+  int im = (S.px && i == 1) ? S.nx : i - 1, ip = (S.px && i == S.nx) ? 1 : i + 1;
+  int jm = (S.py && j == 1) ? S.ny : j - 1, jp = (S.py && j == S.ny) ? 1 : j + 1;
+  int km = (S.pz && k == 1) ? S.nz : k - 1, kp = (S.pz && k == S.nz) ? 1 : k + 1;
+  long long row = (long long)S.nxp * ((long long)j + (long long)S.nyp * k);
+  xm = row + im;
+  xp = row + ip;
+  ym = (long long)i + (long long)S.nxp * ((long long)jm + (long long)S.nyp * k);
+  yp = (long long)i + (long long)S.nxp * ((long long)jp + (long long)S.nyp * k);
+  zm = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * km);
+  zp = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * kp);
+}
+
+__device__ inline void block_sum_store(double v, double* out) {
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int t = threadIdx.x + blockDim.x * threadIdx.y;
+  if ((t & 31) == 0) sh[t >> 5] = v;
+  __syncthreads();
+  if (t == 0) {
+    double s = 0.0;
+    int nw = (blockDim.x * blockDim.y) >> 5;
+    for (int w = 0; w < nw; ++w) s += sh[w];
+    *out = s;
+  }
+}
+
+// b = -C / (dV eps0) everywhere; block partials of b^2 over the interior.
+__global__ void rhs_kernel(KParams P, const double* C, double* b, double* partial) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v2 = 0.0;
+  if (g < P.nodes) {
+    double binv = 1.0 / (P.dV * kEps0);
+    double v = -C[g] * binv;
+    b[g] = v;
+    int i = int(g % P.nxp), j = int((g / P.nxp) % P.nyp), k = int(g / ((long long)P.nxp * P.nyp));
+    if (i >= 1 && i <= P.nx && j >= 1 && j <= P.ny && k >= 1 && k <= P.nz) v2 = v * v;
+  }
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) v2 += __shfl_down_sync(0xffffffffu, v2, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) s += sh[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+// FP64 sweep: Uout = Jacobi(Uin); partial = sum |b - L Uin|^2 of this block.
+__global__ void __launch_bounds__(256) sweep_f64_kernel(Stencil S, JacobiCoef J, const double* __restrict__ Uin,
+                                                        double* __restrict__ Uout, const double* __restrict__ b,
+                                                        double* partial, int zc) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  int k0 = blockIdx.z * zc + 1;
+  double r2 = 0.0;
+  if (i <= S.nx && j <= S.ny) {
+    int k1 = min(k0 + zc - 1, S.nz);
+    for (int k = k0; k <= k1; ++k) {
+      long long c = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * k);
+      long long xm, xp, ym, yp, zm, zp;
+      neighbours(S, i, j, k, xm, xp, ym, yp, zm, zp);
+      double u = Uin[c];
+      double sx = Uin[xp] + Uin[xm], sy = Uin[yp] + Uin[ym], sz = Uin[zp] + Uin[zm];
+      double bc = b[c];
+      double res = bc - ((sx - 2.0 * u) / J.dx2 + (sy - 2.0 * u) / J.dy2 + (sz - 2.0 * u) / J.dz2);
+      r2 += res * res;
+      Uout[c] = J.ax * sx + J.ay * sy + J.az * sz - J.af * bc;
+    }
+  }
+  block_sum_store(r2, partial + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
+}
+
+// FP32 sweep of the increment: res = r - L w, w_out = w - af res.
+// w_zero: the input increment is zero (first sweep after an anchor).
+__global__ void __launch_bounds__(256) sweep_f32_kernel(Stencil S, JacobiCoefF J, const float* __restrict__ win,
+                                                        float* __restrict__ wout, const float* __restrict__ r,
+                                                        double* partial, int zc, int w_zero) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  int k0 = blockIdx.z * zc + 1;
+  float r2 = 0.0f;
+  if (i <= S.nx && j <= S.ny) {
+    int k1 = min(k0 + zc - 1, S.nz);
+    long long plane = (long long)S.nxp * S.nyp;
+    long long c = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * k0);
+    if (w_zero) {
+      for (int k = k0; k <= k1; ++k, c += plane) {
+        float res = __ldg(r + c);
+        r2 += res * res;
+        wout[c] = -J.af * res;
+      }
+    } else {
+      int im = (S.px && i == 1) ? S.nx : i - 1, ip = (S.px && i == S.nx) ? 1 : i + 1;
+      int jm = (S.py && j == 1) ? S.ny : j - 1, jp = (S.py && j == S.ny) ? 1 : j + 1;
+      long long dxm = im - i, dxp = ip - i;
+      long long dym = (long long)(jm - j) * S.nxp, dyp = (long long)(jp - j) * S.nxp;
+      // z pipeline in registers
+      long long cm = (S.pz && k0 == 1) ? c + (long long)(S.nz - 1) * plane : c - plane;
+      float wm = __ldg(win + cm);
+      float wc = __ldg(win + c);
+      for (int k = k0; k <= k1; ++k, c += plane) {
+        long long cp = (S.pz && k == S.nz) ? c - (long long)(S.nz - 1) * plane : c + plane;
+        float wp = __ldg(win + cp);
+        float sx = __ldg(win + c + dxp) + __ldg(win + c + dxm);
+        float sy = __ldg(win + c + dyp) + __ldg(win + c + dym);
+        float sz = wp + wm;
+        float lap = (sx - 2.0f * wc) * J.idx2 + (sy - 2.0f * wc) * J.idy2 + (sz - 2.0f * wc) * J.idz2;
+        float res = __ldg(r + c) - lap;
+        r2 += res * res;
+        wout[c] = wc - J.af * res;
+        wm = wc;
+        wc = wp;
+      }
+    }
+  }
+  block_sum_store((double)r2, partial + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
+}
+
+// Anchor of F32_REFINE: Vout = Vin + sigma w (interior), r = (b - L Vout)/sigma
+// as FP32, partial = sum (b - L Vout)^2 in FP64.
+__global__ void __launch_bounds__(256) anchor_kernel(Stencil S, JacobiCoef J, const double* __restrict__ Vin,
+                                                     double* __restrict__ Vout, const float* __restrict__ w,
+                                                     const double* __restrict__ b, float* __restrict__ r,
+                                                     double sigma, double* partial, int zc, int w_zero) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  int k0 = blockIdx.z * zc + 1;
+  double r2 = 0.0;
+  if (i <= S.nx && j <= S.ny) {
+    int k1 = min(k0 + zc - 1, S.nz);
+    for (int k = k0; k <= k1; ++k) {
+      long long c = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * k);
+      long long xm, xp, ym, yp, zm, zp;
+      neighbours(S, i, j, k, xm, xp, ym, yp, zm, zp);
+      auto val = [&](long long g) { return w_zero ? Vin[g] : Vin[g] + sigma * (double)w[g]; };
+      double u = val(c);
+      double sx = val(xp) + val(xm), sy = val(yp) + val(ym), sz = val(zp) + val(zm);
+      double bc = b[c];
+      double res = bc - ((sx - 2.0 * u) / J.dx2 + (sy - 2.0 * u) / J.dy2 + (sz - 2.0 * u) / J.dz2);
+      r2 += res * res;
+      Vout[c] = u;
+      r[c] = (float)(res / sigma);
+    }
+  }
+  block_sum_store(r2, partial + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
+}
+
+// U = V + sigma w on the interior.
+__global__ void finalize_kernel(Stencil S, const double* V, const float* w, double sigma, double* U, int w_zero) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= S.nodes) return;
+  int i = int(g % S.nxp), j = int((g / S.nxp) % S.nyp), k = int(g / ((long long)S.nxp * S.nyp));
+  bool interior = i >= 1 && i <= S.nx && j >= 1 && j <= S.ny && k >= 1 && k <= S.nz;
+  U[g] = (interior && !w_zero) ? V[g] + sigma * (double)w[g] : V[g];
+}
+
+// Periodic ghost refresh of U (CalcEpotential.f90:100-239 on one rank), in
+// z, y, x order over whole planes.
+__global__ void refresh_periodic_kernel(Stencil S, double* U, int axis) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int nzp = S.nz + 2;
+  if (axis == 2) {
+    long long n = (long long)S.nxp * S.nyp;
+    if (t >= n) return;
+    U[t] = U[t + (long long)S.nz * n];
+    U[t + (long long)(S.nz + 1) * n] = U[t + n];
+  } else if (axis == 1) {
+    long long n = (long long)S.nxp * nzp;
+    if (t >= n) return;
+    int i = int(t % S.nxp), k = int(t / S.nxp);
+    auto at = [&](int j) { return (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * k); };
+    U[at(0)] = U[at(S.ny)];
+    U[at(S.ny + 1)] = U[at(1)];
+  } else {
+    long long n = (long long)S.nyp * nzp;
+    if (t >= n) return;
+    int j = int(t % S.nyp), k = int(t / S.nyp);
+    long long row = (long long)S.nxp * ((long long)j + (long long)S.nyp * k);
+    U[row] = U[row + S.nx];
+    U[row + S.nx + 1] = U[row + 1];
+  }
+}
+
+// Reduce the block partials of `m` consecutive sweeps (one block each) in a
+// fixed order: r2[t] = sum_b partial[t * nb + b].
+__global__ void reduce_sweeps_kernel(const double* partial, int nb, double* r2) {
+  __shared__ double sh[256];
+  const double* p = partial + (long long)blockIdx.x * nb;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += p[b];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) r2[blockIdx.x] = sh[0];
+}
+
+// ------------------------------------------------------ E-field (a11, a12)
+
+// CalcEfield.f90:27-34 + BCfields.f90:31-90 on one rank: interior central
+// differences, open-face ghosts zero, periodic ghosts mirrored.  Writes the
+// FP64 planes (Ex, Ey, Ez) and the FP32 float4 copy used by the CELL32 gather.
+__global__ void efield_kernel(KParams P, const double* __restrict__ U, double* E, float4* E32) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.nodes) return;
+  int i = int(g % P.nxp), j = int((g / P.nxp) % P.nyp), k = int(g / ((long long)P.nxp * P.nyp));
+  int mi = mirror(i, P.nx, P.xflow), mj = mirror(j, P.ny, P.yflow), mk = mirror(k, P.nz, P.zflow);
+  double e[3] = {0.0, 0.0, 0.0};
+  if (mi >= 0 && mj >= 0 && mk >= 0) {
+    // value at the mirrored interior node (equals (i, j, k) when interior)
+    auto u = [&](int a, int b, int c) { return U[node_index(P, a, b, c)]; };
+    int ii = mi, jj = mj, kk = mk;
+    e[2] = -(u(ii, jj, kk + 1) - u(ii, jj, kk - 1)) * 0.5 / P.dz;
+    e[1] = -(u(ii, jj + 1, kk) - u(ii, jj - 1, kk)) * 0.5 / P.dy;
+    e[0] = -(u(ii + 1, jj, kk) - u(ii - 1, jj, kk)) * 0.5 / P.dx;
+  }
+  E[g] = e[0];
+  E[P.nodes + g] = e[1];
+  E[2 * P.nodes + g] = e[2];
+  if (E32) E32[g] = make_float4(float(e[0]), float(e[1]), float(e[2]), 0.0f);
+}
+
+// BCfields.f90:31-90 on one rank: zero the ghost layer of every open face.
+__global__ void bc_fields_kernel(KParams P, double* E, float4* E32) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.nodes) return;
+  int i = int(g % P.nxp), j = int((g / P.nxp) % P.nyp), k = int(g / ((long long)P.nxp * P.nyp));
+  bool ghost = (P.xflow && (i == 0 || i == P.nx + 1)) || (P.yflow && (j == 0 || j == P.ny + 1)) ||
+               (P.zflow && (k == 0 || k == P.nz + 1));
+  if (!ghost) return;
+  E[g] = 0.0;
+  E[P.nodes + g] = 0.0;
+  E[2 * P.nodes + g] = 0.0;
+  if (E32) E32[g] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// Block partials of sum |E + E0|^2 over interior nodes (picard.f90:656-658).
+__global__ void energy_field_kernel(KParams P, const double* E, double* partial) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (g < P.nodes) {
+    int i = int(g % P.nxp), j = int((g / P.nxp) % P.nyp), k = int(g / ((long long)P.nxp * P.nyp));
+    if (i >= 1 && i <= P.nx && j >= 1 && j <= P.ny && k >= 1 && k <= P.nz) {
+      double a = E[g] + P.E0[0], b = E[P.nodes + g] + P.E0[1], c = E[2 * P.nodes + g] + P.E0[2];
+      v = a * a + b * b + c * c;
+    }
+  }
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) s += sh[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__global__ void sum_partials_kernel(const double* partial, int nb, double scale, double* out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[b];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0] * scale;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ wrappers
+
+Stencil make_stencil(const KParams& P) {
+  Stencil S;
+  S.nx = P.nx;
+  S.ny = P.ny;
+  S.nz = P.nz;
+  S.nxp = P.nxp;
+  S.nyp = P.nyp;
+  S.px = !P.xflow;
+  S.py = !P.yflow;
+  S.pz = !P.zflow;
+  S.nodes = P.nodes;
+  return S;
+}
+
+JacobiGeom jacobi_geom(const KParams& P) {
+  JacobiGeom G;
+  G.block = dim3(32, 8, 1);
+  int bx = (P.nx + 31) / 32, by = (P.ny + 7) / 8;
+  // enough z-blocks for ~4 blocks per SM, at least 4 nodes per thread
+  int want = (4 * 148 + bx * by - 1) / (bx * by);
+  int zc = (P.nz + want - 1) / want;
+  if (zc < 4) zc = 4;
+  if (zc > P.nz) zc = P.nz;
+  G.zc = zc;
+  G.grid = dim3(bx, by, (P.nz + zc - 1) / zc);
+  G.nblocks = bx * by * G.grid.z;
+  return G;
+}
+
+JacobiCoef jacobi_coef(const KParams& P) {
+  JacobiCoef J;
+  double dx = P.dx, dy = P.dy, dz = P.dz;
+  double S = (dx * dy) * (dx * dy) + (dx * dz) * (dx * dz) + (dy * dz) * (dy * dz);
+  J.ax = 0.5 * (1.0 / S) * ((dy * dz) * (dy * dz));
+  J.ay = 0.5 * (1.0 / S) * ((dx * dz) * (dx * dz));
+  J.az = 0.5 * (1.0 / S) * ((dx * dy) * (dx * dy));
+  J.af = 0.5 * (1.0 / S) * ((dx * dy * dz) * (dx * dy * dz));
+  J.dx2 = dx * dx;
+  J.dy2 = dy * dy;
+  J.dz2 = dz * dz;
+  return J;
+}
+
+JacobiCoefF jacobi_coef_f(const KParams& P) {
+  JacobiCoef J = jacobi_coef(P);
+  JacobiCoefF F;
+  F.af = float(J.af);
+  F.idx2 = float(1.0 / J.dx2);
+  F.idy2 = float(1.0 / J.dy2);
+  F.idz2 = float(1.0 / J.dz2);
+  return F;
+}
+
+cudaError_t launch_finish_deposit(const KParams& P, const unsigned long long* Nacc, double* N, double* C,
+                                  cudaStream_t st) {
+  finish_deposit_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(P, Nacc, N, C);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finish_flux(const KParams& P, const unsigned long long* Facc, double* F, cudaStream_t st) {
+  finish_flux_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(P, Facc, F);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_potentials(const KParams& P, const double* C, const double* D, double* U, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(U, 0, sizeof(double) * P.nodes, st);
+  if (e != cudaSuccess) return e;
+  const int flows[3] = {P.xflow, P.yflow, P.zflow};
+  for (int axis = 0; axis < 3; ++axis) {
+    if (!flows[axis]) continue;
+    int n1 = axis == 0 ? P.ny : P.nx, n2 = axis == 2 ? P.ny : P.nz;
+    dim3 grid((n1 + kBT - 1) / kBT, (n2 + kBT - 1) / kBT);
+    bc_potentials_kernel<<<grid, dim3(kBT, kBT), 0, st>>>(P, axis, C, D, U);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int rhs_blocks(const KParams& P) { return grid_for(P.nodes); }
+
+cudaError_t launch_rhs(const KParams& P, const double* C, double* b, double* partial, double* bnorm2,
+                       cudaStream_t st) {
+  int nb = grid_for(P.nodes);
+  rhs_kernel<<<nb, kThreads, 0, st>>>(P, C, b, partial);
+  sum_partials_kernel<<<1, 256, 0, st>>>(partial, nb, 1.0, bnorm2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_f64(const KParams& P, const JacobiGeom& G, const double* Uin, double* Uout, const double* b,
+                             double* partial, cudaStream_t st) {
+  sweep_f64_kernel<<<G.grid, G.block, 0, st>>>(make_stencil(P), jacobi_coef(P), Uin, Uout, b, partial, G.zc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_f32(const KParams& P, const JacobiGeom& G, const float* win, float* wout, const float* r,
+                             double* partial, int w_zero, cudaStream_t st) {
+  sweep_f32_kernel<<<G.grid, G.block, 0, st>>>(make_stencil(P), jacobi_coef_f(P), win, wout, r, partial, G.zc,
+                                                w_zero);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_anchor(const KParams& P, const JacobiGeom& G, const double* Vin, double* Vout, const float* w,
+                          const double* b, float* r, double sigma, double* partial, int w_zero, cudaStream_t st) {
+  anchor_kernel<<<G.grid, G.block, 0, st>>>(make_stencil(P), jacobi_coef(P), Vin, Vout, w, b, r, sigma, partial,
+                                             G.zc, w_zero);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const KParams& P, const double* V, const float* w, double sigma, double* U, int w_zero,
+                            cudaStream_t st) {
+  finalize_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(make_stencil(P), V, w, sigma, U, w_zero);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refresh_periodic(const KParams& P, double* U, cudaStream_t st) {
+  Stencil S = make_stencil(P);
+  if (S.pz) refresh_periodic_kernel<<<grid_for((long long)S.nxp * S.nyp), kThreads, 0, st>>>(S, U, 2);
+  if (S.py) refresh_periodic_kernel<<<grid_for((long long)S.nxp * (S.nz + 2)), kThreads, 0, st>>>(S, U, 1);
+  if (S.px) refresh_periodic_kernel<<<grid_for((long long)S.nyp * (S.nz + 2)), kThreads, 0, st>>>(S, U, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_sweeps(const double* partial, int nb, int m, double* r2, cudaStream_t st) {
+  if (m <= 0) return cudaSuccess;
+  reduce_sweeps_kernel<<<m, 256, 0, st>>>(partial, nb, r2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_efield(const KParams& P, const double* U, double* E, float4* E32, cudaStream_t st) {
+  efield_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(P, U, E, E32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_fields(const KParams& P, double* E, float4* E32, cudaStream_t st) {
+  bc_fields_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(P, E, E32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_energy_field(const KParams& P, const double* E, double* partial, double* out, cudaStream_t st) {
+  int nb = grid_for(P.nodes);
+  energy_field_kernel<<<nb, kThreads, 0, st>>>(P, E, partial);
+  sum_partials_kernel<<<1, 256, 0, st>>>(partial, nb, 0.5 * kEps0 * P.dV, out);
+  return cudaGetLastError();
+}
+
+}  // namespace picard

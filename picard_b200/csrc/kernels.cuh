@@ -1,0 +1,92 @@
+// kernels.cuh -- launch wrappers shared between the translation units of
+// libpicard_gpu.  Each wrapper enqueues work on `st` and returns the launch
+// status; none of them synchronises.
+#pragma once
+
+#include "common.cuh"
+
+namespace picard {
+
+// One inflow face of BCinflow.f90 on one rank: loop `outer` x `inner`, the
+// fixed index of the face axis, and the lower-edge coordinate of that axis.
+struct InflowFace {
+  int axis;         // 0 = x face, 1 = y face, 2 = z face
+  int fixed;        // 1-based index of the guard layer (1 or N+2)
+  int o_lo, o_n;    // outer loop start (1-based) and length
+  int i_lo, i_n;    // inner loop start (1-based) and length
+  double edge;      // x0 / y0 / z0 of the guard layer
+  long long first;  // index of the face's first guard cell in the enumeration
+};
+struct InflowTable {
+  int nfaces;
+  InflowFace f[6];
+  long long cells;   // guard cells over all faces
+  int per_cell;      // particles created per guard cell
+  int group_prefix[9];  // slots before species s inside one cell's block
+};
+
+struct ReduceBuf {
+  double* partial;      // one per block
+  double* result;       // device scalar(s)
+  int max_blocks;
+};
+
+// ---------------------------------------------------------- exact FP64 unit
+cudaError_t launch_calc_distance(const KParams& P, double* D, cudaStream_t st);
+cudaError_t launch_init_f64(const KParams& P, PartF64 out, long long start, cudaStream_t st);
+cudaError_t launch_init_c32(const KParams& P, PartC32 out, long long start, cudaStream_t st);
+cudaError_t launch_inflow_f64(const KParams& P, const InflowTable& T, int iteration, PartF64 out, long long start,
+                              cudaStream_t st);
+cudaError_t launch_inflow_c32(const KParams& P, const InflowTable& T, int iteration, PartC32 out, long long start,
+                              cudaStream_t st);
+// Fused inflow (fast path): candidates are generated, advanced by dt and kept
+// only if BCoutflow would keep them; survivors are appended at *count.
+cudaError_t launch_inflow_fused_c32(const KParams& P, const InflowTable& T, int iteration, PartC32 out, int* count,
+                                    long long capacity, int* err, cudaStream_t st);
+cudaError_t launch_inflow_fused_f64(const KParams& P, const InflowTable& T, int iteration, PartF64 out, int* count,
+                                    long long capacity, int* err, cudaStream_t st);
+// ParticlesProduce: per-cell counts, then emission at offsets[].
+cudaError_t launch_produce_count(const KParams& P, int iteration, int* counts, cudaStream_t st);
+// Appends at *count (device); offsets[cells] holds the total, added to *count.
+cudaError_t launch_produce_emit_f64(const KParams& P, int iteration, const int* offsets, PartF64 out, int* count,
+                                    long long capacity, int* err, cudaStream_t st);
+cudaError_t launch_produce_emit_c32(const KParams& P, int iteration, const int* offsets, PartC32 out, int* count,
+                                    long long capacity, int* err, cudaStream_t st);
+cudaError_t launch_advance_position_f64(const KParams& P, PartF64 a, long long n, double dt, cudaStream_t st);
+cudaError_t launch_transfer_f64(const KParams& P, PartF64 a, long long n, cudaStream_t st);
+// wrap != 0 also applies the ParticlesTransfer periodic wrap to survivors.
+cudaError_t launch_compact_outflow_f64(const KParams& P, PartF64 in, PartF64 out, long long n, int* block_counts,
+                                       int* block_offsets, int* new_count, int wrap, cudaStream_t st);
+cudaError_t launch_advance_velocity_f64(const KParams& P, PartF64 a, long long n, const double* E, double dt,
+                                        double deltat, int mode, cudaStream_t st);
+cudaError_t launch_deposit_f64(const KParams& P, PartF64 a, long long n, unsigned long long* Nacc,
+                               unsigned long long* Facc, cudaStream_t st);
+cudaError_t launch_energy_particles_f64(const KParams& P, PartF64 a, long long n, ReduceBuf rb, cudaStream_t st);
+cudaError_t launch_cell_indices_f64(const KParams& P, PartF64 a, long long n, int* ijk, cudaStream_t st);
+
+// ------------------------------------------------------------ CELL32 unit
+cudaError_t launch_advance_position_c32(const KParams& P, PartC32 a, long long n, double dt, cudaStream_t st);
+cudaError_t launch_transfer_c32(const KParams& P, PartC32 a, long long n, cudaStream_t st);
+cudaError_t launch_compact_outflow_c32(const KParams& P, PartC32 in, PartC32 out, long long n, int* block_counts,
+                                       int* block_offsets, int* new_count, int wrap, cudaStream_t st);
+cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
+                                        double deltat, int mode, cudaStream_t st);
+cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
+                               unsigned long long* Facc, cudaStream_t st);
+cudaError_t launch_energy_particles_c32(const KParams& P, PartC32 a, long long n, ReduceBuf rb, cudaStream_t st);
+cudaError_t launch_c32_to_f64(const KParams& P, PartC32 a, long long n, PartF64 out, cudaStream_t st);
+cudaError_t launch_f64_to_c32(const KParams& P, PartF64 a, long long n, PartC32 out, cudaStream_t st);
+// Fused step kernel: optional Boris push with E (mode >= 0), position
+// advance, outflow and periodic wrap, deterministic order-preserving
+// compaction into `out` starting at out_base.
+cudaError_t launch_push_fused_c32(const KParams& P, PartC32 in, PartC32 out, const int* n_in, int* n_out,
+                                  const float4* E, int push, int* tile_state, int* tile_ticket, long long capacity,
+                                  double* up_partial, int* err, cudaStream_t st);
+
+// ------------------------------------------------------------ scans
+// Exclusive scan of n int32 counts into offsets; *total receives the sum.
+cudaError_t launch_scan_int(const int* in, int* out, int n, int* total, int* scratch, cudaStream_t st);
+int scan_scratch_ints(int n);
+int compact_blocks(long long n);
+
+}  // namespace picard

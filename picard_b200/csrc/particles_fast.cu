@@ -1,0 +1,515 @@
+// particles_fast.cu -- CELL32 particle kernels (the performance layout) and
+// the integer scan used by compaction and production.
+//
+// A CELL32 particle is its CIC base node (i, j, k), packed in one uint32, the
+// in-cell fractions f = (x - Lx_min)/dx + 1/2 - i in [0, 1) as FP32, and the
+// velocity as FP32: 28 bytes plus one species byte.  Node i sits at
+// x = Lx_min + (i - 1/2) dx, so the CIC weights are (1 - f, f) directly and
+// the position advance is one FP32 add per axis.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace picard {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int persistent_grid(long long n) {
+  long long b = (n + kThreads - 1) / kThreads;
+  if (b > 148LL * 16) b = 148LL * 16;
+  return b < 1 ? 1 : int(b);
+}
+
+// ------------------------------------------------------------------ scan
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ inline int block_scan_excl(int v, int& total) {
+  __shared__ int warp_sums[32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = (lane < int(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    warp_sums[lane] = w;
+  }
+  __syncthreads();
+  int prefix = (warp > 0 ? warp_sums[warp - 1] : 0) + x - v;
+  total = warp_sums[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return prefix;
+}
+
+__global__ void scan_tiles_kernel(const int* in, int* out, int n, int* tile_sums) {
+  long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    long long i = base + q;
+    v[q] = i < n ? in[i] : 0;
+    s += v[q];
+  }
+  int total;
+  int run = block_scan_excl(s, total);
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    long long i = base + q;
+    if (i < n) out[i] = run;
+    run += v[q];
+  }
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void scan_add_kernel(int* out, int n, const int* tile_offsets) {
+  long long base = (long long)blockIdx.x * kScanTile;
+  int add = tile_offsets[blockIdx.x];
+  for (int q = threadIdx.x; q < kScanTile; q += blockDim.x) {
+    long long i = base + q;
+    if (i < n) out[i] += add;
+  }
+}
+
+// ------------------------------------------------------------ CELL32 ops
+
+struct C32 {
+  int i, j, k;
+  float f[3];
+};
+
+__device__ inline C32 load_pos(const PartC32& a, long long p) {
+  C32 r;
+  unpack_cell(a.cell[p], r.i, r.j, r.k);
+  r.f[0] = a.fx[p];
+  r.f[1] = a.fy[p];
+  r.f[2] = a.fz[p];
+  return r;
+}
+
+// Move one axis by d cells (in cell units) and renormalise to [0, 1).
+// Open axes pin far-out particles at the outer guard node (they are outside
+// the domain and BCoutflow removes them); periodic axes shift by whole
+// periods so the index stays representable.
+__device__ inline void move_axis(int& i, float& f, float d, int n, int open) {
+  float t = f + d;
+  float fl = floorf(t);
+  int di = int(fl);
+  t = t - fl;
+  if (t >= 1.0f) {
+    t = 0.0f;
+    di += 1;
+  }
+  i += di;
+  if (open) {
+    if (i < -1) i = -1, t = 0.0f;
+    if (i > n + 1) i = n + 1, t = 0.5f;
+  } else {
+    while (i < -1) i += n;
+    while (i > n + 1) i -= n;
+  }
+  f = t;
+}
+
+// x < min  <=>  i + f < 1/2;  x > max  <=>  i + f > n + 1/2.
+__device__ inline bool below(int i, float f) { return i < 0 || (i == 0 && f < 0.5f); }
+__device__ inline bool above(int i, float f, int n) { return i > n || (i == n && f > 0.5f); }
+
+// BCoutflow.f90:28-53 in cell coordinates (true = keep).
+__device__ inline bool keep_c32(const KParams& P, const C32& c) {
+  if (P.xflow && (below(c.i, c.f[0]) || above(c.i, c.f[0], P.nx))) return false;
+  if (P.yflow && (below(c.j, c.f[1]) || above(c.j, c.f[1], P.ny))) return false;
+  if (P.zflow && (below(c.k, c.f[2]) || above(c.k, c.f[2], P.nz))) return false;
+  return true;
+}
+
+// ParticlesTransfer.f90:494-519 in cell coordinates: whole-period shifts.
+__device__ inline void wrap_c32(const KParams& P, C32& c) {
+  if (below(c.k, c.f[2])) c.k += P.nz;
+  if (above(c.k, c.f[2], P.nz)) c.k -= P.nz;
+  if (below(c.j, c.f[1])) c.j += P.ny;
+  if (above(c.j, c.f[1], P.ny)) c.j -= P.ny;
+  if (below(c.i, c.f[0])) c.i += P.nx;
+  if (above(c.i, c.f[0], P.nx)) c.i -= P.nx;
+}
+
+__global__ void advance_position_c32_kernel(KParams P, PartC32 a, long long n, float dtdx, float dtdy, float dtdz) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    C32 c = load_pos(a, p);
+    move_axis(c.i, c.f[0], a.vx[p] * dtdx, P.nx, P.xflow);
+    move_axis(c.j, c.f[1], a.vy[p] * dtdy, P.ny, P.yflow);
+    move_axis(c.k, c.f[2], a.vz[p] * dtdz, P.nz, P.zflow);
+    a.cell[p] = pack_cell(c.i, c.j, c.k);
+    a.fx[p] = c.f[0];
+    a.fy[p] = c.f[1];
+    a.fz[p] = c.f[2];
+  }
+}
+
+__global__ void transfer_c32_kernel(KParams P, PartC32 a, long long n) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    C32 c = load_pos(a, p);
+    wrap_c32(P, c);
+    a.cell[p] = pack_cell(c.i, c.j, c.k);
+  }
+}
+
+constexpr int kCompactThreads = 256;
+constexpr int kCompactItems = 8;
+constexpr int kCompactTile = kCompactThreads * kCompactItems;
+
+__global__ void outflow_count_c32(KParams P, PartC32 a, long long n, int* block_counts) {
+  long long base = (long long)blockIdx.x * kCompactTile;
+  int c = 0;
+  for (int q = 0; q < kCompactItems; ++q) {
+    long long p = base + (long long)q * kCompactThreads + threadIdx.x;
+    if (p < n && keep_c32(P, load_pos(a, p))) ++c;
+  }
+  int total;
+  block_scan_excl(c, total);
+  if (threadIdx.x == 0) block_counts[blockIdx.x] = total;
+}
+
+// Order-preserving scatter: item q of thread t is particle base + q*256 + t;
+// survivors keep their order inside the tile (warp ballots per item row).
+__global__ void outflow_scatter_c32(KParams P, PartC32 a, PartC32 o, long long n, const int* block_offsets, int wrap) {
+  __shared__ int row_count[kCompactItems][kCompactThreads / 32];
+  long long base = (long long)blockIdx.x * kCompactTile;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool keep[kCompactItems];
+  for (int q = 0; q < kCompactItems; ++q) {
+    long long p = base + (long long)q * kCompactThreads + threadIdx.x;
+    keep[q] = p < n && keep_c32(P, load_pos(a, p));
+    unsigned m = __ballot_sync(0xffffffffu, keep[q]);
+    if (lane == 0) row_count[q][warp] = __popc(m);
+  }
+  __syncthreads();
+  // prefix over (row, warp) in row-major order = particle order
+  int off = block_offsets[blockIdx.x];
+  for (int q = 0; q < kCompactItems; ++q) {
+    long long p = base + (long long)q * kCompactThreads + threadIdx.x;
+    int before = 0;
+    for (int r = 0; r < q; ++r)
+      for (int w = 0; w < kCompactThreads / 32; ++w) before += row_count[r][w];
+    for (int w = 0; w < warp; ++w) before += row_count[q][w];
+    unsigned m = __ballot_sync(0xffffffffu, keep[q]);
+    if (keep[q]) {
+      long long d = off + before + __popc(m & ((1u << lane) - 1u));
+      uint32_t cell = a.cell[p];
+      if (wrap) {
+        C32 c = load_pos(a, p);
+        wrap_c32(P, c);
+        cell = pack_cell(c.i, c.j, c.k);
+      }
+      o.cell[d] = cell;
+      o.fx[d] = a.fx[p];
+      o.fy[d] = a.fy[p];
+      o.fz[d] = a.fz[p];
+      o.vx[d] = a.vx[p];
+      o.vy[d] = a.vy[p];
+      o.vz[d] = a.vz[p];
+      o.sp[d] = a.sp[p];
+    }
+  }
+}
+
+// Per-species push constants in FP32.
+struct SpeciesF32 {
+  float etadt2[8];
+  float tB[8][3];
+  float sB[8][3];
+};
+
+__device__ inline void gather_c32(const KParams& P, const C32& c, const float4* __restrict__ E, float Ep[3]) {
+  float wx[2] = {1.0f - c.f[0], c.f[0]}, wy[2] = {1.0f - c.f[1], c.f[1]}, wz[2] = {1.0f - c.f[2], c.f[2]};
+  int i0 = min(max(c.i, 0), P.nx + 1), j0 = min(max(c.j, 0), P.ny + 1), k0 = min(max(c.k, 0), P.nz + 1);
+  int i1 = min(max(c.i + 1, 0), P.nx + 1), j1 = min(max(c.j + 1, 0), P.ny + 1), k1 = min(max(c.k + 1, 0), P.nz + 1);
+  Ep[0] = Ep[1] = Ep[2] = 0.0f;
+  const int ii[2] = {i0, i1}, jj[2] = {j0, j1}, kk[2] = {k0, k1};
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      long long row = (long long)P.nxp * ((long long)jj[dj] + (long long)P.nyp * kk[dk]);
+      float4 e0 = __ldg(E + row + ii[0]);
+      float4 e1 = __ldg(E + row + ii[1]);
+      float w = wy[dj] * wz[dk];
+      float a0 = wx[0] * w, a1 = wx[1] * w;
+      Ep[0] += e0.x * a0 + e1.x * a1;
+      Ep[1] += e0.y * a0 + e1.y * a1;
+      Ep[2] += e0.z * a0 + e1.z * a1;
+    }
+}
+
+// AdvanceVelocity.f90:85-119 in FP32 (mode 0); Exp / Imp half steps
+// (modes 1 / 2, AdvanceVelocity.f90:201-230, 311-340).
+__device__ inline void boris_c32(const KParams& P, const SpeciesF32& S, int s, int mode, const float Ep[3], float v[3]) {
+  if (P.fluid[s]) {
+    if (P.gyration[s]) {
+      float B[3] = {float(P.B0[0]), float(P.B0[1]), float(P.B0[2])};
+      float vb = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];
+      float ib = 1.0f / (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+      float vd0 = vb * B[0] + (Ep[1] * B[2] - Ep[2] * B[1]);
+      float vd1 = vb * B[1] + (Ep[2] * B[0] - Ep[0] * B[2]);
+      float vd2 = vb * B[2] + (Ep[0] * B[1] - Ep[1] * B[0]);
+      v[0] = vd0 * ib;
+      v[1] = vd1 * ib;
+      v[2] = vd2 * ib;
+    }
+    return;
+  }
+  const float ve0 = float(P.ve[0]), ve1 = float(P.ve[1]), ve2 = float(P.ve[2]);
+  const float e = S.etadt2[s];
+  const float* tB = S.tB[s];
+  float vmin[3], vmid[3];
+  if (mode == 1) {
+    vmin[0] = v[0] - ve0;
+    vmin[1] = v[1] - ve1;
+    vmin[2] = v[2] - ve2;
+  } else {
+    vmin[0] = v[0] - ve0 + e * Ep[0];
+    vmin[1] = v[1] - ve1 + e * Ep[1];
+    vmin[2] = v[2] - ve2 + e * Ep[2];
+  }
+  vmid[0] = vmin[0] + vmin[1] * tB[2] - vmin[2] * tB[1];
+  vmid[1] = vmin[1] + vmin[2] * tB[0] - vmin[0] * tB[2];
+  vmid[2] = vmin[2] + vmin[0] * tB[1] - vmin[1] * tB[0];
+  if (mode == 0) {
+    const float* sB = S.sB[s];
+    v[0] = vmin[0] + vmid[1] * sB[2] - vmid[2] * sB[1] + ve0 + e * Ep[0];
+    v[1] = vmin[1] + vmid[2] * sB[0] - vmid[0] * sB[2] + ve1 + e * Ep[1];
+    v[2] = vmin[2] + vmid[0] * sB[1] - vmid[1] * sB[0] + ve2 + e * Ep[2];
+    return;
+  }
+  float smid = vmid[0] * vmid[0] + vmid[1] * vmid[1] + vmid[2] * vmid[2];
+  if (smid > 0.0f) {
+    float smin = vmin[0] * vmin[0] + vmin[1] * vmin[1] + vmin[2] * vmin[2];
+    float f = sqrtf(smin / smid);
+    vmid[0] *= f;
+    vmid[1] *= f;
+    vmid[2] *= f;
+  }
+  if (mode == 1) {
+    v[0] = vmid[0] + ve0 + e * Ep[0];
+    v[1] = vmid[1] + ve1 + e * Ep[1];
+    v[2] = vmid[2] + ve2 + e * Ep[2];
+  } else {
+    v[0] = vmid[0] + ve0;
+    v[1] = vmid[1] + ve1;
+    v[2] = vmid[2] + ve2;
+  }
+}
+
+__global__ void advance_velocity_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, long long n, const float4* E, int mode) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    C32 c = load_pos(a, p);
+    float Ep[3];
+    gather_c32(P, c, E, Ep);
+    float v[3] = {a.vx[p], a.vy[p], a.vz[p]};
+    boris_c32(P, S, a.sp[p], mode, Ep, v);
+    a.vx[p] = v[0];
+    a.vy[p] = v[1];
+    a.vz[p] = v[2];
+  }
+}
+
+__device__ inline int fold_index(int i, int n, int open) {
+  if (open) return i < 1 ? 1 : (i > n ? n : i);
+  while (i < 1) i += n;
+  while (i > n) i -= n;
+  return i;
+}
+
+__device__ inline unsigned long long stencil_key(int i, int j, int k, int s) {
+  auto c = [](int v) { v += 2; return (unsigned long long)(v < 0 ? 0 : (v > 0xFFFFF ? 0xFFFFF : v)); };
+  return (c(i) | (c(j) << 20) | (c(k) << 40)) << 4 | (unsigned long long)s;
+}
+
+// Warp-aggregated fixed-point deposit (see particles_exact.cu deposit8).
+__device__ inline void deposit8(unsigned long long key, bool active, const long long w[8], const long long nodes[8],
+                                unsigned long long* plane) {
+  unsigned act = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  unsigned grp = __match_any_sync(act, key);
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(grp) - 1;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    unsigned long long u = (unsigned long long)(w[q] + (1LL << 36));
+    unsigned lo = unsigned(u & 0x3FFFFu), hi = unsigned(u >> 18);
+    unsigned slo = __reduce_add_sync(grp, lo);
+    unsigned shi = __reduce_add_sync(grp, hi);
+    if (lane == leader) {
+      long long cnt = __popc(grp);
+      long long sum = (long long)(((unsigned long long)shi << 18) + (unsigned long long)slo) - cnt * (1LL << 36);
+      atomicAdd(plane + nodes[q], (unsigned long long)sum);
+    }
+  }
+}
+
+// ParticlesGridify.f90:65-123 with FP32 weights rounded to 2^-36 and ghost
+// folds applied to the node indices.
+__global__ void deposit_c32_kernel(KParams P, PartC32 a, long long n, unsigned long long* Nacc,
+                                   unsigned long long* Facc) {
+  long long stride = (long long)gridDim.x * blockDim.x;
+  long long n_round = ((n + 31) / 32) * 32;
+  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n_round; p += stride) {
+    bool active = p < n;
+    long long w[8] = {0, 0, 0, 0, 0, 0, 0, 0}, nodes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float Fw[8];
+    int s = 0;
+    unsigned long long key = ~0ull;
+    if (active) {
+      C32 c = load_pos(a, p);
+      s = a.sp[p];
+      float wx[2] = {1.0f - c.f[0], c.f[0]}, wy[2] = {1.0f - c.f[1], c.f[1]}, wz[2] = {1.0f - c.f[2], c.f[2]};
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        Fw[q] = wx[off[q][0]] * wy[off[q][1]] * wz[off[q][2]];
+        w[q] = __float2ll_rn(Fw[q] * float(kDepositScale));
+        int i = fold_index(c.i + off[q][0], P.nx, P.xflow), j = fold_index(c.j + off[q][1], P.ny, P.yflow),
+            k = fold_index(c.k + off[q][2], P.nz, P.zflow);
+        nodes[q] = node_index(P, i, j, k);
+      }
+      key = stencil_key(c.i, c.j, c.k, s);
+    }
+    deposit8(key, active, w, nodes, Nacc + (long long)s * P.nodes);
+    if (Facc && active) {
+      float vel[3] = {a.vx[p], a.vy[p], a.vz[p]};
+      for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 8; ++q)
+          atomicAdd(Facc + ((long long)s * 3 + c) * P.nodes + nodes[q],
+                    (unsigned long long)__double2ll_rn((double)Fw[q] * (double)vel[c] * kFluxScale));
+    }
+  }
+}
+
+__global__ void energy_particles_c32_kernel(KParams P, PartC32 a, long long n, double* partial) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    int s = a.sp[p];
+    double vx = a.vx[p], vy = a.vy[p], vz = a.vz[p];
+    acc += P.n2p[s] * P.mass[s] * (vx * vx + vy * vy + vz * vz);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t += sh[w];
+    partial[blockIdx.x] = t;
+  }
+}
+
+__global__ void finish_sum_kernel(const double* partial, int nb, double scale, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double t = 0.0;
+    for (int b = 0; b < nb; ++b) t += partial[b];
+    *out = t * scale;
+  }
+}
+
+SpeciesF32 species_f32(const KParams& P, double dt, double deltat, int mode) {
+  SpeciesF32 S;
+  for (int s = 0; s < 8; ++s) {
+    double e = mode == 0 ? 0.5 * dt * P.eta[s] : 0.5 * dt * P.eta[s] * 2.0 * deltat / dt;
+    S.etadt2[s] = float(e);
+    for (int c = 0; c < 3; ++c) {
+      S.tB[s][c] = float(mode == 0 ? P.tB[s][c] : P.tB[s][c] * 2.0 * deltat / dt);
+      S.sB[s][c] = float(P.sB[s][c]);
+    }
+  }
+  return S;
+}
+
+}  // namespace
+
+int scan_scratch_ints(int n) {
+  if (n <= kScanTile) return 0;
+  int nb = (n + kScanTile - 1) / kScanTile;
+  return 2 * nb + 2 + scan_scratch_ints(nb);
+}
+
+cudaError_t launch_scan_int(const int* in, int* out, int n, int* total, int* scratch, cudaStream_t st) {
+  if (n <= 0) return cudaMemsetAsync(total, 0, sizeof(int), st);
+  if (n <= kScanTile) {
+    scan_tiles_kernel<<<1, kScanThreads, 0, st>>>(in, out, n, total);
+    return cudaGetLastError();
+  }
+  int nb = (n + kScanTile - 1) / kScanTile;
+  int* sums = scratch;
+  int* offs = scratch + nb + 1;
+  scan_tiles_kernel<<<nb, kScanThreads, 0, st>>>(in, out, n, sums);
+  cudaError_t e = launch_scan_int(sums, offs, nb, total, offs + nb + 1, st);
+  if (e != cudaSuccess) return e;
+  scan_add_kernel<<<nb, kScanThreads, 0, st>>>(out, n, offs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_advance_position_c32(const KParams& P, PartC32 a, long long n, double dt, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  advance_position_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, float(dt / P.dx), float(dt / P.dy),
+                                                                       float(dt / P.dz));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transfer_c32(const KParams& P, PartC32 a, long long n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  transfer_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compact_outflow_c32(const KParams& P, PartC32 in, PartC32 out, long long n, int* block_counts,
+                                       int* block_offsets, int* new_count, int wrap, cudaStream_t st) {
+  if (n <= 0) return cudaMemsetAsync(new_count, 0, sizeof(int), st);
+  int nb = int((n + kCompactTile - 1) / kCompactTile);
+  outflow_count_c32<<<nb, kCompactThreads, 0, st>>>(P, in, n, block_counts);
+  cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, new_count, block_offsets + nb + 1, st);
+  if (e != cudaSuccess) return e;
+  outflow_scatter_c32<<<nb, kCompactThreads, 0, st>>>(P, in, out, n, block_offsets, wrap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
+                                        double deltat, int mode, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  SpeciesF32 S = species_f32(P, dt, deltat, mode);
+  advance_velocity_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, S, a, n, E, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
+                               unsigned long long* Facc, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  deposit_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, Nacc, Facc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_energy_particles_c32(const KParams& P, PartC32 a, long long n, ReduceBuf rb, cudaStream_t st) {
+  int nb = persistent_grid(n > 0 ? n : 1);
+  if (nb > rb.max_blocks) nb = rb.max_blocks;
+  energy_particles_c32_kernel<<<nb, kThreads, 0, st>>>(P, a, n, rb.partial);
+  finish_sum_kernel<<<1, 32, 0, st>>>(rb.partial, nb, 0.5, rb.result);
+  return cudaGetLastError();
+}
+
+}  // namespace picard

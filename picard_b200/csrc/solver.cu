@@ -1,0 +1,213 @@
+// solver.cu -- CalcEpotential (CalcEpotential.f90:4-246) on the device.
+//
+// The host walks the sweep sequence in batches.  A batch starts at iterate a
+// (the anchor), runs up to m sweeps, reduces each sweep's residual partials
+// in a fixed order and reads the m residual norms back with one copy.  The
+// first iterate d that meets the reference's test -- checked at the top of
+// sweep d+1, so only while d+1 <= maxit -- ends the solve; if d is not the
+// last iterate of the batch it is rebuilt by replaying d - a sweeps from the
+// anchor.  Without a hit the loop stops after 2*maxit+1 sweeps, like the
+// reference, and reports PICARD_ERR_NOT_CONVERGED.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "context.cuh"
+#include "picard_gpu.h"
+
+using namespace picard;
+
+namespace {
+
+// Next batch length: sweeps until the predicted hit, from the last two
+// residual norms, clamped to [16, m_max].
+int next_batch(double r2_prev, double r2_last, double tol2, int m_max) {
+  if (!(r2_prev > 0.0) || !(r2_last > 0.0) || !(r2_last < r2_prev)) return 64;
+  double per = std::log(r2_last / r2_prev);  // < 0
+  double need = std::log(tol2 / r2_last) / per;
+  if (!(need > 0.0)) return 16;
+  double m = need * 0.9;
+  if (m < 16) m = 16;
+  if (m > m_max) m = m_max;
+  return int(m);
+}
+
+bool passes(double r2, double tol) { return std::sqrt(r2) <= tol; }
+
+int read_r2(picard_ctx* c, int count) {
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->r2, sizeof(double) * count, cudaMemcpyDeviceToHost, c->st));
+  PICARD_CUDA(cudaStreamSynchronize(c->st));
+  return PICARD_OK;
+}
+
+// ------------------------------------------------------------- FP64 sweeps
+int solve_f64(picard_ctx* c, double tol, long long smax, int maxit, long long* sweeps, bool* converged) {
+  const KParams& K = c->K;
+  const int nb = c->G.nblocks;
+  double* buf[2] = {c->U, c->U1};
+  PICARD_CUDA(cudaMemcpyAsync(c->U1, c->U, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+  long long a = 0;
+  int m = 64;
+  double r2_prev = 0.0, r2_last = 0.0;
+  const double tol2 = tol * tol;
+  for (;;) {
+    int m_eff = int(std::min<long long>(m, smax - a));
+    PICARD_CUDA(cudaMemcpyAsync(c->Usnap, buf[a % 2], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+    for (int t = 1; t <= m_eff; ++t) {
+      long long s = a + t;
+      PICARD_CUDA(launch_sweep_f64(K, c->G, buf[(s - 1) % 2], buf[s % 2], c->b, c->partials + (size_t)(t - 1) * nb,
+                                   c->st));
+    }
+    PICARD_CUDA(launch_reduce_sweeps(c->partials, nb, m_eff, c->r2, c->st));
+    PICARD_TRY(read_r2(c, m_eff));
+    long long hit = -1;
+    for (int t = 1; t <= m_eff; ++t) {
+      long long d = a + t - 1;  // sweep a+t measured the residual of iterate d
+      double r2 = c->h_pinned[t - 1];
+      if (d >= 1) {
+        r2_prev = r2_last;
+        r2_last = r2;
+        c->last_residual = std::sqrt(r2);
+      }
+      if (d >= 1 && d + 1 <= maxit && passes(r2, tol)) {
+        hit = d;
+        break;
+      }
+    }
+    if (hit >= 0) {
+      long long last = a + m_eff;
+      if (hit != last - 1) {  // rebuild iterate `hit` from the anchor
+        PICARD_CUDA(cudaMemcpyAsync(buf[a % 2], c->Usnap, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+        for (long long s = a + 1; s <= hit; ++s)
+          PICARD_CUDA(launch_sweep_f64(K, c->G, buf[(s - 1) % 2], buf[s % 2], c->b, c->partials, c->st));
+      }
+      if (hit % 2 == 1)
+        PICARD_CUDA(cudaMemcpyAsync(c->U, c->U1, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+      *sweeps = hit;
+      *converged = true;
+      return PICARD_OK;
+    }
+    a += m_eff;
+    if (a >= smax) {
+      if (a % 2 == 1)
+        PICARD_CUDA(cudaMemcpyAsync(c->U, c->U1, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+      *sweeps = a;
+      *converged = false;
+      return PICARD_OK;
+    }
+    m = next_batch(r2_prev, r2_last, tol2, c->m_max);
+  }
+}
+
+// ---------------------------------------------- FP32 increment + FP64 anchor
+int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma, long long* sweeps,
+              bool* converged) {
+  const KParams& K = c->K;
+  const int nb = c->G.nblocks;
+  double* V[2] = {c->U, c->U1};
+  float* R[2] = {c->r, c->r + K.nodes};  // anchor residuals, one per live anchor
+  int vcur = 0, rcur = 0;
+  PICARD_CUDA(cudaMemcpyAsync(c->U1, c->U, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+  // anchor 0: r = (b - L U_0) / sigma
+  PICARD_CUDA(launch_anchor(K, c->G, V[vcur], V[1 - vcur], nullptr, c->b, R[rcur], sigma, c->partials, 1, c->st));
+  vcur = 1 - vcur;
+  long long a = 0;
+  int m = 64;
+  double r2_prev = 0.0, r2_last = 0.0;
+  const double tol2 = tol * tol;
+  for (;;) {
+    int m_eff = int(std::min<long long>(m, smax - a));
+    for (int t = 1; t <= m_eff; ++t) {
+      long long s = a + t;
+      PICARD_CUDA(launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rcur],
+                                   c->partials + (size_t)(t - 1) * nb, t == 1 ? 1 : 0, c->st));
+    }
+    // next anchor: fold w_{a+m_eff} into V, exact FP64 residual of that iterate
+    long long an = a + m_eff;
+    PICARD_CUDA(launch_anchor(K, c->G, V[vcur], V[1 - vcur], c->w[an % 2], c->b, R[1 - rcur], sigma,
+                              c->partials + (size_t)m_eff * nb, 0, c->st));
+    PICARD_CUDA(launch_reduce_sweeps(c->partials, nb, m_eff + 1, c->r2, c->st));
+    PICARD_TRY(read_r2(c, m_eff + 1));
+    long long hit = -1;
+    // sweep a+t (t >= 2) measured iterate a+t-1 in FP32 (scaled by sigma^2);
+    // the anchor measured iterate a+m_eff in FP64
+    for (int t = 2; t <= m_eff + 1; ++t) {
+      long long d = a + t - 1;
+      double r2 = t <= m_eff ? c->h_pinned[t - 1] * sigma * sigma : c->h_pinned[m_eff];
+      r2_prev = r2_last;
+      r2_last = r2;
+      c->last_residual = std::sqrt(r2);
+      if (d >= 1 && d + 1 <= maxit && passes(r2, tol)) {
+        hit = d;
+        break;
+      }
+    }
+    if (hit >= 0) {
+      if (hit == an) {
+        // the new anchor holds the iterate
+        if (V[1 - vcur] != c->U)
+          PICARD_CUDA(cudaMemcpyAsync(c->U, V[1 - vcur], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+      } else {
+        // replay sweeps a+1..hit from the old anchor (unchanged in V[vcur])
+        for (long long s = a + 1; s <= hit; ++s)
+          PICARD_CUDA(launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rcur], c->partials,
+                                       s == a + 1 ? 1 : 0, c->st));
+        PICARD_CUDA(launch_finalize(K, V[vcur], c->w[hit % 2], sigma, c->U, 0, c->st));
+      }
+      *sweeps = hit;
+      *converged = true;
+      return PICARD_OK;
+    }
+    vcur = 1 - vcur;
+    rcur = 1 - rcur;
+    a = an;
+    if (a >= smax) {
+      if (V[vcur] != c->U)
+        PICARD_CUDA(cudaMemcpyAsync(c->U, V[vcur], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+      *sweeps = a;
+      *converged = false;
+      return PICARD_OK;
+    }
+    m = next_batch(r2_prev, r2_last, tol2, c->m_max);
+  }
+}
+
+}  // namespace
+
+extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t maxit, int32_t* sweeps_out) {
+  if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
+  if (maxit < 0) return fail(PICARD_ERR_BAD_ARG, "maxit must be >= 0");
+  const KParams& K = c->K;
+  // b = -C/(dV eps0) and ||b||^2 over the interior (CalcEpotential.f90:50-54)
+  PICARD_CUDA(launch_rhs(K, c->C, c->b, c->red_partial, c->red_result + 4, c->st));
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->red_result + 4, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  PICARD_CUDA(cudaStreamSynchronize(c->st));
+  const double b2 = c->h_pinned[0];
+  const double bnorm = std::sqrt(b2);
+  const double tol = maxerr * bnorm;
+  const long long smax = 2LL * maxit + 1;
+  c->last_bnorm = bnorm;
+  long long sweeps = 0;
+  bool converged = true;
+  // the check at the top of sweep 1 uses r_global = ||b||^2 (CalcEpotential.f90:55-61)
+  if (1 <= maxit && std::sqrt(b2) <= tol) {
+    sweeps = 0;
+    c->last_residual = bnorm;
+  } else if (c->solver == PICARD_SOLVER_F64) {
+    PICARD_TRY(solve_f64(c, tol, smax, maxit, &sweeps, &converged));
+  } else {
+    long long nint = (long long)K.nx * K.ny * K.nz;
+    double sigma = std::sqrt(b2 / (double)nint);
+    if (!(sigma > 0.0)) sigma = 1.0;
+    PICARD_TRY(solve_f32(c, tol, smax, maxit, sigma, &sweeps, &converged));
+  }
+  PICARD_CUDA(launch_refresh_periodic(K, c->U, c->st));
+  c->last_sweeps = sweeps;
+  if (sweeps_out) *sweeps_out = int32_t(sweeps);
+  if (!converged)
+    return fail(PICARD_ERR_NOT_CONVERGED,
+                "Jacobi reached 2*maxit+1 = " + std::to_string(smax) + " sweeps without meeting maxerr");
+  return PICARD_OK;
+}

@@ -1,0 +1,294 @@
+"""Parity of the sm_100a kernels (through the C ABI) with the FP64 oracle.
+
+Bars: integer and index results (cell indices, removed / wrapped particle
+sets, species, particle counts, D) bit-exact; FP64-layout positions bit-exact
+and velocities within 1e-13 relative (libm log/sin differ from CUDA's by an
+ulp); fixed-point deposits within 1e-10 relative L2; potential and field
+within 1e-6 relative L2 of the FP64 oracle (the
+FP64 solver meets 1e-10).  CELL32 (FP32 particles) is held to tolerances
+written beside each check.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from picard_b200 import capi
+from picard_b200.simulation import Simulation
+from tests.helpers import cell_indices, rel_l2, small_haser, small_plasma, sort_particles
+
+pytestmark = pytest.mark.gpu
+
+F64 = dict(layout=capi.LAYOUT_F64, solver=capi.SOLVER_F64)
+F64_REFINE = dict(layout=capi.LAYOUT_F64, solver=capi.SOLVER_F32_REFINE)
+C32 = dict(layout=capi.LAYOUT_CELL32, solver=capi.SOLVER_F32_REFINE)
+
+
+def make(p, **kw):
+    q = O.derive(p)
+    return q, O.OracleState(q), Simulation(q, derive=False, **kw)
+
+
+def assert_same_particles(rp_g, ip_g, rp_o, ip_o, vel_rtol=1e-13):
+    assert rp_g.shape == rp_o.shape
+    np.testing.assert_array_equal(ip_g, ip_o)
+    np.testing.assert_array_equal(rp_g[:, :3], rp_o[:, :3])
+    np.testing.assert_allclose(rp_g[:, 3:6], rp_o[:, 3:6], rtol=vel_rtol, atol=1e-9)
+
+
+# ------------------------------------------------------------- per routine
+
+def test_initialize_matches_oracle():
+    p, o, g = make(small_plasma(n=8, ppc=4), **F64)
+    o.initialize()
+    g.particles_initialize()
+    rp, ip = g.particles()
+    ro, io = o.particles()
+    assert_same_particles(rp, ip, ro, io)
+
+
+@pytest.mark.parametrize("yflow", [1, 0])
+def test_inflow_matches_oracle(yflow):
+    p, o, g = make(small_plasma(n=6, ppc=3, yflow=yflow), **F64)
+    o.bc_inflow(5)
+    g.bc_inflow(5)
+    assert g.num_local == o.num_local
+    assert_same_particles(*g.particles(), *o.particles())
+
+
+def test_produce_matches_oracle():
+    p, o, g = make(small_haser(nx=8, ny=8, nz=8, ppc=1, q=3e24, dt_scaled=0), **F64)
+    o.produce(2)
+    g.particles_produce(2)
+    assert o.num_local > 0 and g.num_local == o.num_local
+    assert_same_particles(*g.particles(), *o.particles(), vel_rtol=0)
+
+
+def test_advance_outflow_transfer_sets_bit_exact():
+    p, o, g = make(small_plasma(n=6, ppc=3, zflow=0, seed=4), **F64)
+    o.initialize()
+    g.set_particles(*o.particles())
+    for s in (o, g):
+        s.advance_position(p.dt * 3000)
+    np.testing.assert_array_equal(g.particles()[0], o.particles()[0])
+    o.bc_outflow()
+    g.bc_outflow()
+    o.transfer()
+    g.particles_transfer()
+    assert g.num_local == o.num_local
+    rg, ig = sort_particles(*g.particles())
+    ro, io = sort_particles(*o.particles())
+    np.testing.assert_array_equal(rg, ro)
+    np.testing.assert_array_equal(ig, io)
+    np.testing.assert_array_equal(cell_indices(p, rg), cell_indices(p, ro))
+
+
+def test_calc_distance_bit_exact():
+    p, o, g = make(small_plasma(n=6, ppc=1, xflow=0), **F64)
+    o.calc_distance()
+    g.calc_distance()
+    np.testing.assert_array_equal(g.field(capi.FIELD_D), o.D)
+
+
+@pytest.mark.parametrize("periodic", [None, "x"])
+def test_gridify_matches_oracle(periodic):
+    kw = {} if periodic is None else {periodic + "flow": 0}
+    p, o, g = make(small_plasma(n=8, ppc=4, seed=2, **kw), **F64)
+    o.initialize()
+    o.advance_position(p.dt * 2500)
+    o.bc_outflow()
+    o.transfer()
+    g.set_particles(*o.particles())
+    o.gridify()
+    g.particles_gridify()
+    assert rel_l2(g.field(capi.FIELD_N), o.N) < 1e-10
+    # C = sum_s q_s N_s cancels between species: compare against the charge scale
+    scale = max(abs(p.charge[s]) * np.abs(o.N[..., s]).max() for s in range(p.species))
+    assert np.abs(g.field(capi.FIELD_C) - o.C).max() < 1e-10 * scale
+    o.gridify_all()
+    g.particles_gridify_all()
+    assert rel_l2(g.field(capi.FIELD_F), o.F) < 1e-9
+
+
+def _charged_state(p, o, steps=1):
+    o.calc_distance()
+    o.initialize()
+    for it in range(1, steps + 1):
+        o.step(it)
+
+
+def test_bc_potentials_matches_oracle():
+    p, o, g = make(small_plasma(n=8, ppc=4, seed=3), **F64)
+    _charged_state(p, o)
+    o.gridify()
+    g.calc_distance()
+    g.set_field(capi.FIELD_C, o.C)
+    o.bc_potentials()
+    g.bc_potentials()
+    assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-12
+
+
+@pytest.mark.parametrize("mode", ["F64", "F64_REFINE"])
+def test_jacobi_matches_oracle(mode):
+    kw = F64 if mode == "F64" else F64_REFINE
+    p, o, g = make(small_plasma(n=12, ppc=4, seed=5), **kw)
+    _charged_state(p, o)
+    o.gridify()
+    o.bc_potentials()
+    g.set_field(capi.FIELD_C, o.C)
+    g.set_field(capi.FIELD_U, o.U)
+    sweeps_o, conv, _ = o.calc_epotential()
+    sweeps_g = g.calc_epotential()
+    assert conv and sweeps_o > 50
+    if mode == "F64":
+        assert sweeps_g == sweeps_o
+        assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-10
+    else:
+        assert abs(sweeps_g - sweeps_o) <= 1
+        assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-6
+
+
+def test_jacobi_cap_reports_not_converged():
+    p, o, g = make(small_plasma(n=6, ppc=1), **F64)
+    C = np.zeros_like(o.C)
+    C[2:-2, 2:-2, 2:-2] = 1e-15
+    o.C[...] = C
+    g.set_field(capi.FIELD_C, C)
+    g.set_field(capi.FIELD_U, np.zeros_like(o.U))
+    s_o, conv, _ = o.calc_epotential(maxerr=1e-12, maxit=3)
+    with pytest.raises(capi.PicardError) as e:
+        g._call("picard_gpu_calc_epotential", 1e-12, 3, None)
+    assert e.value.code == capi.ERR_NOT_CONVERGED
+    assert not conv and s_o == 7
+    assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-12
+
+
+def test_efield_matches_oracle():
+    p, o, g = make(small_plasma(n=8, ppc=4, seed=6, zflow=0), **F64)
+    _charged_state(p, o)
+    g.set_field(capi.FIELD_U, o.U)
+    o.calc_efield()
+    o.bc_fields()
+    g.calc_efield()
+    g.bc_fields()
+    assert rel_l2(g.field(capi.FIELD_E), o.E) < 1e-13
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_advance_velocity_bit_exact_given_field(mode):
+    p, o, g = make(small_plasma(n=8, ppc=4, seed=8), **F64)
+    _charged_state(p, o)
+    g.set_particles(*o.particles())
+    g.set_field(capi.FIELD_E, o.E)
+    o.advance_velocity(mode=mode, deltat=0.5 * p.dt)
+    if mode == 0:
+        g.advance_velocity()
+    elif mode == 1:
+        g.advance_velocity_exp(0.5 * p.dt)
+    else:
+        g.advance_velocity_imp(0.5 * p.dt)
+    rg, ig = g.particles()
+    ro, io = o.particles()
+    np.testing.assert_array_equal(rg[:, :6], ro[:, :6])
+
+
+def test_energy_matches_oracle():
+    p, o, g = make(small_plasma(n=8, ppc=4, seed=9), **F64)
+    _charged_state(p, o)
+    g.set_particles(*o.particles())
+    g.set_field(capi.FIELD_E, o.E)
+    np.testing.assert_allclose(g.energy(), o.energy(), rtol=1e-12)
+
+
+# ---------------------------------------------------------------- full step
+
+def test_one_step_parity_f64_layout():
+    p, o, g = make(small_plasma(n=10, ppc=4, seed=12), **F64)
+    o.calc_distance()
+    o.initialize()
+    o.step(1)
+    g.calc_distance()
+    g.set_particles(*o.particles())
+    o.step(2)
+    g.run(1, 2)
+    assert g.num_local == o.num_local
+    rg, ig = sort_particles(*g.particles())
+    ro, io = sort_particles(*o.particles())
+    # positions were advanced with identical velocities: bit-exact
+    np.testing.assert_array_equal(rg[:, :3], ro[:, :3])
+    np.testing.assert_array_equal(ig, io)
+    np.testing.assert_array_equal(cell_indices(p, rg), cell_indices(p, ro))
+    np.testing.assert_allclose(rg[:, 3:6], ro[:, 3:6], rtol=1e-9, atol=1e-6)
+    assert rel_l2(g.field(capi.FIELD_N), o.N) < 1e-10
+    assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-10
+    assert rel_l2(g.field(capi.FIELD_E), o.E) < 1e-9
+
+
+def test_one_step_parity_cell32_layout():
+    p, o, g = make(small_plasma(n=10, ppc=4, seed=13), **C32)
+    o.calc_distance()
+    o.initialize()
+    o.step(1)
+    g.calc_distance()
+    g.set_particles(*o.particles())
+    o.step(2)
+    g.run(1, 2)
+    assert abs(g.num_local - o.num_local) <= 2
+    rg, ig = g.particles()
+    ro, io = o.particles()
+    # FP32 offsets: cell indices equal except for particles within 1e-5 cells of a face
+    d = np.array(list(p.dxyz))
+    if g.num_local == o.num_local:
+        rg, ig = sort_particles(rg, ig)
+        ro, io = sort_particles(ro, io)
+        np.testing.assert_allclose(rg[:, :3], ro[:, :3], rtol=0, atol=1e-5 * d.min())
+        mism = np.any(cell_indices(p, rg) != cell_indices(p, ro), axis=1)
+        assert mism.sum() <= 2
+    # fields: N within 1e-6, U and E within the north-star 1e-6 relative L2
+    assert rel_l2(g.field(capi.FIELD_N), o.N) < 1e-6
+    assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-6
+    assert rel_l2(g.field(capi.FIELD_E), o.E) < 1e-5
+
+
+@pytest.mark.parametrize("kw,tol", [(F64, 1e-9), (C32, 2e-5)])
+def test_multi_step_energy_moments(kw, tol):
+    p, o, g = make(small_plasma(n=8, ppc=4, seed=21), **kw)
+    o.calc_distance()
+    o.initialize()
+    g.calc_distance()
+    g.particles_initialize()
+    for it in range(1, 6):
+        o.step(it)
+    g.run(0, 5)
+    assert abs(g.num_local - o.num_local) <= (0 if kw is F64 else 3)
+    eg, eo = g.energy(), o.energy()
+    assert abs(eg[0] - eo[0]) <= tol * eo[0]                 # particle kinetic energy
+    assert abs(eg[1] - eo[1]) <= max(tol, 1e-4) * eo[1]      # field energy
+    assert eg[2] == pytest.approx(eo[2], rel=1e-12)
+
+
+def test_fused_loop_equals_plain_loop_f64():
+    p = O.derive(small_plasma(n=8, ppc=4, seed=31))
+    a = Simulation(p, derive=False, **F64)
+    b = Simulation(p, derive=False, **F64)
+    for s in (a, b):
+        s.calc_distance()
+        s.particles_initialize()
+    sa = a.run(0, 3)
+    sb = b.run_fused(0, 3)
+    assert sa == sb
+    assert a.num_local == b.num_local
+    ra, ia = sort_particles(*a.particles())
+    rb, ib = sort_particles(*b.particles())
+    np.testing.assert_array_equal(ia, ib)
+    np.testing.assert_array_equal(ra[:, :3], rb[:, :3])
+    np.testing.assert_allclose(ra[:, 3:6], rb[:, 3:6], rtol=1e-12, atol=1e-9)
+
+
+def test_capacity_error_is_reported():
+    p = small_plasma(n=6, ppc=2)
+    p.max_per_proc = 100
+    q = O.derive(p)
+    g = Simulation(q, derive=False, **C32)
+    with pytest.raises(capi.PicardError) as e:
+        g.particles_initialize()
+    assert e.value.code == capi.ERR_CAPACITY
