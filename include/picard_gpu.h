@@ -176,6 +176,35 @@ PICARD_API int picard_gpu_advance_velocity_imp(picard_ctx* ctx, double deltat,
  * FP64), *num = num_local. */
 PICARD_API int picard_gpu_energy(picard_ctx* ctx, double out[3], int32_t* num);
 
+/* ------------------------------------------------------------ statistics */
+
+/* Counters of the work a context has done since creation or the last
+ * picard_gpu_reset_stats.  sweep_ms is the device time of the Jacobi sweep
+ * kernels, taken with CUDA events on the context's stream around every batch
+ * of sweeps (the hottest kernel of the loop); kernel_launches counts the
+ * kernels this library launched in the process over the same interval. */
+typedef struct picard_stats {
+  int64_t kernel_launches;
+  int64_t solves;          /* CalcEpotential calls                          */
+  int64_t sweeps;          /* Jacobi iterations accepted, summed over solves */
+  int64_t sweep_launches;  /* sweep kernels run (replays and overshoot too)  */
+  double sweep_ms;         /* device time of those sweep launches            */
+  int64_t anchor_launches; /* FP64 anchor passes (F32_REFINE solver)         */
+  double anchor_ms;
+  double last_residual;    /* ||b - L U|| of the last accepted iterate       */
+  double last_bnorm;       /* ||b|| of the last solve                        */
+  int64_t steps;           /* main-loop iterations run                       */
+  int64_t particle_steps;  /* live particles summed over those iterations   */
+  int64_t h2d_bytes;       /* host-to-device bytes copied by the library     */
+  int64_t d2h_bytes;       /* device-to-host bytes copied by the library     */
+} picard_stats;
+
+PICARD_API int picard_gpu_get_stats(picard_ctx* ctx, picard_stats* out);
+PICARD_API int picard_gpu_reset_stats(picard_ctx* ctx);
+/* The cudaStream_t every kernel of this context runs on (for callers that
+ * record their own CUDA events around library calls). */
+PICARD_API int picard_gpu_get_stream(picard_ctx* ctx, void** stream);
+
 /* ----------------------------------------------------------- main loop */
 
 /* One line of the reference's energy log (picard.f90:667-671). */

@@ -60,6 +60,7 @@ def lib():
         L.orc_particles_gridify.argtypes = [P, dp, ip, C.c_int32, dp, dp]
         L.orc_particles_gridify_all.argtypes = [P, dp, ip, C.c_int32, dp, dp, dp]
         L.orc_bc_potentials.argtypes = [P, dp, dp, dp]
+        L.orc_bc_potentials_sampled.argtypes = [P, dp, dp, dp, C.c_int]
         L.orc_calc_epotential.argtypes = [P, dp, dp, C.c_double, C.c_int, C.POINTER(C.c_int), dp]
         L.orc_calc_epotential.restype = C.c_int
         L.orc_calc_efield.argtypes = [P, dp, dp]
@@ -183,6 +184,9 @@ class OracleState:
 
     def bc_potentials(self):
         lib().orc_bc_potentials(C.byref(self.p), _d(self.U), _d(self.C), _d(self.D))
+
+    def bc_potentials_sampled(self, stride: int):
+        lib().orc_bc_potentials_sampled(C.byref(self.p), _d(self.U), _d(self.C), _d(self.D), stride)
 
     def calc_epotential(self, maxerr: float | None = None, maxit: int | None = None):
         conv = C.c_int(0)

@@ -396,10 +396,23 @@ static int create_group(const picard_params* p, uint64_t seed, uint32_t tag, uin
   return n;
 }
 
-/* ParticlesInitialize.f90:54-119 */
+/* particles created per cell by one ParticlesInitialize / BCinflow cell loop */
+static int per_cell_count(const picard_params* p) {
+  int c = 0;
+  for (int s = 0; s < p->species; ++s) c += p->ipp[s] * (1 + p->epp[s] + p->hpp[s]);
+  return c;
+}
+
+/* ParticlesInitialize.f90:54-119.  Every cell creates the same number of
+ * particles, so cell (ii, jj, kk) owns a fixed block of slots in the
+ * reference's append order and the cells can be filled in parallel. */
 EXPORT int orc_particles_initialize(const picard_params* p, double* rp, int32_t* ip, int32_t* num_local) {
   const double* dxyz = p->dxyz;
-  int n = *num_local;
+  const int n0 = *num_local;
+  const long long per_cell = per_cell_count(p);
+  const long long cells = (long long)p->nx * p->ny * p->nz;
+  if (!append_guard(n0, (int)(cells * per_cell), p->max_per_proc) || n0 + cells * per_cell > 2147483647LL) return 2;
+#pragma omp parallel for collapse(2) schedule(static)
   for (int kk = 2; kk <= p->nz + 1; ++kk)
     for (int jj = 2; jj <= p->ny + 1; ++jj)
       for (int ii = 2; ii <= p->nx + 1; ++ii) {
@@ -407,35 +420,60 @@ EXPORT int orc_particles_initialize(const picard_params* p, double* rp, int32_t*
         double y0 = p->Ly_min + dxyz[1] * (jj - 2);
         double z0 = p->Lz_min + dxyz[2] * (kk - 2);
         uint32_t a = (uint32_t)G3(ii, jj, kk);
+        long long cell = (ii - 2) + (long long)p->nx * ((jj - 2) + (long long)p->ny * (kk - 2));
+        int n = (int)(n0 + cell * per_cell);
         for (int ss = 1; ss <= p->species; ++ss)
-          for (int pp = 1; pp <= p->ipp[ss - 1]; ++pp) {
-            int add = 1 + p->epp[ss - 1] + p->hpp[ss - 1];
-            if (!append_guard(n, add, p->max_per_proc)) return 2;
-            n += create_group(p, p->seed, 1, 0, a, ss, pp, x0, y0, z0, rp, ip, n);
-          }
+          for (int pp = 1; pp <= p->ipp[ss - 1]; ++pp) n += create_group(p, p->seed, 1, 0, a, ss, pp, x0, y0, z0, rp, ip, n);
       }
-  *num_local = n;
+  *num_local = (int)(n0 + cells * per_cell);
   return 0;
 }
 
 /* ---------------------------------------------------- BCinflow (a3) */
 
-static int inflow_cell(const picard_params* p, int iteration, int ii, int jj, int kk, int ss_first, double x0,
-                       double y0, double z0, double* rp, int32_t* ip, int* n) {
-  uint32_t a = (uint32_t)G3(ii, jj, kk);
-  for (int ss = ss_first; ss <= p->species; ++ss)
-    for (int pp = 1; pp <= p->ipp[ss - 1]; ++pp) {
-      int add = 1 + p->epp[ss - 1] + p->hpp[ss - 1];
-      if (!append_guard(*n, add, p->max_per_proc)) return 2;
-      *n += create_group(p, p->seed, 2, (uint32_t)iteration, a, ss, pp, x0, y0, z0, rp, ip, *n);
+/* One face of BCinflow: `outer` x `inner` loop over guard cells in the
+ * reference's order.  Every guard cell creates the same number of particles,
+ * so each owns a fixed block of slots and the cells run in parallel.
+ * axis 0: (outer kk, inner jj) at ii = fixed; axis 1: (outer kk, inner ii) at
+ * jj = fixed; axis 2: (outer jj, inner ii) at kk = fixed.  `edge` is the
+ * lower edge of the guard layer along the face normal. */
+static void inflow_face(const picard_params* p, int iteration, int axis, int fixed, int o_lo, int o_hi, int i_lo,
+                        int i_hi, double edge, double* rp, int32_t* ip, int* n) {
+  const double* dxyz = p->dxyz;
+  const long long per_cell = per_cell_count(p);
+  const int o_n = o_hi - o_lo + 1, i_n = i_hi - i_lo + 1;
+  if (o_n <= 0 || i_n <= 0) return;
+  const int n0 = *n;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int o = o_lo; o <= o_hi; ++o)
+    for (int in = i_lo; in <= i_hi; ++in) {
+      int ii, jj, kk;
+      double x0, y0, z0;
+      if (axis == 0) {
+        ii = fixed, kk = o, jj = in;
+        x0 = edge, y0 = p->Ly_min + dxyz[1] * (jj - 2), z0 = p->Lz_min + dxyz[2] * (kk - 2);
+      } else if (axis == 1) {
+        jj = fixed, kk = o, ii = in;
+        x0 = p->Lx_min + dxyz[0] * (ii - 2), y0 = edge, z0 = p->Lz_min + dxyz[2] * (kk - 2);
+      } else {
+        kk = fixed, jj = o, ii = in;
+        x0 = p->Lx_min + dxyz[0] * (ii - 2), y0 = p->Ly_min + dxyz[1] * (jj - 2), z0 = edge;
+      }
+      uint32_t a = (uint32_t)G3(ii, jj, kk);
+      int slot = (int)(n0 + ((long long)(o - o_lo) * i_n + (in - i_lo)) * per_cell);
+      for (int ss = 1; ss <= p->species; ++ss)
+        for (int pp = 1; pp <= p->ipp[ss - 1]; ++pp)
+          slot += create_group(p, p->seed, 2, (uint32_t)iteration, a, ss, pp, x0, y0, z0, rp, ip, slot);
     }
-  return 0;
+  *n = (int)(n0 + (long long)o_n * i_n * per_cell);
 }
 
 /* BCinflow.f90:23-476 on one rank.  Each guard cell of the open faces is
  * filled once: x faces span the extended y and z range, y faces extend z on
  * the +z side (+y face) or the -z side (-y face), z faces extend y on the -y
- * side (+z face) or the +y side (-z face). */
+ * side (+z face) or the +y side (-z face).  The x faces loop over species
+ * 1..S and the y and z faces over 2..S (BCinflow.f90:63, 204); ipp(1) = 0
+ * makes the two the same. */
 EXPORT int orc_bc_inflow(const picard_params* p, int iteration, double* rp, int32_t* ip, int32_t* num_local) {
   const double* dxyz = p->dxyz;
   const int Nx = p->nx, Ny = p->ny, Nz = p->nz;
@@ -443,49 +481,24 @@ EXPORT int orc_bc_inflow(const picard_params* p, int iteration, double* rp, int3
   int yneg = (p->yflow && (p->Ly_min - 0.5 * dxyz[1] < p->ymin)) ? 1 : 0;
   int zpos = (p->zflow && (p->Lz_max + 0.5 * dxyz[2] > p->zmax)) ? 1 : 0;
   int zneg = (p->zflow && (p->Lz_min - 0.5 * dxyz[2] < p->zmin)) ? 1 : 0;
-  int n = *num_local, rc;
-  if (p->xflow && (p->Lx_max + 0.5 * dxyz[0] > p->xmax)) {
-    for (int kk = 2 - zneg; kk <= Nz + 1 + zpos; ++kk)
-      for (int jj = 2 - yneg; jj <= Ny + 1 + ypos; ++jj) {
-        double x0 = p->Lx_max, y0 = p->Ly_min + dxyz[1] * (jj - 2), z0 = p->Lz_min + dxyz[2] * (kk - 2);
-        if ((rc = inflow_cell(p, iteration, Nx + 2, jj, kk, 1, x0, y0, z0, rp, ip, &n))) return rc;
-      }
+  int xpos = (p->xflow && (p->Lx_max + 0.5 * dxyz[0] > p->xmax)) ? 1 : 0;
+  int xneg = (p->xflow && (p->Lx_min - 0.5 * dxyz[0] < p->xmin)) ? 1 : 0;
+  long long per_cell = per_cell_count(p);
+  long long cells = (long long)(xpos + xneg) * (Nz + zneg + zpos) * (Ny + yneg + ypos) +
+                    (long long)ypos * (Nz + zpos) * Nx + (long long)yneg * (Nz + zneg) * Nx +
+                    (long long)zpos * (Ny + yneg) * Nx + (long long)zneg * (Ny + ypos) * Nx;
+  int n = *num_local;
+  if ((long long)n + cells * per_cell > p->max_per_proc) {
+    fprintf(stderr, "oracle: particle capacity %d exceeded\n", p->max_per_proc);
+    return 2;
   }
-  if (p->xflow && (p->Lx_min - 0.5 * dxyz[0] < p->xmin)) {
-    for (int kk = 2 - zneg; kk <= Nz + 1 + zpos; ++kk)
-      for (int jj = 2 - yneg; jj <= Ny + 1 + ypos; ++jj) {
-        double x0 = p->Lx_min - dxyz[0], y0 = p->Ly_min + dxyz[1] * (jj - 2), z0 = p->Lz_min + dxyz[2] * (kk - 2);
-        if ((rc = inflow_cell(p, iteration, 1, jj, kk, 1, x0, y0, z0, rp, ip, &n))) return rc;
-      }
-  }
-  if (ypos > 0) {
-    for (int kk = 2; kk <= Nz + 1 + zpos; ++kk)
-      for (int ii = 2; ii <= Nx + 1; ++ii) {
-        double x0 = p->Lx_min + dxyz[0] * (ii - 2), y0 = p->Ly_max, z0 = p->Lz_min + dxyz[2] * (kk - 2);
-        if ((rc = inflow_cell(p, iteration, ii, Ny + 2, kk, 2, x0, y0, z0, rp, ip, &n))) return rc;
-      }
-  }
-  if (yneg > 0) {
-    for (int kk = 2 - zneg; kk <= Nz + 1; ++kk)
-      for (int ii = 2; ii <= Nx + 1; ++ii) {
-        double x0 = p->Lx_min + dxyz[0] * (ii - 2), y0 = p->Ly_min - dxyz[1], z0 = p->Lz_min + dxyz[2] * (kk - 2);
-        if ((rc = inflow_cell(p, iteration, ii, 1, kk, 2, x0, y0, z0, rp, ip, &n))) return rc;
-      }
-  }
-  if (zpos > 0) {
-    for (int jj = 2 - yneg; jj <= Ny + 1; ++jj)
-      for (int ii = 2; ii <= Nx + 1; ++ii) {
-        double x0 = p->Lx_min + dxyz[0] * (ii - 2), y0 = p->Ly_min + dxyz[1] * (jj - 2), z0 = p->Lz_max;
-        if ((rc = inflow_cell(p, iteration, ii, jj, Nz + 2, 2, x0, y0, z0, rp, ip, &n))) return rc;
-      }
-  }
-  if (zneg > 0) {
-    for (int jj = 2; jj <= Ny + 1 + ypos; ++jj)
-      for (int ii = 2; ii <= Nx + 1; ++ii) {
-        double x0 = p->Lx_min + dxyz[0] * (ii - 2), y0 = p->Ly_min + dxyz[1] * (jj - 2), z0 = p->Lz_min - dxyz[2];
-        if ((rc = inflow_cell(p, iteration, ii, jj, 1, 2, x0, y0, z0, rp, ip, &n))) return rc;
-      }
-  }
+  if (xpos) inflow_face(p, iteration, 0, Nx + 2, 2 - zneg, Nz + 1 + zpos, 2 - yneg, Ny + 1 + ypos, p->Lx_max, rp, ip, &n);
+  if (xneg)
+    inflow_face(p, iteration, 0, 1, 2 - zneg, Nz + 1 + zpos, 2 - yneg, Ny + 1 + ypos, p->Lx_min - dxyz[0], rp, ip, &n);
+  if (ypos) inflow_face(p, iteration, 1, Ny + 2, 2, Nz + 1 + zpos, 2, Nx + 1, p->Ly_max, rp, ip, &n);
+  if (yneg) inflow_face(p, iteration, 1, 1, 2 - zneg, Nz + 1, 2, Nx + 1, p->Ly_min - dxyz[1], rp, ip, &n);
+  if (zpos) inflow_face(p, iteration, 2, Nz + 2, 2 - yneg, Ny + 1, 2, Nx + 1, p->Lz_max, rp, ip, &n);
+  if (zneg) inflow_face(p, iteration, 2, 1, 2, Ny + 1 + ypos, 2, Nx + 1, p->Lz_min - dxyz[2], rp, ip, &n);
   *num_local = n;
   return 0;
 }
@@ -807,8 +820,10 @@ EXPORT void orc_particles_gridify_all(const picard_params* p, const double* rp, 
 
 /* -------------------------------------------- BCpotentials (a9) */
 
-/* BCpotentials.f90:36-139 on one rank (bi = bj = bk = 0, Nx = Nx_local). */
-EXPORT void orc_bc_potentials(const picard_params* p, double* U, const double* C, const double* D) {
+/* BCpotentials.f90:36-139 on one rank (bi = bj = bk = 0, Nx = Nx_local).
+ * stride > 1 computes only every stride-th node of each face (in the face's
+ * loop order) -- a bounded sample for timing the CPU baseline. */
+static void bc_potentials_core(const picard_params* p, double* U, const double* C, const double* D, int stride) {
   const int Nx = p->nx, Ny = p->ny, Nz = p->nz;
   const size_t nn = (size_t)NXP * NYP * NZP;
   const int DX = 2 * Nx + 1, DY = 2 * Ny + 1;
@@ -830,6 +845,7 @@ EXPORT void orc_bc_potentials(const picard_params* p, double* U, const double* C
 #pragma omp parallel for collapse(2) schedule(dynamic)
     for (int kk = 1; kk <= Nz; ++kk)
       for (int jj = 1; jj <= Ny; ++jj) {
+        if (stride > 1 && ((jj - 1) + Ny * (kk - 1)) % stride) continue;
         int dj = Ny + 1 + (1 - jj), dk = Nz + 1 + (1 - kk);
         double u0, u1;
         WINDOW_SUM(Nx + 2, dj, dk, u0);
@@ -842,6 +858,7 @@ EXPORT void orc_bc_potentials(const picard_params* p, double* U, const double* C
 #pragma omp parallel for collapse(2) schedule(dynamic)
     for (int kk = 1; kk <= Nz; ++kk)
       for (int ii = 1; ii <= Nx; ++ii) {
+        if (stride > 1 && ((ii - 1) + Nx * (kk - 1)) % stride) continue;
         int di = Nx + 1 + (1 - ii), dk = Nz + 1 + (1 - kk);
         double u0, u1;
         WINDOW_SUM(di, Ny + 2, dk, u0);
@@ -854,6 +871,7 @@ EXPORT void orc_bc_potentials(const picard_params* p, double* U, const double* C
 #pragma omp parallel for collapse(2) schedule(dynamic)
     for (int jj = 1; jj <= Ny; ++jj)
       for (int ii = 1; ii <= Nx; ++ii) {
+        if (stride > 1 && ((ii - 1) + Nx * (jj - 1)) % stride) continue;
         int di = Nx + 1 + (1 - ii), dj = Ny + 1 + (1 - jj);
         double u0, u1;
         WINDOW_SUM(di, dj, Nz + 2, u0);
@@ -864,6 +882,15 @@ EXPORT void orc_bc_potentials(const picard_params* p, double* U, const double* C
   }
 #undef WINDOW_SUM
 #undef DD
+}
+
+EXPORT void orc_bc_potentials(const picard_params* p, double* U, const double* C, const double* D) {
+  bc_potentials_core(p, U, C, D, 1);
+}
+
+EXPORT void orc_bc_potentials_sampled(const picard_params* p, double* U, const double* C, const double* D,
+                                      int stride) {
+  bc_potentials_core(p, U, C, D, stride < 1 ? 1 : stride);
 }
 
 /* ----------------------------------------- CalcEpotential (a10) */

@@ -30,6 +30,27 @@ SOLVER_F32_REFINE = 1
 
 FIELD_U, FIELD_E, FIELD_N, FIELD_C, FIELD_F, FIELD_D = range(6)
 
+class PicardStats(C.Structure):
+    _fields_ = [
+        ("kernel_launches", C.c_int64),
+        ("solves", C.c_int64),
+        ("sweeps", C.c_int64),
+        ("sweep_launches", C.c_int64),
+        ("sweep_ms", C.c_double),
+        ("anchor_launches", C.c_int64),
+        ("anchor_ms", C.c_double),
+        ("last_residual", C.c_double),
+        ("last_bnorm", C.c_double),
+        ("steps", C.c_int64),
+        ("particle_steps", C.c_int64),
+        ("h2d_bytes", C.c_int64),
+        ("d2h_bytes", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 LOG_FN = C.CFUNCTYPE(None, C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_void_p)
 
 
@@ -85,6 +106,9 @@ def lib():
         "picard_gpu_energy": [ctx, dp, ip],
         "picard_gpu_run": [ctx, C.c_int32, C.c_int32, C.c_int32, LOG_FN, C.c_void_p, C.POINTER(C.c_int64)],
         "picard_gpu_run_fused": [ctx, C.c_int32, C.c_int32, C.POINTER(C.c_int64)],
+        "picard_gpu_get_stats": [ctx, C.POINTER(PicardStats)],
+        "picard_gpu_reset_stats": [ctx],
+        "picard_gpu_get_stream": [ctx, C.POINTER(C.c_void_p)],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -24,10 +24,11 @@ constexpr double kKb = 1.380650e-23;
 constexpr double kMu0 = 1.25663706143591729538505735331180e-6;
 
 // Fixed-point scale of the deposit accumulators: one macro-particle's CIC
-// weight (in [0, 1]) is stored as round(w * 2^36) in an int64, so a node can
-// hold 2^27 particles and the sum is exact and order-independent.
-constexpr int kDepositShift = 36;
-constexpr double kDepositScale = 68719476736.0;  // 2^36
+// weight (in [0, 1]) is stored as round(w * 2^40) in an int64, so the sum is
+// exact and order-independent and a node holds up to 2^23 particle weights
+// per species.
+constexpr int kDepositShift = 40;
+constexpr double kDepositScale = 1099511627776.0;  // 2^40
 // Flux accumulators hold round(w * v * 2^20) (v in m/s).
 constexpr int kFluxShift = 20;
 constexpr double kFluxScale = 1048576.0;  // 2^20
@@ -132,6 +133,11 @@ struct PartC32 {
   float *fx, *fy, *fz, *vx, *vy, *vz;
   int8_t* sp;
 };
+
+// Process-wide count of kernels launched by this library (every launch
+// wrapper calls it once per launch); reported by picard_gpu_get_stats.
+void note_launch();
+long long launches_so_far();
 
 // Status word written by kernels (first error wins).
 enum DevError : int { kDevOk = 0, kDevCapacity = 1, kDevRange = 2 };

@@ -15,9 +15,15 @@
 
 using namespace picard;
 
+#include <atomic>
+
 namespace picard {
 
 static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
@@ -185,6 +191,7 @@ int validate(const picard_params* p, int layout, int solver) {
 int sync_count(picard_ctx* c) {
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i, c->d_count + c->cur, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += sizeof(int);
   c->num_local = c->h_pinned_i[0];
   return PICARD_OK;
 }
@@ -193,12 +200,14 @@ int push_count(picard_ctx* c) {
   c->h_pinned_i[1] = int(c->num_local);
   PICARD_CUDA(cudaMemcpyAsync(c->d_count + c->cur, c->h_pinned_i + 1, sizeof(int), cudaMemcpyHostToDevice, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.h2d_bytes += sizeof(int);
   return PICARD_OK;
 }
 
 int check_dev_err(picard_ctx* c) {
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 2, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += sizeof(int);
   int e = c->h_pinned_i[2];
   if (e == kDevCapacity) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
@@ -310,7 +319,10 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
   if ((rc = check_cuda(cudaMallocHost((void**)&c->h_pinned, sizeof(double) * (c->m_max + 16)), "cudaMallocHost")))
     return bail(rc);
   if ((rc = check_cuda(cudaMallocHost((void**)&c->h_pinned_i, sizeof(int) * 16), "cudaMallocHost"))) return bail(rc);
+  for (int e = 0; e < 4; ++e)
+    if ((rc = check_cuda(cudaEventCreate(&c->ev[e]), "cudaEventCreate"))) return bail(rc);
   if ((rc = check_cuda(cudaStreamSynchronize(c->st), "create"))) return bail(rc);
+  c->launches_at_reset = launches_so_far();
   *out = c;
   return PICARD_OK;
 }
@@ -321,6 +333,8 @@ int picard_gpu_destroy(picard_ctx* c) {
   for (void* q : c->allocs) cudaFree(q);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   if (c->h_pinned_i) cudaFreeHost(c->h_pinned_i);
+  for (int e = 0; e < 4; ++e)
+    if (c->ev[e]) cudaEventDestroy(c->ev[e]);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return PICARD_OK;
@@ -329,6 +343,26 @@ int picard_gpu_destroy(picard_ctx* c) {
 int picard_gpu_synchronize(picard_ctx* c) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  return PICARD_OK;
+}
+
+int picard_gpu_get_stats(picard_ctx* c, picard_stats* out) {
+  if (!c || !out) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  *out = c->stats;
+  out->kernel_launches = launches_so_far() - c->launches_at_reset;
+  return PICARD_OK;
+}
+
+int picard_gpu_reset_stats(picard_ctx* c) {
+  if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
+  c->stats = picard_stats{};
+  c->launches_at_reset = launches_so_far();
+  return PICARD_OK;
+}
+
+int picard_gpu_get_stream(picard_ctx* c, void** stream) {
+  if (!c || !stream) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  *stream = (void*)c->st;
   return PICARD_OK;
 }
 
@@ -375,6 +409,7 @@ int picard_gpu_set_particles(picard_ctx* c, const double* rp, const int32_t* ip,
   if (c->layout == PICARD_LAYOUT_CELL32) PICARD_CUDA(launch_f64_to_c32(c->K, dst, n, c->c32[c->cur], c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
   for (void* q : tmp) cudaFree(q);
+  c->stats.h2d_bytes += (int64_t)n * 49;
   c->num_local = n;
   return push_count(c);
 }
@@ -412,6 +447,7 @@ int picard_gpu_get_particles(picard_ctx* c, double* rp, int32_t* ip, int32_t cap
   PICARD_CUDA(cudaMemcpyAsync(sp.data(), src.sp, n, cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
   for (void* q : tmp) cudaFree(q);
+  c->stats.d2h_bytes += (int64_t)n * 49;
   for (long long p = 0; p < n; ++p) {
     if (rp) {
       for (int q = 0; q < 6; ++q) rp[(size_t)8 * p + q] = soa[(size_t)q * n + p];
@@ -462,6 +498,7 @@ int picard_gpu_get_field(picard_ctx* c, int32_t which, double* out) {
   std::vector<double> h((size_t)ncomp * n);
   PICARD_CUDA(cudaMemcpyAsync(h.data(), dev, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += (int64_t)(sizeof(double) * h.size());
   for (int pl = 0; pl < ncomp; ++pl)
     for (long long g = 0; g < n; ++g) out[ref_index(which, c->prm.species, pl, g)] = h[(size_t)pl * n + g];
   return PICARD_OK;
@@ -478,6 +515,7 @@ int picard_gpu_set_field(picard_ctx* c, int32_t which, const double* in) {
   for (int pl = 0; pl < ncomp; ++pl)
     for (long long g = 0; g < n; ++g) h[(size_t)pl * n + g] = in[ref_index(which, c->prm.species, pl, g)];
   PICARD_CUDA(cudaMemcpyAsync(dev, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->st));
+  c->stats.h2d_bytes += (int64_t)(sizeof(double) * h.size());
   if (which == PICARD_FIELD_E && c->E32) {
     std::vector<float4> e32(n);
     for (long long g = 0; g < n; ++g)
@@ -544,6 +582,7 @@ int picard_gpu_particles_produce(picard_ctx* c, int32_t iteration) {
   PICARD_CUDA(launch_scan_int(c->cell_counts, c->cell_offsets, cells, total, c->cell_offsets + cells + 2, c->st));
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 3, total, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += sizeof(int);
   long long add = c->h_pinned_i[3];
   if (add == 0) return PICARD_OK;
   PICARD_TRY(ensure_capacity(c, add));
@@ -669,6 +708,7 @@ int picard_gpu_energy(picard_ctx* c, double out[3], int32_t* num) {
   PICARD_CUDA(launch_energy_field(c->K, c->E, rf.partial, rf.result, c->st));
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->red_result, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += 2 * sizeof(double);
   out[0] = c->h_pinned[0];
   out[1] = c->h_pinned[1];
   // B is uniform (updateBfield is not implemented in the reference)

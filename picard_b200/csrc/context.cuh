@@ -67,6 +67,11 @@ struct picard_ctx {
 
   picard::InflowTable inflow;
   std::vector<void*> allocs;
+
+  // statistics (picard_gpu_get_stats)
+  picard_stats stats = {};
+  long long launches_at_reset = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace picard {

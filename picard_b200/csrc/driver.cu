@@ -188,6 +188,8 @@ int picard_gpu_run(picard_ctx* c, int32_t iter_start, int32_t iter_end, int32_t 
     PICARD_TRY(picard_gpu_bc_fields(c));
     // ParticlesModifyImp(): empty (ParticlesModify.f90:9-14)
     PICARD_TRY(picard_gpu_advance_velocity(c, p.dt));
+    c->stats.steps += 1;
+    c->stats.particle_steps += c->num_local;
     if (log_interval > 0 && it % log_interval == 0) PICARD_TRY(log_energy(c, it, time, log_fn, user));
   }
   PICARD_CUDA(cudaStreamSynchronize(c->st));
@@ -246,6 +248,8 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
     if (sweeps_total) *sweeps_total += sw;
     PICARD_TRY(picard_gpu_calc_efield(c));
     PICARD_TRY(picard_gpu_advance_velocity(c, p.dt));
+    c->stats.steps += 1;
+    c->stats.particle_steps += c->num_local;
   }
   PICARD_CUDA(cudaStreamSynchronize(c->st));
   if (nc) return fail(PICARD_ERR_NOT_CONVERGED, "at least one Jacobi solve hit 2*maxit+1 sweeps");

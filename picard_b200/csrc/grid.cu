@@ -46,7 +46,7 @@ __device__ inline int mirror(int i, int n, int open) {
   return i < 1 ? i + n : i - n;
 }
 
-// N_s = n2p_s * acc * 2^-36 at every node (ParticlesGridify.f90:98-121 with the
+// N_s = n2p_s * acc * 2^-40 at every node (ParticlesGridify.f90:98-121 with the
 // folds of 149-278), C = sum_s q_s N_s (288-293).
 __global__ void finish_deposit_kernel(KParams P, const unsigned long long* Nacc, double* N, double* Cout) {
   long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -534,11 +534,13 @@ JacobiCoefF jacobi_coef_f(const KParams& P) {
 
 cudaError_t launch_finish_deposit(const KParams& P, const unsigned long long* Nacc, double* N, double* C,
                                   cudaStream_t st) {
+  note_launch();
   finish_deposit_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(P, Nacc, N, C);
   return cudaGetLastError();
 }
 
 cudaError_t launch_finish_flux(const KParams& P, const unsigned long long* Facc, double* F, cudaStream_t st) {
+  note_launch();
   finish_flux_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(P, Facc, F);
   return cudaGetLastError();
 }
@@ -551,6 +553,7 @@ cudaError_t launch_bc_potentials(const KParams& P, const double* C, const double
     if (!flows[axis]) continue;
     int n1 = axis == 0 ? P.ny : P.nx, n2 = axis == 2 ? P.ny : P.nz;
     dim3 grid((n1 + kBT - 1) / kBT, (n2 + kBT - 1) / kBT);
+    note_launch();
     bc_potentials_kernel<<<grid, dim3(kBT, kBT), 0, st>>>(P, axis, C, D, U);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -563,19 +566,23 @@ int rhs_blocks(const KParams& P) { return grid_for(P.nodes); }
 cudaError_t launch_rhs(const KParams& P, const double* C, double* b, double* partial, double* bnorm2,
                        cudaStream_t st) {
   int nb = grid_for(P.nodes);
+  note_launch();
   rhs_kernel<<<nb, kThreads, 0, st>>>(P, C, b, partial);
+  note_launch();
   sum_partials_kernel<<<1, 256, 0, st>>>(partial, nb, 1.0, bnorm2);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sweep_f64(const KParams& P, const JacobiGeom& G, const double* Uin, double* Uout, const double* b,
                              double* partial, cudaStream_t st) {
+  note_launch();
   sweep_f64_kernel<<<G.grid, G.block, 0, st>>>(make_stencil(P), jacobi_coef(P), Uin, Uout, b, partial, G.zc);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sweep_f32(const KParams& P, const JacobiGeom& G, const float* win, float* wout, const float* r,
                              double* partial, int w_zero, cudaStream_t st) {
+  note_launch();
   sweep_f32_kernel<<<G.grid, G.block, 0, st>>>(make_stencil(P), jacobi_coef_f(P), win, wout, r, partial, G.zc,
                                                 w_zero);
   return cudaGetLastError();
@@ -583,6 +590,7 @@ cudaError_t launch_sweep_f32(const KParams& P, const JacobiGeom& G, const float*
 
 cudaError_t launch_anchor(const KParams& P, const JacobiGeom& G, const double* Vin, double* Vout, const float* w,
                           const double* b, float* r, double sigma, double* partial, int w_zero, cudaStream_t st) {
+  note_launch();
   anchor_kernel<<<G.grid, G.block, 0, st>>>(make_stencil(P), jacobi_coef(P), Vin, Vout, w, b, r, sigma, partial,
                                              G.zc, w_zero);
   return cudaGetLastError();
@@ -590,37 +598,52 @@ cudaError_t launch_anchor(const KParams& P, const JacobiGeom& G, const double* V
 
 cudaError_t launch_finalize(const KParams& P, const double* V, const float* w, double sigma, double* U, int w_zero,
                             cudaStream_t st) {
+  note_launch();
   finalize_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(make_stencil(P), V, w, sigma, U, w_zero);
   return cudaGetLastError();
 }
 
 cudaError_t launch_refresh_periodic(const KParams& P, double* U, cudaStream_t st) {
   Stencil S = make_stencil(P);
-  if (S.pz) refresh_periodic_kernel<<<grid_for((long long)S.nxp * S.nyp), kThreads, 0, st>>>(S, U, 2);
-  if (S.py) refresh_periodic_kernel<<<grid_for((long long)S.nxp * (S.nz + 2)), kThreads, 0, st>>>(S, U, 1);
-  if (S.px) refresh_periodic_kernel<<<grid_for((long long)S.nyp * (S.nz + 2)), kThreads, 0, st>>>(S, U, 0);
+  if (S.pz) {
+    note_launch();
+    refresh_periodic_kernel<<<grid_for((long long)S.nxp * S.nyp), kThreads, 0, st>>>(S, U, 2);
+  }
+  if (S.py) {
+    note_launch();
+    refresh_periodic_kernel<<<grid_for((long long)S.nxp * (S.nz + 2)), kThreads, 0, st>>>(S, U, 1);
+  }
+  if (S.px) {
+    note_launch();
+    refresh_periodic_kernel<<<grid_for((long long)S.nyp * (S.nz + 2)), kThreads, 0, st>>>(S, U, 0);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_reduce_sweeps(const double* partial, int nb, int m, double* r2, cudaStream_t st) {
   if (m <= 0) return cudaSuccess;
+  note_launch();
   reduce_sweeps_kernel<<<m, 256, 0, st>>>(partial, nb, r2);
   return cudaGetLastError();
 }
 
 cudaError_t launch_efield(const KParams& P, const double* U, double* E, float4* E32, cudaStream_t st) {
+  note_launch();
   efield_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(P, U, E, E32);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bc_fields(const KParams& P, double* E, float4* E32, cudaStream_t st) {
+  note_launch();
   bc_fields_kernel<<<grid_for(P.nodes), kThreads, 0, st>>>(P, E, E32);
   return cudaGetLastError();
 }
 
 cudaError_t launch_energy_field(const KParams& P, const double* E, double* partial, double* out, cudaStream_t st) {
   int nb = grid_for(P.nodes);
+  note_launch();
   energy_field_kernel<<<nb, kThreads, 0, st>>>(P, E, partial);
+  note_launch();
   sum_partials_kernel<<<1, 256, 0, st>>>(partial, nb, 0.5 * kEps0 * P.dV, out);
   return cudaGetLastError();
 }

@@ -639,7 +639,7 @@ __device__ inline int fold_index(int i, int n, int open) {
   return i;
 }
 
-// Warp-aggregated fixed-point deposit of 8 weights (each in [0, 2^36]) at
+// Warp-aggregated fixed-point deposit of 8 weights (each in [0, 2^40]) at
 // the nodes of `key`'s stencil.  Lanes with equal keys are summed with
 // 32-bit warp reductions of the weights split at bit 18, then one lane per
 // group issues the 8 atomics.
@@ -653,14 +653,14 @@ __device__ inline void deposit8(unsigned long long key, bool active, const long 
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
     long long v = w[q];
-    // Weights are in [-2^36, 2^36]; bias them into [0, 2^37] for the split.
-    unsigned long long u = (unsigned long long)(v + (1LL << 36));
+    // Weights are in [-2^40, 2^40]; bias them into [0, 2^41] for the split.
+    unsigned long long u = (unsigned long long)(v + (1LL << kDepositShift));
     unsigned lo = unsigned(u & 0x3FFFFu), hi = unsigned(u >> 18);
     unsigned slo = __reduce_add_sync(grp, lo);
     unsigned shi = __reduce_add_sync(grp, hi);
     if (lane == leader) {
       long long cnt = __popc(grp);
-      long long sum = (long long)(((unsigned long long)shi << 18) + (unsigned long long)slo) - cnt * (1LL << 36);
+      long long sum = (long long)(((unsigned long long)shi << 18) + (unsigned long long)slo) - cnt * (1LL << kDepositShift);
       atomicAdd(plane + nodes[q], (unsigned long long)sum);
     }
   }
@@ -829,6 +829,7 @@ int compact_blocks(long long n) { return int((n + kCompactTile - 1) / kCompactTi
 
 cudaError_t launch_calc_distance(const KParams& P, double* D, cudaStream_t st) {
   long long total = (long long)(P.nx + 1) * (P.ny + 1) * (P.nz + 1);
+  note_launch();
   calc_distance_kernel<<<grid_for(total), kThreads, 0, st>>>(P, D);
   return cudaGetLastError();
 }
@@ -837,6 +838,7 @@ cudaError_t launch_init_f64(const KParams& P, PartF64 out, long long start, cuda
   GroupPrefix G = group_prefix(P);
   long long total = (long long)P.nx * P.ny * P.nz * G.p[P.species];
   if (total == 0) return cudaSuccess;
+  note_launch();
   init_kernel<<<grid_for(total), kThreads, 0, st>>>(P, G, start, total, StoreF64{out});
   return cudaGetLastError();
 }
@@ -845,6 +847,7 @@ cudaError_t launch_init_c32(const KParams& P, PartC32 out, long long start, cuda
   GroupPrefix G = group_prefix(P);
   long long total = (long long)P.nx * P.ny * P.nz * G.p[P.species];
   if (total == 0) return cudaSuccess;
+  note_launch();
   init_kernel<<<grid_for(total), kThreads, 0, st>>>(P, G, start, total, StoreC32{P, out});
   return cudaGetLastError();
 }
@@ -853,6 +856,7 @@ cudaError_t launch_inflow_f64(const KParams& P, const InflowTable& T, int iterat
                               cudaStream_t st) {
   long long total = T.cells * T.per_cell;
   if (total == 0) return cudaSuccess;
+  note_launch();
   inflow_kernel<<<grid_for(total), kThreads, 0, st>>>(P, T, iteration, start, total, StoreF64{out});
   return cudaGetLastError();
 }
@@ -861,6 +865,7 @@ cudaError_t launch_inflow_c32(const KParams& P, const InflowTable& T, int iterat
                               cudaStream_t st) {
   long long total = T.cells * T.per_cell;
   if (total == 0) return cudaSuccess;
+  note_launch();
   inflow_kernel<<<grid_for(total), kThreads, 0, st>>>(P, T, iteration, start, total, StoreC32{P, out});
   return cudaGetLastError();
 }
@@ -869,6 +874,7 @@ cudaError_t launch_inflow_fused_c32(const KParams& P, const InflowTable& T, int 
                                     long long capacity, int* err, cudaStream_t st) {
   long long total = T.cells * T.per_cell;
   if (total == 0) return cudaSuccess;
+  note_launch();
   inflow_fused_kernel<<<grid_for(total), kThreads, 0, st>>>(P, T, iteration, total, count, capacity, err,
                                                             StoreC32{P, out});
   return cudaGetLastError();
@@ -878,6 +884,7 @@ cudaError_t launch_inflow_fused_f64(const KParams& P, const InflowTable& T, int 
                                     long long capacity, int* err, cudaStream_t st) {
   long long total = T.cells * T.per_cell;
   if (total == 0) return cudaSuccess;
+  note_launch();
   inflow_fused_kernel<<<grid_for(total), kThreads, 0, st>>>(P, T, iteration, total, count, capacity, err,
                                                             StoreF64{out});
   return cudaGetLastError();
@@ -885,6 +892,7 @@ cudaError_t launch_inflow_fused_f64(const KParams& P, const InflowTable& T, int 
 
 cudaError_t launch_produce_count(const KParams& P, int iteration, int* counts, cudaStream_t st) {
   long long cells = (long long)P.nx * P.ny * P.nz;
+  note_launch();
   produce_count_kernel<<<grid_for(cells), kThreads, 0, st>>>(P, iteration, counts);
   return cudaGetLastError();
 }
@@ -897,8 +905,10 @@ __global__ void add_count_kernel(int* count, const int* add, long long capacity)
 cudaError_t launch_produce_emit_f64(const KParams& P, int iteration, const int* offsets, PartF64 out, int* count,
                                     long long capacity, int* err, cudaStream_t st) {
   long long cells = (long long)P.nx * P.ny * P.nz;
+  note_launch();
   produce_emit_kernel<<<grid_for(cells), kThreads, 0, st>>>(P, iteration, offsets, count, capacity, err,
                                                             StoreF64{out});
+  note_launch();
   add_count_kernel<<<1, 1, 0, st>>>(count, offsets + cells, capacity);
   return cudaGetLastError();
 }
@@ -906,8 +916,10 @@ cudaError_t launch_produce_emit_f64(const KParams& P, int iteration, const int* 
 cudaError_t launch_produce_emit_c32(const KParams& P, int iteration, const int* offsets, PartC32 out, int* count,
                                     long long capacity, int* err, cudaStream_t st) {
   long long cells = (long long)P.nx * P.ny * P.nz;
+  note_launch();
   produce_emit_kernel<<<grid_for(cells), kThreads, 0, st>>>(P, iteration, offsets, count, capacity, err,
                                                             StoreC32{P, out});
+  note_launch();
   add_count_kernel<<<1, 1, 0, st>>>(count, offsets + cells, capacity);
   return cudaGetLastError();
 }
@@ -920,12 +932,14 @@ static int persistent_grid(long long n) {
 
 cudaError_t launch_advance_position_f64(const KParams& P, PartF64 a, long long n, double dt, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   advance_position_f64_kernel<<<persistent_grid(n), kThreads, 0, st>>>(a, n, dt);
   return cudaGetLastError();
 }
 
 cudaError_t launch_transfer_f64(const KParams& P, PartF64 a, long long n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   transfer_f64_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n);
   return cudaGetLastError();
 }
@@ -934,9 +948,11 @@ cudaError_t launch_compact_outflow_f64(const KParams& P, PartF64 in, PartF64 out
                                        int* block_offsets, int* new_count, int wrap, cudaStream_t st) {
   int nb = compact_blocks(n);
   if (n <= 0) return cudaMemsetAsync(new_count, 0, sizeof(int), st);
+  note_launch();
   outflow_count_f64<<<nb, kCompactThreads, 0, st>>>(P, in, n, block_counts);
   cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, new_count, block_offsets + nb + 1, st);
   if (e != cudaSuccess) return e;
+  note_launch();
   outflow_scatter_f64<<<nb, kCompactThreads, 0, st>>>(P, in, out, n, block_offsets, wrap);
   return cudaGetLastError();
 }
@@ -944,6 +960,7 @@ cudaError_t launch_compact_outflow_f64(const KParams& P, PartF64 in, PartF64 out
 cudaError_t launch_advance_velocity_f64(const KParams& P, PartF64 a, long long n, const double* E, double dt,
                                         double deltat, int mode, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   advance_velocity_f64_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, E, dt, deltat, mode);
   return cudaGetLastError();
 }
@@ -951,6 +968,7 @@ cudaError_t launch_advance_velocity_f64(const KParams& P, PartF64 a, long long n
 cudaError_t launch_deposit_f64(const KParams& P, PartF64 a, long long n, unsigned long long* Nacc,
                                unsigned long long* Facc, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   deposit_f64_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, Nacc, Facc);
   return cudaGetLastError();
 }
@@ -958,13 +976,16 @@ cudaError_t launch_deposit_f64(const KParams& P, PartF64 a, long long n, unsigne
 cudaError_t launch_energy_particles_f64(const KParams& P, PartF64 a, long long n, ReduceBuf rb, cudaStream_t st) {
   int nb = persistent_grid(n > 0 ? n : 1);
   if (nb > rb.max_blocks) nb = rb.max_blocks;
+  note_launch();
   energy_particles_f64_kernel<<<nb, kThreads, 0, st>>>(P, a, n, rb.partial);
+  note_launch();
   finish_sum_kernel<<<1, 32, 0, st>>>(rb.partial, nb, 0.5, rb.result);
   return cudaGetLastError();
 }
 
 cudaError_t launch_cell_indices_f64(const KParams& P, PartF64 a, long long n, int* ijk, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   cell_indices_f64_kernel<<<grid_for(n), kThreads, 0, st>>>(P, a, n, ijk);
   return cudaGetLastError();
 }
@@ -974,11 +995,13 @@ cudaError_t launch_cell_indices_f64(const KParams& P, PartF64 a, long long n, in
 namespace picard {
 cudaError_t launch_c32_to_f64(const KParams& P, PartC32 a, long long n, PartF64 out, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   c32_to_f64_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, out);
   return cudaGetLastError();
 }
 cudaError_t launch_f64_to_c32(const KParams& P, PartF64 a, long long n, PartC32 out, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   f64_to_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, out);
   return cudaGetLastError();
 }

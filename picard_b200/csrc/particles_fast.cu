@@ -352,19 +352,19 @@ __device__ inline void deposit8(unsigned long long key, bool active, const long 
   int leader = __ffs(grp) - 1;
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
-    unsigned long long u = (unsigned long long)(w[q] + (1LL << 36));
+    unsigned long long u = (unsigned long long)(w[q] + (1LL << kDepositShift));
     unsigned lo = unsigned(u & 0x3FFFFu), hi = unsigned(u >> 18);
     unsigned slo = __reduce_add_sync(grp, lo);
     unsigned shi = __reduce_add_sync(grp, hi);
     if (lane == leader) {
       long long cnt = __popc(grp);
-      long long sum = (long long)(((unsigned long long)shi << 18) + (unsigned long long)slo) - cnt * (1LL << 36);
+      long long sum = (long long)(((unsigned long long)shi << 18) + (unsigned long long)slo) - cnt * (1LL << kDepositShift);
       atomicAdd(plane + nodes[q], (unsigned long long)sum);
     }
   }
 }
 
-// ParticlesGridify.f90:65-123 with FP32 weights rounded to 2^-36 and ghost
+// ParticlesGridify.f90:65-123 with FP32 weights rounded to 2^-40 and ghost
 // folds applied to the node indices.
 __global__ void deposit_c32_kernel(KParams P, PartC32 a, long long n, unsigned long long* Nacc,
                                    unsigned long long* Facc) {
@@ -452,21 +452,25 @@ int scan_scratch_ints(int n) {
 cudaError_t launch_scan_int(const int* in, int* out, int n, int* total, int* scratch, cudaStream_t st) {
   if (n <= 0) return cudaMemsetAsync(total, 0, sizeof(int), st);
   if (n <= kScanTile) {
+    note_launch();
     scan_tiles_kernel<<<1, kScanThreads, 0, st>>>(in, out, n, total);
     return cudaGetLastError();
   }
   int nb = (n + kScanTile - 1) / kScanTile;
   int* sums = scratch;
   int* offs = scratch + nb + 1;
+  note_launch();
   scan_tiles_kernel<<<nb, kScanThreads, 0, st>>>(in, out, n, sums);
   cudaError_t e = launch_scan_int(sums, offs, nb, total, offs + nb + 1, st);
   if (e != cudaSuccess) return e;
+  note_launch();
   scan_add_kernel<<<nb, kScanThreads, 0, st>>>(out, n, offs);
   return cudaGetLastError();
 }
 
 cudaError_t launch_advance_position_c32(const KParams& P, PartC32 a, long long n, double dt, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   advance_position_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, float(dt / P.dx), float(dt / P.dy),
                                                                        float(dt / P.dz));
   return cudaGetLastError();
@@ -474,6 +478,7 @@ cudaError_t launch_advance_position_c32(const KParams& P, PartC32 a, long long n
 
 cudaError_t launch_transfer_c32(const KParams& P, PartC32 a, long long n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   transfer_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n);
   return cudaGetLastError();
 }
@@ -482,9 +487,11 @@ cudaError_t launch_compact_outflow_c32(const KParams& P, PartC32 in, PartC32 out
                                        int* block_offsets, int* new_count, int wrap, cudaStream_t st) {
   if (n <= 0) return cudaMemsetAsync(new_count, 0, sizeof(int), st);
   int nb = int((n + kCompactTile - 1) / kCompactTile);
+  note_launch();
   outflow_count_c32<<<nb, kCompactThreads, 0, st>>>(P, in, n, block_counts);
   cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, new_count, block_offsets + nb + 1, st);
   if (e != cudaSuccess) return e;
+  note_launch();
   outflow_scatter_c32<<<nb, kCompactThreads, 0, st>>>(P, in, out, n, block_offsets, wrap);
   return cudaGetLastError();
 }
@@ -493,6 +500,7 @@ cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n
                                         double deltat, int mode, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   SpeciesF32 S = species_f32(P, dt, deltat, mode);
+  note_launch();
   advance_velocity_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, S, a, n, E, mode);
   return cudaGetLastError();
 }
@@ -500,6 +508,7 @@ cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n
 cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
                                unsigned long long* Facc, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  note_launch();
   deposit_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, Nacc, Facc);
   return cudaGetLastError();
 }
@@ -507,7 +516,9 @@ cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigne
 cudaError_t launch_energy_particles_c32(const KParams& P, PartC32 a, long long n, ReduceBuf rb, cudaStream_t st) {
   int nb = persistent_grid(n > 0 ? n : 1);
   if (nb > rb.max_blocks) nb = rb.max_blocks;
+  note_launch();
   energy_particles_c32_kernel<<<nb, kThreads, 0, st>>>(P, a, n, rb.partial);
+  note_launch();
   finish_sum_kernel<<<1, 32, 0, st>>>(rb.partial, nb, 0.5, rb.result);
   return cudaGetLastError();
 }

@@ -36,9 +36,18 @@ int next_batch(double r2_prev, double r2_last, double tol2, int m_max) {
 
 bool passes(double r2, double tol) { return std::sqrt(r2) <= tol; }
 
+// Device time between two events recorded on the context stream (call after
+// the stream has been synchronised past the second one).
+double elapsed_ms(picard_ctx* c, int a, int b) {
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) != cudaSuccess) return 0.0;
+  return ms;
+}
+
 int read_r2(picard_ctx* c, int count) {
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->r2, sizeof(double) * count, cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += (int64_t)sizeof(double) * count;
   return PICARD_OK;
 }
 
@@ -55,13 +64,17 @@ int solve_f64(picard_ctx* c, double tol, long long smax, int maxit, long long* s
   for (;;) {
     int m_eff = int(std::min<long long>(m, smax - a));
     PICARD_CUDA(cudaMemcpyAsync(c->Usnap, buf[a % 2], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+    PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
     for (int t = 1; t <= m_eff; ++t) {
       long long s = a + t;
       PICARD_CUDA(launch_sweep_f64(K, c->G, buf[(s - 1) % 2], buf[s % 2], c->b, c->partials + (size_t)(t - 1) * nb,
                                    c->st));
     }
+    PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
     PICARD_CUDA(launch_reduce_sweeps(c->partials, nb, m_eff, c->r2, c->st));
     PICARD_TRY(read_r2(c, m_eff));
+    c->stats.sweep_launches += m_eff;
+    c->stats.sweep_ms += elapsed_ms(c, 0, 1);
     long long hit = -1;
     for (int t = 1; t <= m_eff; ++t) {
       long long d = a + t - 1;  // sweep a+t measured the residual of iterate d
@@ -82,6 +95,7 @@ int solve_f64(picard_ctx* c, double tol, long long smax, int maxit, long long* s
         PICARD_CUDA(cudaMemcpyAsync(buf[a % 2], c->Usnap, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
         for (long long s = a + 1; s <= hit; ++s)
           PICARD_CUDA(launch_sweep_f64(K, c->G, buf[(s - 1) % 2], buf[s % 2], c->b, c->partials, c->st));
+        c->stats.sweep_launches += hit - a;
       }
       if (hit % 2 == 1)
         PICARD_CUDA(cudaMemcpyAsync(c->U, c->U1, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
@@ -119,17 +133,24 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
   const double tol2 = tol * tol;
   for (;;) {
     int m_eff = int(std::min<long long>(m, smax - a));
+    PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
     for (int t = 1; t <= m_eff; ++t) {
       long long s = a + t;
       PICARD_CUDA(launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rcur],
                                    c->partials + (size_t)(t - 1) * nb, t == 1 ? 1 : 0, c->st));
     }
+    PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
     // next anchor: fold w_{a+m_eff} into V, exact FP64 residual of that iterate
     long long an = a + m_eff;
     PICARD_CUDA(launch_anchor(K, c->G, V[vcur], V[1 - vcur], c->w[an % 2], c->b, R[1 - rcur], sigma,
                               c->partials + (size_t)m_eff * nb, 0, c->st));
+    PICARD_CUDA(cudaEventRecord(c->ev[2], c->st));
     PICARD_CUDA(launch_reduce_sweeps(c->partials, nb, m_eff + 1, c->r2, c->st));
     PICARD_TRY(read_r2(c, m_eff + 1));
+    c->stats.sweep_launches += m_eff;
+    c->stats.sweep_ms += elapsed_ms(c, 0, 1);
+    c->stats.anchor_launches += 1;
+    c->stats.anchor_ms += elapsed_ms(c, 1, 2);
     long long hit = -1;
     // sweep a+t (t >= 2) measured iterate a+t-1 in FP32 (scaled by sigma^2);
     // the anchor measured iterate a+m_eff in FP64
@@ -154,6 +175,7 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
         for (long long s = a + 1; s <= hit; ++s)
           PICARD_CUDA(launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rcur], c->partials,
                                        s == a + 1 ? 1 : 0, c->st));
+        c->stats.sweep_launches += hit - a;
         PICARD_CUDA(launch_finalize(K, V[vcur], c->w[hit % 2], sigma, c->U, 0, c->st));
       }
       *sweeps = hit;
@@ -184,6 +206,7 @@ extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t 
   PICARD_CUDA(launch_rhs(K, c->C, c->b, c->red_partial, c->red_result + 4, c->st));
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->red_result + 4, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += sizeof(double);
   const double b2 = c->h_pinned[0];
   const double bnorm = std::sqrt(b2);
   const double tol = maxerr * bnorm;
@@ -205,6 +228,10 @@ extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t 
   }
   PICARD_CUDA(launch_refresh_periodic(K, c->U, c->st));
   c->last_sweeps = sweeps;
+  c->stats.solves += 1;
+  c->stats.sweeps += sweeps;
+  c->stats.last_residual = c->last_residual;
+  c->stats.last_bnorm = bnorm;
   if (sweeps_out) *sweeps_out = int32_t(sweeps);
   if (!converged)
     return fail(PICARD_ERR_NOT_CONVERGED,

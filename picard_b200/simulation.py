@@ -162,6 +162,21 @@ class Simulation:
         self._call("picard_gpu_energy", out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n))
         return out
 
+    # ----------------------------------------------------------- statistics
+    def stats(self) -> dict:
+        st = capi.PicardStats()
+        self._call("picard_gpu_get_stats", C.byref(st))
+        return st.as_dict()
+
+    def reset_stats(self) -> None:
+        self._call("picard_gpu_reset_stats")
+
+    @property
+    def stream_handle(self) -> int:
+        h = C.c_void_p()
+        self._call("picard_gpu_get_stream", C.byref(h))
+        return int(h.value or 0)
+
     # ------------------------------------------------------------ main loop
     def run(self, iter_start: int, iter_end: int, log_interval: int = 0, log=None) -> int:
         """picard.f90:554-674; returns the total Jacobi sweeps."""
