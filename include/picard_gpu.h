@@ -172,6 +172,32 @@ PICARD_API int picard_gpu_advance_velocity_exp(picard_ctx* ctx, double deltat,
                                     double dt);                      /* AdvanceVelocity.f90:128-236  */
 PICARD_API int picard_gpu_advance_velocity_imp(picard_ctx* ctx, double deltat,
                                     double dt);                      /* AdvanceVelocity.f90:239-347  */
+/* Largest species*(Nx+2)*(Ny+2)*(Nz+2) that picard_gpu_particles_gridify_noalloc
+ * accepts: its scratch is a fixed 16 MiB array of int64 accumulators. */
+#define PICARD_NOALLOC_MAX_WORDS 2097152
+
+/* The charge deposit of picard_gpu_particles_gridify for callers that cannot
+ * allocate device memory when they call it -- for example a Fortran host whose
+ * device arrays live in a pool another runtime (OpenACC, CUDA Fortran)
+ * reserved up front, or a server that has already committed all of the HBM to
+ * resident runs.  It has no counterpart in the reference: it is an extra
+ * entry point of this library, not a replacement of a Picard subroutine.
+ * Nothing is allocated: the caller passes device pointers to the FP64
+ * positions x, y, z and the 1-based species numbers (int_particles) of
+ * num_local particles, and device outputs N (species x (Nx+2)(Ny+2)(Nz+2),
+ * species fastest, as ParticlesGridify's N) and C ((Nx+2)(Ny+2)(Nz+2)); the
+ * work is queued on `stream` (a cudaStream_t, NULL for the default stream).
+ * Scratch is one fixed array of PICARD_NOALLOC_MAX_WORDS int64 words that
+ * every device holds from the first use of the library until exit; larger
+ * grids are rejected with PICARD_ERR_BAD_ARG.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race and must be ordered by the caller.  Particles
+ * whose species number is outside 1..species are not deposited. */
+PICARD_API int picard_gpu_particles_gridify_noalloc(const picard_params* p, const double* x, const double* y,
+                                                    const double* z, const int32_t* int_particles,
+                                                    int32_t num_local, double* N, double* C, void* stream);
+
 /* picard.f90:651-665: out[0] = uP, out[1] = uE, out[2] = uB (un-normalised,
  * FP64), *num = num_local. */
 PICARD_API int picard_gpu_energy(picard_ctx* ctx, double out[3], int32_t* num);

@@ -109,6 +109,8 @@ def lib():
         "picard_gpu_get_stats": [ctx, C.POINTER(PicardStats)],
         "picard_gpu_reset_stats": [ctx],
         "picard_gpu_get_stream": [ctx, C.POINTER(C.c_void_p)],
+        "picard_gpu_particles_gridify_noalloc": [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p],
     }
     for name, args in sig.items():
         f = getattr(L, name)

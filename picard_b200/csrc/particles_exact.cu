@@ -1006,3 +1006,138 @@ cudaError_t launch_f64_to_c32(const KParams& P, PartF64 a, long long n, PartC32 
   return cudaGetLastError();
 }
 }  // namespace picard
+
+// ---------------------------------------------------------------------------
+// Allocation-free deposit: picard_gpu_particles_gridify_noalloc.
+//
+// Some callers cannot allocate device memory at the point where they need a
+// charge deposit: a host whose device memory is owned by another runtime's
+// fixed pool (a Fortran program that manages its arrays through OpenACC or
+// CUDA Fortran data regions), a serving loop that has already promised all of
+// the HBM to resident runs, or a pipeline that cannot afford the device-wide
+// synchronisation cudaFree implies.  For them this entry point takes the
+// particle arrays and the output grids from the caller and keeps its only
+// scratch -- the int64 fixed-point accumulators -- in the file-scope array
+// below, so it calls no cudaMalloc, cudaFree or allocating library routine.
+#include <mutex>
+#include <string>
+
+namespace picard {
+KParams make_kparams(const picard_params& p);
+int fail(int code, const std::string& msg);
+
+namespace {
+
+// Every device that loads the library holds this array (16 MiB) until the
+// process exits.  All calls share it, so calls that overlap on the GPU race.
+static __device__ __align__(256) unsigned long long g_noalloc_acc[PICARD_NOALLOC_MAX_WORDS];
+
+// Device address of g_noalloc_acc, looked up once per device.
+std::mutex g_noalloc_mutex;
+constexpr int kNoAllocMaxDevices = 64;
+unsigned long long* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// ParticlesGridify.f90:65-123 for caller-owned FP64 arrays; int_particles
+// holds the reference's 1-based species numbers, others are not deposited.
+__global__ void deposit_noalloc_kernel(KParams P, const double* __restrict__ x, const double* __restrict__ y,
+                                       const double* __restrict__ z, const int32_t* __restrict__ sp1, long long n,
+                                       unsigned long long* acc) {
+  long long stride = (long long)gridDim.x * blockDim.x;
+  long long n_round = ((n + 31) / 32) * 32;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n_round; p += stride) {
+    int s = (p < n) ? sp1[p] - 1 : -1;
+    bool active = s >= 0 && s < P.species;
+    long long w[8] = {0, 0, 0, 0, 0, 0, 0, 0}, nodes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long key = ~0ull;
+    if (active) {
+      Cic64 c;
+      cic64(P, x[p], y[p], z[p], c);
+      for (int q = 0; q < 8; ++q) {
+        w[q] = __double2ll_rn(c.F[q] / P.dV * kDepositScale);
+        int i = fold_index(c.i + kOff[q][0], P.nx, P.xflow), j = fold_index(c.j + kOff[q][1], P.ny, P.yflow),
+            k = fold_index(c.k + kOff[q][2], P.nz, P.zflow);
+        nodes[q] = node_index(P, i, j, k);
+      }
+      key = stencil_key(c.i, c.j, c.k, s);
+    } else {
+      s = 0;
+    }
+    deposit8(key, active, w, nodes, acc + (long long)s * P.nodes);
+  }
+}
+
+// N(s, node) = n2p_s * acc * 2^-40 in the reference layout (species fastest),
+// with the ghost folds of ParticlesGridify.f90:149-278; C = sum_s q_s N_s.
+__global__ void finish_noalloc_kernel(KParams P, const unsigned long long* acc, double* N, double* C) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.nodes) return;
+  int i = int(g % P.nxp), j = int((g / P.nxp) % P.nyp), k = int(g / ((long long)P.nxp * P.nyp));
+  auto mirror = [](int v, int nn, int open) { return (v >= 1 && v <= nn) ? v : (open ? -1 : (v < 1 ? v + nn : v - nn)); };
+  int mi = mirror(i, P.nx, P.xflow), mj = mirror(j, P.ny, P.yflow), mk = mirror(k, P.nz, P.zflow);
+  double c = 0.0;
+  for (int s = 0; s < P.species; ++s) {
+    double v = 0.0;
+    if (mi >= 0 && mj >= 0 && mk >= 0) {
+      long long a = (long long)acc[(long long)s * P.nodes + node_index(P, mi, mj, mk)];
+      v = P.n2p[s] * ((double)a * (1.0 / kDepositScale));
+    }
+    N[(long long)s + (long long)P.species * g] = v;
+    c = c + v * P.charge[s];
+  }
+  C[g] = c;
+}
+
+}  // namespace
+}  // namespace picard
+
+extern "C" int picard_gpu_particles_gridify_noalloc(const picard_params* p, const double* x, const double* y,
+                                                    const double* z, const int32_t* int_particles, int32_t num_local,
+                                                    double* N, double* C, void* stream) {
+  using namespace picard;
+  if (!p) return fail(PICARD_ERR_BAD_ARG, "params is NULL");
+  if (!(p->dxyz[0] > 0.0 && p->dxyz[1] > 0.0 && p->dxyz[2] > 0.0))
+    return fail(PICARD_ERR_BAD_ARG, "params not derived (call picard_params_derive first)");
+  if (p->species < 2 || p->species > 8) return fail(PICARD_ERR_BAD_ARG, "species must be in 2..8");
+  if (p->nx < 1 || p->ny < 1 || p->nz < 1) return fail(PICARD_ERR_BAD_ARG, "grid dimensions must be positive");
+  const long long nodes = (long long)(p->nx + 2) * (p->ny + 2) * (p->nz + 2);
+  const long long words = nodes * p->species;
+  if (words > (long long)PICARD_NOALLOC_MAX_WORDS)
+    return fail(PICARD_ERR_BAD_ARG, "the allocation-free deposit needs species*(Nx+2)*(Ny+2)*(Nz+2) = " +
+                                        std::to_string(words) + " accumulator words; its fixed scratch holds " +
+                                        std::to_string((long long)PICARD_NOALLOC_MAX_WORDS));
+  if (num_local < 0) return fail(PICARD_ERR_BAD_ARG, "num_local must be >= 0");
+  if (num_local > 0 && (!x || !y || !z || !int_particles)) return fail(PICARD_ERR_BAD_ARG, "particle array is NULL");
+  if (!N || !C) return fail(PICARD_ERR_BAD_ARG, "output array is NULL");
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(PICARD_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(PICARD_ERR_BAD_ARG, "device ordinal out of range");
+  unsigned long long* acc = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      // the host-side name of the array is not a device address: look the
+      // address up on this device (once), with this device current
+      void* q = nullptr;
+      e = cudaGetSymbolAddress(&q, g_noalloc_acc);
+      if (e != cudaSuccess) return fail(PICARD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = static_cast<unsigned long long*>(q);
+    }
+    acc = g_noalloc_ptr[dev];
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const KParams K = make_kparams(*p);
+  // the array keeps the previous call's sums: clear the part this call uses
+  e = cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * (size_t)words, st);
+  if (e != cudaSuccess) return fail(PICARD_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+  if (num_local > 0) {
+    note_launch();
+    deposit_noalloc_kernel<<<persistent_grid(num_local), kThreads, 0, st>>>(K, x, y, z, int_particles, num_local,
+                                                                             acc);
+  }
+  note_launch();
+  finish_noalloc_kernel<<<grid_for(nodes), kThreads, 0, st>>>(K, acc, N, C);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(PICARD_ERR_CUDA, std::string("deposit launch: ") + cudaGetErrorString(e));
+  return PICARD_OK;
+}
