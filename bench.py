@@ -46,7 +46,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["picard", "reference"], default="picard")
-    ap.add_argument("--workload", choices=["scale", "plain32"], default="scale")
+    ap.add_argument("--workload", choices=["scale", "plain32", "poisson"], default="scale")
+    ap.add_argument("--poisson-n", type=int, default=256)
+    ap.add_argument("--poisson-sweeps", type=int, default=400)
     ap.add_argument("--layout", choices=["cell32", "f64"], default="cell32")
     ap.add_argument("--solver", choices=["refine", "f64"], default="refine")
     ap.add_argument("--no-e2e", action="store_true")
@@ -247,6 +249,7 @@ def run_picard(args, rank, world, local_rank):
             "impl": "picard",
             "gpu_launches": st["kernel_launches"],
             "jacobi_sweeps_per_step": sweeps_per_step,
+            "phase_ms_per_step": {k: round(v / K, 3) for k, v in st["phase_ms"].items()},
             "particles_final": num_final,
             "roofline": {"bound": "hbm", "kernel": "sweep_f32_kernel" if solver else "sweep_f64_kernel",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -326,6 +329,66 @@ def cpu_baseline(args, sweeps_per_step=None, steps: int = 1) -> dict:
             "seconds_per_step": total / steps, "phase_seconds": {k: round(v, 4) for k, v in phases.items()}}
 
 
+def blob_charge(n: int, seed: int, blobs: int = 32):
+    """Charge of the standalone Poisson workload: `blobs` Gaussian blobs
+    (centres uniform in the box, sigma uniform in [4, 16] cells, amplitudes
+    N(0, 1) e per cell) plus 1% uniform noise, on an n^3 box with ghosts."""
+    import numpy as np
+
+    from picard_b200 import params as P
+
+    rng = np.random.default_rng(seed)
+    ax = np.arange(n + 2, dtype=np.float64)
+    C = np.zeros((n + 2,) * 3)
+    for _ in range(blobs):
+        c = rng.uniform(1, n, 3)
+        s = rng.uniform(4, 16)
+        a = rng.standard_normal()
+        gx, gy, gz = (np.exp(-0.5 * ((ax - c[d]) / s) ** 2) for d in range(3))
+        C += a * gz[:, None, None] * gy[None, :, None] * gx[None, None, :]
+    C += 0.01 * rng.uniform(-1, 1, C.shape)
+    C[0, :, :] = C[-1, :, :] = 0
+    C[:, 0, :] = C[:, -1, :] = 0
+    C[:, :, 0] = C[:, :, -1] = 0
+    return C * P.EC
+
+
+def run_poisson(args, local_rank):
+    """Jacobi-only workload: an n^3 open box, blob charge, zero boundary
+    potential, `--poisson-sweeps` sweeps (maxit bounded, no stop).  Reports the
+    sweep kernel's device time and roofline.  Used for kernel profiling on a
+    working set larger than L2."""
+    import torch
+
+    from picard_b200 import capi
+    from picard_b200 import params as P
+    from picard_b200.simulation import Simulation
+
+    torch.cuda.set_device(local_rank)
+    n = args.poisson_n
+    p = P.config_plain_32(n=n, ppc=1, capacity=1024)
+    solver = capi.SOLVER_F32_REFINE if args.solver == "refine" else capi.SOLVER_F64
+    sim = Simulation(p, layout=capi.LAYOUT_F64, solver=solver)
+    sim.set_field(capi.FIELD_C, blob_charge(n, seed=0))
+    sim.set_field(capi.FIELD_U, __import__("numpy").zeros((n + 2,) * 3))
+    maxit = max(1, args.poisson_sweeps // 2)
+    sim.calc_epotential(maxerr=1e-300, maxit=maxit)  # warm-up solve
+    sim.reset_stats()
+    sim.set_field(capi.FIELD_U, __import__("numpy").zeros((n + 2,) * 3))
+    sim.calc_epotential(maxerr=1e-300, maxit=maxit)
+    st = sim.stats()
+    sim.close()
+    cells = n ** 3
+    bpn = 12 if solver == capi.SOLVER_F32_REFINE else 24
+    ms = st["sweep_ms"] / max(st["sweep_launches"], 1)
+    peak, kind = measured_peaks()
+    ach = bpn * cells / (ms * 1e-3) / 1e9
+    print(json.dumps({"workload": f"poisson {n}^3", "sweeps": st["sweep_launches"], "sweep_ms": ms,
+                      "achieved_gbs": ach, "peak_gbs": peak, "frac": ach / peak, "peak_kind": kind,
+                      "anchor_ms": st["anchor_ms"] / max(st["anchor_launches"], 1),
+                      "gpu_launches": st["kernel_launches"]}), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -351,6 +414,9 @@ def main():
     rank, world, local_rank = env_rank()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "poisson":
+        run_poisson(args, local_rank)
         return
     if world > 1:
         import torch

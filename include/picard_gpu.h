@@ -223,6 +223,11 @@ typedef struct picard_stats {
   int64_t particle_steps;  /* live particles summed over those iterations   */
   int64_t h2d_bytes;       /* host-to-device bytes copied by the library     */
   int64_t d2h_bytes;       /* device-to-host bytes copied by the library     */
+  /* device time of the phases of picard_gpu_run_fused iterations (CUDA
+   * events at the phase boundaries, host waits included): particle movement
+   * (advance, produce, outflow, wrap, inflow), deposit, BCpotentials, Jacobi
+   * solve, E-field + velocity push */
+  double phase_ms[5];
 } picard_stats;
 
 PICARD_API int picard_gpu_get_stats(picard_ctx* ctx, picard_stats* out);

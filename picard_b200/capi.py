@@ -45,10 +45,15 @@ class PicardStats(C.Structure):
         ("particle_steps", C.c_int64),
         ("h2d_bytes", C.c_int64),
         ("d2h_bytes", C.c_int64),
+        ("phase_ms", C.c_double * 5),
     ]
 
+    PHASES = ("particles", "deposit", "bc_potentials", "jacobi", "field_push")
+
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "phase_ms"}
+        d["phase_ms"] = {n: self.phase_ms[i] for i, n in enumerate(self.PHASES)}
+        return d
 
 
 LOG_FN = C.CFUNCTYPE(None, C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_void_p)

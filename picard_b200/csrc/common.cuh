@@ -140,6 +140,6 @@ void note_launch();
 long long launches_so_far();
 
 // Status word written by kernels (first error wins).
-enum DevError : int { kDevOk = 0, kDevCapacity = 1, kDevRange = 2 };
+enum DevError : int { kDevOk = 0, kDevCapacity = 1, kDevRange = 2, kDevTimeout = 3 };
 
 }  // namespace picard

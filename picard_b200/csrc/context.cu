@@ -247,7 +247,7 @@ int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver,
   b += (double)s.nodes * (8.0 * s.species /*Nacc*/ + 8.0 * s.species /*N*/ + 8 * 3 /*C,U,b*/ + 24 /*E*/ + 8 /*U1*/);
   if (layout == PICARD_LAYOUT_CELL32) b += 16.0 * s.nodes;
   if (solver == PICARD_SOLVER_F64) b += 8.0 * s.nodes;
-  else b += 16.0 * s.nodes;
+  else b += 16.0 * (double)f32_elems(make_kparams(*p));
   b += 8.0 * (double)s.dsize;
   b += 8.0 * (double)s.cells;                // produce counts + offsets
   b += 8.0 * (double)s.nb_compact * 3;       // compaction scratch
@@ -301,7 +301,16 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
   if (solver == PICARD_SOLVER_F64) {
     if ((rc = dalloc(c, c->Usnap, nn))) return bail(rc);
   } else {
-    if ((rc = dalloc(c, c->w[0], nn)) || (rc = dalloc(c, c->w[1], nn)) || (rc = dalloc(c, c->r, 2 * nn))) return bail(rc);
+    const long long fe = f32_elems(c->K);
+    if ((rc = dalloc(c, c->w[0], fe)) || (rc = dalloc(c, c->w[1], fe)) || (rc = dalloc(c, c->r, 2 * fe))) return bail(rc);
+    if (c->G.tma) {
+      int e0 = make_tensor_map(&c->tmw[0], c->w[0], c->K, 10, c->G.zc + 2);
+      int e1 = make_tensor_map(&c->tmw[1], c->w[1], c->K, 10, c->G.zc + 2);
+      int e2 = make_tensor_map(&c->tmr[0], c->r, c->K, 8, c->G.zc);
+      int e3 = make_tensor_map(&c->tmr[1], c->r + fe, c->K, 8, c->G.zc);
+      if (e0 || e1 || e2 || e3)
+        return bail(fail(PICARD_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(e0 | e1 | e2 | e3) + ")"));
+    }
   }
   if ((rc = dalloc(c, c->partials, (size_t)(c->m_max + 1) * c->G.nblocks)) ||
       (rc = dalloc(c, c->r2, c->m_max + 1)))
@@ -321,6 +330,8 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
   if ((rc = check_cuda(cudaMallocHost((void**)&c->h_pinned_i, sizeof(int) * 16), "cudaMallocHost"))) return bail(rc);
   for (int e = 0; e < 4; ++e)
     if ((rc = check_cuda(cudaEventCreate(&c->ev[e]), "cudaEventCreate"))) return bail(rc);
+  for (int e = 0; e < 6; ++e)
+    if ((rc = check_cuda(cudaEventCreate(&c->pev[e]), "cudaEventCreate"))) return bail(rc);
   if ((rc = check_cuda(cudaStreamSynchronize(c->st), "create"))) return bail(rc);
   c->launches_at_reset = launches_so_far();
   *out = c;
@@ -335,6 +346,8 @@ int picard_gpu_destroy(picard_ctx* c) {
   if (c->h_pinned_i) cudaFreeHost(c->h_pinned_i);
   for (int e = 0; e < 4; ++e)
     if (c->ev[e]) cudaEventDestroy(c->ev[e]);
+  for (int e = 0; e < 6; ++e)
+    if (c->pev[e]) cudaEventDestroy(c->pev[e]);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return PICARD_OK;

@@ -39,8 +39,10 @@ struct picard_ctx {
   double* b = nullptr;
   double* U1 = nullptr;     // second FP64 iterate / anchor buffer
   double* Usnap = nullptr;  // FP64 solver: iterate at the batch start
-  float* w[2] = {nullptr, nullptr};
-  float* r = nullptr;
+  float* w[2] = {nullptr, nullptr};  // padded FP32 layout (grid.cuh f32_pitch)
+  float* r = nullptr;                 // two padded FP32 arrays
+  CUtensorMap tmw[2];                 // TMA descriptors of w[0], w[1] (w boxes)
+  CUtensorMap tmr[2];                 // TMA descriptors of r, r + f32_elems (r boxes)
   double* partials = nullptr;  // [m_max + 1][nblocks]
   double* r2 = nullptr;        // [m_max + 1]
   picard::JacobiGeom G;
@@ -72,6 +74,7 @@ struct picard_ctx {
   picard_stats stats = {};
   long long launches_at_reset = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t pev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // phase boundaries
 };
 
 namespace picard {

@@ -207,6 +207,7 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
   const int cells = p.nx * p.ny * p.nz;
   bool nc = false;
   for (int32_t it = iter_start + 1; it <= iter_end; ++it) {
+    PICARD_CUDA(cudaEventRecord(c->pev[0], c->st));
     // AdvancePosition on the particles present before BCinflow
     PICARD_TRY(picard_gpu_advance_position(c, p.dt));
     // ParticlesProduce, appended behind them (device-side count)
@@ -237,8 +238,11 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
       PICARD_CUDA(launch_inflow_fused_c32(K, c->inflow, it, c->c32[c->cur], c->d_count + c->cur, c->capacity,
                                           c->d_err, c->st));
     PICARD_TRY(sync_count_public(c));
+    PICARD_CUDA(cudaEventRecord(c->pev[1], c->st));
     PICARD_TRY(picard_gpu_particles_gridify(c));
+    PICARD_CUDA(cudaEventRecord(c->pev[2], c->st));
     PICARD_TRY(picard_gpu_bc_potentials(c));
+    PICARD_CUDA(cudaEventRecord(c->pev[3], c->st));
     int32_t sw = 0;
     int rc = picard_gpu_calc_epotential(c, p.maxerr, p.maxit, &sw);
     if (rc == PICARD_ERR_NOT_CONVERGED)
@@ -246,8 +250,15 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
     else if (rc != PICARD_OK)
       return rc;
     if (sweeps_total) *sweeps_total += sw;
+    PICARD_CUDA(cudaEventRecord(c->pev[4], c->st));
     PICARD_TRY(picard_gpu_calc_efield(c));
     PICARD_TRY(picard_gpu_advance_velocity(c, p.dt));
+    PICARD_CUDA(cudaEventRecord(c->pev[5], c->st));
+    PICARD_CUDA(cudaEventSynchronize(c->pev[5]));
+    for (int ph = 0; ph < 5; ++ph) {
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, c->pev[ph], c->pev[ph + 1]) == cudaSuccess) c->stats.phase_ms[ph] += ms;
+    }
     c->stats.steps += 1;
     c->stats.particle_steps += c->num_local;
   }

@@ -197,7 +197,16 @@ struct Stencil {
   int nx, ny, nz, nxp, nyp;
   int px, py, pz;  // periodic axes
   long long nodes;
+  int fpitch;      // row pitch (floats) of the FP32 solver arrays
 };
+
+// FP32 solver arrays (increment w, scaled residual r) are padded: node
+// (i, j, k) sits at column i + 3 of a row of fpitch floats, fpitch a multiple
+// of 8.  Interior rows then start on 16-byte boundaries (column 4) and every
+// TMA box origin (column 32 b) is 16-byte aligned.
+__host__ __device__ inline long long fidx(const Stencil& S, int i, int j, int k) {
+  return (long long)(i + 3) + (long long)S.fpitch * ((long long)j + (long long)S.nyp * k);
+}
 
 __device__ inline void neighbours(const Stencil& S, int i, int j, int k, long long& xm, long long& xp, long long& ym,
                                   long long& yp, long long& zm, long long& zp) {
@@ -285,8 +294,8 @@ __global__ void __launch_bounds__(256) sweep_f32_kernel(Stencil S, JacobiCoefF J
   float r2 = 0.0f;
   if (i <= S.nx && j <= S.ny) {
     int k1 = min(k0 + zc - 1, S.nz);
-    long long plane = (long long)S.nxp * S.nyp;
-    long long c = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * k0);
+    long long plane = (long long)S.fpitch * S.nyp;
+    long long c = fidx(S, i, j, k0);
     if (w_zero) {
       for (int k = k0; k <= k1; ++k, c += plane) {
         float res = __ldg(r + c);
@@ -297,7 +306,7 @@ __global__ void __launch_bounds__(256) sweep_f32_kernel(Stencil S, JacobiCoefF J
       int im = (S.px && i == 1) ? S.nx : i - 1, ip = (S.px && i == S.nx) ? 1 : i + 1;
       int jm = (S.py && j == 1) ? S.ny : j - 1, jp = (S.py && j == S.ny) ? 1 : j + 1;
       long long dxm = im - i, dxp = ip - i;
-      long long dym = (long long)(jm - j) * S.nxp, dyp = (long long)(jp - j) * S.nxp;
+      long long dym = (long long)(jm - j) * S.fpitch, dyp = (long long)(jp - j) * S.fpitch;
       // z pipeline in registers
       long long cm = (S.pz && k0 == 1) ? c + (long long)(S.nz - 1) * plane : c - plane;
       float wm = __ldg(win + cm);
@@ -336,14 +345,19 @@ __global__ void __launch_bounds__(256) anchor_kernel(Stencil S, JacobiCoef J, co
       long long c = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * k);
       long long xm, xp, ym, yp, zm, zp;
       neighbours(S, i, j, k, xm, xp, ym, yp, zm, zp);
-      auto val = [&](long long g) { return w_zero ? Vin[g] : Vin[g] + sigma * (double)w[g]; };
+      // FP32 index of a node given its FP64 index (same (i, j, k))
+      auto fof = [&](long long g) {
+        long long ii = g % S.nxp, rest = g / S.nxp;
+        return (ii + 3) + (long long)S.fpitch * rest;
+      };
+      auto val = [&](long long g) { return w_zero ? Vin[g] : Vin[g] + sigma * (double)w[fof(g)]; };
       double u = val(c);
       double sx = val(xp) + val(xm), sy = val(yp) + val(ym), sz = val(zp) + val(zm);
       double bc = b[c];
       double res = bc - ((sx - 2.0 * u) / J.dx2 + (sy - 2.0 * u) / J.dy2 + (sz - 2.0 * u) / J.dz2);
       r2 += res * res;
       Vout[c] = u;
-      r[c] = (float)(res / sigma);
+      r[fidx(S, i, j, k)] = (float)(res / sigma);
     }
   }
   block_sum_store(r2, partial + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
@@ -355,7 +369,109 @@ __global__ void finalize_kernel(Stencil S, const double* V, const float* w, doub
   if (g >= S.nodes) return;
   int i = int(g % S.nxp), j = int((g / S.nxp) % S.nyp), k = int(g / ((long long)S.nxp * S.nyp));
   bool interior = i >= 1 && i <= S.nx && j >= 1 && j <= S.ny && k >= 1 && k <= S.nz;
-  U[g] = (interior && !w_zero) ? V[g] + sigma * (double)w[g] : V[g];
+  U[g] = (interior && !w_zero) ? V[g] + sigma * (double)w[fidx(S, i, j, k)] : V[g];
+}
+
+// ------------------------------------------------- TMA-staged FP32 sweep
+
+// One block owns a 32 x 8 x ZC column of interior nodes.  Its single elected
+// thread issues two TMA tile loads into shared memory -- the increment w with
+// a one-node halo (box 40 x 10 x (ZC+2) from the 16-byte aligned column
+// 32 bx) and the scaled residual r (box 40 x 8 x ZC) -- completing on one
+// mbarrier.  The block then sweeps its column plane by plane from shared
+// memory and writes w' with coalesced stores.  Open axes only: the ghost
+// layer of w is zero, which the box supplies (and TMA zero-fills outside the
+// array).  Waits are bounded: on timeout the block records kDevTimeout in
+// *err, waits (bounded) for its copies to land and returns.
+constexpr int kTmaTx = 32, kTmaTy = 8, kTmaBoxX = 40;
+constexpr long long kMbarSpin = 1LL << 24;
+
+__device__ inline bool mbar_wait(uint32_t mbar, uint32_t phase, long long limit) {
+  for (long long it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int ZC>
+__global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ CUtensorMap tw,
+                                                        const __grid_constant__ CUtensorMap tr, Stencil S,
+                                                        JacobiCoefF J, float* __restrict__ wout, double* partial,
+                                                        int w_zero, int* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* sw = reinterpret_cast<float*>(smem_raw);                       // [ZC+2][10][40]
+  float* sr = sw + (ZC + 2) * (kTmaTy + 2) * kTmaBoxX;                  // [ZC][8][40]
+  __shared__ __align__(8) unsigned long long mbar;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + kTmaTx * ty;
+  const int x0 = blockIdx.x * kTmaTx, y0 = blockIdx.y * kTmaTy, z0 = blockIdx.z * ZC;
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t bytes = (uint32_t)(ZC * kTmaTy * kTmaBoxX * sizeof(float));
+    if (!w_zero) bytes += (uint32_t)((ZC + 2) * (kTmaTy + 2) * kTmaBoxX * sizeof(float));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+    if (!w_zero)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+          ::"r"((uint32_t)__cvta_generic_to_shared(sw)), "l"((unsigned long long)&tw), "r"(x0), "r"(y0), "r"(z0),
+          "r"(mb)
+          : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)&tr), "r"(x0), "r"(y0 + 1),
+        "r"(z0 + 1), "r"(mb)
+        : "memory");
+  }
+  if (!mbar_wait(mb, 0, kMbarSpin)) {
+    if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+    mbar_wait(mb, 0, kMbarSpin);  // let the copies land before the block exits
+    return;
+  }
+  const int i = x0 + tx + 1, j = y0 + ty + 1;
+  float r2 = 0.0f;
+  if (i <= S.nx && j <= S.ny) {
+    const int kend = min(ZC, S.nz - z0);
+    const long long plane = (long long)S.fpitch * S.nyp;
+    long long c = fidx(S, i, j, z0 + 1);
+    const int col = tx + 4;  // smem column of node i
+    if (w_zero) {
+      for (int kk = 1; kk <= kend; ++kk, c += plane) {
+        float res = sr[((kk - 1) * kTmaTy + ty) * kTmaBoxX + col];
+        r2 += res * res;
+        wout[c] = -J.af * res;
+      }
+    } else {
+      auto W = [&](int kk, int row, int cc) { return sw[(kk * (kTmaTy + 2) + row) * kTmaBoxX + cc]; };
+      float wm = W(0, ty + 1, col);
+      float wc = W(1, ty + 1, col);
+      for (int kk = 1; kk <= kend; ++kk, c += plane) {
+        float wp = W(kk + 1, ty + 1, col);
+        float sx = W(kk, ty + 1, col + 1) + W(kk, ty + 1, col - 1);
+        float sy = W(kk, ty + 2, col) + W(kk, ty, col);
+        float sz = wp + wm;
+        float lap = (sx - 2.0f * wc) * J.idx2 + (sy - 2.0f * wc) * J.idy2 + (sz - 2.0f * wc) * J.idz2;
+        float res = sr[((kk - 1) * kTmaTy + ty) * kTmaBoxX + col] - lap;
+        r2 += res * res;
+        wout[c] = wc - J.af * res;
+        wm = wc;
+        wc = wp;
+      }
+    }
+  }
+  block_sum_store((double)r2, partial + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
 }
 
 // Periodic ghost refresh of U (CalcEpotential.f90:100-239 on one rank), in
@@ -490,8 +606,12 @@ Stencil make_stencil(const KParams& P) {
   S.py = !P.yflow;
   S.pz = !P.zflow;
   S.nodes = P.nodes;
+  S.fpitch = f32_pitch(P);
   return S;
 }
+
+int f32_pitch(const KParams& P) { return ((P.nx + 5 + 7) / 8) * 8; }
+long long f32_elems(const KParams& P) { return (long long)f32_pitch(P) * P.nyp * P.nzp; }
 
 JacobiGeom jacobi_geom(const KParams& P) {
   JacobiGeom G;
@@ -502,6 +622,12 @@ JacobiGeom jacobi_geom(const KParams& P) {
   int zc = (P.nz + want - 1) / want;
   if (zc < 4) zc = 4;
   if (zc > P.nz) zc = P.nz;
+  G.tma = P.xflow && P.yflow && P.zflow;
+  if (G.tma) {
+    // TMA column depth: 8 planes (26 KB of shared memory, 8 blocks per SM),
+    // 4 for shallow grids
+    zc = P.nz >= 64 ? 8 : 4;
+  }
   G.zc = zc;
   G.grid = dim3(bx, by, (P.nz + zc - 1) / zc);
   G.nblocks = bx * by * G.grid.z;
@@ -586,6 +712,55 @@ cudaError_t launch_sweep_f32(const KParams& P, const JacobiGeom& G, const float*
   sweep_f32_kernel<<<G.grid, G.block, 0, st>>>(make_stencil(P), jacobi_coef_f(P), win, wout, r, partial, G.zc,
                                                 w_zero);
   return cudaGetLastError();
+}
+
+int make_tensor_map(CUtensorMap* m, float* base, const KParams& P, int box_y, int box_z) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return (int)CUDA_ERROR_NOT_FOUND;
+    encode = reinterpret_cast<Encode>(fn);
+  }
+  const int pitch = f32_pitch(P);
+  cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)P.nyp, (cuuint64_t)P.nzp};
+  cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(float), (cuuint64_t)pitch * P.nyp * sizeof(float)};
+  cuuint32_t box[3] = {(cuuint32_t)kTmaBoxX, (cuuint32_t)box_y, (cuuint32_t)box_z};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return (int)encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
+
+template <int ZC>
+static cudaError_t launch_tma_zc(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                                 float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
+  const size_t smem = ((size_t)(ZC + 2) * (kTmaTy + 2) * kTmaBoxX + (size_t)ZC * kTmaTy * kTmaBoxX) * sizeof(float);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(sweep_tma_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  note_launch();
+  sweep_tma_kernel<ZC><<<G.grid, dim3(kTmaTx, kTmaTy), smem, st>>>(*tw, *tr, make_stencil(P), jacobi_coef_f(P), wout,
+                                                                     partial, w_zero, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_tma(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                             float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
+  switch (G.zc) {
+    case 4: return launch_tma_zc<4>(P, G, tw, tr, wout, partial, w_zero, err, st);
+    case 8: return launch_tma_zc<8>(P, G, tw, tr, wout, partial, w_zero, err, st);
+    case 16: return launch_tma_zc<16>(P, G, tw, tr, wout, partial, w_zero, err, st);
+  }
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_anchor(const KParams& P, const JacobiGeom& G, const double* Vin, double* Vout, const float* w,

@@ -1,6 +1,8 @@
 // grid.cuh -- launch wrappers of grid.cu (node-array kernels).
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace picard {
@@ -19,7 +21,18 @@ struct JacobiGeom {
   dim3 grid, block;
   int zc;
   int nblocks;
+  int tma;  // all axes open: the TMA-staged sweep kernel is used (zc in {4, 8, 16})
 };
+
+// Row pitch (floats) of the padded FP32 solver arrays: node (i, j, k) at
+// column i + 3, rows a multiple of 8 floats (32 bytes).
+int f32_pitch(const KParams& P);
+long long f32_elems(const KParams& P);
+// TMA descriptors of one padded FP32 array: w boxes (40 x 10 x zc+2) and
+// r boxes (40 x 8 x zc).  Returns a CUresult.
+int make_tensor_map(CUtensorMap* m, float* base, const KParams& P, int box_y, int box_z);
+cudaError_t launch_sweep_tma(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                             float* wout, double* partial, int w_zero, int* err, cudaStream_t st);
 
 JacobiGeom jacobi_geom(const KParams& P);
 JacobiCoef jacobi_coef(const KParams& P);

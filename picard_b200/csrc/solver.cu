@@ -44,6 +44,18 @@ double elapsed_ms(picard_ctx* c, int a, int b) {
   return ms;
 }
 
+// A sweep that gave up waiting for its TMA tiles recorded kDevTimeout.
+int check_timeout(picard_ctx* c) {
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 4, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += sizeof(int);
+  if (c->h_pinned_i[4] == kDevTimeout) {
+    PICARD_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+    return fail(PICARD_ERR_TIMEOUT, "a Jacobi sweep timed out waiting for its TMA tiles");
+  }
+  return PICARD_OK;
+}
+
 int read_r2(picard_ctx* c, int count) {
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->r2, sizeof(double) * count, cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
@@ -121,7 +133,14 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
   const KParams& K = c->K;
   const int nb = c->G.nblocks;
   double* V[2] = {c->U, c->U1};
-  float* R[2] = {c->r, c->r + K.nodes};  // anchor residuals, one per live anchor
+  float* R[2] = {c->r, c->r + f32_elems(K)};  // anchor residuals, one per live anchor
+  // sweep s reads w[(s-1)%2] (TMA descriptor tmw[(s-1)%2]) and R[rcur] (tmr[rcur])
+  auto sweep = [&](long long s, int rc_, double* partial, int w_zero) -> cudaError_t {
+    if (c->G.tma)
+      return launch_sweep_tma(K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[rc_], c->w[s % 2], partial, w_zero, c->d_err,
+                              c->st);
+    return launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rc_], partial, w_zero, c->st);
+  };
   int vcur = 0, rcur = 0;
   PICARD_CUDA(cudaMemcpyAsync(c->U1, c->U, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
   // anchor 0: r = (b - L U_0) / sigma
@@ -136,8 +155,7 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
     PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
     for (int t = 1; t <= m_eff; ++t) {
       long long s = a + t;
-      PICARD_CUDA(launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rcur],
-                                   c->partials + (size_t)(t - 1) * nb, t == 1 ? 1 : 0, c->st));
+      PICARD_CUDA(sweep(s, rcur, c->partials + (size_t)(t - 1) * nb, t == 1 ? 1 : 0));
     }
     PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
     // next anchor: fold w_{a+m_eff} into V, exact FP64 residual of that iterate
@@ -147,6 +165,7 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
     PICARD_CUDA(cudaEventRecord(c->ev[2], c->st));
     PICARD_CUDA(launch_reduce_sweeps(c->partials, nb, m_eff + 1, c->r2, c->st));
     PICARD_TRY(read_r2(c, m_eff + 1));
+    PICARD_TRY(check_timeout(c));
     c->stats.sweep_launches += m_eff;
     c->stats.sweep_ms += elapsed_ms(c, 0, 1);
     c->stats.anchor_launches += 1;
@@ -173,8 +192,7 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
       } else {
         // replay sweeps a+1..hit from the old anchor (unchanged in V[vcur])
         for (long long s = a + 1; s <= hit; ++s)
-          PICARD_CUDA(launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rcur], c->partials,
-                                       s == a + 1 ? 1 : 0, c->st));
+          PICARD_CUDA(sweep(s, rcur, c->partials, s == a + 1 ? 1 : 0));
         c->stats.sweep_launches += hit - a;
         PICARD_CUDA(launch_finalize(K, V[vcur], c->w[hit % 2], sigma, c->U, 0, c->st));
       }
