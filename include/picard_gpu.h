@@ -236,6 +236,16 @@ PICARD_API int picard_gpu_reset_stats(picard_ctx* ctx);
  * record their own CUDA events around library calls). */
 PICARD_API int picard_gpu_get_stream(picard_ctx* ctx, void** stream);
 
+/* ---------------------------------------------------------------- options */
+
+typedef enum picard_option {
+  /* 1: BCpotentials on the tensor cores (three-way BF16 split, FP32
+   * accumulation folded into FP64 every 512 K-values; the default of the
+   * CELL32 layout).  0: FP64 direct sum (the default of the F64 layout). */
+  PICARD_OPT_BCPOT_TENSOR = 0
+} picard_option;
+PICARD_API int picard_gpu_set_option(picard_ctx* ctx, int32_t option, int32_t value);
+
 /* ----------------------------------------------------------- main loop */
 
 /* One line of the reference's energy log (picard.f90:667-671). */

@@ -24,6 +24,7 @@ UNITS = {
     "particles_exact.cu": ["--fmad=false"],
     "particles_fast.cu": [],
     "grid.cu": [],
+    "bcpot_tc.cu": [],
     "solver.cu": [],
     "context.cu": [],
     "driver.cu": [],

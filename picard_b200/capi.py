@@ -29,6 +29,7 @@ SOLVER_F64 = 0
 SOLVER_F32_REFINE = 1
 
 FIELD_U, FIELD_E, FIELD_N, FIELD_C, FIELD_F, FIELD_D = range(6)
+OPT_BCPOT_TENSOR = 0
 
 class PicardStats(C.Structure):
     _fields_ = [
@@ -114,6 +115,7 @@ def lib():
         "picard_gpu_get_stats": [ctx, C.POINTER(PicardStats)],
         "picard_gpu_reset_stats": [ctx],
         "picard_gpu_get_stream": [ctx, C.POINTER(C.c_void_p)],
+        "picard_gpu_set_option": [ctx, C.c_int32, C.c_int32],
         "picard_gpu_particles_gridify_noalloc": [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                                  C.c_void_p, C.c_void_p, C.c_void_p],
     }

@@ -1,0 +1,397 @@
+// bcpot_tc.cu -- BCpotentials (BCpotentials.f90:51-139) on the 5th-generation
+// tensor cores.
+//
+// For one face axis, with (p1, p2) the in-plane coordinates of a face node and
+// q the coordinate along the normal,
+//   U_f(p1, p2) = sum_q sum_q1 sum_q2 C(q, q1, q2) D_f(q, q1 - p1, q2 - p2),
+// where f = 0, 1 are the two faces of the axis (they differ only in the normal
+// offset of D).  For a fixed plane q and row shift d = q1 - p1 this is a GEMM
+//   U_f(p1, :) += C(q, p1 + d, :) . T_{q,d,f},  T[q2, p2] = D_f(q, d, q2 - p2)
+// (T is Toeplitz).  A CTA owns a 128 x 256 output tile -- 128 rows p1, and
+// 128 columns p2 of each face side by side -- and accumulates it in tensor
+// memory over a slice of the (q, d) pairs (split-K over all SMs).
+//
+// Precision: every FP64 operand is split into three BF16 parts
+// (x = x1 + x2 + x3, 24 significant bits) and each K-step issues the six
+// products x_i y_j with i + j <= 4.  The FP32 accumulator in TMEM is folded
+// into an FP64 partial of the CTA every kFlushChunks K-chunks, so FP32
+// rounding only accumulates over short runs.  A reduction kernel sums the
+// per-CTA partials in a fixed order.
+//
+// Operands are built by the CTA's threads in shared memory in the canonical
+// K-major no-swizzle layout of tcgen05 (8-row x 16-byte core matrices):
+// element (r, k) of a tile with R rows lives at byte
+//   (k / 8) * (R * 16) + (r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2,
+// i.e. leading-byte offset R * 16 between the two K core matrices of an
+// instruction and stride-byte offset 128 between 8-row groups.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "common.cuh"
+#include "grid.cuh"
+
+namespace picard {
+
+namespace {
+
+constexpr int kTcM = 128;          // rows p1 per tile
+constexpr int kTcHalfN = 128;      // columns p2 per face
+constexpr int kTcN = 2 * kTcHalfN; // both faces
+constexpr int kTcKC = 64;          // K (q2) per chunk
+constexpr int kTcThreads = 128;
+constexpr int kFlushChunks = 8;    // K-chunks between FP64 folds of the accumulator
+constexpr long long kTcSpin = 1LL << 26;
+
+constexpr int kAsplit = kTcM * kTcKC;  // bf16 elements of one A split
+constexpr int kBsplit = kTcN * kTcKC;  // bf16 elements of one B split
+constexpr int kWinPad = 64;            // zero padding on both sides of a D window
+
+struct TcAxis {
+  int axis;        // normal axis
+  int n1, n2, nn;  // in-plane extents (p1, p2) and normal extent
+  int n2pad;       // n2 rounded up to kTcKC
+  int mtiles, ntiles, splits;
+};
+
+__device__ inline uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
+// K-major, M = 128, N = 256.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
+                            ((uint32_t)(kTcM >> 4) << 24);
+
+__device__ inline void split3(float x, __nv_bfloat16& a, __nv_bfloat16& b, __nv_bfloat16& c) {
+  a = __float2bfloat16_rn(x);
+  float r = x - __bfloat162float(a);
+  b = __float2bfloat16_rn(r);
+  r = r - __bfloat162float(b);
+  c = __float2bfloat16_rn(r);
+}
+
+__device__ inline bool mbar_wait_tc(uint32_t mbar, uint32_t phase) {
+  for (long long it = 0; it < kTcSpin; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// C (FP64 node array) -> three BF16 planes per face axis,
+// Cs[s][q][row][q2] with row = p1 - 1 in [0, n1), q2 - 1 in [0, n2pad).
+__global__ void split_charge_kernel(KParams P, TcAxis X, const double* __restrict__ C, __nv_bfloat16* Cs) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long per = (long long)X.nn * X.n1 * X.n2pad;
+  if (t >= per) return;
+  int q2 = int(t % X.n2pad);
+  int row = int((t / X.n2pad) % X.n1);
+  int q = int(t / ((long long)X.n2pad * X.n1));
+  float v = 0.0f;
+  if (q2 < X.n2) {
+    int ci, cj, ck;
+    if (X.axis == 0) ci = q + 1, cj = row + 1, ck = q2 + 1;
+    else if (X.axis == 1) ci = row + 1, cj = q + 1, ck = q2 + 1;
+    else ci = row + 1, cj = q2 + 1, ck = q + 1;
+    v = (float)C[node_index(P, ci, cj, ck)];
+  }
+  __nv_bfloat16 a, b, c;
+  split3(v, a, b, c);
+  Cs[t] = a;
+  Cs[per + t] = b;
+  Cs[2 * per + t] = c;
+}
+
+// D index (1-based) of face f for plane q, shift d (along p1), offset o2 (along p2).
+__device__ inline long long d_index(const KParams& P, const TcAxis& X, int f, int q, int d, int o2) {
+  int on = f == 0 ? q : q - (X.nn + 1);
+  int a, b, c;
+  if (X.axis == 0) a = P.nx + 1 + on, b = P.ny + 1 + d, c = P.nz + 1 + o2;
+  else if (X.axis == 1) a = P.nx + 1 + d, b = P.ny + 1 + on, c = P.nz + 1 + o2;
+  else a = P.nx + 1 + d, b = P.ny + 1 + o2, c = P.nz + 1 + on;
+  long long DX = 2LL * P.nx + 1, DY = 2LL * P.ny + 1;
+  return (long long)(a - 1) + DX * ((long long)(b - 1) + DY * (long long)(c - 1));
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    bcpot_tc_kernel(KParams P, TcAxis X, const __nv_bfloat16* __restrict__ Cs, const double* __restrict__ D,
+                    double* partial, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(smem);                  // [3][kAsplit]
+  __nv_bfloat16* sB = sA + 3 * kAsplit;                                          // [3][kBsplit]
+  __nv_bfloat16* sW = sB + 3 * kBsplit;                                          // [2][3][2*n2+2*pad]
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wlen = 2 * X.n2 - 1 + 2 * kWinPad;
+
+  // tile and slice of (q, d) pairs of this CTA
+  const int tile = blockIdx.x / X.splits, split = blockIdx.x % X.splits;
+  const int mt = tile / X.ntiles, nt = tile % X.ntiles;
+  const int m0 = mt * kTcM, n0 = nt * kTcHalfN;
+  // shifts d = q1 - p1 with at least one valid row (q1, p1 both in [1, n1])
+  const int rows_hi = (m0 + kTcM < X.n1) ? m0 + kTcM : X.n1;
+  const int dlo = 1 - rows_hi, dhi = X.n1 - m0 - 1;
+  const long long npairs = (long long)X.nn * (dhi - dlo + 1);
+  const long long pbeg = npairs * split / X.splits, pend = npairs * (split + 1) / X.splits;
+  const int nchunks = X.n2pad / kTcKC;
+  double* part = partial + (long long)blockIdx.x * kTcM * kTcN;
+
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (warp == 0) {
+    uint32_t dst = (uint32_t)__cvta_generic_to_shared(&tmem_base);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTcN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int e = tid; e < kTcM * kTcN; e += kTcThreads) part[e] = 0.0;
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  uint32_t phase = 0;
+  bool pending = false;   // MMAs committed and not yet waited for
+  int since_flush = 0;    // chunks accumulated in TMEM
+  bool ok = true;
+
+  auto wait_mma = [&]() -> bool {
+    if (!pending) return true;
+    bool r = mbar_wait_tc(mb, phase);
+    phase ^= 1;
+    pending = false;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return r;
+  };
+  // fold the FP32 accumulator into the FP64 partial (each thread owns row
+  // 32*warp + lane of the tile: TMEM lane = row)
+  auto flush = [&]() {
+    for (int col = 0; col < kTcN; col += 16) {
+      uint32_t r[16];
+      uint32_t addr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)col;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      double* row = part + (long long)(32 * warp + lane) * kTcN + col;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) row[j] += (double)__uint_as_float(r[j]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  };
+
+  for (long long pr = pbeg; pr < pend && ok; ++pr) {
+    const int q = int(pr / (dhi - dlo + 1)) + 1;
+    const int d = dlo + int(pr % (dhi - dlo + 1));
+    // previous MMAs read sW / sA / sB: wait before rewriting them
+    if (!wait_mma()) { ok = false; break; }
+    __syncthreads();
+    // D windows of both faces: index o2 + n2 - 1 + pad, o2 in [-(n2-1), n2-1]
+    for (int e = tid; e < 2 * wlen; e += kTcThreads) {
+      int f = e / wlen, w = e % wlen;
+      int o2 = w - kWinPad - (X.n2 - 1);
+      float v = 0.0f;
+      if (o2 >= -(X.n2 - 1) && o2 <= X.n2 - 1) v = (float)D[d_index(P, X, f, q, d, o2)];
+      __nv_bfloat16 a, b, c;
+      split3(v, a, b, c);
+      sW[(f * 3 + 0) * wlen + w] = a;
+      sW[(f * 3 + 1) * wlen + w] = b;
+      sW[(f * 3 + 2) * wlen + w] = c;
+    }
+    __syncthreads();
+    for (int kc = 0; kc < nchunks && ok; ++kc) {
+      if (kc > 0) {
+        if (!wait_mma()) { ok = false; break; }
+        __syncthreads();
+      }
+      const int k0 = kc * kTcKC;
+      // A: rows r = p1 - 1 - m0, source row p1 + d - 1 of plane q
+      for (int e = tid; e < 3 * kTcM * (kTcKC / 8); e += kTcThreads) {
+        int s = e / (kTcM * (kTcKC / 8)), rem = e % (kTcM * (kTcKC / 8));
+        int r = rem / (kTcKC / 8), c8 = rem % (kTcKC / 8);
+        int src = m0 + r + d;  // 0-based source row
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (src >= 0 && src < X.n1 && m0 + r < X.n1) {
+          long long per = (long long)X.nn * X.n1 * X.n2pad;
+          const __nv_bfloat16* g = Cs + s * per + ((long long)(q - 1) * X.n1 + src) * X.n2pad + k0 + c8 * 8;
+          v = *reinterpret_cast<const uint4*>(g);
+        }
+        unsigned char* dst = reinterpret_cast<unsigned char*>(sA + s * kAsplit) + c8 * (kTcM * 16) +
+                             (r >> 3) * 128 + (r & 7) * 16;
+        *reinterpret_cast<uint4*>(dst) = v;
+      }
+      // B: column n = f * 128 + p (p2 = n0 + p + 1), k -> q2 = k0 + k + 1
+      for (int e = tid; e < 3 * kTcN * (kTcKC / 8); e += kTcThreads) {
+        int s = e / (kTcN * (kTcKC / 8)), rem = e % (kTcN * (kTcKC / 8));
+        int n = rem / (kTcKC / 8), c8 = rem % (kTcKC / 8);
+        int f = n / kTcHalfN, p = n % kTcHalfN;
+        int p2 = n0 + p + 1;
+        __align__(16) __nv_bfloat16 v[8];
+        const __nv_bfloat16* win = sW + (f * 3 + s) * wlen;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          int q2 = k0 + c8 * 8 + j + 1;
+          bool valid = q2 <= X.n2 && p2 <= X.n2;
+          int w = q2 - p2 + (X.n2 - 1) + kWinPad;
+          v[j] = valid ? win[w] : __float2bfloat16_rn(0.0f);
+        }
+        unsigned char* dst = reinterpret_cast<unsigned char*>(sB + s * kBsplit) + c8 * (kTcN * 16) +
+                             (n >> 3) * 128 + (n & 7) * 16;
+        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t aBase = (uint32_t)__cvta_generic_to_shared(sA);
+        const uint32_t bBase = (uint32_t)__cvta_generic_to_shared(sB);
+        const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
+#pragma unroll
+        for (int ks = 0; ks < kTcKC / 16; ++ks) {
+#pragma unroll
+          for (int t = 0; t < 6; ++t) {
+            uint32_t a_addr = aBase + pa[t] * kAsplit * 2 + ks * 2 * (kTcM * 16);
+            uint32_t b_addr = bBase + pb[t] * kBsplit * 2 + ks * 2 * (kTcN * 16);
+            uint64_t adesc = smem_desc(a_addr, kTcM * 16, 128);
+            uint64_t bdesc = smem_desc(b_addr, kTcN * 16, 128);
+            uint32_t acc = (since_flush == 0 && ks == 0 && t == 0) ? 0u : 1u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                ::"r"(tmem), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(acc)
+                : "memory");
+          }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
+                     : "memory");
+      }
+      pending = true;
+      ++since_flush;
+      if (since_flush == kFlushChunks) {
+        if (!wait_mma()) { ok = false; break; }
+        flush();
+        __syncthreads();
+        since_flush = 0;
+      }
+    }
+  }
+  if (ok && !wait_mma()) ok = false;
+  if (ok && since_flush > 0) flush();
+  if (!ok) {
+    if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+    wait_mma();  // bounded: let outstanding MMAs finish before TMEM is released
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN) : "memory");
+  }
+}
+
+// U on both faces of the axis = (sum over splits of the partial tiles) / (4 pi eps0).
+__global__ void bcpot_reduce_kernel(KParams P, TcAxis X, const double* partial, double* U) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long total = (long long)X.mtiles * X.ntiles * kTcM * kTcN;
+  if (t >= total) return;
+  int col = int(t % kTcN);
+  int row = int((t / kTcN) % kTcM);
+  int tile = int(t / ((long long)kTcN * kTcM));
+  int mt = tile / X.ntiles, nt = tile % X.ntiles;
+  int f = col / kTcHalfN;
+  int p1 = mt * kTcM + row + 1, p2 = nt * kTcHalfN + col % kTcHalfN + 1;
+  if (p1 > X.n1 || p2 > X.n2) return;
+  double s = 0.0;
+  for (int sp = 0; sp < X.splits; ++sp)
+    s += partial[((long long)(tile * X.splits + sp) * kTcM + row) * kTcN + col];
+  const double scale = 1.0 / (2.0 * kTau * kEps0);
+  int fixed = f == 0 ? 0 : (X.axis == 0 ? P.nx + 1 : (X.axis == 1 ? P.ny + 1 : P.nz + 1));
+  long long g;
+  if (X.axis == 0) g = node_index(P, fixed, p1, p2);
+  else if (X.axis == 1) g = node_index(P, p1, fixed, p2);
+  else g = node_index(P, p1, p2, fixed);
+  U[g] = s * scale;
+}
+
+TcAxis tc_axis(const KParams& P, int axis, int sms) {
+  TcAxis X;
+  X.axis = axis;
+  if (axis == 0) X.n1 = P.ny, X.n2 = P.nz, X.nn = P.nx;
+  else if (axis == 1) X.n1 = P.nx, X.n2 = P.nz, X.nn = P.ny;
+  else X.n1 = P.nx, X.n2 = P.ny, X.nn = P.nz;
+  X.n2pad = (X.n2 + kTcKC - 1) / kTcKC * kTcKC;
+  X.mtiles = (X.n1 + kTcM - 1) / kTcM;
+  X.ntiles = (X.n2 + kTcHalfN - 1) / kTcHalfN;
+  int tiles = X.mtiles * X.ntiles;
+  X.splits = sms / tiles;
+  if (X.splits < 1) X.splits = 1;
+  return X;
+}
+
+}  // namespace
+
+size_t bcpot_tc_smem_bytes(const KParams& P) {
+  int n2max = P.nx > P.ny ? (P.nx > P.nz ? P.nx : P.nz) : (P.ny > P.nz ? P.ny : P.nz);
+  return (size_t)(3 * kAsplit + 3 * kBsplit) * 2 + (size_t)2 * 3 * (2 * n2max - 1 + 2 * kWinPad) * 2 + 16;
+}
+
+void bcpot_tc_scratch(const KParams& P, long long* cs_elems, long long* partial_elems) {
+  long long cs = 0, pe = 0;
+  for (int axis = 0; axis < 3; ++axis) {
+    TcAxis X = tc_axis(P, axis, 148);
+    long long c = 3LL * X.nn * X.n1 * X.n2pad;
+    long long p = (long long)X.mtiles * X.ntiles * X.splits * kTcM * kTcN;
+    cs = c > cs ? c : cs;
+    pe = p > pe ? p : pe;
+  }
+  *cs_elems = cs;
+  *partial_elems = pe;
+}
+
+cudaError_t launch_bc_potentials_tc(const KParams& P, const double* C, const double* D, double* U, void* cs_buf,
+                                    double* partial, int* err, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(U, 0, sizeof(double) * P.nodes, st);
+  if (e != cudaSuccess) return e;
+  const size_t smem = bcpot_tc_smem_bytes(P);
+  static size_t attr = 0;
+  if (attr < smem) {
+    e = cudaFuncSetAttribute(bcpot_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = smem;
+  }
+  const int flows[3] = {P.xflow, P.yflow, P.zflow};
+  __nv_bfloat16* Cs = static_cast<__nv_bfloat16*>(cs_buf);
+  for (int axis = 0; axis < 3; ++axis) {
+    if (!flows[axis]) continue;
+    TcAxis X = tc_axis(P, axis, 148);
+    long long per = (long long)X.nn * X.n1 * X.n2pad;
+    note_launch();
+    split_charge_kernel<<<(unsigned)((per + 255) / 256), 256, 0, st>>>(P, X, C, Cs);
+    note_launch();
+    bcpot_tc_kernel<<<X.mtiles * X.ntiles * X.splits, kTcThreads, smem, st>>>(P, X, Cs, D, partial, err);
+    long long outs = (long long)X.mtiles * X.ntiles * kTcM * kTcN;
+    note_launch();
+    bcpot_reduce_kernel<<<(unsigned)((outs + 255) / 256), 256, 0, st>>>(P, X, partial, U);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace picard

@@ -216,6 +216,17 @@ int check_dev_err(picard_ctx* c) {
   return PICARD_OK;
 }
 
+int check_dev_err_timeout(picard_ctx* c) {
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 5, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  PICARD_CUDA(cudaStreamSynchronize(c->st));
+  c->stats.d2h_bytes += sizeof(int);
+  if (c->h_pinned_i[5] == kDevTimeout) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+    return fail(PICARD_ERR_TIMEOUT, "a tensor-core BCpotentials block timed out waiting for its MMAs");
+  }
+  return PICARD_OK;
+}
+
 int ensure_capacity(picard_ctx* c, long long add) {
   if (c->num_local + add > c->capacity)
     return fail(PICARD_ERR_CAPACITY, "particle count " + std::to_string(c->num_local + add) +
@@ -267,6 +278,7 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
   c->capacity = p->max_per_proc;
   c->inflow = make_inflow_table(*p);
   c->G = jacobi_geom(c->K);
+  c->bcpot_tensor = layout == PICARD_LAYOUT_CELL32 ? 1 : 0;
   int rc = PICARD_OK;
   auto bail = [&](int code) {
     picard_gpu_destroy(c);
@@ -665,9 +677,30 @@ int picard_gpu_particles_gridify_all(picard_ctx* c) {
   return deposit(c, true);
 }
 
+int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
+  if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
+  if (option == PICARD_OPT_BCPOT_TENSOR) {
+    c->bcpot_tensor = value != 0;
+    return PICARD_OK;
+  }
+  return fail(PICARD_ERR_BAD_ARG, "unknown option");
+}
+
 // BCpotentials.f90:1-145
 int picard_gpu_bc_potentials(picard_ctx* c) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
+  if (c->bcpot_tensor) {
+    if (!c->tc_cs) {
+      long long cs = 0, pe = 0;
+      bcpot_tc_scratch(c->K, &cs, &pe);
+      unsigned short* csb = nullptr;
+      PICARD_TRY(dalloc(c, csb, (size_t)cs));
+      PICARD_TRY(dalloc(c, c->tc_partial, (size_t)pe));
+      c->tc_cs = csb;
+    }
+    PICARD_CUDA(launch_bc_potentials_tc(c->K, c->C, c->D, c->U, c->tc_cs, c->tc_partial, c->d_err, c->st));
+    return check_dev_err_timeout(c);
+  }
   PICARD_CUDA(launch_bc_potentials(c->K, c->C, c->D, c->U, c->st));
   return PICARD_OK;
 }

@@ -61,6 +61,11 @@ struct picard_ctx {
   double* h_pinned = nullptr;    // [m_max + 16] host staging
   int* h_pinned_i = nullptr;     // [16]
 
+  // tensor-core BCpotentials (bcpot_tc.cu)
+  int bcpot_tensor = 0;
+  void* tc_cs = nullptr;
+  double* tc_partial = nullptr;
+
   // fused-path scratch
   int* tile_state = nullptr;
   int* tile_ticket = nullptr;

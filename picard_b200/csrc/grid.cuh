@@ -41,6 +41,12 @@ cudaError_t launch_finish_deposit(const KParams& P, const unsigned long long* Na
                                   cudaStream_t st);
 cudaError_t launch_finish_flux(const KParams& P, const unsigned long long* Facc, double* F, cudaStream_t st);
 cudaError_t launch_bc_potentials(const KParams& P, const double* C, const double* D, double* U, cudaStream_t st);
+// Tensor-core BCpotentials (bcpot_tc.cu): scratch sizes (bf16 split charge,
+// FP64 per-CTA partial tiles) and the launch.
+void bcpot_tc_scratch(const KParams& P, long long* cs_elems, long long* partial_elems);
+size_t bcpot_tc_smem_bytes(const KParams& P);
+cudaError_t launch_bc_potentials_tc(const KParams& P, const double* C, const double* D, double* U, void* cs_buf,
+                                    double* partial, int* err, cudaStream_t st);
 int rhs_blocks(const KParams& P);
 cudaError_t launch_rhs(const KParams& P, const double* C, double* b, double* partial, double* bnorm2,
                        cudaStream_t st);

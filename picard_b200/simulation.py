@@ -51,6 +51,9 @@ class Simulation:
     def _call(self, name: str, *args, allow=(capi.OK,)) -> int:
         return capi.check(getattr(capi.lib(), name)(self._h, *args), name, allow)
 
+    def set_option(self, option: int, value: int) -> None:
+        self._call("picard_gpu_set_option", option, value)
+
     def synchronize(self) -> None:
         self._call("picard_gpu_synchronize")
 

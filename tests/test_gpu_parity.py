@@ -127,6 +127,34 @@ def test_bc_potentials_matches_oracle():
     assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-12
 
 
+@pytest.mark.parametrize("dims", [(16, 16, 16), (160, 24, 20), (40, 136, 12)])
+def test_bc_potentials_tensor_cores_vs_fp64(dims):
+    # three-way BF16 split, FP32 accumulation folded into FP64 every 512
+    # K-values: the face potentials agree with the FP64 sum to ~1e-6 relative
+    nx, ny, nz = dims
+    p = small_plasma(n=8, ppc=2, seed=23)
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.xmin, p.xmax = -500.0 * nx, 500.0 * nx
+    p.ymin, p.ymax = -500.0 * ny, 500.0 * ny
+    p.zmin, p.zmax = -500.0 * nz, 500.0 * nz
+    p.max_per_proc = nx * ny * nz * 8 + 100000
+    q, o, g = make(p, **F64)
+    o.calc_distance()
+    o.initialize()
+    o.step(1)
+    o.step(2)
+    o.gridify()
+    o.bc_potentials()
+    g.calc_distance()
+    g.set_field(capi.FIELD_C, o.C)
+    g.set_option(capi.OPT_BCPOT_TENSOR, 1)
+    g.bc_potentials()
+    U = g.field(capi.FIELD_U)
+    err = rel_l2(U, o.U)
+    print(f"tensor-core BCpotentials {dims}: rel L2 vs FP64 = {err:.3e}")
+    assert err < 1e-5
+
+
 @pytest.mark.parametrize("mode", ["F64", "F64_REFINE"])
 def test_jacobi_matches_oracle(mode):
     kw = F64 if mode == "F64" else F64_REFINE
