@@ -54,14 +54,16 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=25.0, help="rough budget of the CPU baseline sample")
+    ap.add_argument("--ppc", type=int, default=None,
+                    help="ions per cell of the at-scale workload (default 32; smaller for profiling runs)")
     return ap.parse_args()
 
 
-def workload(name: str, seed: int):
+def workload(name: str, seed: int, ppc: int | None = None):
     from picard_b200 import params as P
 
     if name == "scale":
-        p = P.config_plain_scale(seed=seed)
+        p = P.config_plain_scale(seed=seed) if ppc is None else P.config_plain_scale(seed=seed, ppc_ion=ppc)
         desc = {"workload": "plain-at-scale 256x128x128 cells, 64 ppc (32 H+ + 32 e-), Haser source Q=1e27/s",
                 "grid": [256, 128, 128], "ppc_total": 64, "species": 3}
     else:
@@ -135,6 +137,20 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def combine_ranks(ms: float, work: float, dist=None, device: str = "cpu"):
+    """Whole-job timing of independent runs, one per rank: the slowest rank's
+    device time and the work summed over ranks (every rank takes part)."""
+    if dist is None:
+        return ms, work
+    import torch
+
+    t = torch.tensor([ms, work], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(t[1])
+
+
 # ---------------------------------------------------------------- GPU arm
 
 def run_picard(args, rank, world, local_rank):
@@ -149,7 +165,9 @@ def run_picard(args, rank, world, local_rank):
         import torch.distributed as dist
     layout = capi.LAYOUT_CELL32 if args.layout == "cell32" else capi.LAYOUT_F64
     solver = capi.SOLVER_F32_REFINE if args.solver == "refine" else capi.SOLVER_F64
-    p, desc = workload(args.workload, seed=rank)
+    p, desc = workload(args.workload, seed=rank, ppc=args.ppc)
+    if args.ppc is not None:
+        desc = dict(desc, ppc_total=2 * args.ppc, workload=desc["workload"] + f" (ppc override {args.ppc})")
     W, K = args.warmup, args.steps
 
     sim = Simulation(p, layout=layout, solver=solver)
@@ -221,15 +239,7 @@ def run_picard(args, rank, world, local_rank):
                "path": "picard_gpu_run (per-subroutine C-ABI calls) incl. context creation and initialisation",
                "ms": e_ms}
 
-    # reductions over ranks: max time, summed work
-    if dist is not None:
-        t = torch.tensor([ms, float(particle_steps)], dtype=torch.float64, device="cuda")
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        ms_max, total_ps = float(tmax[0]), float(t[1])
-    else:
-        ms_max, total_ps = ms, float(particle_steps)
+    ms_max, total_ps = combine_ranks(ms, float(particle_steps), dist, "cuda")
     value = total_ps / (ms_max * 1e-3)
 
     cpu = None
