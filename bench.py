@@ -46,7 +46,12 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["picard", "reference"], default="picard")
-    ap.add_argument("--workload", choices=["scale", "plain32", "poisson"], default="scale")
+    ap.add_argument("--workload", choices=["scale", "plain32", "poisson", "serving"], default="scale")
+    ap.add_argument("--requests", type=int, default=12, help="serving workload: runs in the arrival stream")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving workload: mean arrivals per second")
+    ap.add_argument("--run-steps", type=int, default=200, help="serving workload: iterations per run")
+    ap.add_argument("--slots", type=int, default=8, help="serving workload: runs in flight at once")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving workload: HBM budget of admitted runs")
     ap.add_argument("--poisson-n", type=int, default=256)
     ap.add_argument("--poisson-sweeps", type=int, default=400)
     ap.add_argument("--layout", choices=["cell32", "f64"], default="cell32")
@@ -261,7 +266,9 @@ def run_picard(args, rank, world, local_rank):
             "jacobi_sweeps_per_step": sweeps_per_step,
             "phase_ms_per_step": {k: round(v / K, 3) for k, v in st["phase_ms"].items()},
             "particles_final": num_final,
-            "roofline": {"bound": "hbm", "kernel": "sweep_f32_kernel" if solver else "sweep_f64_kernel",
+            "roofline": {"bound": "hbm",
+                         "kernel": ("sweep_tma_kernel" if p.xflow and p.yflow and p.zflow else "sweep_f32_kernel")
+                         if solver else "sweep_f64_kernel",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "launch_ms": sweep_avg_ms,
@@ -399,6 +406,114 @@ def run_poisson(args, local_rank):
                       "gpu_launches": st["kernel_launches"]}), flush=True)
 
 
+def run_serving(args, local_rank):
+    """Serving workload: a Poisson stream of parameter-sweep runs (cubic grids
+    of 24..128 cells, 8..64 ppc, Haser Q log-uniform in [1e25, 1e28] s^-1,
+    --run-steps iterations each) served two ways on one GPU.
+      plain:  one run after another through picard_gpu_run (the per-subroutine
+              call sequence of picard.f90), the arrival stream replayed against
+              the measured service times;
+      served: the picard_server request loop -- admission under the HBM
+              budget, --slots runs in flight on their own streams, requests
+              submitted at their arrival times.
+    Both arms create, initialise, run and release every run inside the timed
+    region.  Throughput = particle-steps of all runs / (last finish - first
+    arrival); latency = finish - arrival."""
+    import numpy as np
+    import torch
+
+    from picard_b200 import capi
+    from picard_b200 import params as P
+    from picard_b200.server import Server
+    from picard_b200.simulation import Simulation
+
+    torch.cuda.set_device(local_rank)
+    stream = P.serving_stream(seed=0, count=args.requests, rate_per_s=args.rate)
+    reqs = []
+    for t, p, steps in stream:
+        if args.run_steps != steps:
+            p = P._size_capacity(p, args.run_steps, max(1, int(p.ppc[1])))
+        reqs.append((t, capi.params_derive(p), args.run_steps))
+    layout, solver = capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE
+
+    # warm-up: load the kernels, tune nothing that the timed arms reuse
+    w = P.config_plain_scale(seed=99, nx=16, ny=16, nz=16, ppc_ion=2)
+    sim = Simulation(w, layout=layout, solver=solver)
+    sim.calc_distance()
+    sim.particles_initialize()
+    sim.run_fused(0, 2)
+    sim.close()
+    torch.cuda.synchronize()
+
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = ClockSampler(int(visible.split(",")[local_rank]) if visible else local_rank)
+    clocks.start()
+    plain = []
+    for t, p, steps in reqs:
+        a = time.perf_counter()
+        sim = Simulation(p, derive=False, layout=layout, solver=solver)
+        sim.calc_distance()
+        sim.particles_initialize()
+        sweeps = sim.run(0, steps)
+        st = sim.stats()
+        U = sim.field(capi.FIELD_U)
+        sim.close()
+        plain.append({"service_s": time.perf_counter() - a, "particle_steps": st["particle_steps"],
+                      "sweeps": sweeps, "u_sum": float(U.sum())})
+    clock = reqs[0][0]
+    plain_lat = []
+    for (t, _, _), r in zip(reqs, plain):
+        start = max(clock, t)
+        clock = start + r["service_s"]
+        plain_lat.append(clock - t)
+    plain_makespan = clock - reqs[0][0]
+
+    with Server(int(args.budget_gb * 1e9), args.slots) as srv:
+        base = srv.now_ms()
+        for i, (t, p, steps) in enumerate(reqs):
+            wait = base + t * 1e3 - srv.now_ms()
+            if wait > 0:
+                time.sleep(wait * 1e-3)
+            srv.submit(i, p, steps, layout=layout, solver=solver, arrival_ms=base + t * 1e3)
+        res = sorted(srv.poll(wait_all=True), key=lambda r: r["id"])
+    clk = clocks.stop()
+    bad = [r for r in res if r["status"] != capi.OK]
+    served_lat = [(r["finish_ms"] - r["arrival_ms"]) * 1e-3 for r in res]
+    served_makespan = (max(r["finish_ms"] for r in res) - (base + reqs[0][0] * 1e3)) * 1e-3
+    ps_served = sum(r["particle_steps"] for r in res)
+    ps_plain = sum(r["particle_steps"] for r in plain)
+    u_diff = max(abs(r["u_sum"] - q["u_sum"]) / max(abs(q["u_sum"]), 1e-300) for r, q in zip(res, plain))
+
+    def pct(v, q):
+        return float(np.percentile(np.asarray(v), q))
+
+    served_tput = ps_served / served_makespan
+    plain_tput = ps_plain / plain_makespan
+    line = {
+        "metric": "particle-steps/s & run p50/p99 latency, served vs plain", "value": served_tput,
+        "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "impl": "picard",
+        "workload": "serving", "vs_baseline": None,
+        "dtype": "f32 particles, f32 Jacobi sweeps with f64 anchors",
+        "data": "synthetic (seeded Philox plasma, run seeds 0..requests-1)",
+        "config": {"workload": f"serving stream: {len(reqs)} runs, Poisson arrivals {args.rate}/s, cubic grids "
+                               f"24..128 cells, 8..64 ppc, Haser Q log-uniform [1e25, 1e28] s^-1, "
+                               f"{args.run_steps} steps each",
+                   "grids": [int(p.nx) for _, p, _ in reqs], "budget_gb": args.budget_gb, "slots": args.slots},
+        "served": {"particle_steps_per_s": served_tput, "makespan_s": served_makespan,
+                   "p50_latency_s": pct(served_lat, 50), "p99_latency_s": pct(served_lat, 99),
+                   "failed": len(bad)},
+        "plain": {"particle_steps_per_s": plain_tput, "makespan_s": plain_makespan,
+                  "p50_latency_s": pct(plain_lat, 50), "p99_latency_s": pct(plain_lat, 99),
+                  "busy_s": sum(r["service_s"] for r in plain)},
+        "served_over_plain": served_tput / plain_tput,
+        "offered_load": {"arrivals_per_s": args.rate,
+                         "plain_service_rate_per_s": len(reqs) / sum(r["service_s"] for r in plain)},
+        "u_sum_max_rel_diff_served_vs_plain": u_diff,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -427,6 +542,10 @@ def main():
         return
     if args.workload == "poisson":
         run_poisson(args, local_rank)
+        return
+    if args.workload == "serving":
+        if rank == 0:
+            run_serving(args, local_rank)
         return
     if world > 1:
         import torch

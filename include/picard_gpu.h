@@ -242,8 +242,17 @@ typedef enum picard_option {
   /* 1: BCpotentials on the tensor cores (three-way BF16 split, FP32
    * accumulation folded into FP64 every 512 K-values; the default of the
    * CELL32 layout).  0: FP64 direct sum (the default of the F64 layout). */
-  PICARD_OPT_BCPOT_TENSOR = 0
+  PICARD_OPT_BCPOT_TENSOR = 0,
+  /* Launch shape of the TMA Jacobi sweep (open boundaries with the F32_REFINE
+   * solver).  It never changes a result bit.  SWEEP_CTAS: > 0 persistent grid
+   * of that many CTAs, -1 one CTA per tile, 0 re-run the launch tuner (which
+   * picks both knobs at context creation).  SWEEP_PDL: 1 programmatic
+   * dependent launch between consecutive sweeps, 0 plain stream order. */
+  PICARD_OPT_SWEEP_CTAS = 1,
+  PICARD_OPT_SWEEP_PDL = 2
 } picard_option;
+/* Reads an option's current value (SWEEP_CTAS: 0 means one CTA per tile). */
+PICARD_API int picard_gpu_get_option(picard_ctx* ctx, int32_t option, int32_t* value);
 PICARD_API int picard_gpu_set_option(picard_ctx* ctx, int32_t option, int32_t value);
 
 /* ----------------------------------------------------------- main loop */

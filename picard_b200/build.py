@@ -28,6 +28,7 @@ UNITS = {
     "solver.cu": [],
     "context.cu": [],
     "driver.cu": [],
+    "server.cu": [],
 }
 
 
@@ -42,7 +43,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     headers = [os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith(".cuh")]
-    headers.append(os.path.join(ROOT, "include", "picard_gpu.h"))
+    headers += [os.path.join(ROOT, "include", h) for h in ("picard_gpu.h", "picard_server.h")]
     objs = []
     for unit, extra in UNITS.items():
         src = os.path.join(SRC, unit)
@@ -55,7 +56,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
     if force or not _newer(LIB, objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lpthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

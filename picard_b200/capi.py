@@ -30,6 +30,8 @@ SOLVER_F32_REFINE = 1
 
 FIELD_U, FIELD_E, FIELD_N, FIELD_C, FIELD_F, FIELD_D = range(6)
 OPT_BCPOT_TENSOR = 0
+OPT_SWEEP_CTAS = 1
+OPT_SWEEP_PDL = 2
 
 class PicardStats(C.Structure):
     _fields_ = [
@@ -54,6 +56,40 @@ class PicardStats(C.Structure):
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "phase_ms"}
         d["phase_ms"] = {n: self.phase_ms[i] for i, n in enumerate(self.PHASES)}
+        return d
+
+
+class PicardRequest(C.Structure):
+    """include/picard_server.h picard_request."""
+    _fields_ = [
+        ("id", C.c_int64),
+        ("params", PicardParams),
+        ("layout", C.c_int32),
+        ("solver", C.c_int32),
+        ("steps", C.c_int32),
+        ("arrival_ms", C.c_double),
+    ]
+
+
+class PicardResult(C.Structure):
+    """include/picard_server.h picard_result."""
+    _fields_ = [
+        ("id", C.c_int64),
+        ("status", C.c_int32),
+        ("num_local", C.c_int32),
+        ("arrival_ms", C.c_double),
+        ("start_ms", C.c_double),
+        ("finish_ms", C.c_double),
+        ("sweeps", C.c_int64),
+        ("particle_steps", C.c_int64),
+        ("energy", C.c_double * 3),
+        ("u_sum", C.c_double),
+        ("u_abs_sum", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "energy"}
+        d["energy"] = tuple(self.energy)
         return d
 
 
@@ -116,6 +152,13 @@ def lib():
         "picard_gpu_reset_stats": [ctx],
         "picard_gpu_get_stream": [ctx, C.POINTER(C.c_void_p)],
         "picard_gpu_set_option": [ctx, C.c_int32, C.c_int32],
+        "picard_gpu_get_option": [ctx, C.c_int32, ip],
+        "picard_server_create": [C.c_uint64, C.c_int32, C.POINTER(C.c_void_p)],
+        "picard_server_submit": [C.c_void_p, C.POINTER(PicardRequest)],
+        "picard_server_now_ms": [C.c_void_p, dp],
+        "picard_server_poll": [C.c_void_p, C.POINTER(PicardResult), C.c_int32, ip, C.c_int32],
+        "picard_server_load": [C.c_void_p, ip, ip, C.POINTER(C.c_uint64)],
+        "picard_server_destroy": [C.c_void_p],
         "picard_gpu_particles_gridify_noalloc": [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                                  C.c_void_p, C.c_void_p, C.c_void_p],
     }

@@ -145,9 +145,11 @@ template <class T>
 int dalloc(picard_ctx* c, T*& p, size_t n) {
   void* q = nullptr;
   size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
-  cudaError_t e = cudaMalloc(&q, bytes);
+  // stream-ordered: creating or destroying a context does not synchronise
+  // the device, so contexts of concurrent runs come and go independently
+  cudaError_t e = cudaMallocAsync(&q, bytes, c->st);
   if (e != cudaSuccess)
-    return fail(PICARD_ERR_CUDA, "cudaMalloc(" + std::to_string(bytes) + " B): " + cudaGetErrorString(e));
+    return fail(PICARD_ERR_CUDA, "cudaMallocAsync(" + std::to_string(bytes) + " B): " + cudaGetErrorString(e));
   c->allocs.push_back(q);
   e = cudaMemsetAsync(q, 0, bytes, c->st);
   if (e != cudaSuccess) return check_cuda(e, "cudaMemsetAsync");
@@ -263,6 +265,11 @@ int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver,
   b += 8.0 * (double)s.cells;                // produce counts + offsets
   b += 8.0 * (double)s.nb_compact * 3;       // compaction scratch
   b += 8.0 * 1025.0 * s.nb_jacobi;           // sweep partials
+  if (layout == PICARD_LAYOUT_CELL32) {      // tensor-core BCpotentials scratch
+    long long cs = 0, pe = 0;
+    bcpot_tc_scratch(make_kparams(*p), &cs, &pe);
+    b += 2.0 * (double)cs + 8.0 * (double)pe;
+  }
   *bytes = (uint64_t)b;
   return PICARD_OK;
 }
@@ -344,6 +351,7 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
     if ((rc = check_cuda(cudaEventCreate(&c->ev[e]), "cudaEventCreate"))) return bail(rc);
   for (int e = 0; e < 6; ++e)
     if ((rc = check_cuda(cudaEventCreate(&c->pev[e]), "cudaEventCreate"))) return bail(rc);
+  if ((rc = tune_sweep(c, false))) return bail(rc);
   if ((rc = check_cuda(cudaStreamSynchronize(c->st), "create"))) return bail(rc);
   c->launches_at_reset = launches_so_far();
   *out = c;
@@ -352,8 +360,10 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
 
 int picard_gpu_destroy(picard_ctx* c) {
   if (!c) return PICARD_OK;
-  if (c->st) cudaStreamSynchronize(c->st);
-  for (void* q : c->allocs) cudaFree(q);
+  if (c->st) {
+    for (void* q : c->allocs) cudaFreeAsync(q, c->st);
+    cudaStreamSynchronize(c->st);
+  }
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   if (c->h_pinned_i) cudaFreeHost(c->h_pinned_i);
   for (int e = 0; e < 4; ++e)
@@ -416,8 +426,8 @@ int picard_gpu_set_particles(picard_ctx* c, const double* rp, const int32_t* ip,
   } else {
     double* buf = nullptr;
     int8_t* sb = nullptr;
-    PICARD_CUDA(cudaMalloc(&buf, sizeof(double) * 6 * std::max<int32_t>(n, 1)));
-    PICARD_CUDA(cudaMalloc(&sb, std::max<int32_t>(n, 1)));
+    PICARD_CUDA(cudaMallocAsync(&buf, sizeof(double) * 6 * std::max<int32_t>(n, 1), c->st));
+    PICARD_CUDA(cudaMallocAsync(&sb, std::max<int32_t>(n, 1), c->st));
     tmp = {buf, sb};
     dst.x = buf;
     dst.y = buf + n;
@@ -432,8 +442,8 @@ int picard_gpu_set_particles(picard_ctx* c, const double* rp, const int32_t* ip,
     PICARD_CUDA(cudaMemcpyAsync(cols[q], soa.data() + (size_t)q * n, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
   PICARD_CUDA(cudaMemcpyAsync(dst.sp, sp.data(), n, cudaMemcpyHostToDevice, c->st));
   if (c->layout == PICARD_LAYOUT_CELL32) PICARD_CUDA(launch_f64_to_c32(c->K, dst, n, c->c32[c->cur], c->st));
+  for (void* q : tmp) cudaFreeAsync(q, c->st);
   PICARD_CUDA(cudaStreamSynchronize(c->st));
-  for (void* q : tmp) cudaFree(q);
   c->stats.h2d_bytes += (int64_t)n * 49;
   c->num_local = n;
   return push_count(c);
@@ -452,8 +462,8 @@ int picard_gpu_get_particles(picard_ctx* c, double* rp, int32_t* ip, int32_t cap
   } else {
     double* buf = nullptr;
     int8_t* sb = nullptr;
-    PICARD_CUDA(cudaMalloc(&buf, sizeof(double) * 6 * std::max<long long>(n, 1)));
-    PICARD_CUDA(cudaMalloc(&sb, std::max<long long>(n, 1)));
+    PICARD_CUDA(cudaMallocAsync(&buf, sizeof(double) * 6 * std::max<long long>(n, 1), c->st));
+    PICARD_CUDA(cudaMallocAsync(&sb, std::max<long long>(n, 1), c->st));
     tmp = {buf, sb};
     src.x = buf;
     src.y = buf + n;
@@ -470,8 +480,8 @@ int picard_gpu_get_particles(picard_ctx* c, double* rp, int32_t* ip, int32_t cap
   for (int q = 0; q < 6; ++q)
     PICARD_CUDA(cudaMemcpyAsync(soa.data() + (size_t)q * n, cols[q], sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaMemcpyAsync(sp.data(), src.sp, n, cudaMemcpyDeviceToHost, c->st));
+  for (void* q : tmp) cudaFreeAsync(q, c->st);
   PICARD_CUDA(cudaStreamSynchronize(c->st));
-  for (void* q : tmp) cudaFree(q);
   c->stats.d2h_bytes += (int64_t)n * 49;
   for (long long p = 0; p < n; ++p) {
     if (rp) {
@@ -682,6 +692,29 @@ int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
   if (option == PICARD_OPT_BCPOT_TENSOR) {
     c->bcpot_tensor = value != 0;
     return PICARD_OK;
+  }
+  if (option == PICARD_OPT_SWEEP_CTAS) {
+    if (value < -1) return fail(PICARD_ERR_BAD_ARG, "SWEEP_CTAS must be -1, 0 or a CTA count");
+    if (value == 0) {
+      c->G.ctas = -1;  // forget the cached shape of this context
+      return tune_sweep(c, true);
+    }
+    c->G.ctas = value < 0 ? 0 : value;
+    return PICARD_OK;
+  }
+  if (option == PICARD_OPT_SWEEP_PDL) {
+    c->G.pdl = value != 0;
+    return PICARD_OK;
+  }
+  return fail(PICARD_ERR_BAD_ARG, "unknown option");
+}
+
+int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
+  if (!c || !value) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  switch (option) {
+    case PICARD_OPT_BCPOT_TENSOR: *value = c->bcpot_tensor; return PICARD_OK;
+    case PICARD_OPT_SWEEP_CTAS: *value = c->G.ctas; return PICARD_OK;
+    case PICARD_OPT_SWEEP_PDL: *value = c->G.pdl; return PICARD_OK;
   }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");
 }

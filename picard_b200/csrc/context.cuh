@@ -90,6 +90,9 @@ picard::InflowTable make_inflow_table(const picard_params& p);
 // Reads the device particle count into ctx->num_local after surfacing any
 // device-side capacity error.
 int sync_count_public(picard_ctx* c);
+// Times the launch shapes of the TMA sweep on this context's buffers and keeps
+// the fastest (cached per grid and device unless `fresh`).
+int tune_sweep(picard_ctx* c, bool fresh);
 }  // namespace picard
 
 #define PICARD_CUDA(expr)                                          \

@@ -20,6 +20,7 @@
 // r and its FP64 norm (the exact stopping test of the anchor iterate).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -374,15 +375,30 @@ __global__ void finalize_kernel(Stencil S, const double* V, const float* w, doub
 
 // ------------------------------------------------- TMA-staged FP32 sweep
 
-// One block owns a 32 x 8 x ZC column of interior nodes.  Its single elected
-// thread issues two TMA tile loads into shared memory -- the increment w with
-// a one-node halo (box 40 x 10 x (ZC+2) from the 16-byte aligned column
-// 32 bx) and the scaled residual r (box 40 x 8 x ZC) -- completing on one
-// mbarrier.  The block then sweeps its column plane by plane from shared
-// memory and writes w' with coalesced stores.  Open axes only: the ghost
-// layer of w is zero, which the box supplies (and TMA zero-fills outside the
-// array).  Waits are bounded: on timeout the block records kDevTimeout in
-// *err, waits (bounded) for its copies to land and returns.
+// The interior is cut into 32 x 8 x ZC columns of nodes ("tiles", x fastest).
+// A CTA walks the tiles t = blockIdx.x, + gridDim.x, ... through a two-stage
+// shared-memory pipeline: while it sweeps tile t from one stage, the TMA
+// engine fills the other stage with tile t + gridDim.x.  Per tile one elected
+// thread issues two TMA tile loads completing on the stage's mbarrier -- the
+// increment w with a one-node halo (box 40 x 10 x (ZC+2) from the 16-byte
+// aligned column 32 bx) and the scaled residual r (box 40 x 8 x ZC) -- and
+// the block then sweeps the column plane by plane from shared memory and
+// writes w' with coalesced stores.  Open axes only: the ghost layer of w is
+// zero, which the box supplies (and TMA zero-fills outside the array).
+//
+// The grid size is a tuning knob (a multiple of the SM count, or one CTA per
+// tile): each node's update and each tile's partial sum of squared residuals
+// are computed the same way whatever the grid, so results do not depend on it.
+//
+// Launched with programmatic dependent launch: the CTAs of sweep s+1 are
+// scheduled while sweep s drains and block in griddepcontrol.wait -- which
+// returns once sweep s has completed and its stores are visible -- before
+// their first load.
+//
+// Waits are bounded: when a stage's copies do not land within the limit the
+// block (deciding together, so that no thread is left at a barrier) records
+// kDevTimeout in *err, waits (bounded) for the copies it has in flight and
+// returns.
 constexpr int kTmaTx = 32, kTmaTy = 8, kTmaBoxX = 40;
 constexpr long long kMbarSpin = 1LL << 24;
 
@@ -402,76 +418,119 @@ __device__ inline bool mbar_wait(uint32_t mbar, uint32_t phase, long long limit)
 }
 
 template <int ZC>
+struct TmaStage {
+  static constexpr int kW = (ZC + 2) * (kTmaTy + 2) * kTmaBoxX;  // floats of the w box
+  static constexpr int kR = ZC * kTmaTy * kTmaBoxX;              // floats of the r box
+  static constexpr int kFloats = kW + kR;
+  static constexpr size_t kBytes = sizeof(float) * kFloats;
+  static_assert(kBytes % 128 == 0, "stage buffers stay 128-byte aligned");
+};
+
+template <int ZC>
+__device__ inline void tma_issue_tile(const CUtensorMap* tw, const CUtensorMap* tr, float* stage, uint32_t mb, int t,
+                                      int gx, int gy, int w_zero) {
+  const int bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
+  const int x0 = bx * kTmaTx, y0 = by * kTmaTy, z0 = bz * ZC;
+  float* sw = stage;
+  float* sr = stage + TmaStage<ZC>::kW;
+  uint32_t bytes = (uint32_t)(TmaStage<ZC>::kR * sizeof(float));
+  if (!w_zero) bytes += (uint32_t)(TmaStage<ZC>::kW * sizeof(float));
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+  if (!w_zero)
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"((uint32_t)__cvta_generic_to_shared(sw)), "l"((unsigned long long)tw), "r"(x0), "r"(y0), "r"(z0), "r"(mb)
+        : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)tr), "r"(x0), "r"(y0 + 1), "r"(z0 + 1),
+      "r"(mb)
+      : "memory");
+}
+
+template <int ZC>
 __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ CUtensorMap tw,
                                                         const __grid_constant__ CUtensorMap tr, Stencil S,
                                                         JacobiCoefF J, float* __restrict__ wout, double* partial,
-                                                        int w_zero, int* err) {
+                                                        int w_zero, int gx, int gy, int ntiles, int* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  float* sw = reinterpret_cast<float*>(smem_raw);                       // [ZC+2][10][40]
-  float* sr = sw + (ZC + 2) * (kTmaTy + 2) * kTmaBoxX;                  // [ZC][8][40]
-  __shared__ __align__(8) unsigned long long mbar;
+  float* stages = reinterpret_cast<float*>(smem_raw);  // [2][TmaStage<ZC>::kFloats]
+  __shared__ __align__(8) unsigned long long mbar[2];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + kTmaTx * ty;
-  const int x0 = blockIdx.x * kTmaTx, y0 = blockIdx.y * kTmaTy, z0 = blockIdx.z * ZC;
-  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  const uint32_t mb0 = (uint32_t)__cvta_generic_to_shared(&mbar[0]);
+  const uint32_t mb1 = (uint32_t)__cvta_generic_to_shared(&mbar[1]);
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((unsigned long long)&tw) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((unsigned long long)&tr) : "memory");
   }
   __syncthreads();
-  if (tid == 0) {
-    uint32_t bytes = (uint32_t)(ZC * kTmaTy * kTmaBoxX * sizeof(float));
-    if (!w_zero) bytes += (uint32_t)((ZC + 2) * (kTmaTy + 2) * kTmaBoxX * sizeof(float));
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
-    if (!w_zero)
-      asm volatile(
-          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-          ::"r"((uint32_t)__cvta_generic_to_shared(sw)), "l"((unsigned long long)&tw), "r"(x0), "r"(y0), "r"(z0),
-          "r"(mb)
-          : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-        ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)&tr), "r"(x0), "r"(y0 + 1),
-        "r"(z0 + 1), "r"(mb)
-        : "memory");
-  }
-  if (!mbar_wait(mb, 0, kMbarSpin)) {
-    if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
-    mbar_wait(mb, 0, kMbarSpin);  // let the copies land before the block exits
-    return;
-  }
-  const int i = x0 + tx + 1, j = y0 + ty + 1;
-  float r2 = 0.0f;
-  if (i <= S.nx && j <= S.ny) {
-    const int kend = min(ZC, S.nz - z0);
-    const long long plane = (long long)S.fpitch * S.nyp;
-    long long c = fidx(S, i, j, z0 + 1);
-    const int col = tx + 4;  // smem column of node i
-    if (w_zero) {
-      for (int kk = 1; kk <= kend; ++kk, c += plane) {
-        float res = sr[((kk - 1) * kTmaTy + ty) * kTmaBoxX + col];
-        r2 += res * res;
-        wout[c] = -J.af * res;
-      }
-    } else {
-      auto W = [&](int kk, int row, int cc) { return sw[(kk * (kTmaTy + 2) + row) * kTmaBoxX + cc]; };
-      float wm = W(0, ty + 1, col);
-      float wc = W(1, ty + 1, col);
-      for (int kk = 1; kk <= kend; ++kk, c += plane) {
-        float wp = W(kk + 1, ty + 1, col);
-        float sx = W(kk, ty + 1, col + 1) + W(kk, ty + 1, col - 1);
-        float sy = W(kk, ty + 2, col) + W(kk, ty, col);
-        float sz = wp + wm;
-        float lap = (sx - 2.0f * wc) * J.idx2 + (sy - 2.0f * wc) * J.idy2 + (sz - 2.0f * wc) * J.idz2;
-        float res = sr[((kk - 1) * kTmaTy + ty) * kTmaBoxX + col] - lap;
-        r2 += res * res;
-        wout[c] = wc - J.af * res;
-        wm = wc;
-        wc = wp;
+  // the previous sweep wrote the w this one reads: wait for it, then let the
+  // next sweep's CTAs be scheduled as this grid's CTAs retire
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  int t = blockIdx.x;
+  if (t >= ntiles) return;
+  if (tid == 0) tma_issue_tile<ZC>(&tw, &tr, stages, mb0, t, gx, gy, w_zero);
+  const long long plane = (long long)S.fpitch * S.nyp;
+  for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
+    const int st = it & 1;
+    const uint32_t phase = (uint32_t)((it >> 1) & 1);
+    const uint32_t mb = st ? mb1 : mb0;
+    const int tn = t + gridDim.x;
+    // the other stage was last read in iteration it-1, which ended at a barrier
+    if (tid == 0 && tn < ntiles)
+      tma_issue_tile<ZC>(&tw, &tr, stages + (st ^ 1) * TmaStage<ZC>::kFloats, st ? mb0 : mb1, tn, gx, gy, w_zero);
+    const bool ok = __syncthreads_and(mbar_wait(mb, phase, kMbarSpin) ? 1 : 0);
+    if (!ok) {
+      if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+      // let the copies in flight land before the block exits
+      mbar_wait(mb, phase, kMbarSpin);
+      if (tn < ntiles) mbar_wait(st ? mb0 : mb1, (uint32_t)(((it + 1) >> 1) & 1), kMbarSpin);
+      return;
+    }
+    const float* sw = stages + st * TmaStage<ZC>::kFloats;
+    const float* sr = sw + TmaStage<ZC>::kW;
+    const int bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
+    const int x0 = bx * kTmaTx, y0 = by * kTmaTy, z0 = bz * ZC;
+    const int i = x0 + tx + 1, j = y0 + ty + 1;
+    float r2 = 0.0f;
+    if (i <= S.nx && j <= S.ny) {
+      const int kend = min(ZC, S.nz - z0);
+      long long c = fidx(S, i, j, z0 + 1);
+      const int col = tx + 4;  // smem column of node i
+      if (w_zero) {
+        for (int kk = 1; kk <= kend; ++kk, c += plane) {
+          float res = sr[((kk - 1) * kTmaTy + ty) * kTmaBoxX + col];
+          r2 += res * res;
+          wout[c] = -J.af * res;
+        }
+      } else {
+        auto W = [&](int kk, int row, int cc) { return sw[(kk * (kTmaTy + 2) + row) * kTmaBoxX + cc]; };
+        float wm = W(0, ty + 1, col);
+        float wc = W(1, ty + 1, col);
+        for (int kk = 1; kk <= kend; ++kk, c += plane) {
+          float wp = W(kk + 1, ty + 1, col);
+          float sx = W(kk, ty + 1, col + 1) + W(kk, ty + 1, col - 1);
+          float sy = W(kk, ty + 2, col) + W(kk, ty, col);
+          float sz = wp + wm;
+          float lap = (sx - 2.0f * wc) * J.idx2 + (sy - 2.0f * wc) * J.idy2 + (sz - 2.0f * wc) * J.idz2;
+          float res = sr[((kk - 1) * kTmaTy + ty) * kTmaBoxX + col] - lap;
+          r2 += res * res;
+          wout[c] = wc - J.af * res;
+          wm = wc;
+          wc = wp;
+        }
       }
     }
+    block_sum_store((double)r2, partial + t);
+    // every thread is done with this stage (and thread 0 with the reduction
+    // scratch) before the stage is refilled in the next iteration
+    __syncthreads();
   }
-  block_sum_store((double)r2, partial + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
 }
 
 // Periodic ghost refresh of U (CalcEpotential.f90:100-239 on one rank), in
@@ -740,17 +799,48 @@ int make_tensor_map(CUtensorMap* m, float* base, const KParams& P, int box_y, in
 template <int ZC>
 static cudaError_t launch_tma_zc(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
                                  float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
-  const size_t smem = ((size_t)(ZC + 2) * (kTmaTy + 2) * kTmaBoxX + (size_t)ZC * kTmaTy * kTmaBoxX) * sizeof(float);
+  const size_t smem = 2 * TmaStage<ZC>::kBytes;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(sweep_tma_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
+  const int ntiles = G.nblocks;
+  const int ctas = G.ctas > 0 ? std::min(G.ctas, ntiles) : ntiles;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(kTmaTx, kTmaTy);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = G.pdl ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
   note_launch();
-  sweep_tma_kernel<ZC><<<G.grid, dim3(kTmaTx, kTmaTy), smem, st>>>(*tw, *tr, make_stencil(P), jacobi_coef_f(P), wout,
-                                                                     partial, w_zero, err);
-  return cudaGetLastError();
+  return cudaLaunchKernelEx(&cfg, sweep_tma_kernel<ZC>, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout, partial,
+                            w_zero, (int)G.grid.x, (int)G.grid.y, ntiles, err);
+}
+
+template <int ZC>
+static int occupancy_zc() {
+  const size_t smem = 2 * TmaStage<ZC>::kBytes;
+  if (cudaFuncSetAttribute(sweep_tma_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_tma_kernel<ZC>, kTmaTx * kTmaTy, smem) != cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+
+int sweep_tma_occupancy(const JacobiGeom& G) {
+  switch (G.zc) {
+    case 4: return occupancy_zc<4>();
+    case 8: return occupancy_zc<8>();
+    case 16: return occupancy_zc<16>();
+  }
+  return 1;
 }
 
 cudaError_t launch_sweep_tma(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,

@@ -22,7 +22,13 @@ struct JacobiGeom {
   int zc;
   int nblocks;
   int tma;  // all axes open: the TMA-staged sweep kernel is used (zc in {4, 8, 16})
+  // TMA sweep launch shape (results do not depend on it): CTAs of the
+  // persistent grid (0: one per tile) and programmatic dependent launch
+  int ctas = 0;
+  int pdl = 1;
 };
+// CTAs of one SM the TMA sweep kernel of this geometry can hold.
+int sweep_tma_occupancy(const JacobiGeom& G);
 
 // Row pitch (floats) of the padded FP32 solver arrays: node (i, j, k) at
 // column i + 3, rows a multiple of 8 floats (32 bytes).

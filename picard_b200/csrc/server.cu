@@ -1,0 +1,206 @@
+// server.cu -- the request loop of the serving workload: runs admitted by HBM
+// budget, state resident on the device for the whole run, concurrent runs
+// overlapping on the device, latencies reported per run.
+//
+// Each admitted request becomes a picard_ctx on its own CUDA stream, driven by
+// one worker thread: CalcDistance, ParticlesInitialize, `steps` iterations of
+// the fused loop, the energy diagnostics, release.  A request is admitted when
+// a worker is free and its device footprint (picard_gpu_footprint) fits in
+// what the budget has left; requests are admitted in arrival order, so a
+// large request waits for memory instead of being overtaken forever.  While a
+// run waits on its own stream for the host (the Jacobi stop test), the
+// kernels of the other runs keep the device busy -- that overlap is the
+// continuous batching of the loop.  Context memory comes from the
+// stream-ordered allocator, so admitting or retiring a run does not
+// synchronise the device.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "context.cuh"
+#include "picard_gpu.h"
+#include "picard_server.h"
+
+using namespace picard;
+
+struct picard_server {
+  uint64_t budget = 0;
+  uint64_t in_use = 0;
+  int device = 0;
+  int max_slots = 1;
+  int running = 0;
+  bool stopping = false;
+  std::deque<std::pair<picard_request, uint64_t>> queue;  // request, footprint
+  std::vector<picard_result> done;
+  std::mutex mu;
+  std::condition_variable cv_work;  // a worker may be able to start a request
+  std::condition_variable cv_done;  // a request finished
+  std::vector<std::thread> workers;
+  std::chrono::steady_clock::time_point t0;
+  int64_t submitted = 0, finished = 0;
+};
+
+namespace {
+
+double now_ms(const picard_server* s) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s->t0).count();
+}
+
+int run_request(const picard_request& rq, picard_result* out) {
+  picard_ctx* c = nullptr;
+  PICARD_TRY(picard_gpu_create(&rq.params, rq.layout, rq.solver, &c));
+  int rc = picard_gpu_calc_distance(c);
+  if (rc == PICARD_OK) rc = picard_gpu_particles_initialize(c);
+  int64_t sweeps = 0;
+  if (rc == PICARD_OK) {
+    rc = picard_gpu_run_fused(c, 0, rq.steps, &sweeps);
+    if (rc == PICARD_ERR_NOT_CONVERGED) rc = PICARD_OK;  // the reference carries on too
+  }
+  if (rc == PICARD_OK) rc = picard_gpu_energy(c, out->energy, &out->num_local);
+  picard_stats st;
+  if (rc == PICARD_OK) rc = picard_gpu_get_stats(c, &st);
+  if (rc == PICARD_OK) {
+    out->sweeps = sweeps;
+    out->particle_steps = st.particle_steps;
+    // checksum of the final potential (sum over all nodes, FP64)
+    const long long nn = c->K.nodes;
+    std::vector<double> h((size_t)nn);
+    rc = check_cuda(cudaMemcpyAsync(h.data(), c->U, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st), "U");
+    if (rc == PICARD_OK) rc = check_cuda(cudaStreamSynchronize(c->st), "sync");
+    double s = 0.0, a = 0.0;
+    for (long long g = 0; g < nn; ++g) s += h[(size_t)g], a += std::fabs(h[(size_t)g]);
+    out->u_sum = s;
+    out->u_abs_sum = a;
+  }
+  picard_gpu_destroy(c);
+  return rc;
+}
+
+void worker_main(picard_server* s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    std::pair<picard_request, uint64_t> job;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] {
+        if (s->stopping && s->queue.empty()) return true;
+        return !s->queue.empty() && s->queue.front().second <= s->budget - s->in_use;
+      });
+      if (s->queue.empty()) return;
+      job = s->queue.front();
+      s->queue.pop_front();
+      s->in_use += job.second;
+      s->running += 1;
+    }
+    s->cv_work.notify_all();
+    picard_result r;
+    std::memset(&r, 0, sizeof(r));
+    r.id = job.first.id;
+    r.start_ms = now_ms(s);
+    r.status = run_request(job.first, &r);
+    r.finish_ms = now_ms(s);
+    r.arrival_ms = job.first.arrival_ms;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->in_use -= job.second;
+      s->running -= 1;
+      s->finished += 1;
+      s->done.push_back(r);
+    }
+    s->cv_work.notify_all();
+    s->cv_done.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int picard_server_create(uint64_t hbm_budget_bytes, int32_t max_slots, picard_server** out) {
+  if (!out || max_slots < 1 || hbm_budget_bytes == 0) return fail(PICARD_ERR_BAD_ARG, "bad server arguments");
+  picard_server* s = new picard_server();
+  s->budget = hbm_budget_bytes;
+  s->max_slots = max_slots;
+  s->t0 = std::chrono::steady_clock::now();
+  if (cudaGetDevice(&s->device) != cudaSuccess) {
+    delete s;
+    return fail(PICARD_ERR_CUDA, "no CUDA device");
+  }
+  // keep freed context memory in the pool between runs
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+    uint64_t keep = hbm_budget_bytes;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  for (int i = 0; i < max_slots; ++i) s->workers.emplace_back(worker_main, s);
+  *out = s;
+  return PICARD_OK;
+}
+
+int picard_server_submit(picard_server* s, const picard_request* rq) {
+  if (!s || !rq) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  uint64_t fp = 0;
+  PICARD_TRY(picard_gpu_footprint(&rq->params, rq->layout, rq->solver, &fp));
+  if (fp > s->budget)
+    return fail(PICARD_ERR_CAPACITY, "request needs " + std::to_string(fp) + " B, more than the whole HBM budget");
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) return fail(PICARD_ERR_STATE, "server is shutting down");
+    picard_request copy = *rq;
+    if (copy.arrival_ms < 0) copy.arrival_ms = now_ms(s);
+    s->queue.emplace_back(copy, fp);
+    s->submitted += 1;
+  }
+  s->cv_work.notify_all();
+  return PICARD_OK;
+}
+
+int picard_server_now_ms(picard_server* s, double* ms) {
+  if (!s || !ms) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  *ms = now_ms(s);
+  return PICARD_OK;
+}
+
+int picard_server_poll(picard_server* s, picard_result* out, int32_t max, int32_t* n, int32_t wait_all) {
+  if (!s || !n) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (wait_all) s->cv_done.wait(lk, [&] { return s->finished == s->submitted; });
+  int32_t k = 0;
+  while (k < max && !s->done.empty()) {
+    out[k++] = s->done.front();
+    s->done.erase(s->done.begin());
+  }
+  *n = k;
+  return PICARD_OK;
+}
+
+int picard_server_load(picard_server* s, int32_t* running, int32_t* queued, uint64_t* bytes_in_use) {
+  if (!s) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (running) *running = s->running;
+  if (queued) *queued = int32_t(s->queue.size());
+  if (bytes_in_use) *bytes_in_use = s->in_use;
+  return PICARD_OK;
+}
+
+int picard_server_destroy(picard_server* s) {
+  if (!s) return PICARD_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+  }
+  s->cv_work.notify_all();
+  for (auto& t : s->workers) t.join();
+  delete s;
+  return PICARD_OK;
+}
+
+}  // extern "C"

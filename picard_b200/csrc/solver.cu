@@ -12,7 +12,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
+#include <vector>
 
 #include "context.cuh"
 #include "picard_gpu.h"
@@ -256,3 +260,73 @@ extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t 
                 "Jacobi reached 2*maxit+1 = " + std::to_string(smax) + " sweeps without meeting maxerr");
   return PICARD_OK;
 }
+
+// ------------------------------------------------------- sweep launch tuner
+//
+// Picks the launch shape of the TMA sweep -- the persistent grid size (k CTAs
+// per SM for k up to the kernel's occupancy, or one CTA per tile) and whether
+// programmatic dependent launch is used -- by timing a short run of sweeps of
+// each candidate on this context's own buffers.  The shape does not change a
+// single bit of the results, so the choice is free to differ from process to
+// process.  Choices are cached per (grid, tile depth, device) for the life of
+// the process.
+namespace picard {
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_tuned;
+}  // namespace
+
+int tune_sweep(picard_ctx* c, bool fresh) {
+  if (!c->G.tma || !c->w[0]) return PICARD_OK;
+  const auto key = std::make_tuple(c->K.nx, c->K.ny, c->K.nz, c->G.zc, c->device);
+  if (!fresh) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      c->G.ctas = it->second.first;
+      c->G.pdl = it->second.second;
+      return PICARD_OK;
+    }
+  }
+  int sms = 148;
+  PICARD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  const int occ = sweep_tma_occupancy(c->G);
+  std::vector<std::pair<int, int>> cand;
+  for (int pdl = 1; pdl >= 0; --pdl) {
+    for (int k = 1; k <= occ; ++k)
+      if ((long long)k * sms < c->G.nblocks) cand.emplace_back(k * sms, pdl);
+    cand.emplace_back(0, pdl);
+  }
+  constexpr int kReps = 24;
+  std::vector<float> best(cand.size(), 1e30f);
+  for (int round = 0; round < 2; ++round) {
+    for (size_t q = 0; q < cand.size(); ++q) {
+      c->G.ctas = cand[q].first;
+      c->G.pdl = cand[q].second;
+      for (int s = 1; s <= 2; ++s)
+        PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
+                                     c->d_err, c->st));
+      PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
+      for (int s = 1; s <= kReps; ++s)
+        PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
+                                     c->d_err, c->st));
+      PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
+      PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
+      float ms = 0.0f;
+      PICARD_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+      best[q] = std::min(best[q], ms);
+    }
+  }
+  PICARD_TRY(check_timeout(c));
+  size_t pick = 0;
+  for (size_t q = 1; q < cand.size(); ++q)
+    if (best[q] < best[pick]) pick = q;
+  c->G.ctas = cand[pick].first;
+  c->G.pdl = cand[pick].second;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[key] = cand[pick];
+  return PICARD_OK;
+}
+
+}  // namespace picard

@@ -168,3 +168,106 @@ def config_plain_scale(seed: int = 0, nx: int = 256, ny: int = 128, nz: int = 12
     face = 2 * ((ny + 2) * (nz + 2) + (nx + 2) * (nz + 2) + (nx + 2) * (ny + 2))
     p.max_per_proc = capacity if capacity is not None else int(cells * ppc_ion * 2 * 1.05 + face * ppc_ion * 2 + 1_000_000)
     return p
+
+
+def expected_produced(p: PicardParams, steps: int) -> float:
+    """Expected number of particles ParticlesProduce adds in ``steps``
+    iterations (ions plus their co-produced electrons and protons), from the
+    Haser density at each cell (ParticlesProduce.f90:40-70); ``p`` must be
+    derived.  Used to size max_per_proc for runs with a neutral source."""
+    import numpy as np
+
+    dx, dy, dz = p.dxyz[0], p.dxyz[1], p.dxyz[2]
+    dV = dx * dy * dz
+    x0 = p.Lx_min + dx * np.arange(p.nx)
+    y0 = p.Ly_min + dy * np.arange(p.ny)
+    z0 = p.Lz_min + dz * np.arange(p.nz)
+    X, Y, Z = np.meshgrid(x0, y0, z0, indexing="ij")
+    r1 = np.sqrt((X + 0.5 * dx) ** 2 + (Y + 0.5 * dy) ** 2 + (Z + 0.5 * dz) ** 2)
+    near = (4.0 * r1) ** 3 < dV
+    if near.any():
+        s = np.zeros(int(near.sum()))
+        for fx in (0.25, 0.75):
+            for fy in (0.25, 0.75):
+                for fz in (0.25, 0.75):
+                    s += np.sqrt((X[near] + fx * dx) ** 2 + (Y[near] + fy * dy) ** 2 + (Z[near] + fz * dz) ** 2)
+        r1[near] = s / 8.0
+    total = 0.0
+    for s in range(p.species):
+        if p.vn[s] <= 0.0 or p.n2p[s] <= 0.0:
+            continue
+        nden = p.Qn[s] / (2.0 * TAU * r1 * r1 * p.vn[s]) * np.exp(-p.nu_d[s] * r1 / p.vn[s])
+        rate = p.nu_i[s] * nden * dV / p.n2p[s]
+        if p.produce_dt_scaled:
+            rate = rate * p.dt
+        total += float(rate.sum()) * (1 + p.epp[s] + p.hpp[s])
+    return total * steps
+
+
+def _size_capacity(p: PicardParams, steps: int, ppc_ion: int) -> PicardParams:
+    """max_per_proc for a run of ``steps`` iterations: the initial plasma with
+    5% spare, a face of inflow, and the expected Haser production with 20%
+    spare."""
+    from .capi import params_derive
+
+    q = params_derive(p)
+    cells = p.nx * p.ny * p.nz
+    face = 2 * ((p.ny + 2) * (p.nz + 2) + (p.nx + 2) * (p.nz + 2) + (p.nx + 2) * (p.ny + 2))
+    p.max_per_proc = int(cells * ppc_ion * 2 * 1.05 + face * ppc_ion * 2 + 1.2 * expected_produced(q, steps) + 65536)
+    return p
+
+
+def config_batch_run(rng, seed: int) -> tuple[PicardParams, int]:
+    """One run of the batched parameter sweep: a cubic grid of edge drawn from
+    16..96 cells (1 km cells), 8..32 macro-particles per cell in total (half
+    H+, half electrons), drift drawn from 300..800 km/s along +x, |B| drawn from
+    1..10 nT in an isotropic random direction, the 32^3 workload's plasma
+    otherwise, no neutral source, 100 steps.  ``rng`` is a numpy Generator."""
+    n = int(rng.integers(16, 97))
+    ppc_ion = max(1, int(rng.integers(8, 33)) // 2)
+    p = config_plain_32(seed=seed, n=n, ppc=ppc_ion)
+    v = float(rng.uniform(300e3, 800e3))
+    for s in range(8):
+        p.v0[s][0] = v
+    bmag = float(rng.uniform(1e-9, 10e-9))
+    u = rng.normal(size=3)
+    u = u / math.sqrt(float((u * u).sum()))
+    p.B0[0], p.B0[1], p.B0[2] = (bmag * float(c) for c in u)
+    steps = 100
+    return _size_capacity(p, steps, ppc_ion), steps
+
+
+def config_serving_run(rng, seed: int) -> tuple[PicardParams, int]:
+    """One request of the serving stream: the at-scale plasma with a Haser
+    source on a cubic grid of edge drawn from 24..128 cells, 8..64
+    macro-particles per cell in total, Q log-uniform in [1e25, 1e28] s^-1,
+    200 steps."""
+    n = int(rng.integers(24, 129))
+    ppc_ion = max(1, int(rng.integers(8, 65)) // 2)
+    p = config_plain_scale(seed=seed, nx=n, ny=n, nz=n, ppc_ion=ppc_ion)
+    p.Qn[2] = float(10.0 ** rng.uniform(25.0, 28.0))
+    steps = 200
+    return _size_capacity(p, steps, ppc_ion), steps
+
+
+def serving_stream(seed: int, count: int, rate_per_s: float = 20.0):
+    """``count`` requests with Poisson arrivals at ``rate_per_s``: a list of
+    (arrival seconds, params, steps), run seeds seed*1000 + i."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += float(rng.exponential(1.0 / rate_per_s))
+        p, steps = config_serving_run(rng, seed * 1000 + i)
+        out.append((t, p, steps))
+    return out
+
+
+def batch_set(seed: int, count: int = 64):
+    """The batched sweep's ``count`` runs: a list of (params, steps)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    return [config_batch_run(rng, seed * 1000 + i) for i in range(count)]

@@ -54,6 +54,11 @@ class Simulation:
     def set_option(self, option: int, value: int) -> None:
         self._call("picard_gpu_set_option", option, value)
 
+    def get_option(self, option: int) -> int:
+        v = C.c_int32(0)
+        self._call("picard_gpu_get_option", option, C.byref(v))
+        return int(v.value)
+
     def synchronize(self) -> None:
         self._call("picard_gpu_synchronize")
 

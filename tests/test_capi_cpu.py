@@ -1,9 +1,10 @@
 """The C-ABI library without a GPU: it loads, exports every entry point that
-include/picard_gpu.h declares, and its host-only routines (parameter defaults
+include/*.h declares, and its host-only routines (parameter defaults
 and derivation, footprint) agree with the reference and the oracle."""
 import ctypes as C
 import os
 import re
+import subprocess
 
 import numpy as np
 import pytest
@@ -16,7 +17,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "picard_gpu.h")).read()
+    inc = os.path.join(ROOT, "include")
+    text = "".join(open(os.path.join(inc, h)).read() for h in sorted(os.listdir(inc)) if h.endswith(".h"))
     return sorted(set(re.findall(r"PICARD_API\s+[\w\s\*]+?\b(picard_\w+)\s*\(", text)))
 
 
@@ -69,7 +71,12 @@ def test_footprint_scales_with_capacity():
     p2.max_per_proc = p.max_per_proc * 2
     big = capi.footprint(p2, capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE)
     assert big - small == pytest.approx(2 * 29 * p.max_per_proc, rel=0.01)
-    assert capi.footprint(p, capi.LAYOUT_F64, capi.SOLVER_F64) > small
+    # where particles dominate, the FP64 layout (49 B/particle) holds more
+    # than CELL32 (29 B/particle) even with CELL32's tensor-core scratch
+    p3 = p.copy()
+    p3.max_per_proc = 10_000_000
+    assert capi.footprint(p3, capi.LAYOUT_F64, capi.SOLVER_F64) > capi.footprint(
+        p3, capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE)
 
 
 def test_bad_arguments_are_rejected_without_a_device():
@@ -84,3 +91,52 @@ def test_bad_arguments_are_rejected_without_a_device():
     underived = P.config_plain_32(n=8, ppc=2)
     rc = capi.lib().picard_gpu_create(C.byref(underived), capi.LAYOUT_F64, capi.SOLVER_F64, C.byref(h))
     assert rc == capi.ERR_BAD_ARG and "derive" in capi.last_error()
+
+
+_LAYOUT_PROBE = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "picard_server.h"
+#define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m))
+int main(void) {
+  printf("picard_params %zu\n", sizeof(picard_params));
+  printf("picard_stats %zu\n", sizeof(picard_stats));
+  printf("picard_request %zu\n", sizeof(picard_request));
+  printf("picard_result %zu\n", sizeof(picard_result));
+  F(picard_request, params); F(picard_request, layout); F(picard_request, steps); F(picard_request, arrival_ms);
+  F(picard_result, status); F(picard_result, sweeps); F(picard_result, energy); F(picard_result, u_abs_sum);
+  F(picard_stats, phase_ms); F(picard_params, u0);
+  return 0;
+}
+"""
+
+
+def test_ctypes_structs_match_the_c_compiler(tmp_path):
+    """Every struct that crosses the C ABI has the size and field offsets gcc
+    gives it from the headers."""
+    src = tmp_path / "probe.c"
+    src.write_text(_LAYOUT_PROBE)
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                        check=True).stdout.splitlines())
+    assert int(got["picard_params"]) == C.sizeof(P.PicardParams)
+    assert int(got["picard_stats"]) == C.sizeof(capi.PicardStats)
+    assert int(got["picard_request"]) == C.sizeof(capi.PicardRequest)
+    assert int(got["picard_result"]) == C.sizeof(capi.PicardResult)
+    for key, val in got.items():
+        if "." not in key:
+            continue
+        sname, field = key.split(".")
+        cls = {"picard_request": capi.PicardRequest, "picard_result": capi.PicardResult,
+               "picard_stats": capi.PicardStats, "picard_params": P.PicardParams}[sname]
+        assert getattr(cls, field).offset == int(val), key
+
+
+def test_server_rejects_bad_arguments_without_a_device():
+    L = capi.lib()
+    out = C.c_void_p()
+    assert L.picard_server_create(0, 2, C.byref(out)) == capi.ERR_BAD_ARG
+    assert L.picard_server_create(1 << 30, 0, C.byref(out)) == capi.ERR_BAD_ARG
+    assert L.picard_server_submit(None, None) == capi.ERR_BAD_ARG
+    assert L.picard_server_destroy(None) == capi.OK
