@@ -247,9 +247,12 @@ typedef enum picard_option {
    * solver).  It never changes a result bit.  SWEEP_CTAS: > 0 persistent grid
    * of that many CTAs, -1 one CTA per tile, 0 re-run the launch tuner (which
    * picks both knobs at context creation).  SWEEP_PDL: 1 programmatic
-   * dependent launch between consecutive sweeps, 0 plain stream order. */
+   * dependent launch between consecutive sweeps, 0 plain stream order.
+   * SWEEP_STAGES: shared-memory stages per CTA, 1 or 2 (2 prefetches the
+   * CTA's next tile). */
   PICARD_OPT_SWEEP_CTAS = 1,
-  PICARD_OPT_SWEEP_PDL = 2
+  PICARD_OPT_SWEEP_PDL = 2,
+  PICARD_OPT_SWEEP_STAGES = 3
 } picard_option;
 /* Reads an option's current value (SWEEP_CTAS: 0 means one CTA per tile). */
 PICARD_API int picard_gpu_get_option(picard_ctx* ctx, int32_t option, int32_t* value);

@@ -32,6 +32,7 @@ FIELD_U, FIELD_E, FIELD_N, FIELD_C, FIELD_F, FIELD_D = range(6)
 OPT_BCPOT_TENSOR = 0
 OPT_SWEEP_CTAS = 1
 OPT_SWEEP_PDL = 2
+OPT_SWEEP_STAGES = 3
 
 class PicardStats(C.Structure):
     _fields_ = [

@@ -381,14 +381,17 @@ __global__ void finalize_kernel(Stencil S, const double* V, const float* w, doub
 // engine fills the other stage with tile t + gridDim.x.  Per tile one elected
 // thread issues two TMA tile loads completing on the stage's mbarrier -- the
 // increment w with a one-node halo (box 40 x 10 x (ZC+2) from the 16-byte
-// aligned column 32 bx) and the scaled residual r (box 40 x 8 x ZC) -- and
+// aligned column 32 bx) and the scaled residual r (box 32 x 8 x ZC from the
+// tile's first interior column, 32 bx + 4, also 16-byte aligned) -- and
 // the block then sweeps the column plane by plane from shared memory and
 // writes w' with coalesced stores.  Open axes only: the ghost layer of w is
 // zero, which the box supplies (and TMA zero-fills outside the array).
 //
-// The grid size is a tuning knob (a multiple of the SM count, or one CTA per
-// tile): each node's update and each tile's partial sum of squared residuals
-// are computed the same way whatever the grid, so results do not depend on it.
+// The grid size (a multiple of the SM count, or one CTA per tile) and the
+// number of stages (1: the next tile is loaded after the current one is
+// consumed) are tuning knobs: each node's update and each tile's partial sum
+// of squared residuals are computed the same way whatever they are, so results
+// do not depend on them.
 //
 // Launched with programmatic dependent launch: the CTAs of sweep s+1 are
 // scheduled while sweep s drains and block in griddepcontrol.wait -- which
@@ -420,7 +423,7 @@ __device__ inline bool mbar_wait(uint32_t mbar, uint32_t phase, long long limit)
 template <int ZC>
 struct TmaStage {
   static constexpr int kW = (ZC + 2) * (kTmaTy + 2) * kTmaBoxX;  // floats of the w box
-  static constexpr int kR = ZC * kTmaTy * kTmaBoxX;              // floats of the r box
+  static constexpr int kR = ZC * kTmaTy * kTmaTx;                // floats of the r box
   static constexpr int kFloats = kW + kR;
   static constexpr size_t kBytes = sizeof(float) * kFloats;
   static_assert(kBytes % 128 == 0, "stage buffers stay 128-byte aligned");
@@ -443,18 +446,18 @@ __device__ inline void tma_issue_tile(const CUtensorMap* tw, const CUtensorMap* 
         : "memory");
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-      ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)tr), "r"(x0), "r"(y0 + 1), "r"(z0 + 1),
+      ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)tr), "r"(x0 + 4), "r"(y0 + 1), "r"(z0 + 1),
       "r"(mb)
       : "memory");
 }
 
-template <int ZC>
+template <int ZC, int STAGES>
 __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ CUtensorMap tw,
                                                         const __grid_constant__ CUtensorMap tr, Stencil S,
                                                         JacobiCoefF J, float* __restrict__ wout, double* partial,
                                                         int w_zero, int gx, int gy, int ntiles, int* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  float* stages = reinterpret_cast<float*>(smem_raw);  // [2][TmaStage<ZC>::kFloats]
+  float* stages = reinterpret_cast<float*>(smem_raw);  // [STAGES][TmaStage<ZC>::kFloats]
   __shared__ __align__(8) unsigned long long mbar[2];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + kTmaTx * ty;
@@ -477,19 +480,20 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
   if (tid == 0) tma_issue_tile<ZC>(&tw, &tr, stages, mb0, t, gx, gy, w_zero);
   const long long plane = (long long)S.fpitch * S.nyp;
   for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
-    const int st = it & 1;
-    const uint32_t phase = (uint32_t)((it >> 1) & 1);
+    const int st = STAGES == 2 ? (it & 1) : 0;
+    const uint32_t phase = (uint32_t)(STAGES == 2 ? ((it >> 1) & 1) : (it & 1));
     const uint32_t mb = st ? mb1 : mb0;
     const int tn = t + gridDim.x;
-    // the other stage was last read in iteration it-1, which ended at a barrier
-    if (tid == 0 && tn < ntiles)
+    // two stages: prefetch the next tile into the other stage, which was last
+    // read in iteration it-1 (ended at a barrier)
+    if (STAGES == 2 && tid == 0 && tn < ntiles)
       tma_issue_tile<ZC>(&tw, &tr, stages + (st ^ 1) * TmaStage<ZC>::kFloats, st ? mb0 : mb1, tn, gx, gy, w_zero);
     const bool ok = __syncthreads_and(mbar_wait(mb, phase, kMbarSpin) ? 1 : 0);
     if (!ok) {
       if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
       // let the copies in flight land before the block exits
       mbar_wait(mb, phase, kMbarSpin);
-      if (tn < ntiles) mbar_wait(st ? mb0 : mb1, (uint32_t)(((it + 1) >> 1) & 1), kMbarSpin);
+      if (STAGES == 2 && tn < ntiles) mbar_wait(st ? mb0 : mb1, (uint32_t)(((it + 1) >> 1) & 1), kMbarSpin);
       return;
     }
     const float* sw = stages + st * TmaStage<ZC>::kFloats;
@@ -504,7 +508,7 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
       const int col = tx + 4;  // smem column of node i
       if (w_zero) {
         for (int kk = 1; kk <= kend; ++kk, c += plane) {
-          float res = sr[((kk - 1) * kTmaTy + ty) * kTmaBoxX + col];
+          float res = sr[((kk - 1) * kTmaTy + ty) * kTmaTx + tx];
           r2 += res * res;
           wout[c] = -J.af * res;
         }
@@ -518,7 +522,7 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
           float sy = W(kk, ty + 2, col) + W(kk, ty, col);
           float sz = wp + wm;
           float lap = (sx - 2.0f * wc) * J.idx2 + (sy - 2.0f * wc) * J.idy2 + (sz - 2.0f * wc) * J.idz2;
-          float res = sr[((kk - 1) * kTmaTy + ty) * kTmaBoxX + col] - lap;
+          float res = sr[((kk - 1) * kTmaTy + ty) * kTmaTx + tx] - lap;
           r2 += res * res;
           wout[c] = wc - J.af * res;
           wm = wc;
@@ -528,8 +532,9 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
     }
     block_sum_store((double)r2, partial + t);
     // every thread is done with this stage (and thread 0 with the reduction
-    // scratch) before the stage is refilled in the next iteration
+    // scratch) before the stage is refilled
     __syncthreads();
+    if (STAGES == 1 && tid == 0 && tn < ntiles) tma_issue_tile<ZC>(&tw, &tr, stages, mb0, tn, gx, gy, w_zero);
   }
 }
 
@@ -773,7 +778,7 @@ cudaError_t launch_sweep_f32(const KParams& P, const JacobiGeom& G, const float*
   return cudaGetLastError();
 }
 
-int make_tensor_map(CUtensorMap* m, float* base, const KParams& P, int box_y, int box_z) {
+int make_tensor_map(CUtensorMap* m, float* base, const KParams& P, int box_x, int box_y, int box_z) {
   using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -789,20 +794,21 @@ int make_tensor_map(CUtensorMap* m, float* base, const KParams& P, int box_y, in
   const int pitch = f32_pitch(P);
   cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)P.nyp, (cuuint64_t)P.nzp};
   cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(float), (cuuint64_t)pitch * P.nyp * sizeof(float)};
-  cuuint32_t box[3] = {(cuuint32_t)kTmaBoxX, (cuuint32_t)box_y, (cuuint32_t)box_z};
+  cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_z};
   cuuint32_t estr[3] = {1, 1, 1};
   return (int)encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
-template <int ZC>
-static cudaError_t launch_tma_zc(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+template <int ZC, int STAGES>
+static cudaError_t launch_tma_zs(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
                                  float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
-  const size_t smem = 2 * TmaStage<ZC>::kBytes;
+  const size_t smem = STAGES * TmaStage<ZC>::kBytes;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(sweep_tma_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(sweep_tma_kernel<ZC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -819,26 +825,38 @@ static cudaError_t launch_tma_zc(const KParams& P, const JacobiGeom& G, const CU
   cfg.attrs = at;
   cfg.numAttrs = 1;
   note_launch();
-  return cudaLaunchKernelEx(&cfg, sweep_tma_kernel<ZC>, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout, partial,
-                            w_zero, (int)G.grid.x, (int)G.grid.y, ntiles, err);
+  return cudaLaunchKernelEx(&cfg, sweep_tma_kernel<ZC, STAGES>, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout,
+                            partial, w_zero, (int)G.grid.x, (int)G.grid.y, ntiles, err);
 }
 
 template <int ZC>
-static int occupancy_zc() {
-  const size_t smem = 2 * TmaStage<ZC>::kBytes;
-  if (cudaFuncSetAttribute(sweep_tma_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+static cudaError_t launch_tma_zc(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                                 float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
+  return G.stages == 2 ? launch_tma_zs<ZC, 2>(P, G, tw, tr, wout, partial, w_zero, err, st)
+                       : launch_tma_zs<ZC, 1>(P, G, tw, tr, wout, partial, w_zero, err, st);
+}
+
+template <int ZC, int STAGES>
+static int occupancy_zs() {
+  const size_t smem = STAGES * TmaStage<ZC>::kBytes;
+  if (cudaFuncSetAttribute(sweep_tma_kernel<ZC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
     return 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_tma_kernel<ZC>, kTmaTx * kTmaTy, smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_tma_kernel<ZC, STAGES>, kTmaTx * kTmaTy, smem) !=
+      cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
 }
 
-int sweep_tma_occupancy(const JacobiGeom& G) {
-  switch (G.zc) {
-    case 4: return occupancy_zc<4>();
-    case 8: return occupancy_zc<8>();
-    case 16: return occupancy_zc<16>();
+int sweep_tma_occupancy(const JacobiGeom& G, int stages) {
+  switch (G.zc * 4 + (stages == 2 ? 1 : 0)) {
+    case 16: return occupancy_zs<4, 1>();
+    case 17: return occupancy_zs<4, 2>();
+    case 32: return occupancy_zs<8, 1>();
+    case 33: return occupancy_zs<8, 2>();
+    case 64: return occupancy_zs<16, 1>();
+    case 65: return occupancy_zs<16, 2>();
   }
   return 1;
 }

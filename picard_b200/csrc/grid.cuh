@@ -26,17 +26,19 @@ struct JacobiGeom {
   // persistent grid (0: one per tile) and programmatic dependent launch
   int ctas = 0;
   int pdl = 1;
+  int stages = 1;  // shared-memory stages per CTA (2: the next tile is prefetched)
 };
 // CTAs of one SM the TMA sweep kernel of this geometry can hold.
-int sweep_tma_occupancy(const JacobiGeom& G);
+int sweep_tma_occupancy(const JacobiGeom& G, int stages);
 
 // Row pitch (floats) of the padded FP32 solver arrays: node (i, j, k) at
 // column i + 3, rows a multiple of 8 floats (32 bytes).
 int f32_pitch(const KParams& P);
 long long f32_elems(const KParams& P);
-// TMA descriptors of one padded FP32 array: w boxes (40 x 10 x zc+2) and
-// r boxes (40 x 8 x zc).  Returns a CUresult.
-int make_tensor_map(CUtensorMap* m, float* base, const KParams& P, int box_y, int box_z);
+// TMA descriptor of one padded FP32 array with box_x x box_y x box_z boxes
+// (w: 40 x 10 x zc+2 from the aligned column below the tile's halo; r: 32 x 8
+// x zc from the tile's first interior column).  Returns a CUresult.
+int make_tensor_map(CUtensorMap* m, float* base, const KParams& P, int box_x, int box_y, int box_z);
 cudaError_t launch_sweep_tma(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
                              float* wout, double* partial, int w_zero, int* err, cudaStream_t st);
 

@@ -12,6 +12,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <string>
@@ -263,18 +265,23 @@ extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t 
 
 // ------------------------------------------------------- sweep launch tuner
 //
-// Picks the launch shape of the TMA sweep -- the persistent grid size (k CTAs
-// per SM for k up to the kernel's occupancy, or one CTA per tile) and whether
-// programmatic dependent launch is used -- by timing a short run of sweeps of
-// each candidate on this context's own buffers.  The shape does not change a
+// Picks the launch shape of the TMA sweep -- one CTA per tile with one
+// shared-memory stage, or a persistent grid of k CTAs per SM (two stages, k up
+// to the kernel's occupancy; or one stage at full occupancy), each with and
+// without programmatic dependent launch -- by timing a short run of sweeps of
+// each candidate on this context's own buffers.  PICARD_TUNE_LOG=1 prints the
+// timings to stderr.  The shape does not change a
 // single bit of the results, so the choice is free to differ from process to
 // process.  Choices are cached per (grid, tile depth, device) for the life of
 // the process.
 namespace picard {
 
 namespace {
+struct SweepShape {
+  int ctas, pdl, stages;
+};
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_tuned;
+std::map<std::tuple<int, int, int, int, int>, SweepShape> g_tuned;
 }  // namespace
 
 int tune_sweep(picard_ctx* c, bool fresh) {
@@ -284,26 +291,29 @@ int tune_sweep(picard_ctx* c, bool fresh) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) {
-      c->G.ctas = it->second.first;
-      c->G.pdl = it->second.second;
+      c->G.ctas = it->second.ctas;
+      c->G.pdl = it->second.pdl;
+      c->G.stages = it->second.stages;
       return PICARD_OK;
     }
   }
   int sms = 148;
   PICARD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  const int occ = sweep_tma_occupancy(c->G);
-  std::vector<std::pair<int, int>> cand;
+  const int occ1 = sweep_tma_occupancy(c->G, 1), occ2 = sweep_tma_occupancy(c->G, 2);
+  std::vector<SweepShape> cand;
   for (int pdl = 1; pdl >= 0; --pdl) {
-    for (int k = 1; k <= occ; ++k)
-      if ((long long)k * sms < c->G.nblocks) cand.emplace_back(k * sms, pdl);
-    cand.emplace_back(0, pdl);
+    cand.push_back({0, pdl, 1});  // one CTA per tile
+    for (int k = 1; k <= occ2; ++k)
+      if ((long long)k * sms < c->G.nblocks) cand.push_back({k * sms, pdl, 2});
+    if ((long long)occ1 * sms < c->G.nblocks) cand.push_back({occ1 * sms, pdl, 1});
   }
   constexpr int kReps = 24;
   std::vector<float> best(cand.size(), 1e30f);
   for (int round = 0; round < 2; ++round) {
     for (size_t q = 0; q < cand.size(); ++q) {
-      c->G.ctas = cand[q].first;
-      c->G.pdl = cand[q].second;
+      c->G.ctas = cand[q].ctas;
+      c->G.pdl = cand[q].pdl;
+      c->G.stages = cand[q].stages;
       for (int s = 1; s <= 2; ++s)
         PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
                                      c->d_err, c->st));
@@ -315,15 +325,22 @@ int tune_sweep(picard_ctx* c, bool fresh) {
       PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
       float ms = 0.0f;
       PICARD_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
-      best[q] = std::min(best[q], ms);
+      best[q] = std::min(best[q], ms / kReps);
     }
   }
   PICARD_TRY(check_timeout(c));
   size_t pick = 0;
   for (size_t q = 1; q < cand.size(); ++q)
     if (best[q] < best[pick]) pick = q;
-  c->G.ctas = cand[pick].first;
-  c->G.pdl = cand[pick].second;
+  if (const char* v = std::getenv("PICARD_TUNE_LOG"); v && *v && *v != '0') {
+    for (size_t q = 0; q < cand.size(); ++q)
+      std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: ctas=%d pdl=%d stages=%d  %.3f us%s\n", c->K.nx,
+                   c->K.ny, c->K.nz, c->G.zc, cand[q].ctas, cand[q].pdl, cand[q].stages, best[q] * 1e3,
+                   q == pick ? "  <- picked" : "");
+  }
+  c->G.ctas = cand[pick].ctas;
+  c->G.pdl = cand[pick].pdl;
+  c->G.stages = cand[pick].stages;
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tuned[key] = cand[pick];
   return PICARD_OK;

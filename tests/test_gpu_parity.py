@@ -176,8 +176,8 @@ def test_jacobi_matches_oracle(mode):
 
 
 def test_sweep_launch_shape_does_not_change_bits():
-    # the TMA sweep's persistent grid size and programmatic dependent launch
-    # are tuning knobs only: every shape gives the same potential bit for bit
+    # the TMA sweep's persistent grid size, stage count and programmatic
+    # dependent launch are tuning knobs only: every shape gives the same potential bit for bit
     # and the same sweep count, within 1e-6 of the FP64 oracle
     nx, ny, nz = 72, 40, 36  # 3 x 5 x 9 = 135 tiles of 32 x 8 x 4
     p = small_plasma(n=8, ppc=1, seed=31)
@@ -189,7 +189,8 @@ def test_sweep_launch_shape_does_not_change_bits():
     q, o, g = make(p, **C32)
     rng = np.random.default_rng(5)
     C = np.zeros_like(o.C)
-    x, y, z = np.meshgrid(np.arange(nx + 2), np.arange(ny + 2), np.arange(nz + 2), indexing="ij")
+    # reference layout C(0:nx+1, 0:ny+1, 0:nz+1), column-major: numpy shape (nz+2, ny+2, nx+2)
+    z, y, x = np.meshgrid(np.arange(nz + 2), np.arange(ny + 2), np.arange(nx + 2), indexing="ij")
     for _ in range(4):
         c = rng.uniform([8, 8, 8], [nx - 8, ny - 8, nz - 8])
         C += rng.normal() * 1e-12 * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / 18.0)
@@ -199,9 +200,10 @@ def test_sweep_launch_shape_does_not_change_bits():
     sweeps_o, conv, _ = o.calc_epotential()
     assert conv
     results = []
-    for ctas, pdl in [(-1, 0), (-1, 1), (7, 1), (40, 0), (64, 1)]:
+    for ctas, pdl, stages in [(-1, 0, 1), (-1, 1, 1), (7, 1, 2), (40, 0, 2), (64, 1, 1), (-1, 1, 2)]:
         g.set_option(capi.OPT_SWEEP_CTAS, ctas)
         g.set_option(capi.OPT_SWEEP_PDL, pdl)
+        g.set_option(capi.OPT_SWEEP_STAGES, stages)
         g.set_field(capi.FIELD_C, C)
         g.set_field(capi.FIELD_U, np.zeros_like(o.U))
         sweeps = g.calc_epotential()

@@ -67,7 +67,7 @@ def test_served_run_equals_the_direct_fused_loop():
     g.particles_initialize()
     g.run_fused(0, steps)
     e = g.energy()
-    n = g.num_local()
+    n = g.num_local
     U = g.field(capi.FIELD_U)
     with Server(4 * GB, 2) as s:
         s.submit(0, p, steps)
