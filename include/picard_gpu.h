@@ -252,7 +252,13 @@ typedef enum picard_option {
    * CTA's next tile). */
   PICARD_OPT_SWEEP_CTAS = 1,
   PICARD_OPT_SWEEP_PDL = 2,
-  PICARD_OPT_SWEEP_STAGES = 3
+  PICARD_OPT_SWEEP_STAGES = 3,
+  /* Register-resident sweeps (one cooperative launch per batch of sweeps, w
+   * in registers, r in shared memory): 0 off (the TMA kernel with the shape
+   * above), 1..5 on with CTA shape 0..4 (32 x 8 x 8 up to 32 x 32 x 32 nodes)
+   * when that grid fits on the device, else PICARD_ERR_STATE.  Never changes
+   * a result bit. */
+  PICARD_OPT_SWEEP_RESIDENT = 4
 } picard_option;
 /* Reads an option's current value (SWEEP_CTAS: 0 means one CTA per tile). */
 PICARD_API int picard_gpu_get_option(picard_ctx* ctx, int32_t option, int32_t* value);

@@ -26,6 +26,7 @@ UNITS = {
     "grid.cu": [],
     "bcpot_tc.cu": [],
     "solver.cu": [],
+    "jacobi_resident.cu": [],
     "context.cu": [],
     "driver.cu": [],
     "server.cu": [],

@@ -33,6 +33,7 @@ OPT_BCPOT_TENSOR = 0
 OPT_SWEEP_CTAS = 1
 OPT_SWEEP_PDL = 2
 OPT_SWEEP_STAGES = 3
+OPT_SWEEP_RESIDENT = 4
 
 class PicardStats(C.Structure):
     _fields_ = [

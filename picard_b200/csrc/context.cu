@@ -157,6 +157,19 @@ int dalloc(picard_ctx* c, T*& p, size_t n) {
   return PICARD_OK;
 }
 
+}  // namespace
+
+namespace picard {
+int dev_alloc(picard_ctx* c, void** p, size_t bytes) {
+  unsigned char* q = nullptr;
+  PICARD_TRY(dalloc(c, q, bytes));
+  *p = q;
+  return PICARD_OK;
+}
+}  // namespace picard
+
+namespace {
+
 struct Sizes {
   long long cap, nodes, cells, dsize;
   int species, nb_compact, nb_jacobi;
@@ -706,6 +719,10 @@ int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
     c->G.pdl = value != 0;
     return PICARD_OK;
   }
+  if (option == PICARD_OPT_SWEEP_RESIDENT) {
+    if (value < 0 || value > kResidentShapes) return fail(PICARD_ERR_BAD_ARG, "SWEEP_RESIDENT must be 0..5");
+    return set_resident(c, value);
+  }
   if (option == PICARD_OPT_SWEEP_STAGES) {
     if (value != 1 && value != 2) return fail(PICARD_ERR_BAD_ARG, "SWEEP_STAGES must be 1 or 2");
     c->G.stages = value;
@@ -721,6 +738,7 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
     case PICARD_OPT_SWEEP_CTAS: *value = c->G.ctas; return PICARD_OK;
     case PICARD_OPT_SWEEP_PDL: *value = c->G.pdl; return PICARD_OK;
     case PICARD_OPT_SWEEP_STAGES: *value = c->G.stages; return PICARD_OK;
+    case PICARD_OPT_SWEEP_RESIDENT: *value = resident_option_value(c); return PICARD_OK;
   }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");
 }

@@ -61,6 +61,11 @@ struct picard_ctx {
   double* h_pinned = nullptr;    // [m_max + 16] host staging
   int* h_pinned_i = nullptr;     // [16]
 
+  // register-resident sweeps (jacobi_resident.cu)
+  float* res_faces = nullptr;
+  unsigned int* res_bar = nullptr;
+  long long res_faces_cap = 0;  // floats
+
   // tensor-core BCpotentials (bcpot_tc.cu)
   int bcpot_tensor = 0;
   void* tc_cs = nullptr;
@@ -90,9 +95,14 @@ picard::InflowTable make_inflow_table(const picard_params& p);
 // Reads the device particle count into ctx->num_local after surfacing any
 // device-side capacity error.
 int sync_count_public(picard_ctx* c);
+// Device memory owned by the context (zeroed, freed with it).
+int dev_alloc(picard_ctx* c, void** p, size_t bytes);
 // Times the launch shapes of the TMA sweep on this context's buffers and keeps
 // the fastest (cached per grid and device unless `fresh`).
 int tune_sweep(picard_ctx* c, bool fresh);
+// PICARD_OPT_SWEEP_RESIDENT: 0 off, q + 1 resident with CTA shape q.
+int set_resident(picard_ctx* c, int value);
+int resident_option_value(const picard_ctx* c);
 }  // namespace picard
 
 #define PICARD_CUDA(expr)                                          \

@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "grid.cuh"
+#include "stencil.cuh"
 
 namespace picard {
 
@@ -194,21 +195,6 @@ __global__ void bc_potentials_kernel(KParams P, int axis, const double* __restri
 
 // ------------------------------------------------------------- Jacobi
 
-struct Stencil {
-  int nx, ny, nz, nxp, nyp;
-  int px, py, pz;  // periodic axes
-  long long nodes;
-  int fpitch;      // row pitch (floats) of the FP32 solver arrays
-};
-
-// FP32 solver arrays (increment w, scaled residual r) are padded: node
-// (i, j, k) sits at column i + 3 of a row of fpitch floats, fpitch a multiple
-// of 8.  Interior rows then start on 16-byte boundaries (column 4) and every
-// TMA box origin (column 32 b) is 16-byte aligned.
-__host__ __device__ inline long long fidx(const Stencil& S, int i, int j, int k) {
-  return (long long)(i + 3) + (long long)S.fpitch * ((long long)j + (long long)S.nyp * k);
-}
-
 __device__ inline void neighbours(const Stencil& S, int i, int j, int k, long long& xm, long long& xp, long long& ym,
                                   long long& yp, long long& zm, long long& zp) {
   int im = (S.px && i == 1) ? S.nx : i - 1, ip = (S.px && i == S.nx) ? 1 : i + 1;
@@ -300,8 +286,8 @@ __global__ void __launch_bounds__(256) sweep_f32_kernel(Stencil S, JacobiCoefF J
     if (w_zero) {
       for (int k = k0; k <= k1; ++k, c += plane) {
         float res = __ldg(r + c);
-        r2 += res * res;
-        wout[c] = -J.af * res;
+        r2 = acc_r2_f32(r2, res);
+        wout[c] = jacobi_next_f32(J, 0.0f, res);
       }
     } else {
       int im = (S.px && i == 1) ? S.nx : i - 1, ip = (S.px && i == S.nx) ? 1 : i + 1;
@@ -315,13 +301,10 @@ __global__ void __launch_bounds__(256) sweep_f32_kernel(Stencil S, JacobiCoefF J
       for (int k = k0; k <= k1; ++k, c += plane) {
         long long cp = (S.pz && k == S.nz) ? c - (long long)(S.nz - 1) * plane : c + plane;
         float wp = __ldg(win + cp);
-        float sx = __ldg(win + c + dxp) + __ldg(win + c + dxm);
-        float sy = __ldg(win + c + dyp) + __ldg(win + c + dym);
-        float sz = wp + wm;
-        float lap = (sx - 2.0f * wc) * J.idx2 + (sy - 2.0f * wc) * J.idy2 + (sz - 2.0f * wc) * J.idz2;
-        float res = __ldg(r + c) - lap;
-        r2 += res * res;
-        wout[c] = wc - J.af * res;
+        float res = jacobi_res_f32(J, wc, __ldg(win + c + dxm), __ldg(win + c + dxp), __ldg(win + c + dym),
+                                   __ldg(win + c + dyp), wm, wp, __ldg(r + c));
+        r2 = acc_r2_f32(r2, res);
+        wout[c] = jacobi_next_f32(J, wc, res);
         wm = wc;
         wc = wp;
       }
@@ -509,8 +492,8 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
       if (w_zero) {
         for (int kk = 1; kk <= kend; ++kk, c += plane) {
           float res = sr[((kk - 1) * kTmaTy + ty) * kTmaTx + tx];
-          r2 += res * res;
-          wout[c] = -J.af * res;
+          r2 = acc_r2_f32(r2, res);
+          wout[c] = jacobi_next_f32(J, 0.0f, res);
         }
       } else {
         auto W = [&](int kk, int row, int cc) { return sw[(kk * (kTmaTy + 2) + row) * kTmaBoxX + cc]; };
@@ -518,13 +501,10 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
         float wc = W(1, ty + 1, col);
         for (int kk = 1; kk <= kend; ++kk, c += plane) {
           float wp = W(kk + 1, ty + 1, col);
-          float sx = W(kk, ty + 1, col + 1) + W(kk, ty + 1, col - 1);
-          float sy = W(kk, ty + 2, col) + W(kk, ty, col);
-          float sz = wp + wm;
-          float lap = (sx - 2.0f * wc) * J.idx2 + (sy - 2.0f * wc) * J.idy2 + (sz - 2.0f * wc) * J.idz2;
-          float res = sr[((kk - 1) * kTmaTy + ty) * kTmaTx + tx] - lap;
-          r2 += res * res;
-          wout[c] = wc - J.af * res;
+          float res = jacobi_res_f32(J, wc, W(kk, ty + 1, col - 1), W(kk, ty + 1, col + 1), W(kk, ty, col),
+                                     W(kk, ty + 2, col), wm, wp, sr[((kk - 1) * kTmaTy + ty) * kTmaTx + tx]);
+          r2 = acc_r2_f32(r2, res);
+          wout[c] = jacobi_next_f32(J, wc, res);
           wm = wc;
           wc = wp;
         }

@@ -27,7 +27,24 @@ struct JacobiGeom {
   int ctas = 0;
   int pdl = 1;
   int stages = 1;  // shared-memory stages per CTA (2: the next tile is prefetched)
+  // register-resident sweeps (jacobi_resident.cu): one cooperative launch per
+  // batch of sweeps over CTAs of 32 x res_by x res_nz nodes
+  int res = 0;
+  int res_by = 0, res_nz = 0, res_cgx = 0, res_cgy = 0, res_cgz = 0, res_ctas = 0;
 };
+// Plans the resident sweep with CTA shape `shape_index` (0 = smallest);
+// returns 1 and fills G.res* when all its CTAs can be co-resident on the
+// current device, else 0 (G.res = 0).
+int resident_plan(const KParams& P, JacobiGeom& G, int shape_index);
+constexpr int kResidentShapes = 5;
+// Floats of the face-exchange buffer the planned resident sweep needs.
+long long resident_face_floats(const JacobiGeom& G);
+// m sweeps (the first from w = 0 when w_zero, else from win) in one
+// cooperative launch: partial[t * nblocks + tile] for t < m, w of the last
+// sweep to wout.  bar: one counter, zeroed here.
+cudaError_t launch_sweeps_resident(const KParams& P, const JacobiGeom& G, const float* r, const float* win,
+                                   float* wout, float* faces, unsigned int* bar, double* partial, int m, int w_zero,
+                                   int* err, cudaStream_t st);
 // CTAs of one SM the TMA sweep kernel of this geometry can hold.
 int sweep_tma_occupancy(const JacobiGeom& G, int stages);
 

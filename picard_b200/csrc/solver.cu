@@ -27,6 +27,8 @@ using namespace picard;
 
 namespace {
 
+std::mutex g_resident_mu;
+
 // Next batch length: sweeps until the predicted hit, from the last two
 // residual norms, clamped to [16, m_max].
 int next_batch(double r2_prev, double r2_last, double tol2, int m_max) {
@@ -141,11 +143,27 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
   double* V[2] = {c->U, c->U1};
   float* R[2] = {c->r, c->r + f32_elems(K)};  // anchor residuals, one per live anchor
   // sweep s reads w[(s-1)%2] (TMA descriptor tmw[(s-1)%2]) and R[rcur] (tmr[rcur])
-  auto sweep = [&](long long s, int rc_, double* partial, int w_zero) -> cudaError_t {
+  auto sweep = [&](long long s, int rsel, double* partial, int w_zero) -> cudaError_t {
     if (c->G.tma)
-      return launch_sweep_tma(K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[rc_], c->w[s % 2], partial, w_zero, c->d_err,
+      return launch_sweep_tma(K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[rsel], c->w[s % 2], partial, w_zero, c->d_err,
                               c->st);
-    return launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rc_], partial, w_zero, c->st);
+    return launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rsel], partial, w_zero, c->st);
+  };
+  // sweeps a0+1 .. a0+count from w = 0 (the anchor), partials of sweep a0+t at
+  // partial_base + (t-1) nb
+  auto run_sweeps = [&](long long a0, int count, int rsel, double* partial_base) -> int {
+    if (c->G.res) {
+      // one resident launch at a time on the device: its CTAs must all be
+      // resident together, which another cooperative grid could prevent
+      std::lock_guard<std::mutex> lk(g_resident_mu);
+      PICARD_CUDA(launch_sweeps_resident(K, c->G, R[rsel], nullptr, c->w[(a0 + count) % 2], c->res_faces,
+                                         c->res_bar, partial_base, count, 1, c->d_err, c->st));
+      PICARD_CUDA(cudaStreamSynchronize(c->st));
+      return PICARD_OK;
+    }
+    for (int t = 1; t <= count; ++t)
+      PICARD_CUDA(sweep(a0 + t, rsel, partial_base + (size_t)(t - 1) * nb, t == 1 ? 1 : 0));
+    return PICARD_OK;
   };
   int vcur = 0, rcur = 0;
   PICARD_CUDA(cudaMemcpyAsync(c->U1, c->U, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
@@ -159,10 +177,7 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
   for (;;) {
     int m_eff = int(std::min<long long>(m, smax - a));
     PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
-    for (int t = 1; t <= m_eff; ++t) {
-      long long s = a + t;
-      PICARD_CUDA(sweep(s, rcur, c->partials + (size_t)(t - 1) * nb, t == 1 ? 1 : 0));
-    }
+    PICARD_TRY(run_sweeps(a, m_eff, rcur, c->partials));
     PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
     // next anchor: fold w_{a+m_eff} into V, exact FP64 residual of that iterate
     long long an = a + m_eff;
@@ -197,8 +212,7 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
           PICARD_CUDA(cudaMemcpyAsync(c->U, V[1 - vcur], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
       } else {
         // replay sweeps a+1..hit from the old anchor (unchanged in V[vcur])
-        for (long long s = a + 1; s <= hit; ++s)
-          PICARD_CUDA(sweep(s, rcur, c->partials, s == a + 1 ? 1 : 0));
+        PICARD_TRY(run_sweeps(a, int(hit - a), rcur, c->partials));
         c->stats.sweep_launches += hit - a;
         PICARD_CUDA(launch_finalize(K, V[vcur], c->w[hit % 2], sigma, c->U, 0, c->st));
       }
@@ -265,11 +279,13 @@ extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t 
 
 // ------------------------------------------------------- sweep launch tuner
 //
-// Picks the launch shape of the TMA sweep -- one CTA per tile with one
-// shared-memory stage, or a persistent grid of k CTAs per SM (two stages, k up
-// to the kernel's occupancy; or one stage at full occupancy), each with and
-// without programmatic dependent launch -- by timing a short run of sweeps of
-// each candidate on this context's own buffers.  PICARD_TUNE_LOG=1 prints the
+// Picks how the FP32 sweeps run -- the TMA sweep kernel with one CTA per tile
+// and one shared-memory stage, or a persistent grid of k CTAs per SM (two
+// stages, k up to the kernel's occupancy; or one stage at full occupancy),
+// each with and without programmatic dependent launch; or the
+// register-resident sweep with each CTA shape whose grid fits on the device
+// at once -- by timing a short run of sweeps of each candidate on this
+// context's own buffers.  PICARD_TUNE_LOG=1 prints the
 // timings to stderr.  The shape does not change a
 // single bit of the results, so the choice is free to differ from process to
 // process.  Choices are cached per (grid, tile depth, device) for the life of
@@ -279,51 +295,120 @@ namespace picard {
 namespace {
 struct SweepShape {
   int ctas, pdl, stages;
+  int res;  // 0: TMA sweep kernel; q + 1: resident sweep with CTA shape q
 };
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, SweepShape> g_tuned;
+
+int apply_shape(picard_ctx* c, const SweepShape& sh) {
+  c->G.ctas = sh.ctas;
+  c->G.pdl = sh.pdl;
+  c->G.stages = sh.stages;
+  c->G.res = 0;
+  if (sh.res > 0) {
+    if (!resident_plan(c->K, c->G, sh.res - 1)) return fail(PICARD_ERR_STATE, "resident sweep shape does not fit");
+    const long long need = resident_face_floats(c->G);
+    if (need > c->res_faces_cap) {
+      void* q = nullptr;
+      PICARD_TRY(dev_alloc(c, &q, sizeof(float) * (size_t)need));
+      c->res_faces = static_cast<float*>(q);
+      c->res_faces_cap = need;
+    }
+    if (!c->res_bar) {
+      void* q = nullptr;
+      PICARD_TRY(dev_alloc(c, &q, sizeof(unsigned int)));
+      c->res_bar = static_cast<unsigned int*>(q);
+    }
+  }
+  return PICARD_OK;
+}
 }  // namespace
+
+int set_resident(picard_ctx* c, int value) {
+  if (value == 0) {
+    c->G.res = 0;
+    return PICARD_OK;
+  }
+  if (!c->G.tma || !c->w[0]) return fail(PICARD_ERR_STATE, "resident sweeps need open boundaries and the F32_REFINE solver");
+  SweepShape sh{0, 0, 1, value};
+  JacobiGeom g = c->G;
+  if (!resident_plan(c->K, g, value - 1)) return fail(PICARD_ERR_STATE, "resident sweep shape does not fit the device");
+  c->G.res = 0;
+  c->G.res_by = 0;
+  // keep the TMA launch shape, switch the sweeps to the resident kernel
+  const int ctas = c->G.ctas, pdl = c->G.pdl, stages = c->G.stages;
+  sh.ctas = ctas;
+  sh.pdl = pdl;
+  sh.stages = stages;
+  return apply_shape(c, sh);
+}
+
+int resident_option_value(const picard_ctx* c) {
+  if (!c->G.res) return 0;
+  for (int q = 0; q < kResidentShapes; ++q) {
+    JacobiGeom g = c->G;
+    if (resident_plan(c->K, g, q) && g.res_by == c->G.res_by && g.res_nz == c->G.res_nz) return q + 1;
+  }
+  return 0;
+}
 
 int tune_sweep(picard_ctx* c, bool fresh) {
   if (!c->G.tma || !c->w[0]) return PICARD_OK;
   const auto key = std::make_tuple(c->K.nx, c->K.ny, c->K.nz, c->G.zc, c->device);
+  auto apply = [&](const SweepShape& sh) -> int { return apply_shape(c, sh); };
   if (!fresh) {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tuned.find(key);
-    if (it != g_tuned.end()) {
-      c->G.ctas = it->second.ctas;
-      c->G.pdl = it->second.pdl;
-      c->G.stages = it->second.stages;
-      return PICARD_OK;
+    SweepShape cached;
+    bool hit = false;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tuned.find(key);
+      if (it != g_tuned.end()) {
+        cached = it->second;
+        hit = true;
+      }
     }
+    if (hit) return apply(cached);
   }
   int sms = 148;
   PICARD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   const int occ1 = sweep_tma_occupancy(c->G, 1), occ2 = sweep_tma_occupancy(c->G, 2);
   std::vector<SweepShape> cand;
   for (int pdl = 1; pdl >= 0; --pdl) {
-    cand.push_back({0, pdl, 1});  // one CTA per tile
+    cand.push_back({0, pdl, 1, 0});  // one CTA per tile
     for (int k = 1; k <= occ2; ++k)
-      if ((long long)k * sms < c->G.nblocks) cand.push_back({k * sms, pdl, 2});
-    if ((long long)occ1 * sms < c->G.nblocks) cand.push_back({occ1 * sms, pdl, 1});
+      if ((long long)k * sms < c->G.nblocks) cand.push_back({k * sms, pdl, 2, 0});
+    if ((long long)occ1 * sms < c->G.nblocks) cand.push_back({occ1 * sms, pdl, 1, 0});
+  }
+  for (int q = 0; q < kResidentShapes; ++q) {
+    JacobiGeom g = c->G;
+    if (resident_plan(c->K, g, q)) cand.push_back({0, 0, 1, q + 1});
   }
   constexpr int kReps = 24;
   std::vector<float> best(cand.size(), 1e30f);
   for (int round = 0; round < 2; ++round) {
     for (size_t q = 0; q < cand.size(); ++q) {
-      c->G.ctas = cand[q].ctas;
-      c->G.pdl = cand[q].pdl;
-      c->G.stages = cand[q].stages;
-      for (int s = 1; s <= 2; ++s)
-        PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
-                                     c->d_err, c->st));
-      PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
-      for (int s = 1; s <= kReps; ++s)
-        PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
-                                     c->d_err, c->st));
-      PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
-      PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
+      PICARD_TRY(apply(cand[q]));
       float ms = 0.0f;
+      if (c->G.res) {
+        std::lock_guard<std::mutex> lk(g_resident_mu);
+        PICARD_CUDA(launch_sweeps_resident(c->K, c->G, c->r, nullptr, c->w[0], c->res_faces, c->res_bar,
+                                           c->partials, 2, 1, c->d_err, c->st));
+        PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
+        PICARD_CUDA(launch_sweeps_resident(c->K, c->G, c->r, nullptr, c->w[0], c->res_faces, c->res_bar,
+                                           c->partials, kReps, 1, c->d_err, c->st));
+        PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
+        PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
+      } else {
+        for (int s = 1; s <= 2; ++s)
+          PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
+                                       c->d_err, c->st));
+        PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
+        for (int s = 1; s <= kReps; ++s)
+          PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
+                                       c->d_err, c->st));
+        PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
+        PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
+      }
       PICARD_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
       best[q] = std::min(best[q], ms / kReps);
     }
@@ -333,14 +418,17 @@ int tune_sweep(picard_ctx* c, bool fresh) {
   for (size_t q = 1; q < cand.size(); ++q)
     if (best[q] < best[pick]) pick = q;
   if (const char* v = std::getenv("PICARD_TUNE_LOG"); v && *v && *v != '0') {
-    for (size_t q = 0; q < cand.size(); ++q)
-      std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: ctas=%d pdl=%d stages=%d  %.3f us%s\n", c->K.nx,
-                   c->K.ny, c->K.nz, c->G.zc, cand[q].ctas, cand[q].pdl, cand[q].stages, best[q] * 1e3,
-                   q == pick ? "  <- picked" : "");
+    for (size_t q = 0; q < cand.size(); ++q) {
+      if (cand[q].res)
+        std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: resident shape %d  %.3f us%s\n", c->K.nx, c->K.ny,
+                     c->K.nz, c->G.zc, cand[q].res - 1, best[q] * 1e3, q == pick ? "  <- picked" : "");
+      else
+        std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: ctas=%d pdl=%d stages=%d  %.3f us%s\n", c->K.nx,
+                     c->K.ny, c->K.nz, c->G.zc, cand[q].ctas, cand[q].pdl, cand[q].stages, best[q] * 1e3,
+                     q == pick ? "  <- picked" : "");
+    }
   }
-  c->G.ctas = cand[pick].ctas;
-  c->G.pdl = cand[pick].pdl;
-  c->G.stages = cand[pick].stages;
+  PICARD_TRY(apply(cand[pick]));
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tuned[key] = cand[pick];
   return PICARD_OK;

@@ -175,11 +175,14 @@ def test_jacobi_matches_oracle(mode):
         assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-6
 
 
-def test_sweep_launch_shape_does_not_change_bits():
-    # the TMA sweep's persistent grid size, stage count and programmatic
-    # dependent launch are tuning knobs only: every shape gives the same potential bit for bit
-    # and the same sweep count, within 1e-6 of the FP64 oracle
-    nx, ny, nz = 72, 40, 36  # 3 x 5 x 9 = 135 tiles of 32 x 8 x 4
+@pytest.mark.parametrize("dims", [(72, 40, 36), (40, 24, 72)])
+def test_sweep_variant_does_not_change_bits(dims):
+    # how the FP32 sweeps run -- the TMA kernel's persistent grid size, stage
+    # count and programmatic dependent launch, or the register-resident kernel
+    # with any CTA shape -- never changes a bit: the same potential and the
+    # same sweep count, within 1e-6 of the FP64 oracle.  (72, 40, 36): 3 x 5 x
+    # 9 tiles of 32 x 8 x 4; (40, 24, 72): 2 x 3 x 9 tiles of 32 x 8 x 8.
+    nx, ny, nz = dims
     p = small_plasma(n=8, ppc=1, seed=31)
     p.nx, p.ny, p.nz = nx, ny, nz
     p.xmin, p.xmax = -500.0 * nx, 500.0 * nx
@@ -192,27 +195,34 @@ def test_sweep_launch_shape_does_not_change_bits():
     # reference layout C(0:nx+1, 0:ny+1, 0:nz+1), column-major: numpy shape (nz+2, ny+2, nx+2)
     z, y, x = np.meshgrid(np.arange(nz + 2), np.arange(ny + 2), np.arange(nx + 2), indexing="ij")
     for _ in range(4):
-        c = rng.uniform([8, 8, 8], [nx - 8, ny - 8, nz - 8])
+        c = rng.uniform([6, 6, 6], [nx - 6, ny - 6, nz - 6])
         C += rng.normal() * 1e-12 * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / 18.0)
     C[0, :, :] = C[-1, :, :] = C[:, 0, :] = C[:, -1, :] = C[:, :, 0] = C[:, :, -1] = 0.0
     o.C[...] = C
     o.U[...] = 0.0
     sweeps_o, conv, _ = o.calc_epotential()
     assert conv
+    variants = [("tma", -1, 0, 1), ("tma", -1, 1, 1), ("tma", 7, 1, 2), ("tma", 40, 0, 2), ("tma", 64, 1, 1),
+                ("tma", -1, 1, 2)] + [("resident", q, 0, 0) for q in range(1, 6)]
     results = []
-    for ctas, pdl, stages in [(-1, 0, 1), (-1, 1, 1), (7, 1, 2), (40, 0, 2), (64, 1, 1), (-1, 1, 2)]:
-        g.set_option(capi.OPT_SWEEP_CTAS, ctas)
-        g.set_option(capi.OPT_SWEEP_PDL, pdl)
-        g.set_option(capi.OPT_SWEEP_STAGES, stages)
+    for kind, a, b, c_ in variants:
+        if kind == "tma":
+            g.set_option(capi.OPT_SWEEP_RESIDENT, 0)
+            g.set_option(capi.OPT_SWEEP_CTAS, a)
+            g.set_option(capi.OPT_SWEEP_PDL, b)
+            g.set_option(capi.OPT_SWEEP_STAGES, c_)
+        else:
+            g.set_option(capi.OPT_SWEEP_RESIDENT, a)
+            assert g.get_option(capi.OPT_SWEEP_RESIDENT) == a
         g.set_field(capi.FIELD_C, C)
         g.set_field(capi.FIELD_U, np.zeros_like(o.U))
         sweeps = g.calc_epotential()
-        results.append((sweeps, g.field(capi.FIELD_U)))
-    for sweeps, U in results[1:]:
-        assert sweeps == results[0][0]
-        np.testing.assert_array_equal(U, results[0][1])
-    assert abs(results[0][0] - sweeps_o) <= 1
-    assert rel_l2(results[0][1], o.U) < 1e-6
+        results.append((kind, a, sweeps, g.field(capi.FIELD_U)))
+    for kind, a, sweeps, U in results[1:]:
+        assert sweeps == results[0][2], (kind, a)
+        np.testing.assert_array_equal(U, results[0][3], err_msg=f"{kind} {a}")
+    assert abs(results[0][2] - sweeps_o) <= 1
+    assert rel_l2(results[0][3], o.U) < 1e-6
 
 
 def test_jacobi_cap_reports_not_converged():
