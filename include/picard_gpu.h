@@ -258,7 +258,11 @@ typedef enum picard_option {
    * above), 1..5 on with CTA shape 0..4 (32 x 8 x 8 up to 32 x 32 x 32 nodes)
    * when that grid fits on the device, else PICARD_ERR_STATE.  Never changes
    * a result bit. */
-  PICARD_OPT_SWEEP_RESIDENT = 4
+  PICARD_OPT_SWEEP_RESIDENT = 4,
+  /* TMA sweep tile width: 0 32-wide tiles, one node per thread; 1 64-wide
+   * tiles, two x-adjacent nodes per thread in packed FP32 pair arithmetic.
+   * Never changes a result bit. */
+  PICARD_OPT_SWEEP_PAIRS = 5
 } picard_option;
 /* Reads an option's current value (SWEEP_CTAS: 0 means one CTA per tile). */
 PICARD_API int picard_gpu_get_option(picard_ctx* ctx, int32_t option, int32_t* value);

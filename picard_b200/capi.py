@@ -34,6 +34,7 @@ OPT_SWEEP_CTAS = 1
 OPT_SWEEP_PDL = 2
 OPT_SWEEP_STAGES = 3
 OPT_SWEEP_RESIDENT = 4
+OPT_SWEEP_PAIRS = 5
 
 class PicardStats(C.Structure):
     _fields_ = [

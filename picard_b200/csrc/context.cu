@@ -340,6 +340,10 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
       int e1 = make_tensor_map(&c->tmw[1], c->w[1], c->K, 40, 10, c->G.zc + 2);
       int e2 = make_tensor_map(&c->tmr[0], c->r, c->K, 32, 8, c->G.zc);
       int e3 = make_tensor_map(&c->tmr[1], c->r + fe, c->K, 32, 8, c->G.zc);
+      e0 |= make_tensor_map(&c->tmw2[0], c->w[0], c->K, 72, 10, c->G.zc + 2);
+      e1 |= make_tensor_map(&c->tmw2[1], c->w[1], c->K, 72, 10, c->G.zc + 2);
+      e2 |= make_tensor_map(&c->tmr2[0], c->r, c->K, 64, 8, c->G.zc);
+      e3 |= make_tensor_map(&c->tmr2[1], c->r + fe, c->K, 64, 8, c->G.zc);
       if (e0 || e1 || e2 || e3)
         return bail(fail(PICARD_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(e0 | e1 | e2 | e3) + ")"));
     }
@@ -723,6 +727,10 @@ int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
     if (value < 0 || value > kResidentShapes) return fail(PICARD_ERR_BAD_ARG, "SWEEP_RESIDENT must be 0..5");
     return set_resident(c, value);
   }
+  if (option == PICARD_OPT_SWEEP_PAIRS) {
+    c->G.pairs = value != 0;
+    return PICARD_OK;
+  }
   if (option == PICARD_OPT_SWEEP_STAGES) {
     if (value != 1 && value != 2) return fail(PICARD_ERR_BAD_ARG, "SWEEP_STAGES must be 1 or 2");
     c->G.stages = value;
@@ -738,6 +746,7 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
     case PICARD_OPT_SWEEP_CTAS: *value = c->G.ctas; return PICARD_OK;
     case PICARD_OPT_SWEEP_PDL: *value = c->G.pdl; return PICARD_OK;
     case PICARD_OPT_SWEEP_STAGES: *value = c->G.stages; return PICARD_OK;
+    case PICARD_OPT_SWEEP_PAIRS: *value = c->G.pairs; return PICARD_OK;
     case PICARD_OPT_SWEEP_RESIDENT: *value = resident_option_value(c); return PICARD_OK;
   }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");

@@ -43,6 +43,7 @@ struct picard_ctx {
   float* r = nullptr;                 // two padded FP32 arrays
   CUtensorMap tmw[2];                 // TMA descriptors of w[0], w[1] (w boxes)
   CUtensorMap tmr[2];                 // TMA descriptors of r, r + f32_elems (r boxes)
+  CUtensorMap tmw2[2], tmr2[2];       // the same for the x-pair sweep's wider boxes
   double* partials = nullptr;  // [m_max + 1][nblocks]
   double* r2 = nullptr;        // [m_max + 1]
   picard::JacobiGeom G;

@@ -518,6 +518,205 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
   }
 }
 
+// ------------------------------------------- TMA-staged FP32 sweep, x pairs
+//
+// The same sweep over tiles twice as wide: 64 (x) x 8 (y) x ZC (z) nodes per
+// tile, 32 x 8 threads, each thread updating the two x-adjacent nodes 2 tx and
+// 2 tx + 1 of its row with packed FP32 pair arithmetic (add/sub/mul/fma
+// .rn.f32x2, each lane rounded like the scalar __fadd_rn/.../__fmaf_rn of
+// jacobi_res_f32) and 8-byte shared-memory loads and global stores, the z
+// loop fully unrolled.  The x neighbours outside the pair come from the
+// adjacent lanes by shuffle (the tile's outer columns from shared memory).
+// Boxes: w 72 x 10 x (ZC+2) from the aligned column 64 bx, r 64 x 8 x ZC from
+// the tile's first interior column 64 bx + 4.
+//
+// Each 64-wide tile is two of the 32 x 8 x ZC tiles the residual partials
+// are defined on (lanes 0-15 and 16-31).  Their per-column FP32 sums over z
+// are formed node by node as in sweep_tma_kernel, and the 32-lane shuffle
+// tree of block_sum_store is reproduced exactly: its steps 16, 8, 4, 2 are
+// shuffles by 8, 4, 2, 1 of both pair components, its step 1 the in-lane sum
+// of the pair.  So the two kernels write the same partials bit for bit.
+constexpr int kTma2BoxX = 72, kTma2Tile = 64;
+
+template <int ZC>
+struct Tma2Stage {
+  static constexpr int kW = (ZC + 2) * (kTmaTy + 2) * kTma2BoxX;
+  static constexpr int kR = ZC * kTmaTy * kTma2Tile;
+  static constexpr int kFloats = kW + kR;
+  static constexpr size_t kBytes = sizeof(float) * kFloats;
+  static_assert(kBytes % 128 == 0, "stage buffers stay 128-byte aligned");
+};
+
+__device__ __forceinline__ unsigned long long pk2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float2 up2(unsigned long long v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+template <int ZC>
+__device__ inline void tma2_issue_tile(const CUtensorMap* tw, const CUtensorMap* tr, float* stage, uint32_t mb, int t,
+                                       int gx2, int gy, int w_zero) {
+  const int bx = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
+  const int x0 = bx * kTma2Tile, y0 = by * kTmaTy, z0 = bz * ZC;
+  float* sw = stage;
+  float* sr = stage + Tma2Stage<ZC>::kW;
+  uint32_t bytes = (uint32_t)(Tma2Stage<ZC>::kR * sizeof(float));
+  if (!w_zero) bytes += (uint32_t)(Tma2Stage<ZC>::kW * sizeof(float));
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+  if (!w_zero)
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"((uint32_t)__cvta_generic_to_shared(sw)), "l"((unsigned long long)tw), "r"(x0), "r"(y0), "r"(z0), "r"(mb)
+        : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)tr), "r"(x0 + 4), "r"(y0 + 1),
+      "r"(z0 + 1), "r"(mb)
+      : "memory");
+}
+
+template <int ZC, int STAGES>
+__global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__ CUtensorMap tw,
+                                                         const __grid_constant__ CUtensorMap tr, Stencil S,
+                                                         JacobiCoefF J, float* __restrict__ wout, double* partial,
+                                                         int w_zero, int gx2, int gx, int gy, int ntiles, int* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* stages = reinterpret_cast<float*>(smem_raw);  // [STAGES][Tma2Stage<ZC>::kFloats]
+  __shared__ __align__(8) unsigned long long mbar[2];
+  __shared__ double rows[2][kTmaTy];  // row sums of the two 32-wide partial tiles
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + kTmaTx * ty;
+  const uint32_t mb0 = (uint32_t)__cvta_generic_to_shared(&mbar[0]);
+  const uint32_t mb1 = (uint32_t)__cvta_generic_to_shared(&mbar[1]);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((unsigned long long)&tw) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((unsigned long long)&tr) : "memory");
+  }
+  __syncthreads();
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  int t = blockIdx.x;
+  if (t >= ntiles) return;
+  if (tid == 0) tma2_issue_tile<ZC>(&tw, &tr, stages, mb0, t, gx2, gy, w_zero);
+  const long long plane = (long long)S.fpitch * S.nyp;
+  const unsigned long long m2 = pk2(-2.0f, -2.0f), ix2 = pk2(J.idx2, J.idx2), iy2 = pk2(J.idy2, J.idy2),
+                           iz2 = pk2(J.idz2, J.idz2), naf = pk2(-J.af, -J.af);
+  for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
+    const int st = STAGES == 2 ? (it & 1) : 0;
+    const uint32_t phase = (uint32_t)(STAGES == 2 ? ((it >> 1) & 1) : (it & 1));
+    const uint32_t mb = st ? mb1 : mb0;
+    const int tn = t + gridDim.x;
+    if (STAGES == 2 && tid == 0 && tn < ntiles)
+      tma2_issue_tile<ZC>(&tw, &tr, stages + (st ^ 1) * Tma2Stage<ZC>::kFloats, st ? mb0 : mb1, tn, gx2, gy, w_zero);
+    const bool ok = __syncthreads_and(mbar_wait(mb, phase, kMbarSpin) ? 1 : 0);
+    if (!ok) {
+      if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+      mbar_wait(mb, phase, kMbarSpin);
+      if (STAGES == 2 && tn < ntiles) mbar_wait(st ? mb0 : mb1, (uint32_t)(((it + 1) >> 1) & 1), kMbarSpin);
+      return;
+    }
+    const float* sw = stages + st * Tma2Stage<ZC>::kFloats;
+    const float* sr = sw + Tma2Stage<ZC>::kW;
+    const int bx2 = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
+    const int i0 = bx2 * kTma2Tile + 2 * tx + 1, j = by * kTmaTy + ty + 1, z0 = bz * ZC;
+    const bool act0 = i0 <= S.nx && j <= S.ny, act1 = i0 + 1 <= S.nx && j <= S.ny;
+    const int kend = min(ZC, S.nz - z0);
+    // w rows of this thread's pair: plane kk (0 .. ZC+1), row 0 .. 9, columns 2 tx + 4, + 5
+    auto wrow = [&](int kk, int row) {
+      return *reinterpret_cast<const unsigned long long*>(sw + (kk * (kTmaTy + 2) + row) * kTma2BoxX + 2 * tx + 4);
+    };
+    auto wcol = [&](int kk, int row, int col) { return sw[(kk * (kTmaTy + 2) + row) * kTma2BoxX + col]; };
+    unsigned long long wm = w_zero ? 0ull : wrow(0, ty + 1);
+    unsigned long long wc = w_zero ? 0ull : wrow(1, ty + 1);
+    unsigned long long r2 = 0ull;  // (+0.0f, +0.0f)
+    float* out = wout + fidx(S, i0, j, z0 + 1);
+#pragma unroll
+    for (int kk = 1; kk <= ZC; ++kk) {
+      if (kk <= kend) {
+        unsigned long long wp = 0ull, ym = 0ull, yp = 0ull;
+        float xl = 0.0f, xr = 0.0f;
+        const float2 c = up2(wc);
+        if (!w_zero) {
+          wp = wrow(kk + 1, ty + 1);
+          ym = wrow(kk, ty);
+          yp = wrow(kk, ty + 2);
+          xl = wcol(kk, ty + 1, 2 * tx + 3);  // x - 1 of the pair's first node
+          xr = wcol(kk, ty + 1, 2 * tx + 6);  // x + 1 of the pair's second node
+        }
+        const unsigned long long xm = pk2(xl, c.x), xp = pk2(c.y, xr);
+        const unsigned long long rr =
+            *reinterpret_cast<const unsigned long long*>(sr + ((kk - 1) * kTmaTy + ty) * kTma2Tile + 2 * tx);
+        // jacobi_res_f32 on both lanes
+        const unsigned long long sx = add2(xp, xm), sy = add2(yp, ym), sz = add2(wp, wm);
+        unsigned long long lap = mul2(fma2(m2, wc, sx), ix2);
+        lap = fma2(fma2(m2, wc, sy), iy2, lap);
+        lap = fma2(fma2(m2, wc, sz), iz2, lap);
+        const unsigned long long res = sub2(rr, lap);
+        const float2 rf = up2(res);
+        const unsigned long long resm = pk2(act0 ? rf.x : 0.0f, act1 ? rf.y : 0.0f);
+        r2 = fma2(resm, resm, r2);
+        const float2 wn = up2(fma2(naf, res, wc));
+        if (act1) {
+          *reinterpret_cast<float2*>(out) = wn;
+        } else if (act0) {
+          out[0] = wn.x;
+        }
+        out += plane;
+        wm = wc;
+        wc = wp;
+      }
+    }
+    // partials of the two 32-wide tiles, block_sum_store's tree reproduced
+    const float2 rr2 = up2(r2);
+    double v0 = (double)rr2.x, v1 = (double)rr2.y;
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      v0 += __shfl_down_sync(0xffffffffu, v0, o);
+      v1 += __shfl_down_sync(0xffffffffu, v1, o);
+    }
+    if ((tx & 15) == 0) rows[tx >> 4][ty] = v0 + v1;
+    __syncthreads();
+    if (tid < 2) {
+      const int bx = 2 * bx2 + tid;
+      if (bx < gx) {
+        double sum = 0.0;
+        for (int q = 0; q < kTmaTy; ++q) sum += rows[tid][q];
+        partial[bx + (long long)gx * (by + (long long)gy * bz)] = sum;
+      }
+    }
+    __syncthreads();
+    if (STAGES == 1 && tid == 0 && tn < ntiles) tma2_issue_tile<ZC>(&tw, &tr, stages, mb0, tn, gx2, gy, w_zero);
+  }
+}
+
 // Periodic ghost refresh of U (CalcEpotential.f90:100-239 on one rank), in
 // z, y, x order over whole planes.
 __global__ void refresh_periodic_kernel(Stencil S, double* U, int axis) {
@@ -839,6 +1038,81 @@ int sweep_tma_occupancy(const JacobiGeom& G, int stages) {
     case 65: return occupancy_zs<16, 2>();
   }
   return 1;
+}
+
+template <int ZC, int STAGES>
+static cudaError_t launch_tma2_zs(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                                  float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
+  const size_t smem = STAGES * Tma2Stage<ZC>::kBytes;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e =
+        cudaFuncSetAttribute(sweep_tma2_kernel<ZC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int gx2 = (P.nx + kTma2Tile - 1) / kTma2Tile;
+  const int ntiles = gx2 * (int)G.grid.y * (int)G.grid.z;
+  const int ctas = G.ctas > 0 ? std::min(G.ctas, ntiles) : ntiles;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(kTmaTx, kTmaTy);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = G.pdl ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, sweep_tma2_kernel<ZC, STAGES>, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout,
+                            partial, w_zero, gx2, (int)G.grid.x, (int)G.grid.y, ntiles, err);
+}
+
+template <int ZC>
+static cudaError_t launch_tma2_zc(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                                  float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
+  return G.stages == 2 ? launch_tma2_zs<ZC, 2>(P, G, tw, tr, wout, partial, w_zero, err, st)
+                       : launch_tma2_zs<ZC, 1>(P, G, tw, tr, wout, partial, w_zero, err, st);
+}
+
+template <int ZC, int STAGES>
+static int occupancy2_zs() {
+  const size_t smem = STAGES * Tma2Stage<ZC>::kBytes;
+  if (cudaFuncSetAttribute(sweep_tma2_kernel<ZC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_tma2_kernel<ZC, STAGES>, kTmaTx * kTmaTy, smem) !=
+      cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+
+int sweep_tma2_occupancy(const JacobiGeom& G, int stages) {
+  switch (G.zc * 4 + (stages == 2 ? 1 : 0)) {
+    case 16: return occupancy2_zs<4, 1>();
+    case 17: return occupancy2_zs<4, 2>();
+    case 32: return occupancy2_zs<8, 1>();
+    case 33: return occupancy2_zs<8, 2>();
+    case 64: return occupancy2_zs<16, 1>();
+    case 65: return occupancy2_zs<16, 2>();
+  }
+  return 1;
+}
+
+int sweep_tma2_tiles(const KParams& P, const JacobiGeom& G) {
+  return ((P.nx + kTma2Tile - 1) / kTma2Tile) * (int)G.grid.y * (int)G.grid.z;
+}
+
+cudaError_t launch_sweep_tma2(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                              float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
+  switch (G.zc) {
+    case 4: return launch_tma2_zc<4>(P, G, tw, tr, wout, partial, w_zero, err, st);
+    case 8: return launch_tma2_zc<8>(P, G, tw, tr, wout, partial, w_zero, err, st);
+    case 16: return launch_tma2_zc<16>(P, G, tw, tr, wout, partial, w_zero, err, st);
+  }
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_sweep_tma(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,

@@ -27,6 +27,7 @@ struct JacobiGeom {
   int ctas = 0;
   int pdl = 1;
   int stages = 1;  // shared-memory stages per CTA (2: the next tile is prefetched)
+  int pairs = 0;   // 1: the x-pair kernel (64-wide tiles)
   // register-resident sweeps (jacobi_resident.cu): one cooperative launch per
   // batch of sweeps over CTAs of 32 x res_by x res_nz nodes
   int res = 0;
@@ -45,6 +46,13 @@ long long resident_face_floats(const JacobiGeom& G);
 cudaError_t launch_sweeps_resident(const KParams& P, const JacobiGeom& G, const float* r, const float* win,
                                    float* wout, float* faces, unsigned int* bar, double* partial, int m, int w_zero,
                                    int* err, cudaStream_t st);
+// The x-pair TMA sweep (64-wide tiles; w boxes 72 x 10 x zc+2, r boxes 64 x
+// 8 x zc): launch, occupancy and tile count.  Writes the same partials (in
+// the 32-wide tile layout) as launch_sweep_tma.
+cudaError_t launch_sweep_tma2(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                              float* wout, double* partial, int w_zero, int* err, cudaStream_t st);
+int sweep_tma2_occupancy(const JacobiGeom& G, int stages);
+int sweep_tma2_tiles(const KParams& P, const JacobiGeom& G);
 // CTAs of one SM the TMA sweep kernel of this geometry can hold.
 int sweep_tma_occupancy(const JacobiGeom& G, int stages);
 

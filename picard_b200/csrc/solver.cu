@@ -144,6 +144,9 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
   float* R[2] = {c->r, c->r + f32_elems(K)};  // anchor residuals, one per live anchor
   // sweep s reads w[(s-1)%2] (TMA descriptor tmw[(s-1)%2]) and R[rcur] (tmr[rcur])
   auto sweep = [&](long long s, int rsel, double* partial, int w_zero) -> cudaError_t {
+    if (c->G.tma && c->G.pairs)
+      return launch_sweep_tma2(K, c->G, &c->tmw2[(s - 1) % 2], &c->tmr2[rsel], c->w[s % 2], partial, w_zero,
+                               c->d_err, c->st);
     if (c->G.tma)
       return launch_sweep_tma(K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[rsel], c->w[s % 2], partial, w_zero, c->d_err,
                               c->st);
@@ -295,7 +298,8 @@ namespace picard {
 namespace {
 struct SweepShape {
   int ctas, pdl, stages;
-  int res;  // 0: TMA sweep kernel; q + 1: resident sweep with CTA shape q
+  int res;    // 0: TMA sweep kernel; q + 1: resident sweep with CTA shape q
+  int pairs;  // TMA sweep: 1 the x-pair kernel
 };
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, SweepShape> g_tuned;
@@ -304,6 +308,7 @@ int apply_shape(picard_ctx* c, const SweepShape& sh) {
   c->G.ctas = sh.ctas;
   c->G.pdl = sh.pdl;
   c->G.stages = sh.stages;
+  c->G.pairs = sh.pairs;
   c->G.res = 0;
   if (sh.res > 0) {
     if (!resident_plan(c->K, c->G, sh.res - 1)) return fail(PICARD_ERR_STATE, "resident sweep shape does not fit");
@@ -330,7 +335,7 @@ int set_resident(picard_ctx* c, int value) {
     return PICARD_OK;
   }
   if (!c->G.tma || !c->w[0]) return fail(PICARD_ERR_STATE, "resident sweeps need open boundaries and the F32_REFINE solver");
-  SweepShape sh{0, 0, 1, value};
+  SweepShape sh{0, 0, 1, value, 0};
   JacobiGeom g = c->G;
   if (!resident_plan(c->K, g, value - 1)) return fail(PICARD_ERR_STATE, "resident sweep shape does not fit the device");
   c->G.res = 0;
@@ -340,6 +345,7 @@ int set_resident(picard_ctx* c, int value) {
   sh.ctas = ctas;
   sh.pdl = pdl;
   sh.stages = stages;
+  sh.pairs = c->G.pairs;
   return apply_shape(c, sh);
 }
 
@@ -371,17 +377,21 @@ int tune_sweep(picard_ctx* c, bool fresh) {
   }
   int sms = 148;
   PICARD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  const int occ1 = sweep_tma_occupancy(c->G, 1), occ2 = sweep_tma_occupancy(c->G, 2);
   std::vector<SweepShape> cand;
-  for (int pdl = 1; pdl >= 0; --pdl) {
-    cand.push_back({0, pdl, 1, 0});  // one CTA per tile
-    for (int k = 1; k <= occ2; ++k)
-      if ((long long)k * sms < c->G.nblocks) cand.push_back({k * sms, pdl, 2, 0});
-    if ((long long)occ1 * sms < c->G.nblocks) cand.push_back({occ1 * sms, pdl, 1, 0});
+  for (int pairs = 0; pairs <= 1; ++pairs) {
+    const int occ1 = pairs ? sweep_tma2_occupancy(c->G, 1) : sweep_tma_occupancy(c->G, 1);
+    const int occ2 = pairs ? sweep_tma2_occupancy(c->G, 2) : sweep_tma_occupancy(c->G, 2);
+    const int tiles = pairs ? sweep_tma2_tiles(c->K, c->G) : c->G.nblocks;
+    for (int pdl = 1; pdl >= 0; --pdl) {
+      cand.push_back({0, pdl, 1, 0, pairs});  // one CTA per tile
+      for (int k = 1; k <= occ2; ++k)
+        if ((long long)k * sms < tiles) cand.push_back({k * sms, pdl, 2, 0, pairs});
+      if ((long long)occ1 * sms < tiles) cand.push_back({occ1 * sms, pdl, 1, 0, pairs});
+    }
   }
   for (int q = 0; q < kResidentShapes; ++q) {
     JacobiGeom g = c->G;
-    if (resident_plan(c->K, g, q)) cand.push_back({0, 0, 1, q + 1});
+    if (resident_plan(c->K, g, q)) cand.push_back({0, 0, 1, q + 1, 0});
   }
   constexpr int kReps = 24;
   std::vector<float> best(cand.size(), 1e30f);
@@ -399,13 +409,15 @@ int tune_sweep(picard_ctx* c, bool fresh) {
         PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
         PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
       } else {
-        for (int s = 1; s <= 2; ++s)
-          PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
-                                       c->d_err, c->st));
+        auto one = [&](int s) {
+          return c->G.pairs ? launch_sweep_tma2(c->K, c->G, &c->tmw2[(s - 1) % 2], &c->tmr2[0], c->w[s % 2],
+                                                c->partials, 0, c->d_err, c->st)
+                            : launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2],
+                                               c->partials, 0, c->d_err, c->st);
+        };
+        for (int s = 1; s <= 2; ++s) PICARD_CUDA(one(s));
         PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
-        for (int s = 1; s <= kReps; ++s)
-          PICARD_CUDA(launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2], c->partials, 0,
-                                       c->d_err, c->st));
+        for (int s = 1; s <= kReps; ++s) PICARD_CUDA(one(s));
         PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
         PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
       }
@@ -423,9 +435,9 @@ int tune_sweep(picard_ctx* c, bool fresh) {
         std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: resident shape %d  %.3f us%s\n", c->K.nx, c->K.ny,
                      c->K.nz, c->G.zc, cand[q].res - 1, best[q] * 1e3, q == pick ? "  <- picked" : "");
       else
-        std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: ctas=%d pdl=%d stages=%d  %.3f us%s\n", c->K.nx,
-                     c->K.ny, c->K.nz, c->G.zc, cand[q].ctas, cand[q].pdl, cand[q].stages, best[q] * 1e3,
-                     q == pick ? "  <- picked" : "");
+        std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: pairs=%d ctas=%d pdl=%d stages=%d  %.3f us%s\n",
+                     c->K.nx, c->K.ny, c->K.nz, c->G.zc, cand[q].pairs, cand[q].ctas, cand[q].pdl, cand[q].stages,
+                     best[q] * 1e3, q == pick ? "  <- picked" : "");
     }
   }
   PICARD_TRY(apply(cand[pick]));
