@@ -18,12 +18,13 @@
 // rounding only accumulates over short runs.  A reduction kernel sums the
 // per-CTA partials in a fixed order.
 //
-// Operands are built by the CTA's threads in shared memory in the canonical
-// K-major no-swizzle layout of tcgen05 (8-row x 16-byte core matrices):
-// element (r, k) of a tile with R rows lives at byte
-//   (k / 8) * (R * 16) + (r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2,
-// i.e. leading-byte offset R * 16 between the two K core matrices of an
-// instruction and stride-byte offset 128 between 8-row groups.
+// Operands sit in shared memory in the canonical K-major no-swizzle layout of
+// tcgen05 (8-row x 16-byte core matrices) with rows 16 bytes apart
+// throughout: element (r, k) of an operand whose K blocks are L bytes apart
+// lives at byte (k / 8) * L + r * 16 + (k % 8) * 2, i.e. leading-byte offset L
+// between the two K core matrices of an instruction and stride-byte offset
+// 128 between 8-row groups.  Uniform 16-byte rows let a row shift be a plain
+// change of the descriptor's start address (see the kernel).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -44,10 +45,6 @@ constexpr int kTcThreads = 128;
 constexpr int kFlushChunks = 8;    // K-chunks between FP64 folds of the accumulator
 constexpr long long kTcSpin = 1LL << 26;
 
-constexpr int kAsplit = kTcM * kTcKC;  // bf16 elements of one A split
-constexpr int kBsplit = kTcN * kTcKC;  // bf16 elements of one B split
-constexpr int kWinPad = 64;            // zero padding on both sides of a D window
-
 struct TcAxis {
   int axis;        // normal axis
   int n1, n2, nn;  // in-plane extents (p1, p2) and normal extent
@@ -59,11 +56,6 @@ __device__ inline uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) 
   return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
-
-// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
-// K-major, M = 128, N = 256.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
-                            ((uint32_t)(kTcM >> 4) << 24);
 
 __device__ inline void split3(float x, __nv_bfloat16& a, __nv_bfloat16& b, __nv_bfloat16& c) {
   a = __float2bfloat16_rn(x);
@@ -123,31 +115,66 @@ __device__ inline long long d_index(const KParams& P, const TcAxis& X, int f, in
   return (long long)(a - 1) + DX * ((long long)(b - 1) + DY * (long long)(c - 1));
 }
 
+// ----------------------------------------------------------------- kernel
+//
+// Per step (q, d, K-chunk kc) the CTA issues, for each face f, the six split
+// products of
+//   Acc_f[r][n'] += sum_k A[r][k] B_f[n'][k],   k = q2 - 1 - k0 in [0, 64),
+// with A[r][k] = C(q, m0 + r + d, q2) and B_f[n'][k] = W_f(q2 - p2), where the
+// output columns are stored reversed, n' = 127 - (p2 - 1 - n0).  Then
+//   q2 - p2 = o_min + k + n',   o_min = k0 - n0 - 127,
+// so B_f is a sliding window: with Z[u] = (w[u], ..., w[u+7]) (16 bytes, w[j] =
+// W_f(o_min + j)), element (n', k) is Z[n' + 8 floor(k/8)][k mod 8], i.e. a
+// K-major no-swizzle operand with rows 16 bytes apart and both core-matrix
+// strides 128 bytes.  A is read from a tall buffer T holding rows m0 + dA ..
+// m0 + dA + 256 of plane q (K-major, rows 16 bytes apart, the eight K blocks
+// kRT * 16 bytes apart): shift d starts (d - dA) * 16 bytes further in.  T is
+// loaded (cp.async, zero-filled outside the face) once per run of up to kDB
+// consecutive shifts; Z is rebuilt per step from a 191-value window of D,
+// double buffered so that the MMAs of one step overlap the build of the next,
+// and the D values of the next step are prefetched into registers.
+constexpr int kDB = 128;            // shifts served by one T buffer
+constexpr int kRT = 257;            // T rows (>= kDB + 127; odd multiple of 16 B keeps cp.async conflict-free)
+constexpr int kZN = 184;            // Z entries per (face, split): n' + 8 floor(k/8) <= 127 + 56
+constexpr int kWL = 192;            // window values per (face, split) (191 used)
+constexpr int kWUsed = 191;
+constexpr size_t kTSplit = (size_t)8 * kRT * 16;     // bytes of one split of T
+constexpr size_t kZFS = (size_t)kZN * 16;            // bytes of one (face, split) Z array
+constexpr size_t kSmemT = 3 * kTSplit;
+constexpr size_t kSmemZ = 2 * 2 * 3 * kZFS;          // [buf][face][split]
+constexpr size_t kSmemW = (size_t)2 * 3 * kWL * 2;   // [face][split][kWL] bf16
+constexpr size_t kTcSmem = kSmemT + kSmemZ + kSmemW;
+// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
+// K-major, M = 128, N = 128 (one face per instruction).
+constexpr uint32_t kIdescFace = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcHalfN >> 3) << 17) |
+                                ((uint32_t)(kTcM >> 4) << 24);
+constexpr int kPrefetch = 3;  // D values per thread per step (2 * 191 <= 3 * 128)
+
 __global__ void __launch_bounds__(kTcThreads, 1)
     bcpot_tc_kernel(KParams P, TcAxis X, const __nv_bfloat16* __restrict__ Cs, const double* __restrict__ D,
                     double* partial, int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(smem);                  // [3][kAsplit]
-  __nv_bfloat16* sB = sA + 3 * kAsplit;                                          // [3][kBsplit]
-  __nv_bfloat16* sW = sB + 3 * kBsplit;                                          // [2][3][2*n2+2*pad]
-  __shared__ __align__(8) unsigned long long mbar;
+  unsigned char* sT = smem;                   // [3][8][kRT][16 B]
+  unsigned char* sZ = smem + kSmemT;          // [2][2][3][kZN][16 B]
+  __nv_bfloat16* sWin = reinterpret_cast<__nv_bfloat16*>(smem + kSmemT + kSmemZ);  // [2][3][kWL]
+  __shared__ __align__(8) unsigned long long mbar[2];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int wlen = 2 * X.n2 - 1 + 2 * kWinPad;
 
-  // tile and slice of (q, d) pairs of this CTA
   const int tile = blockIdx.x / X.splits, split = blockIdx.x % X.splits;
   const int mt = tile / X.ntiles, nt = tile % X.ntiles;
   const int m0 = mt * kTcM, n0 = nt * kTcHalfN;
-  // shifts d = q1 - p1 with at least one valid row (q1, p1 both in [1, n1])
   const int rows_hi = (m0 + kTcM < X.n1) ? m0 + kTcM : X.n1;
   const int dlo = 1 - rows_hi, dhi = X.n1 - m0 - 1;
-  const long long npairs = (long long)X.nn * (dhi - dlo + 1);
+  const int nd = dhi - dlo + 1;
+  const long long npairs = (long long)X.nn * nd;
   const long long pbeg = npairs * split / X.splits, pend = npairs * (split + 1) / X.splits;
   const int nchunks = X.n2pad / kTcKC;
+  const long long per = (long long)X.nn * X.n1 * X.n2pad;  // elements of one split of Cs
   double* part = partial + (long long)blockIdx.x * kTcM * kTcN;
 
-  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  const uint32_t mb0 = (uint32_t)__cvta_generic_to_shared(&mbar[0]);
+  const uint32_t mb1 = (uint32_t)__cvta_generic_to_shared(&mbar[1]);
   if (warp == 0) {
     uint32_t dst = (uint32_t)__cvta_generic_to_shared(&tmem_base);
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTcN)
@@ -155,7 +182,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int e = tid; e < kTcM * kTcN; e += kTcThreads) part[e] = 0.0;
@@ -163,21 +191,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  uint32_t phase = 0;
-  bool pending = false;   // MMAs committed and not yet waited for
-  int since_flush = 0;    // chunks accumulated in TMEM
+  uint32_t phase[2] = {0, 0};
+  bool pending[2] = {false, false};
+  int since_flush = 0;
   bool ok = true;
 
-  auto wait_mma = [&]() -> bool {
-    if (!pending) return true;
-    bool r = mbar_wait_tc(mb, phase);
-    phase ^= 1;
-    pending = false;
+  auto wait_buf = [&](int b) -> bool {
+    if (!pending[b]) return true;
+    bool r = mbar_wait_tc(b ? mb1 : mb0, phase[b]);
+    phase[b] ^= 1;
+    pending[b] = false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     return r;
   };
-  // fold the FP32 accumulator into the FP64 partial (each thread owns row
-  // 32*warp + lane of the tile: TMEM lane = row)
+  auto drain = [&]() -> bool {
+    bool a = wait_buf(0);
+    bool b = wait_buf(1);
+    return a && b;
+  };
+  // fold the FP32 accumulator into the FP64 partial (thread = TMEM lane =
+  // tile row); TMEM column f*128 + n' is partial column f*128 + 127 - n'
   auto flush = [&]() {
     for (int col = 0; col < kTcN; col += 16) {
       uint32_t r[16];
@@ -188,114 +221,159 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
           : "r"(addr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      double* row = part + (long long)(32 * warp + lane) * kTcN + col;
+      const int f = col / kTcHalfN, nbase = col % kTcHalfN;
+      double* row = part + (long long)(32 * warp + lane) * kTcN + f * kTcHalfN;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) row[j] += (double)__uint_as_float(r[j]);
+      for (int j = 0; j < 16; ++j) row[kTcHalfN - 1 - (nbase + j)] += (double)__uint_as_float(r[j]);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   };
 
-  for (long long pr = pbeg; pr < pend && ok; ++pr) {
-    const int q = int(pr / (dhi - dlo + 1)) + 1;
-    const int d = dlo + int(pr % (dhi - dlo + 1));
-    // previous MMAs read sW / sA / sB: wait before rewriting them
-    if (!wait_mma()) { ok = false; break; }
-    __syncthreads();
-    // D windows of both faces: index o2 + n2 - 1 + pad, o2 in [-(n2-1), n2-1]
-    for (int e = tid; e < 2 * wlen; e += kTcThreads) {
-      int f = e / wlen, w = e % wlen;
-      int o2 = w - kWinPad - (X.n2 - 1);
-      float v = 0.0f;
-      if (o2 >= -(X.n2 - 1) && o2 <= X.n2 - 1) v = (float)D[d_index(P, X, f, q, d, o2)];
-      __nv_bfloat16 a, b, c;
-      split3(v, a, b, c);
-      sW[(f * 3 + 0) * wlen + w] = a;
-      sW[(f * 3 + 1) * wlen + w] = b;
-      sW[(f * 3 + 2) * wlen + w] = c;
+  // D values of one step into registers: item e = tid + 128 m -> face e / 191,
+  // window index e % 191
+  double pre[kPrefetch];
+  auto prefetch = [&](int q, int d, int kc) {
+    const int o_min = kc * kTcKC - n0 - (kTcHalfN - 1);
+#pragma unroll
+    for (int m = 0; m < kPrefetch; ++m) {
+      const int e = tid + kTcThreads * m;
+      double v = 0.0;
+      if (e < 2 * kWUsed) {
+        const int f = e / kWUsed, j = e % kWUsed;
+        const int o2 = o_min + j;
+        if (o2 >= -(X.n2 - 1) && o2 <= X.n2 - 1) v = __ldg(D + d_index(P, X, f, q, d, o2));
+      }
+      pre[m] = v;
     }
-    __syncthreads();
-    for (int kc = 0; kc < nchunks && ok; ++kc) {
-      if (kc > 0) {
-        if (!wait_mma()) { ok = false; break; }
+  };
+  auto step_of = [&](int kc, long long pr, int& q, int& d) {
+    q = int(pr / nd) + 1;
+    d = dlo + int(pr % nd);
+    (void)kc;
+  };
+
+  int step = 0;
+  if (pbeg < pend) {
+    int q, d;
+    step_of(0, pbeg, q, d);
+    prefetch(q, d, 0);
+  }
+  for (int kc = 0; kc < nchunks && ok; ++kc) {
+    const int k0 = kc * kTcKC;
+    int Tq = -1, TdA = 0;
+    for (long long pr = pbeg; pr < pend && ok; ++pr) {
+      int q, d;
+      step_of(kc, pr, q, d);
+      if (q != Tq || d >= TdA + kDB) {
+        // every MMA that reads T is done before T is rewritten
+        if (!__syncthreads_and(drain() ? 1 : 0)) { ok = false; break; }
+        Tq = q;
+        TdA = d;
+        const int rho0 = m0 + TdA;
+        const uint32_t tbase = (uint32_t)__cvta_generic_to_shared(sT);
+        for (int e = tid; e < 3 * kRT * 8; e += kTcThreads) {
+          const int kb = e & 7, rest = e >> 3;
+          const int t = rest % kRT, sp = rest / kRT;
+          const int rho = rho0 + t;
+          const bool in = rho >= 0 && rho < X.n1;
+          const __nv_bfloat16* g =
+              in ? Cs + sp * per + ((long long)(q - 1) * X.n1 + rho) * X.n2pad + k0 + kb * 8 : Cs;
+          const uint32_t dst = tbase + (uint32_t)(sp * kTSplit + (size_t)kb * kRT * 16 + (size_t)t * 16);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(g), "r"(in ? 16 : 0)
+                       : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
       }
-      const int k0 = kc * kTcKC;
-      // A: rows r = p1 - 1 - m0, source row p1 + d - 1 of plane q
-      for (int e = tid; e < 3 * kTcM * (kTcKC / 8); e += kTcThreads) {
-        int s = e / (kTcM * (kTcKC / 8)), rem = e % (kTcM * (kTcKC / 8));
-        int r = rem / (kTcKC / 8), c8 = rem % (kTcKC / 8);
-        int src = m0 + r + d;  // 0-based source row
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (src >= 0 && src < X.n1 && m0 + r < X.n1) {
-          long long per = (long long)X.nn * X.n1 * X.n2pad;
-          const __nv_bfloat16* g = Cs + s * per + ((long long)(q - 1) * X.n1 + src) * X.n2pad + k0 + c8 * 8;
-          v = *reinterpret_cast<const uint4*>(g);
-        }
-        unsigned char* dst = reinterpret_cast<unsigned char*>(sA + s * kAsplit) + c8 * (kTcM * 16) +
-                             (r >> 3) * 128 + (r & 7) * 16;
-        *reinterpret_cast<uint4*>(dst) = v;
-      }
-      // B: column n = f * 128 + p (p2 = n0 + p + 1), k -> q2 = k0 + k + 1
-      for (int e = tid; e < 3 * kTcN * (kTcKC / 8); e += kTcThreads) {
-        int s = e / (kTcN * (kTcKC / 8)), rem = e % (kTcN * (kTcKC / 8));
-        int n = rem / (kTcKC / 8), c8 = rem % (kTcKC / 8);
-        int f = n / kTcHalfN, p = n % kTcHalfN;
-        int p2 = n0 + p + 1;
-        __align__(16) __nv_bfloat16 v[8];
-        const __nv_bfloat16* win = sW + (f * 3 + s) * wlen;
+      const int b = step & 1;
+      // the MMAs of step - 2 read Z[b]
+      if (!__syncthreads_and(wait_buf(b) ? 1 : 0)) { ok = false; break; }
+      // window of this step from the prefetched D values
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          int q2 = k0 + c8 * 8 + j + 1;
-          bool valid = q2 <= X.n2 && p2 <= X.n2;
-          int w = q2 - p2 + (X.n2 - 1) + kWinPad;
-          v[j] = valid ? win[w] : __float2bfloat16_rn(0.0f);
+      for (int m = 0; m < kPrefetch; ++m) {
+        const int e = tid + kTcThreads * m;
+        if (e < 2 * kWUsed) {
+          const int f = e / kWUsed, j = e % kWUsed;
+          __nv_bfloat16 a0, a1, a2;
+          split3((float)pre[m], a0, a1, a2);
+          sWin[(f * 3 + 0) * kWL + j] = a0;
+          sWin[(f * 3 + 1) * kWL + j] = a1;
+          sWin[(f * 3 + 2) * kWL + j] = a2;
         }
-        unsigned char* dst = reinterpret_cast<unsigned char*>(sB + s * kBsplit) + c8 * (kTcN * 16) +
-                             (n >> 3) * 128 + (n & 7) * 16;
-        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
+      }
+      if (tid < 6) sWin[tid * kWL + kWUsed] = __float2bfloat16_rn(0.0f);
+      __syncthreads();
+      // Z[b][f][s][u] = w[u .. u+7]
+      unsigned char* zb = sZ + (size_t)b * 2 * 3 * kZFS;
+      for (int e = tid; e < 6 * kZN; e += kTcThreads) {
+        const int fs = e / kZN, u = e % kZN;
+        const __nv_bfloat16* w = sWin + fs * kWL + u;
+        __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = w[j];
+        *reinterpret_cast<uint4*>(zb + (size_t)fs * kZFS + (size_t)u * 16) = *reinterpret_cast<const uint4*>(v);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t aBase = (uint32_t)__cvta_generic_to_shared(sA);
-        const uint32_t bBase = (uint32_t)__cvta_generic_to_shared(sB);
+        const uint32_t tb = (uint32_t)__cvta_generic_to_shared(sT) + (uint32_t)(d - TdA) * 16u;
+        const uint32_t zs = (uint32_t)__cvta_generic_to_shared(zb);
         const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
 #pragma unroll
-        for (int ks = 0; ks < kTcKC / 16; ++ks) {
+        for (int f = 0; f < 2; ++f) {
 #pragma unroll
-          for (int t = 0; t < 6; ++t) {
-            uint32_t a_addr = aBase + pa[t] * kAsplit * 2 + ks * 2 * (kTcM * 16);
-            uint32_t b_addr = bBase + pb[t] * kBsplit * 2 + ks * 2 * (kTcN * 16);
-            uint64_t adesc = smem_desc(a_addr, kTcM * 16, 128);
-            uint64_t bdesc = smem_desc(b_addr, kTcN * 16, 128);
-            uint32_t acc = (since_flush == 0 && ks == 0 && t == 0) ? 0u : 1u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                ::"r"(tmem), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(acc)
-                : "memory");
+          for (int ks = 0; ks < kTcKC / 16; ++ks) {
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+              const uint32_t a_addr = tb + (uint32_t)(pa[t] * kTSplit + (size_t)(2 * ks) * kRT * 16);
+              const uint32_t b_addr = zs + (uint32_t)((f * 3 + pb[t]) * kZFS + ks * 256);
+              const uint64_t adesc = smem_desc(a_addr, kRT * 16, 128);
+              const uint64_t bdesc = smem_desc(b_addr, 128, 128);
+              const uint32_t acc = (since_flush == 0 && ks == 0 && t == 0) ? 0u : 1u;
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\t"
+                  "setp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                  ::"r"(tmem + (uint32_t)(f * kTcHalfN)), "l"(adesc), "l"(bdesc), "r"(kIdescFace), "r"(acc)
+                  : "memory");
+            }
           }
         }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b ? mb1 : mb0)
                      : "memory");
       }
-      pending = true;
-      ++since_flush;
-      if (since_flush == kFlushChunks) {
-        if (!wait_mma()) { ok = false; break; }
+      pending[b] = true;
+      ++step;
+      // D values of the next step
+      {
+        long long npr = pr + 1;
+        int nkc = kc;
+        if (npr >= pend) {
+          npr = pbeg;
+          ++nkc;
+        }
+        if (nkc < nchunks) {
+          int nq, ndd;
+          step_of(nkc, npr, nq, ndd);
+          prefetch(nq, ndd, nkc);
+        }
+      }
+      if (++since_flush == kFlushChunks) {
+        if (!__syncthreads_and(drain() ? 1 : 0)) { ok = false; break; }
         flush();
         __syncthreads();
         since_flush = 0;
       }
     }
   }
-  if (ok && !wait_mma()) ok = false;
+  if (ok && !__syncthreads_and(drain() ? 1 : 0)) ok = false;
   if (ok && since_flush > 0) flush();
   if (!ok) {
     if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
-    wait_mma();  // bounded: let outstanding MMAs finish before TMEM is released
+    drain();  // bounded: let outstanding MMAs finish before TMEM is released
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -347,8 +425,8 @@ TcAxis tc_axis(const KParams& P, int axis, int sms) {
 }  // namespace
 
 size_t bcpot_tc_smem_bytes(const KParams& P) {
-  int n2max = P.nx > P.ny ? (P.nx > P.nz ? P.nx : P.nz) : (P.ny > P.nz ? P.ny : P.nz);
-  return (size_t)(3 * kAsplit + 3 * kBsplit) * 2 + (size_t)2 * 3 * (2 * n2max - 1 + 2 * kWinPad) * 2 + 16;
+  (void)P;
+  return kTcSmem;
 }
 
 void bcpot_tc_scratch(const KParams& P, long long* cs_elems, long long* partial_elems) {
