@@ -143,7 +143,9 @@ constexpr size_t kZFS = (size_t)kZN * 16;            // bytes of one (face, spli
 constexpr size_t kSmemT = 3 * kTSplit;
 constexpr size_t kSmemZ = 2 * 2 * 3 * kZFS;          // [buf][face][split]
 constexpr size_t kSmemW = (size_t)2 * 3 * kWL * 2;   // [face][split][kWL] bf16
-constexpr size_t kTcSmem = kSmemT + kSmemZ + kSmemW;
+constexpr size_t kSmemX = (size_t)4 * 32 * 33 * 8;   // per-warp 32 x 32 FP64 transpose tiles
+constexpr size_t kTcSmem = kSmemT + kSmemZ + kSmemW + kSmemX;
+constexpr int kFoldsPerFlush = 16;  // on-chip folds between FP64 flushes
 // kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
 // K-major, M = 128, N = 128 (one face per instruction).
 constexpr uint32_t kIdescFace = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcHalfN >> 3) << 17) |
@@ -157,6 +159,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   unsigned char* sT = smem;                   // [3][8][kRT][16 B]
   unsigned char* sZ = smem + kSmemT;          // [2][2][3][kZN][16 B]
   __nv_bfloat16* sWin = reinterpret_cast<__nv_bfloat16*>(smem + kSmemT + kSmemZ);  // [2][3][kWL]
+  double* sX = reinterpret_cast<double*>(smem + kSmemT + kSmemZ + kSmemW);         // [4][32][33]
   __shared__ __align__(8) unsigned long long mbar[2];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -177,7 +180,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t mb1 = (uint32_t)__cvta_generic_to_shared(&mbar[1]);
   if (warp == 0) {
     uint32_t dst = (uint32_t)__cvta_generic_to_shared(&tmem_base);
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTcN)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(2 * kTcN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -209,24 +212,78 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     bool b = wait_buf(1);
     return a && b;
   };
-  // fold the FP32 accumulator into the FP64 partial (thread = TMEM lane =
-  // tile row); TMEM column f*128 + n' is partial column f*128 + 127 - n'
-  auto flush = [&]() {
+  // Two on-chip levels before FP64.  The MMAs accumulate a segment of
+  // kFlushChunks steps in TMEM columns [0, 256); fold() adds it (FP32) into
+  // a running sum in columns [256, 512) and is cheap (TMEM loads and stores
+  // only); every kFoldsPerFlush folds flush64() adds the running sum into the
+  // CTA's FP64 partial, staged through a per-warp shared-memory transpose so
+  // that the global read-modify-writes are coalesced.  Thread = TMEM lane =
+  // tile row; TMEM column f*128 + n' is partial column f*128 + 127 - n'.
+  int folds = 0;
+  auto fold = [&]() {
     for (int col = 0; col < kTcN; col += 16) {
-      uint32_t r[16];
-      uint32_t addr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)col;
+      uint32_t a[16], r[16];
+      const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7]),
+            "=r"(a[8]), "=r"(a[9]), "=r"(a[10]), "=r"(a[11]), "=r"(a[12]), "=r"(a[13]), "=r"(a[14]), "=r"(a[15])
+          : "r"(lanebase + (uint32_t)col));
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(lanebase + (uint32_t)(kTcN + col)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const float sum = folds == 0 ? __uint_as_float(a[j]) : __fadd_rn(__uint_as_float(r[j]), __uint_as_float(a[j]));
+        r[j] = __float_as_uint(sum);
+      }
+      asm volatile(
+          "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+          ::"r"(lanebase + (uint32_t)(kTcN + col)), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]),
+            "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]),
+            "r"(r[14]), "r"(r[15])
+          : "memory");
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    ++folds;
+  };
+  auto flush64 = [&]() {
+    double* X = sX + warp * 32 * 33;
+    for (int col = 0; col < kTcN; col += 32) {
+      uint32_t r[32];
+      const uint32_t addr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(kTcN + col);
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
           : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
             "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
           : "r"(addr));
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(addr + 16u));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      const int f = col / kTcHalfN, nbase = col % kTcHalfN;
-      double* row = part + (long long)(32 * warp + lane) * kTcN + f * kTcHalfN;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) row[kTcHalfN - 1 - (nbase + j)] += (double)__uint_as_float(r[j]);
+      for (int j = 0; j < 32; ++j) X[lane * 33 + j] = (double)__uint_as_float(r[j]);
+      __syncwarp();
+      // lane = TMEM column col + lane, i.e. partial column f*128 + 127 - n'
+      const int f = col / kTcHalfN, nprime = col % kTcHalfN + lane;
+      for (int rr = 0; rr < 32; ++rr) {
+        double* g = part + (long long)(32 * warp + rr) * kTcN + f * kTcHalfN + (kTcHalfN - 1 - nprime);
+        *g += X[rr * 33 + lane];
+      }
+      __syncwarp();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    folds = 0;
+  };
+  auto flush = [&]() {
+    fold();
+    if (folds == kFoldsPerFlush) flush64();
   };
 
   // D values of one step into registers: item e = tid + 128 m -> face e / 191,
@@ -370,7 +427,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   }
   if (ok && !__syncthreads_and(drain() ? 1 : 0)) ok = false;
-  if (ok && since_flush > 0) flush();
+  if (ok && since_flush > 0) fold();
+  if (ok && folds > 0) flush64();
   if (!ok) {
     if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
     drain();  // bounded: let outstanding MMAs finish before TMEM is released
@@ -379,9 +437,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTcN) : "memory");
   }
 }
+
 
 // U on both faces of the axis = (sum over splits of the partial tiles) / (4 pi eps0).
 __global__ void bcpot_reduce_kernel(KParams P, TcAxis X, const double* partial, double* U) {
