@@ -46,7 +46,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["picard", "reference"], default="picard")
-    ap.add_argument("--workload", choices=["scale", "plain32", "poisson", "serving"], default="scale")
+    ap.add_argument("--workload", choices=["scale", "plain32", "poisson", "serving", "precision"], default="scale")
+    ap.add_argument("--precision-n", type=int, default=512, help="precision workload: box edge in cells")
+    ap.add_argument("--precision-sweeps", type=int, default=4001, help="precision workload: Jacobi sweeps compared")
     ap.add_argument("--requests", type=int, default=12, help="serving workload: runs in the arrival stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serving workload: mean arrivals per second")
     ap.add_argument("--run-steps", type=int, default=200, help="serving workload: iterations per run")
@@ -514,6 +516,83 @@ def run_serving(args, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_precision(args, local_rank):
+    """Precision study on an n^3 open box (default 512^3) with the blob charge
+    (32 Gaussian blobs, sigma 4..16 cells, N(0,1) e per cell, 1% noise):
+      boundary: the tensor-core BCpotentials (three-way BF16 split, FP32
+                accumulation in TMEM folded on chip, FP64 partials) against the
+                FP64 direct sum, over every face node (the full product, no
+                coarsening of the charge);
+      jacobi:   FP32 sweeps of the increment with FP64 anchors against all-FP64
+                sweeps, the same number of sweeps from the same FP64 boundary
+                potential;
+      end to end: tensor-core boundary + FP32/FP64 Jacobi against FP64 boundary
+                + FP64 Jacobi.
+    Errors are relative L2 over the nodes compared, and the largest pointwise
+    error relative to the largest |U|."""
+    import numpy as np
+    import torch
+
+    from picard_b200 import capi
+    from picard_b200 import params as P
+    from picard_b200.simulation import Simulation
+
+    torch.cuda.set_device(local_rank)
+    n = args.precision_n
+    p = P.config_plain_32(n=n, ppc=1, capacity=1024)
+    C = blob_charge(n, seed=0)
+    maxit = max(1, (args.precision_sweeps - 1) // 2)
+
+    def rel(a, b, mask=None):
+        if mask is not None:
+            a, b = a[mask], b[mask]
+        d = float(np.linalg.norm((a - b).ravel()))
+        return {"rel_l2": d / max(float(np.linalg.norm(b.ravel())), 1e-300),
+                "max_rel": float(np.abs(a - b).max()) / max(float(np.abs(b).max()), 1e-300)}
+
+    def timed(fn, stream):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    out = {"workload": f"precision {n}^3 open box, blob charge", "sweeps_compared": 2 * maxit + 1}
+    g64 = Simulation(p, layout=capi.LAYOUT_F64, solver=capi.SOLVER_F64)
+    s64 = torch.cuda.ExternalStream(g64.stream_handle)
+    g64.calc_distance()
+    g64.set_field(capi.FIELD_C, C)
+    g64.set_option(capi.OPT_BCPOT_TENSOR, 0)
+    out["bcpot_fp64_ms"] = timed(g64.bc_potentials, s64)
+    Ub64 = g64.field(capi.FIELD_U)
+    g64.set_option(capi.OPT_BCPOT_TENSOR, 1)
+    out["bcpot_tensor_ms"] = timed(g64.bc_potentials, s64)
+    Ubtc = g64.field(capi.FIELD_U)
+    face = Ub64 != 0.0
+    out["boundary"] = rel(Ubtc, Ub64, face)
+    out["face_nodes"] = int(face.sum())
+    # FP64 Jacobi from the FP64 boundary potential
+    g64.set_field(capi.FIELD_U, Ub64)
+    out["jacobi_fp64_ms"] = timed(lambda: g64.calc_epotential(maxerr=1e-300, maxit=maxit), s64)
+    U64 = g64.field(capi.FIELD_U)
+    g64.close()
+    g32 = Simulation(p, layout=capi.LAYOUT_F64, solver=capi.SOLVER_F32_REFINE)
+    s32 = torch.cuda.ExternalStream(g32.stream_handle)
+    g32.set_field(capi.FIELD_C, C)
+    g32.set_field(capi.FIELD_U, Ub64)
+    out["jacobi_fp32_refine_ms"] = timed(lambda: g32.calc_epotential(maxerr=1e-300, maxit=maxit), s32)
+    U32 = g32.field(capi.FIELD_U)
+    out["jacobi"] = rel(U32, U64)
+    g32.set_field(capi.FIELD_U, Ubtc)
+    g32.calc_epotential(maxerr=1e-300, maxit=maxit)
+    Ue2e = g32.field(capi.FIELD_U)
+    out["end_to_end"] = rel(Ue2e, U64)
+    g32.close()
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -542,6 +621,10 @@ def main():
         return
     if args.workload == "poisson":
         run_poisson(args, local_rank)
+        return
+    if args.workload == "precision":
+        if rank == 0:
+            run_precision(args, local_rank)
         return
     if args.workload == "serving":
         if rank == 0:
