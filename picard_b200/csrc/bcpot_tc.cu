@@ -7,16 +7,16 @@
 // where f = 0, 1 are the two faces of the axis (they differ only in the normal
 // offset of D).  For a fixed plane q and row shift d = q1 - p1 this is a GEMM
 //   U_f(p1, :) += C(q, p1 + d, :) . T_{q,d,f},  T[q2, p2] = D_f(q, d, q2 - p2)
-// (T is Toeplitz).  A CTA owns a 128 x 256 output tile -- 128 rows p1, and
-// 128 columns p2 of each face side by side -- and accumulates it in tensor
-// memory over a slice of the (q, d) pairs (split-K over all SMs).
+// (T is Toeplitz).  A CTA owns one face of a 128 x 128 output tile -- 128
+// rows p1 by 128 columns p2 -- and accumulates it in tensor memory over a
+// slice of the (q, d) pairs (split-K over all SMs).
 //
 // Precision: every FP64 operand is split into three BF16 parts
 // (x = x1 + x2 + x3, 24 significant bits) and each K-step issues the six
-// products x_i y_j with i + j <= 4.  The FP32 accumulator in TMEM is folded
-// into an FP64 partial of the CTA every kFlushChunks K-chunks, so FP32
-// rounding only accumulates over short runs.  A reduction kernel sums the
-// per-CTA partials in a fixed order.
+// products x_i y_j with i + j <= 4.  Each FP32 MMA accumulation spans one
+// step (128 K-values); the steps are summed in tensor memory with Kahan
+// compensation, and the CTA's result goes out once as FP64.  A reduction
+// kernel sums the per-CTA partials in a fixed order.
 //
 // Operands sit in shared memory in the canonical K-major no-swizzle layout of
 // tcgen05 (8-row x 16-byte core matrices) with rows 16 bytes apart
@@ -40,9 +40,8 @@ namespace {
 constexpr int kTcM = 128;          // rows p1 per tile
 constexpr int kTcHalfN = 128;      // columns p2 per face
 constexpr int kTcN = 2 * kTcHalfN; // both faces
-constexpr int kTcKC = 64;          // K (q2) per chunk
+constexpr int kTcKC = 128;         // K (q2) per chunk
 constexpr int kTcThreads = 128;
-constexpr int kFlushChunks = 8;    // K-chunks between FP64 folds of the accumulator
 constexpr long long kTcSpin = 1LL << 26;
 
 struct TcAxis {
@@ -117,54 +116,80 @@ __device__ inline long long d_index(const KParams& P, const TcAxis& X, int f, in
 
 // ----------------------------------------------------------------- kernel
 //
-// Per step (q, d, K-chunk kc) the CTA issues, for each face f, the six split
-// products of
-//   Acc_f[r][n'] += sum_k A[r][k] B_f[n'][k],   k = q2 - 1 - k0 in [0, 64),
-// with A[r][k] = C(q, m0 + r + d, q2) and B_f[n'][k] = W_f(q2 - p2), where the
+// A CTA owns one face f of a 128 x 128 output tile and a slice of the (q, d)
+// pairs.  Per step (q, d, K-chunk kc) it issues the six split products of
+//   Acc[r][n'] += sum_k A[r][k] B[n'][k],   k = q2 - 1 - k0 in [0, 128),
+// with A[r][k] = C(q, m0 + r + d, q2) and B[n'][k] = W_f(q2 - p2), where the
 // output columns are stored reversed, n' = 127 - (p2 - 1 - n0).  Then
 //   q2 - p2 = o_min + k + n',   o_min = k0 - n0 - 127,
-// so B_f is a sliding window: with Z[u] = (w[u], ..., w[u+7]) (16 bytes, w[j] =
+// so B is a sliding window: with Z[u] = (w[u], ..., w[u+7]) (16 bytes, w[j] =
 // W_f(o_min + j)), element (n', k) is Z[n' + 8 floor(k/8)][k mod 8], i.e. a
 // K-major no-swizzle operand with rows 16 bytes apart and both core-matrix
 // strides 128 bytes.  A is read from a tall buffer T holding rows m0 + dA ..
-// m0 + dA + 256 of plane q (K-major, rows 16 bytes apart, the eight K blocks
+// m0 + dA + 192 of plane q (K-major, rows 16 bytes apart, the 16 K blocks
 // kRT * 16 bytes apart): shift d starts (d - dA) * 16 bytes further in.  T is
 // loaded (cp.async, zero-filled outside the face) once per run of up to kDB
-// consecutive shifts; Z is rebuilt per step from a 191-value window of D,
+// consecutive shifts; Z is rebuilt per step from a 255-value window of D,
 // double buffered so that the MMAs of one step overlap the build of the next,
 // and the D values of the next step are prefetched into registers.
-constexpr int kDB = 128;            // shifts served by one T buffer
-constexpr int kRT = 257;            // T rows (>= kDB + 127; odd multiple of 16 B keeps cp.async conflict-free)
-constexpr int kZN = 184;            // Z entries per (face, split): n' + 8 floor(k/8) <= 127 + 56
-constexpr int kWL = 192;            // window values per (face, split) (191 used)
-constexpr int kWUsed = 191;
-constexpr size_t kTSplit = (size_t)8 * kRT * 16;     // bytes of one split of T
-constexpr size_t kZFS = (size_t)kZN * 16;            // bytes of one (face, split) Z array
+//
+// Accumulation.  Tensor memory holds two FP32 accumulators (columns 0-127 and
+// 128-255) used by alternate steps, and a Kahan-compensated FP32 running sum
+// (sum in 256-383, compensation in 384-511).  While the MMAs of step i run
+// into one accumulator, the threads fold step i-1's accumulator into the
+// running sum, so each FP32 MMA accumulation spans one step (6 x 128
+// K-values) and the sum over steps is compensated.  The CTA writes its FP64
+// partial (sum - compensation) once at the end.
+constexpr int kDB = 64;             // shifts served by one T buffer
+constexpr int kRT = 193;            // T rows (>= kDB + 127; odd multiple of 16 B keeps cp.async conflict-free)
+constexpr int kKB = kTcKC / 8;      // K blocks per chunk
+constexpr int kZN = 128 + kTcKC - 8;  // Z entries per split: n' + 8 floor(k/8) <= 127 + kTcKC - 8
+constexpr int kWUsed = kZN + 7;     // window values used (255)
+constexpr int kWL = kWUsed + 1;
+constexpr size_t kTSplit = (size_t)kKB * kRT * 16;   // bytes of one split of T
+constexpr size_t kZS = (size_t)kZN * 16;             // bytes of one split of Z
 constexpr size_t kSmemT = 3 * kTSplit;
-constexpr size_t kSmemZ = 2 * 2 * 3 * kZFS;          // [buf][face][split]
-constexpr size_t kSmemW = (size_t)2 * 3 * kWL * 2;   // [face][split][kWL] bf16
-constexpr size_t kSmemX = (size_t)4 * 32 * 33 * 8;   // per-warp 32 x 32 FP64 transpose tiles
-constexpr size_t kTcSmem = kSmemT + kSmemZ + kSmemW + kSmemX;
-constexpr int kFoldsPerFlush = 16;  // on-chip folds between FP64 flushes
+constexpr size_t kSmemZ = 2 * 3 * kZS;               // [buf][split]
+constexpr size_t kSmemW = (size_t)3 * kWL * 2;       // [split][kWL] bf16
+constexpr size_t kTcSmem = kSmemT + kSmemZ + kSmemW;
+constexpr uint32_t kColAcc = 0, kColSum = 256, kColComp = 384;
 // kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
-// K-major, M = 128, N = 128 (one face per instruction).
+// K-major, M = 128, N = 128.
 constexpr uint32_t kIdescFace = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcHalfN >> 3) << 17) |
                                 ((uint32_t)(kTcM >> 4) << 24);
-constexpr int kPrefetch = 3;  // D values per thread per step (2 * 191 <= 3 * 128)
+constexpr int kPrefetch = 2;  // D values per thread per step (255 <= 2 * 128)
+
+__device__ inline void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+}
+__device__ inline void tmem_st16(uint32_t addr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          addr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
 
 __global__ void __launch_bounds__(kTcThreads, 1)
     bcpot_tc_kernel(KParams P, TcAxis X, const __nv_bfloat16* __restrict__ Cs, const double* __restrict__ D,
                     double* partial, int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* sT = smem;                   // [3][8][kRT][16 B]
-  unsigned char* sZ = smem + kSmemT;          // [2][2][3][kZN][16 B]
-  __nv_bfloat16* sWin = reinterpret_cast<__nv_bfloat16*>(smem + kSmemT + kSmemZ);  // [2][3][kWL]
-  double* sX = reinterpret_cast<double*>(smem + kSmemT + kSmemZ + kSmemW);         // [4][32][33]
+  unsigned char* sT = smem;                   // [3][kKB][kRT][16 B]
+  unsigned char* sZ = smem + kSmemT;          // [2][3][kZN][16 B]
+  __nv_bfloat16* sWin = reinterpret_cast<__nv_bfloat16*>(smem + kSmemT + kSmemZ);  // [3][kWL]
   __shared__ __align__(8) unsigned long long mbar[2];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  const int tile = blockIdx.x / X.splits, split = blockIdx.x % X.splits;
+  // CTA -> (tile, face, split)
+  const int split = blockIdx.x % X.splits;
+  const int tf = blockIdx.x / X.splits;
+  const int f = tf % 2, tile = tf / 2;
   const int mt = tile / X.ntiles, nt = tile % X.ntiles;
   const int m0 = mt * kTcM, n0 = nt * kTcHalfN;
   const int rows_hi = (m0 + kTcM < X.n1) ? m0 + kTcM : X.n1;
@@ -174,13 +199,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const long long pbeg = npairs * split / X.splits, pend = npairs * (split + 1) / X.splits;
   const int nchunks = X.n2pad / kTcKC;
   const long long per = (long long)X.nn * X.n1 * X.n2pad;  // elements of one split of Cs
-  double* part = partial + (long long)blockIdx.x * kTcM * kTcN;
+  // partial block of (tile, split): [128 rows][256 columns], this face's half
+  double* part = partial + ((long long)tile * X.splits + split) * kTcM * kTcN + f * kTcHalfN;
 
   const uint32_t mb0 = (uint32_t)__cvta_generic_to_shared(&mbar[0]);
   const uint32_t mb1 = (uint32_t)__cvta_generic_to_shared(&mbar[1]);
   if (warp == 0) {
     uint32_t dst = (uint32_t)__cvta_generic_to_shared(&tmem_base);
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(2 * kTcN)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(512)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -189,15 +215,27 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int e = tid; e < kTcM * kTcN; e += kTcThreads) part[e] = 0.0;
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
+  const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's 32 TMEM lanes
   uint32_t phase[2] = {0, 0};
-  bool pending[2] = {false, false};
-  int since_flush = 0;
+  bool pending[2] = {false, false};  // MMAs committed on mbar[b], not yet waited for
+  bool unfolded[2] = {false, false};  // accumulator b holds a step not yet folded
   bool ok = true;
+
+  // running sum and compensation start at zero
+  {
+    uint32_t z[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) z[j] = 0u;
+    for (int col = 0; col < kTcHalfN; col += 16) {
+      tmem_st16(lanebase + kColSum + col, z);
+      tmem_st16(lanebase + kColComp + col, z);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  }
 
   auto wait_buf = [&](int b) -> bool {
     if (!pending[b]) return true;
@@ -212,115 +250,54 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     bool b = wait_buf(1);
     return a && b;
   };
-  // Two on-chip levels before FP64.  The MMAs accumulate a segment of
-  // kFlushChunks steps in TMEM columns [0, 256); fold() adds it (FP32) into
-  // a running sum in columns [256, 512) and is cheap (TMEM loads and stores
-  // only); every kFoldsPerFlush folds flush64() adds the running sum into the
-  // CTA's FP64 partial, staged through a per-warp shared-memory transpose so
-  // that the global read-modify-writes are coalesced.  Thread = TMEM lane =
-  // tile row; TMEM column f*128 + n' is partial column f*128 + 127 - n'.
-  int folds = 0;
-  auto fold = [&]() {
-    for (int col = 0; col < kTcN; col += 16) {
-      uint32_t a[16], r[16];
-      const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7]),
-            "=r"(a[8]), "=r"(a[9]), "=r"(a[10]), "=r"(a[11]), "=r"(a[12]), "=r"(a[13]), "=r"(a[14]), "=r"(a[15])
-          : "r"(lanebase + (uint32_t)col));
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(lanebase + (uint32_t)(kTcN + col)));
+  // Kahan: y = a - c; t = s + y; c = (t - s) - y; s = t
+  auto fold = [&](int b) {
+    if (!unfolded[b]) return;
+    for (int col = 0; col < kTcHalfN; col += 16) {
+      uint32_t a[16], sm[16], cp[16];
+      tmem_ld16(lanebase + kColAcc + (uint32_t)(b * kTcHalfN + col), a);
+      tmem_ld16(lanebase + kColSum + col, sm);
+      tmem_ld16(lanebase + kColComp + col, cp);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
-        const float sum = folds == 0 ? __uint_as_float(a[j]) : __fadd_rn(__uint_as_float(r[j]), __uint_as_float(a[j]));
-        r[j] = __float_as_uint(sum);
+        const float y = __fsub_rn(__uint_as_float(a[j]), __uint_as_float(cp[j]));
+        const float t = __fadd_rn(__uint_as_float(sm[j]), y);
+        cp[j] = __float_as_uint(__fsub_rn(__fsub_rn(t, __uint_as_float(sm[j])), y));
+        sm[j] = __float_as_uint(t);
       }
-      asm volatile(
-          "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
-          ::"r"(lanebase + (uint32_t)(kTcN + col)), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]),
-            "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]),
-            "r"(r[14]), "r"(r[15])
-          : "memory");
+      tmem_st16(lanebase + kColSum + col, sm);
+      tmem_st16(lanebase + kColComp + col, cp);
     }
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    ++folds;
-  };
-  auto flush64 = [&]() {
-    double* X = sX + warp * 32 * 33;
-    for (int col = 0; col < kTcN; col += 32) {
-      uint32_t r[32];
-      const uint32_t addr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(kTcN + col);
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(addr));
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-          : "r"(addr + 16u));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-      for (int j = 0; j < 32; ++j) X[lane * 33 + j] = (double)__uint_as_float(r[j]);
-      __syncwarp();
-      // lane = TMEM column col + lane, i.e. partial column f*128 + 127 - n'
-      const int f = col / kTcHalfN, nprime = col % kTcHalfN + lane;
-      for (int rr = 0; rr < 32; ++rr) {
-        double* g = part + (long long)(32 * warp + rr) * kTcN + f * kTcHalfN + (kTcHalfN - 1 - nprime);
-        *g += X[rr * 33 + lane];
-      }
-      __syncwarp();
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    folds = 0;
-  };
-  auto flush = [&]() {
-    fold();
-    if (folds == kFoldsPerFlush) flush64();
+    unfolded[b] = false;
   };
 
-  // D values of one step into registers: item e = tid + 128 m -> face e / 191,
-  // window index e % 191
+  // D values of one step into registers: item e = tid + 128 m -> window index e
   double pre[kPrefetch];
   auto prefetch = [&](int q, int d, int kc) {
     const int o_min = kc * kTcKC - n0 - (kTcHalfN - 1);
 #pragma unroll
     for (int m = 0; m < kPrefetch; ++m) {
-      const int e = tid + kTcThreads * m;
+      const int j = tid + kTcThreads * m;
       double v = 0.0;
-      if (e < 2 * kWUsed) {
-        const int f = e / kWUsed, j = e % kWUsed;
+      if (j < kWUsed) {
         const int o2 = o_min + j;
         if (o2 >= -(X.n2 - 1) && o2 <= X.n2 - 1) v = __ldg(D + d_index(P, X, f, q, d, o2));
       }
       pre[m] = v;
     }
   };
-  auto step_of = [&](int kc, long long pr, int& q, int& d) {
-    q = int(pr / nd) + 1;
-    d = dlo + int(pr % nd);
-    (void)kc;
-  };
 
   int step = 0;
-  if (pbeg < pend) {
-    int q, d;
-    step_of(0, pbeg, q, d);
-    prefetch(q, d, 0);
-  }
+  if (pbeg < pend) prefetch(int(pbeg / nd) + 1, dlo + int(pbeg % nd), 0);
   for (int kc = 0; kc < nchunks && ok; ++kc) {
     const int k0 = kc * kTcKC;
     int Tq = -1, TdA = 0;
     for (long long pr = pbeg; pr < pend && ok; ++pr) {
-      int q, d;
-      step_of(kc, pr, q, d);
+      const int q = int(pr / nd) + 1;
+      const int d = dlo + int(pr % nd);
       if (q != Tq || d >= TdA + kDB) {
         // every MMA that reads T is done before T is rewritten
         if (!__syncthreads_and(drain() ? 1 : 0)) { ok = false; break; }
@@ -328,8 +305,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         TdA = d;
         const int rho0 = m0 + TdA;
         const uint32_t tbase = (uint32_t)__cvta_generic_to_shared(sT);
-        for (int e = tid; e < 3 * kRT * 8; e += kTcThreads) {
-          const int kb = e & 7, rest = e >> 3;
+        for (int e = tid; e < 3 * kRT * kKB; e += kTcThreads) {
+          const int kb = e % kKB, rest = e / kKB;
           const int t = rest % kRT, sp = rest / kRT;
           const int rho = rho0 + t;
           const bool in = rho >= 0 && rho < X.n1;
@@ -345,32 +322,32 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncthreads();
       }
       const int b = step & 1;
-      // the MMAs of step - 2 read Z[b]
+      // the MMAs of step - 2 (accumulator b, Z[b]) are done: fold them
       if (!__syncthreads_and(wait_buf(b) ? 1 : 0)) { ok = false; break; }
+      fold(b);
       // window of this step from the prefetched D values
 #pragma unroll
       for (int m = 0; m < kPrefetch; ++m) {
-        const int e = tid + kTcThreads * m;
-        if (e < 2 * kWUsed) {
-          const int f = e / kWUsed, j = e % kWUsed;
+        const int j = tid + kTcThreads * m;
+        if (j < kWUsed) {
           __nv_bfloat16 a0, a1, a2;
           split3((float)pre[m], a0, a1, a2);
-          sWin[(f * 3 + 0) * kWL + j] = a0;
-          sWin[(f * 3 + 1) * kWL + j] = a1;
-          sWin[(f * 3 + 2) * kWL + j] = a2;
+          sWin[0 * kWL + j] = a0;
+          sWin[1 * kWL + j] = a1;
+          sWin[2 * kWL + j] = a2;
         }
       }
-      if (tid < 6) sWin[tid * kWL + kWUsed] = __float2bfloat16_rn(0.0f);
+      if (tid < 3) sWin[tid * kWL + kWUsed] = __float2bfloat16_rn(0.0f);
       __syncthreads();
-      // Z[b][f][s][u] = w[u .. u+7]
-      unsigned char* zb = sZ + (size_t)b * 2 * 3 * kZFS;
-      for (int e = tid; e < 6 * kZN; e += kTcThreads) {
-        const int fs = e / kZN, u = e % kZN;
-        const __nv_bfloat16* w = sWin + fs * kWL + u;
+      // Z[b][s][u] = w_s[u .. u+7]
+      unsigned char* zb = sZ + (size_t)b * 3 * kZS;
+      for (int e = tid; e < 3 * kZN; e += kTcThreads) {
+        const int sp = e / kZN, u = e % kZN;
+        const __nv_bfloat16* w = sWin + sp * kWL + u;
         __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = w[j];
-        *reinterpret_cast<uint4*>(zb + (size_t)fs * kZFS + (size_t)u * 16) = *reinterpret_cast<const uint4*>(v);
+        *reinterpret_cast<uint4*>(zb + (size_t)sp * kZS + (size_t)u * 16) = *reinterpret_cast<const uint4*>(v);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
@@ -378,31 +355,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tb = (uint32_t)__cvta_generic_to_shared(sT) + (uint32_t)(d - TdA) * 16u;
         const uint32_t zs = (uint32_t)__cvta_generic_to_shared(zb);
+        const uint32_t acc_cols = tmem + kColAcc + (uint32_t)(b * kTcHalfN);
         const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
 #pragma unroll
-        for (int f = 0; f < 2; ++f) {
+        for (int ks = 0; ks < kTcKC / 16; ++ks) {
 #pragma unroll
-          for (int ks = 0; ks < kTcKC / 16; ++ks) {
-#pragma unroll
-            for (int t = 0; t < 6; ++t) {
-              const uint32_t a_addr = tb + (uint32_t)(pa[t] * kTSplit + (size_t)(2 * ks) * kRT * 16);
-              const uint32_t b_addr = zs + (uint32_t)((f * 3 + pb[t]) * kZFS + ks * 256);
-              const uint64_t adesc = smem_desc(a_addr, kRT * 16, 128);
-              const uint64_t bdesc = smem_desc(b_addr, 128, 128);
-              const uint32_t acc = (since_flush == 0 && ks == 0 && t == 0) ? 0u : 1u;
-              asm volatile(
-                  "{\n\t.reg .pred p;\n\t"
-                  "setp.ne.b32 p, %4, 0;\n\t"
-                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                  ::"r"(tmem + (uint32_t)(f * kTcHalfN)), "l"(adesc), "l"(bdesc), "r"(kIdescFace), "r"(acc)
-                  : "memory");
-            }
+          for (int t = 0; t < 6; ++t) {
+            const uint32_t a_addr = tb + (uint32_t)(pa[t] * kTSplit + (size_t)(2 * ks) * kRT * 16);
+            const uint32_t b_addr = zs + (uint32_t)(pb[t] * kZS + ks * 256);
+            const uint64_t adesc = smem_desc(a_addr, kRT * 16, 128);
+            const uint64_t bdesc = smem_desc(b_addr, 128, 128);
+            const uint32_t acc = (ks == 0 && t == 0) ? 0u : 1u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                ::"r"(acc_cols), "l"(adesc), "l"(bdesc), "r"(kIdescFace), "r"(acc)
+                : "memory");
           }
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b ? mb1 : mb0)
                      : "memory");
       }
       pending[b] = true;
+      unfolded[b] = true;
       ++step;
       // D values of the next step
       {
@@ -412,24 +388,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           npr = pbeg;
           ++nkc;
         }
-        if (nkc < nchunks) {
-          int nq, ndd;
-          step_of(nkc, npr, nq, ndd);
-          prefetch(nq, ndd, nkc);
-        }
-      }
-      if (++since_flush == kFlushChunks) {
-        if (!__syncthreads_and(drain() ? 1 : 0)) { ok = false; break; }
-        flush();
-        __syncthreads();
-        since_flush = 0;
+        if (nkc < nchunks) prefetch(int(npr / nd) + 1, dlo + int(npr % nd), nkc);
       }
     }
   }
   if (ok && !__syncthreads_and(drain() ? 1 : 0)) ok = false;
-  if (ok && since_flush > 0) fold();
-  if (ok && folds > 0) flush64();
-  if (!ok) {
+  if (ok) {
+    fold(step & 1);        // the older of the two outstanding steps first
+    fold((step + 1) & 1);
+    // partial = sum - compensation, this thread's row
+    double* row = part + (long long)(32 * warp + lane) * kTcN;
+    for (int col = 0; col < kTcHalfN; col += 16) {
+      uint32_t sm[16], cp[16];
+      tmem_ld16(lanebase + kColSum + col, sm);
+      tmem_ld16(lanebase + kColComp + col, cp);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        row[kTcHalfN - 1 - (col + j)] = (double)__uint_as_float(sm[j]) - (double)__uint_as_float(cp[j]);
+    }
+  } else {
     if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
     drain();  // bounded: let outstanding MMAs finish before TMEM is released
   }
@@ -437,10 +415,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTcN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
   }
 }
-
 
 // U on both faces of the axis = (sum over splits of the partial tiles) / (4 pi eps0).
 __global__ void bcpot_reduce_kernel(KParams P, TcAxis X, const double* partial, double* U) {
@@ -475,7 +452,7 @@ TcAxis tc_axis(const KParams& P, int axis, int sms) {
   X.n2pad = (X.n2 + kTcKC - 1) / kTcKC * kTcKC;
   X.mtiles = (X.n1 + kTcM - 1) / kTcM;
   X.ntiles = (X.n2 + kTcHalfN - 1) / kTcHalfN;
-  int tiles = X.mtiles * X.ntiles;
+  int tiles = X.mtiles * X.ntiles * 2;  // one CTA per face of a tile
   X.splits = sms / tiles;
   if (X.splits < 1) X.splits = 1;
   return X;
@@ -521,7 +498,7 @@ cudaError_t launch_bc_potentials_tc(const KParams& P, const double* C, const dou
     note_launch();
     split_charge_kernel<<<(unsigned)((per + 255) / 256), 256, 0, st>>>(P, X, C, Cs);
     note_launch();
-    bcpot_tc_kernel<<<X.mtiles * X.ntiles * X.splits, kTcThreads, smem, st>>>(P, X, Cs, D, partial, err);
+    bcpot_tc_kernel<<<X.mtiles * X.ntiles * 2 * X.splits, kTcThreads, smem, st>>>(P, X, Cs, D, partial, err);
     long long outs = (long long)X.mtiles * X.ntiles * kTcM * kTcN;
     note_launch();
     bcpot_reduce_kernel<<<(unsigned)((outs + 255) / 256), 256, 0, st>>>(P, X, partial, U);
