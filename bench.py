@@ -55,6 +55,7 @@ def parse_args():
     ap.add_argument("--slots", type=int, default=8, help="serving workload: runs in flight at once")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving workload: HBM budget of admitted runs")
     ap.add_argument("--poisson-n", type=int, default=256)
+    ap.add_argument("--poisson-dims", type=str, default=None, help="poisson workload: nx,ny,nz (default n^3)")
     ap.add_argument("--poisson-sweeps", type=int, default=400)
     ap.add_argument("--layout", choices=["cell32", "f64"], default="cell32")
     ap.add_argument("--solver", choices=["refine", "f64"], default="refine")
@@ -383,26 +384,42 @@ def run_poisson(args, local_rank):
     from picard_b200 import params as P
     from picard_b200.simulation import Simulation
 
+    import numpy as np
+
     torch.cuda.set_device(local_rank)
     n = args.poisson_n
-    p = P.config_plain_32(n=n, ppc=1, capacity=1024)
+    dims = [int(v) for v in args.poisson_dims.split(",")] if args.poisson_dims else [n, n, n]
+    nx, ny, nz = dims
+    p = P.config_plain_32(n=8, ppc=1, capacity=1024)
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.xmin, p.xmax = -500.0 * nx, 500.0 * nx
+    p.ymin, p.ymax = -500.0 * ny, 500.0 * ny
+    p.zmin, p.zmax = -500.0 * nz, 500.0 * nz
     solver = capi.SOLVER_F32_REFINE if args.solver == "refine" else capi.SOLVER_F64
     sim = Simulation(p, layout=capi.LAYOUT_F64, solver=solver)
-    sim.set_field(capi.FIELD_C, blob_charge(n, seed=0))
-    sim.set_field(capi.FIELD_U, __import__("numpy").zeros((n + 2,) * 3))
+    big = blob_charge(max(dims), seed=0)
+    C = np.ascontiguousarray(big[: nz + 2, : ny + 2, : nx + 2])
+    C[-1, :, :] = C[:, -1, :] = C[:, :, -1] = 0.0
+    sim.set_field(capi.FIELD_C, C)
+    sim.set_field(capi.FIELD_U, np.zeros_like(C))
     maxit = max(1, args.poisson_sweeps // 2)
     sim.calc_epotential(maxerr=1e-300, maxit=maxit)  # warm-up solve
     sim.reset_stats()
-    sim.set_field(capi.FIELD_U, __import__("numpy").zeros((n + 2,) * 3))
+    sim.set_field(capi.FIELD_U, np.zeros_like(C))
     sim.calc_epotential(maxerr=1e-300, maxit=maxit)
     st = sim.stats()
+    shape = (sim.get_option(capi.OPT_SWEEP_PAIRS), sim.get_option(capi.OPT_SWEEP_CTAS),
+             sim.get_option(capi.OPT_SWEEP_PDL), sim.get_option(capi.OPT_SWEEP_STAGES),
+             sim.get_option(capi.OPT_SWEEP_RESIDENT))
     sim.close()
-    cells = n ** 3
+    cells = nx * ny * nz
     bpn = 12 if solver == capi.SOLVER_F32_REFINE else 24
     ms = st["sweep_ms"] / max(st["sweep_launches"], 1)
     peak, kind = measured_peaks()
     ach = bpn * cells / (ms * 1e-3) / 1e9
-    print(json.dumps({"workload": f"poisson {n}^3", "sweeps": st["sweep_launches"], "sweep_ms": ms,
+    print(json.dumps({"workload": f"poisson {nx}x{ny}x{nz}", "sweep_shape": {
+                          "pairs": shape[0], "ctas": shape[1], "pdl": shape[2], "stages": shape[3],
+                          "resident": shape[4]}, "sweeps": st["sweep_launches"], "sweep_ms": ms,
                       "achieved_gbs": ach, "peak_gbs": peak, "frac": ach / peak, "peak_kind": kind,
                       "anchor_ms": st["anchor_ms"] / max(st["anchor_launches"], 1),
                       "gpu_launches": st["kernel_launches"]}), flush=True)

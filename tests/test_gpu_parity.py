@@ -129,8 +129,9 @@ def test_bc_potentials_matches_oracle():
 
 @pytest.mark.parametrize("dims", [(16, 16, 16), (160, 24, 20), (40, 136, 12)])
 def test_bc_potentials_tensor_cores_vs_fp64(dims):
-    # three-way BF16 split, FP32 accumulation folded into FP64 every 512
-    # K-values: the face potentials agree with the FP64 sum to ~1e-6 relative
+    # three-way BF16 split, one FP32 MMA accumulation per 128 K-values, the
+    # steps summed with Kahan compensation in tensor memory: the face
+    # potentials agree with the FP64 sum within the north-star 1e-6 relative
     nx, ny, nz = dims
     p = small_plasma(n=8, ppc=2, seed=23)
     p.nx, p.ny, p.nz = nx, ny, nz
@@ -152,7 +153,7 @@ def test_bc_potentials_tensor_cores_vs_fp64(dims):
     U = g.field(capi.FIELD_U)
     err = rel_l2(U, o.U)
     print(f"tensor-core BCpotentials {dims}: rel L2 vs FP64 = {err:.3e}")
-    assert err < 1e-5
+    assert err < 1e-6
 
 
 @pytest.mark.parametrize("mode", ["F64", "F64_REFINE"])
