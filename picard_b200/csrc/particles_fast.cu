@@ -8,6 +8,8 @@
 // the position advance is one FP32 add per axis.
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include <cmath>
 
 #include "common.cuh"
@@ -402,6 +404,138 @@ __global__ void deposit_c32_kernel(KParams P, PartC32 a, long long n, unsigned l
   }
 }
 
+// ParticlesGridify.f90:65-123, shared-memory tiled.  Particles are stored in
+// cell order (initialisation and every append go cell by cell; compaction
+// keeps the order) and move a small fraction of a cell per step, so a chunk
+// of kDepChunk consecutive particles touches a small box of nodes.  Each CTA
+// takes the bounding box of its chunk's CIC stencils (base node + 1 on every
+// axis, by species), accumulates the fixed-point weights there with 32-bit
+// shared-memory atomics -- weights lie in [0, 2^40], split into 20-bit halves
+// so neither half-sum can overflow over a chunk -- and adds every touched node
+// to global memory once, with the ghost folds applied.  A chunk whose box does
+// not fit the tile falls back to one global atomic per particle corner.
+// Integer sums are exact and order-independent: N is bit-identical to the
+// warp-aggregated kernel's.
+constexpr int kDepChunk = 1024;          // particles per CTA iteration (4 per thread)
+constexpr int kDepTile = 8192;           // tile entries (two u32 halves each: 64 KB)
+
+__device__ inline int block_min_max(int v, bool want_max, int* red) {
+  for (int o = 16; o > 0; o >>= 1) {
+    int u = __shfl_xor_sync(0xffffffffu, v, o);
+    v = want_max ? max(v, u) : min(v, u);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = l < (int)(blockDim.x >> 5) ? red[l] : (want_max ? INT_MIN : INT_MAX);
+    for (int o = 16; o > 0; o >>= 1) {
+      int u = __shfl_xor_sync(0xffffffffu, v, o);
+      v = want_max ? max(v, u) : min(v, u);
+    }
+    if (l == 0) red[32] = v;
+  }
+  __syncthreads();
+  v = red[32];
+  __syncthreads();
+  return v;
+}
+
+__global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC32 a, long long n,
+                                                               unsigned long long* Nacc) {
+  extern __shared__ unsigned int dep_tile[];  // [2][kDepTile]: low and high 20-bit halves
+  __shared__ int red[33];
+  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+  unsigned int* lo = dep_tile;
+  unsigned int* hi = dep_tile + kDepTile;
+  constexpr int kPer = kDepChunk / 256;
+  for (long long base = (long long)blockIdx.x * kDepChunk; base < n; base += (long long)gridDim.x * kDepChunk) {
+    C32 c[kPer];
+    int sp[kPer];
+    bool act[kPer];
+    int imin = INT_MAX, imax = INT_MIN, jmin = INT_MAX, jmax = INT_MIN, kmin = INT_MAX, kmax = INT_MIN;
+    int smin = INT_MAX, smax = INT_MIN;
+#pragma unroll
+    for (int m = 0; m < kPer; ++m) {
+      const long long p = base + threadIdx.x + 256 * m;
+      act[m] = p < n;
+      if (act[m]) {
+        c[m] = load_pos(a, p);
+        sp[m] = a.sp[p];
+        imin = min(imin, c[m].i), imax = max(imax, c[m].i);
+        jmin = min(jmin, c[m].j), jmax = max(jmax, c[m].j);
+        kmin = min(kmin, c[m].k), kmax = max(kmax, c[m].k);
+        smin = min(smin, sp[m]), smax = max(smax, sp[m]);
+      }
+    }
+    imin = block_min_max(imin, false, red);
+    imax = block_min_max(imax, true, red);
+    jmin = block_min_max(jmin, false, red);
+    jmax = block_min_max(jmax, true, red);
+    kmin = block_min_max(kmin, false, red);
+    kmax = block_min_max(kmax, true, red);
+    smin = block_min_max(smin, false, red);
+    smax = block_min_max(smax, true, red);
+    const long long bi = (long long)imax - imin + 2, bj = (long long)jmax - jmin + 2, bk = (long long)kmax - kmin + 2,
+                    bs = (long long)smax - smin + 1;
+    const long long vol = bi * bj * bk * bs;
+    if (vol <= kDepTile) {
+      const int vi = int(vol);
+      for (int e = threadIdx.x; e < vi; e += 256) lo[e] = 0u, hi[e] = 0u;
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < kPer; ++m) {
+        if (!act[m]) continue;
+        const float wx[2] = {1.0f - c[m].f[0], c[m].f[0]}, wy[2] = {1.0f - c[m].f[1], c[m].f[1]},
+                    wz[2] = {1.0f - c[m].f[2], c[m].f[2]};
+        const int b0 = (((sp[m] - smin) * int(bk) + (c[m].k - kmin)) * int(bj) + (c[m].j - jmin)) * int(bi) +
+                       (c[m].i - imin);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float F = wx[off[q][0]] * wy[off[q][1]] * wz[off[q][2]];
+          const unsigned long long w = (unsigned long long)__float2ll_rn(F * float(kDepositScale));
+          const int e = b0 + (off[q][2] * int(bj) + off[q][1]) * int(bi) + off[q][0];
+          atomicAdd(lo + e, unsigned(w & 0xFFFFFu));
+          atomicAdd(hi + e, unsigned(w >> 20));
+        }
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < vi; e += 256) {
+        const unsigned l = lo[e], h = hi[e];
+        if ((l | h) == 0u) continue;
+        int r = e;
+        const int ii = r % int(bi) + imin;
+        r /= int(bi);
+        const int jj = r % int(bj) + jmin;
+        r /= int(bj);
+        const int kk = r % int(bk) + kmin;
+        const int ss = r / int(bk) + smin;
+        const int i = fold_index(ii, P.nx, P.xflow), j = fold_index(jj, P.ny, P.yflow),
+                  k = fold_index(kk, P.nz, P.zflow);
+        const unsigned long long v = ((unsigned long long)h << 20) + (unsigned long long)l;
+        atomicAdd(Nacc + (long long)ss * P.nodes + node_index(P, i, j, k), v);
+      }
+      __syncthreads();
+    } else {
+#pragma unroll
+      for (int m = 0; m < kPer; ++m) {
+        if (!act[m]) continue;
+        const float wx[2] = {1.0f - c[m].f[0], c[m].f[0]}, wy[2] = {1.0f - c[m].f[1], c[m].f[1]},
+                    wz[2] = {1.0f - c[m].f[2], c[m].f[2]};
+        unsigned long long* plane = Nacc + (long long)sp[m] * P.nodes;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float F = wx[off[q][0]] * wy[off[q][1]] * wz[off[q][2]];
+          const unsigned long long w = (unsigned long long)__float2ll_rn(F * float(kDepositScale));
+          const int i = fold_index(c[m].i + off[q][0], P.nx, P.xflow), j = fold_index(c[m].j + off[q][1], P.ny, P.yflow),
+                    k = fold_index(c[m].k + off[q][2], P.nz, P.zflow);
+          atomicAdd(plane + node_index(P, i, j, k), w);
+        }
+      }
+    }
+  }
+}
+
 __global__ void energy_particles_c32_kernel(KParams P, PartC32 a, long long n, double* partial) {
   __shared__ double sh[32];
   double acc = 0.0;
@@ -508,6 +642,21 @@ cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n
 cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
                                unsigned long long* Facc, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  if (!Facc) {
+    const size_t smem = 2 * sizeof(unsigned int) * kDepTile;
+    static bool attr = false;
+    if (!attr) {
+      cudaError_t e = cudaFuncSetAttribute(deposit_tile_c32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+      if (e != cudaSuccess) return e;
+      attr = true;
+    }
+    long long chunks = (n + kDepChunk - 1) / kDepChunk;
+    int grid = int(chunks < 148LL * 3 ? chunks : 148LL * 3);
+    note_launch();
+    deposit_tile_c32_kernel<<<grid, 256, smem, st>>>(P, a, n, Nacc);
+    return cudaGetLastError();
+  }
   note_launch();
   deposit_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, a, n, Nacc, Facc);
   return cudaGetLastError();

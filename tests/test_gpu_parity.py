@@ -336,6 +336,28 @@ def test_one_step_parity_cell32_layout():
     assert rel_l2(g.field(capi.FIELD_E), o.E) < 1e-5
 
 
+@pytest.mark.parametrize("order", ["cell", "shuffled"])
+def test_tiled_deposit_equals_warp_aggregated(order):
+    # CELL32 ParticlesGridify runs the shared-memory tiled deposit (and its
+    # per-corner fallback when a chunk's box exceeds the tile: shuffled
+    # order); ParticlesGridifyAll runs the warp-aggregated kernel.  Both sum
+    # the same fixed-point weights, so N must agree bit for bit.
+    p, o, g = make(small_haser(nx=40, ny=24, nz=20, ppc=3, seed=17), **C32)
+    g.calc_distance()
+    g.particles_initialize()
+    g.run_fused(0, 5)
+    if order == "shuffled":
+        rp, ip = g.particles()
+        perm = np.random.default_rng(3).permutation(len(ip))
+        g.set_particles(rp[perm], ip[perm])
+    g.particles_gridify()
+    N_tile = g.field(capi.FIELD_N)
+    g.particles_gridify_all()
+    N_warp = g.field(capi.FIELD_N)
+    assert np.abs(N_tile).sum() > 0
+    np.testing.assert_array_equal(N_tile, N_warp)
+
+
 @pytest.mark.parametrize("kw,tol", [(F64, 1e-9), (C32, 2e-5)])
 def test_multi_step_energy_moments(kw, tol):
     p, o, g = make(small_plasma(n=8, ppc=4, seed=21), **kw)
