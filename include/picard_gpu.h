@@ -262,7 +262,11 @@ typedef enum picard_option {
   /* TMA sweep tile width: 0 32-wide tiles, one node per thread; 1 64-wide
    * tiles, two x-adjacent nodes per thread in packed FP32 pair arithmetic.
    * Never changes a result bit. */
-  PICARD_OPT_SWEEP_PAIRS = 5
+  PICARD_OPT_SWEEP_PAIRS = 5,
+  /* 1: x-pair sweeps two at a time (one launch computes sweeps s and s+1 of
+   * a tile, the intermediate iterate in shared memory); 0 one per launch.
+   * Never changes a result bit. */
+  PICARD_OPT_SWEEP_FUSED = 6
 } picard_option;
 /* Reads an option's current value (SWEEP_CTAS: 0 means one CTA per tile). */
 PICARD_API int picard_gpu_get_option(picard_ctx* ctx, int32_t option, int32_t* value);

@@ -35,6 +35,7 @@ OPT_SWEEP_PDL = 2
 OPT_SWEEP_STAGES = 3
 OPT_SWEEP_RESIDENT = 4
 OPT_SWEEP_PAIRS = 5
+OPT_SWEEP_FUSED = 6
 
 class PicardStats(C.Structure):
     _fields_ = [

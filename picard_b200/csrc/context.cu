@@ -344,6 +344,12 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
       e1 |= make_tensor_map(&c->tmw2[1], c->w[1], c->K, 72, 10, c->G.zc + 2);
       e2 |= make_tensor_map(&c->tmr2[0], c->r, c->K, 64, 8, c->G.zc);
       e3 |= make_tensor_map(&c->tmr2[1], c->r + fe, c->K, 64, 8, c->G.zc);
+      if (c->G.zc <= 8) {
+        e0 |= make_tensor_map(&c->tmw3[0], c->w[0], c->K, 72, 12, c->G.zc + 4);
+        e1 |= make_tensor_map(&c->tmw3[1], c->w[1], c->K, 72, 12, c->G.zc + 4);
+        e2 |= make_tensor_map(&c->tmr3[0], c->r, c->K, 72, 10, c->G.zc + 2);
+        e3 |= make_tensor_map(&c->tmr3[1], c->r + fe, c->K, 72, 10, c->G.zc + 2);
+      }
       if (e0 || e1 || e2 || e3)
         return bail(fail(PICARD_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(e0 | e1 | e2 | e3) + ")"));
     }
@@ -729,6 +735,13 @@ int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
   }
   if (option == PICARD_OPT_SWEEP_PAIRS) {
     c->G.pairs = value != 0;
+    if (!c->G.pairs) c->G.fused2 = 0;
+    return PICARD_OK;
+  }
+  if (option == PICARD_OPT_SWEEP_FUSED) {
+    if (value && (!c->G.tma || c->G.zc > 8)) return fail(PICARD_ERR_STATE, "two-sweep launches need the TMA sweep with zc <= 8");
+    c->G.fused2 = value != 0;
+    if (c->G.fused2) c->G.pairs = 1;
     return PICARD_OK;
   }
   if (option == PICARD_OPT_SWEEP_STAGES) {
@@ -747,6 +760,7 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
     case PICARD_OPT_SWEEP_PDL: *value = c->G.pdl; return PICARD_OK;
     case PICARD_OPT_SWEEP_STAGES: *value = c->G.stages; return PICARD_OK;
     case PICARD_OPT_SWEEP_PAIRS: *value = c->G.pairs; return PICARD_OK;
+    case PICARD_OPT_SWEEP_FUSED: *value = c->G.fused2; return PICARD_OK;
     case PICARD_OPT_SWEEP_RESIDENT: *value = resident_option_value(c); return PICARD_OK;
   }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");

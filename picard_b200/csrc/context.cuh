@@ -44,6 +44,7 @@ struct picard_ctx {
   CUtensorMap tmw[2];                 // TMA descriptors of w[0], w[1] (w boxes)
   CUtensorMap tmr[2];                 // TMA descriptors of r, r + f32_elems (r boxes)
   CUtensorMap tmw2[2], tmr2[2];       // the same for the x-pair sweep's wider boxes
+  CUtensorMap tmw3[2], tmr3[2];       // two-sweep kernel: w boxes 72 x 12 x zc+4, r boxes 72 x 10 x zc+2
   double* partials = nullptr;  // [m_max + 1][nblocks]
   double* r2 = nullptr;        // [m_max + 1]
   picard::JacobiGeom G;

@@ -717,6 +717,206 @@ __global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__
   }
 }
 
+// ---------------------------------- two sweeps per launch (temporal blocking)
+//
+// Sweeps s and s+1 of the x-pair kernel in one launch.  Per 64 x 8 x ZC tile
+// the CTA loads w_{s-1} with a two-node halo (box 72 x 12 x (ZC+4)) and r with
+// a one-node halo (box 72 x 10 x (ZC+2)), computes w_s on the tile and its
+// one-node halo (x pairs from tile column -2 to 65, rows -1..8, planes
+// -1..ZC) into shared memory -- zero outside the interior, the ghost value --
+// and then w_{s+1} on the tile from there.  Every node of either sweep is the
+// same jacobi_res_f32 / jacobi_next_f32 arithmetic on the same inputs as in a
+// single-sweep launch (halo nodes are recomputed by each neighbouring tile,
+// identically), and both sweeps' per-tile partials are formed exactly as in
+// sweep_tma2_kernel (per-column FP32 sums in z order, the 32-lane tree, rows
+// in order), so results are bit-identical to two single sweeps.  L2 traffic
+// per sweep drops from ~15 to ~10.6 bytes per node and launches halve.
+template <int ZC>
+struct Sweep2Smem {
+  static constexpr int kW0 = (ZC + 4) * 12 * kTma2BoxX;  // w_{s-1}: [ZC+4][12][72]
+  static constexpr int kR = (ZC + 2) * 10 * kTma2BoxX;   // r:       [ZC+2][10][72]
+  static constexpr int kW1X = 68;
+  static constexpr int kW1 = (ZC + 2) * 10 * kW1X;       // w_s:     [ZC+2][10][68]
+  static constexpr int kCS = kTmaTy * kTma2Tile;         // sweep-s column sums [8][64]
+  static constexpr size_t kBytes = sizeof(float) * (size_t)(kW0 + kR + kW1 + kCS);
+  static_assert((kW0 * 4) % 128 == 0 && ((kW0 + kR) * 4) % 128 == 0, "TMA destinations 128-byte aligned");
+};
+
+// 32-lane partial tree of block_sum_store on x-pair column sums (lane l holds
+// columns 2l and 2l+1 of a 64-wide row); lanes 0 and 16 return the two
+// 32-wide tiles' row sums.
+__device__ __forceinline__ double pair_row_tree(float c0, float c1) {
+  double v0 = (double)c0, v1 = (double)c1;
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) {
+    v0 += __shfl_down_sync(0xffffffffu, v0, o);
+    v1 += __shfl_down_sync(0xffffffffu, v1, o);
+  }
+  return v0 + v1;
+}
+
+template <int ZC>
+__global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__ CUtensorMap tw,
+                                                         const __grid_constant__ CUtensorMap tr, Stencil S,
+                                                         JacobiCoefF J, float* __restrict__ wout, double* partialA,
+                                                         double* partialB, int w_zero, int gx2, int gx, int gy,
+                                                         int ntiles, int* err) {
+  using L = Sweep2Smem<ZC>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* W0 = reinterpret_cast<float*>(smem_raw);
+  float* R = W0 + L::kW0;
+  float* W1 = R + L::kR;
+  float* CS = W1 + L::kW1;
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ double rows[2][2][kTmaTy];  // [sweep][32-wide tile][row]
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + kTmaTx * ty;
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((unsigned long long)&tw) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((unsigned long long)&tr) : "memory");
+  }
+  __syncthreads();
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const int t = blockIdx.x;
+  if (t >= ntiles) return;
+  const int bx2 = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
+  const int x0 = bx2 * kTma2Tile, y0 = by * kTmaTy, z0 = bz * ZC;
+  if (tid == 0) {
+    uint32_t bytes = (uint32_t)(L::kR * sizeof(float));
+    if (!w_zero) bytes += (uint32_t)(L::kW0 * sizeof(float));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+    if (!w_zero)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+          ::"r"((uint32_t)__cvta_generic_to_shared(W0)), "l"((unsigned long long)&tw), "r"(x0), "r"(y0 - 1),
+          "r"(z0 - 1), "r"(mb)
+          : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"((uint32_t)__cvta_generic_to_shared(R)), "l"((unsigned long long)&tr), "r"(x0), "r"(y0), "r"(z0),
+        "r"(mb)
+        : "memory");
+  }
+  const bool ok = __syncthreads_and(mbar_wait(mb, 0, kMbarSpin) ? 1 : 0);
+  if (!ok) {
+    if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+    mbar_wait(mb, 0, kMbarSpin);
+    return;
+  }
+  const unsigned long long m2 = pk2(-2.0f, -2.0f), ix2 = pk2(J.idx2, J.idx2), iy2 = pk2(J.idy2, J.idy2),
+                           iz2 = pk2(J.idz2, J.idz2), naf = pk2(-J.af, -J.af);
+  auto node_res = [&](unsigned long long wc, float xl, float xr, unsigned long long ym, unsigned long long yp,
+                      unsigned long long wm, unsigned long long wp, unsigned long long rr) {
+    const float2 c = up2(wc);
+    const unsigned long long xm = pk2(xl, c.x), xp = pk2(c.y, xr);
+    const unsigned long long sx = add2(xp, xm), sy = add2(yp, ym), sz = add2(wp, wm);
+    unsigned long long lap = mul2(fma2(m2, wc, sx), ix2);
+    lap = fma2(fma2(m2, wc, sy), iy2, lap);
+    lap = fma2(fma2(m2, wc, sz), iz2, lap);
+    return sub2(rr, lap);
+  };
+  auto u64at = [](const float* base, int idx) { return *reinterpret_cast<const unsigned long long*>(base + idx); };
+
+  // ---- sweep s on the tile and its one-node halo: 34 x-pairs x 10 rows, z marching
+  for (int item = tid; item < 34 * 10; item += 256) {
+    const int p = item % 34, ry = item / 34;
+    const int xr = 2 * p - 2, yr = ry - 1;  // first node of the pair, tile-relative
+    const int i0 = x0 + 1 + xr, j = y0 + 1 + yr;
+    const bool rowin = j >= 1 && j <= S.ny;
+    const bool in0 = rowin && i0 >= 1 && i0 <= S.nx, in1 = rowin && i0 + 1 >= 1 && i0 + 1 <= S.nx;
+    const bool tilecol = p >= 1 && p <= 32 && ry >= 1 && ry <= kTmaTy;
+    // W0[kz][ky][kx]: kz = zr + 2, ky = yr + 2, kx = xr + 4
+    auto w0 = [&](int zr, int dy) { return u64at(W0, ((zr + 2) * 12 + (yr + 2 + dy)) * kTma2BoxX + xr + 4); };
+    auto w0s = [&](int zr, int dx) { return W0[((zr + 2) * 12 + (yr + 2)) * kTma2BoxX + xr + 4 + dx]; };
+    unsigned long long wm = w_zero ? 0ull : w0(-2, 0);
+    unsigned long long wc = w_zero ? 0ull : w0(-1, 0);
+    unsigned long long r2 = 0ull;
+#pragma unroll
+    for (int zr = -1; zr <= ZC; ++zr) {
+      const int k = z0 + 1 + zr;
+      unsigned long long wp = 0ull, ym = 0ull, yp = 0ull;
+      float xl = 0.0f, xrr = 0.0f;
+      if (!w_zero) {
+        wp = w0(zr + 1, 0);
+        ym = w0(zr, -1);
+        yp = w0(zr, 1);
+        xl = w0s(zr, -1);
+        xrr = w0s(zr, 2);
+      }
+      const unsigned long long rr = u64at(R, ((zr + 1) * 10 + (yr + 1)) * kTma2BoxX + xr + 4);
+      const unsigned long long res = node_res(wc, xl, xrr, ym, yp, wm, wp, rr);
+      const bool kin = k >= 1 && k <= S.nz;
+      const float2 rf = up2(res);
+      const float2 wn = up2(fma2(naf, res, wc));
+      const bool a0 = in0 && kin, a1 = in1 && kin;
+      *reinterpret_cast<float2*>(W1 + ((zr + 1) * 10 + ry) * L::kW1X + xr + 2) =
+          make_float2(a0 ? wn.x : 0.0f, a1 ? wn.y : 0.0f);
+      if (tilecol && zr >= 0 && zr < ZC) {
+        const unsigned long long resm = pk2(a0 ? rf.x : 0.0f, a1 ? rf.y : 0.0f);
+        r2 = fma2(resm, resm, r2);
+      }
+      wm = wc;
+      wc = wp;
+    }
+    if (tilecol) *reinterpret_cast<float2*>(CS + (ry - 1) * kTma2Tile + xr) = up2(r2);
+  }
+  __syncthreads();
+
+  // ---- sweep s+1 on the tile from w_s in shared memory
+  const int i0 = x0 + 2 * tx + 1, j = y0 + ty + 1;
+  const bool act0 = i0 <= S.nx && j <= S.ny, act1 = i0 + 1 <= S.nx && j <= S.ny;
+  const int kend = min(ZC, S.nz - z0);
+  // W1[kz][ky][kx]: kz = zr + 1, ky = yr + 1, kx = xr + 2
+  auto w1 = [&](int zr, int dy) { return u64at(W1, ((zr + 1) * 10 + (ty + 1 + dy)) * L::kW1X + 2 * tx + 2); };
+  auto w1s = [&](int zr, int dx) { return W1[((zr + 1) * 10 + (ty + 1)) * L::kW1X + 2 * tx + 2 + dx]; };
+  unsigned long long wm = w1(-1, 0), wc = w1(0, 0), r2 = 0ull;
+  float* out = wout + fidx(S, i0, j, z0 + 1);
+  const long long plane = (long long)S.fpitch * S.nyp;
+#pragma unroll
+  for (int zr = 0; zr < ZC; ++zr) {
+    if (zr < kend) {
+      const unsigned long long wp = w1(zr + 1, 0);
+      const unsigned long long rr = u64at(R, ((zr + 1) * 10 + (ty + 1)) * kTma2BoxX + 2 * tx + 4);
+      const unsigned long long res = node_res(wc, w1s(zr, -1), w1s(zr, 2), w1(zr, -1), w1(zr, 1), wm, wp, rr);
+      const float2 rf = up2(res);
+      const unsigned long long resm = pk2(act0 ? rf.x : 0.0f, act1 ? rf.y : 0.0f);
+      r2 = fma2(resm, resm, r2);
+      const float2 wn = up2(fma2(naf, res, wc));
+      if (act1) {
+        *reinterpret_cast<float2*>(out) = wn;
+      } else if (act0) {
+        out[0] = wn.x;
+      }
+      out += plane;
+      wm = wc;
+      wc = wp;
+    }
+  }
+  // ---- partials of both sweeps for the two 32-wide tiles
+  const float2 ca = *reinterpret_cast<const float2*>(CS + ty * kTma2Tile + 2 * tx);
+  const double rowA = pair_row_tree(ca.x, ca.y);
+  const float2 cb = up2(r2);
+  const double rowB = pair_row_tree(cb.x, cb.y);
+  if ((tx & 15) == 0) {
+    rows[0][tx >> 4][ty] = rowA;
+    rows[1][tx >> 4][ty] = rowB;
+  }
+  __syncthreads();
+  if (tid < 4) {
+    const int sw = tid >> 1, half = tid & 1;
+    const int bx = 2 * bx2 + half;
+    if (bx < gx) {
+      double sum = 0.0;
+      for (int q = 0; q < kTmaTy; ++q) sum += rows[sw][half][q];
+      (sw ? partialB : partialA)[bx + (long long)gx * (by + (long long)gy * bz)] = sum;
+    }
+  }
+}
+
 // Periodic ghost refresh of U (CalcEpotential.f90:100-239 on one rank), in
 // z, y, x order over whole planes.
 __global__ void refresh_periodic_kernel(Stencil S, double* U, int axis) {
@@ -1111,6 +1311,44 @@ cudaError_t launch_sweep_tma2(const KParams& P, const JacobiGeom& G, const CUten
     case 4: return launch_tma2_zc<4>(P, G, tw, tr, wout, partial, w_zero, err, st);
     case 8: return launch_tma2_zc<8>(P, G, tw, tr, wout, partial, w_zero, err, st);
     case 16: return launch_tma2_zc<16>(P, G, tw, tr, wout, partial, w_zero, err, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int ZC>
+static cudaError_t launch_sweep2_zc(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw,
+                                    const CUtensorMap* tr, float* wout, double* partialA, double* partialB,
+                                    int w_zero, int* err, cudaStream_t st) {
+  const size_t smem = Sweep2Smem<ZC>::kBytes;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(sweep2_tma_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int gx2 = (P.nx + kTma2Tile - 1) / kTma2Tile;
+  const int ntiles = gx2 * (int)G.grid.y * (int)G.grid.z;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ntiles);
+  cfg.blockDim = dim3(kTmaTx, kTmaTy);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = G.pdl ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, sweep2_tma_kernel<ZC>, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout, partialA,
+                            partialB, w_zero, gx2, (int)G.grid.x, (int)G.grid.y, ntiles, err);
+}
+
+cudaError_t launch_sweep2_tma(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
+                              float* wout, double* partialA, double* partialB, int w_zero, int* err,
+                              cudaStream_t st) {
+  switch (G.zc) {
+    case 4: return launch_sweep2_zc<4>(P, G, tw, tr, wout, partialA, partialB, w_zero, err, st);
+    case 8: return launch_sweep2_zc<8>(P, G, tw, tr, wout, partialA, partialB, w_zero, err, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -164,7 +164,17 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
       PICARD_CUDA(cudaStreamSynchronize(c->st));
       return PICARD_OK;
     }
-    for (int t = 1; t <= count; ++t)
+    int t = 1;
+    if (c->G.tma && c->G.pairs && c->G.fused2) {
+      // sweeps a0+t and a0+t+1 per launch: reads w[(s-1)%2], writes w[(s+1)%2]
+      for (; t + 1 <= count; t += 2) {
+        const long long s = a0 + t;
+        PICARD_CUDA(launch_sweep2_tma(K, c->G, &c->tmw3[(s - 1) % 2], &c->tmr3[rsel], c->w[(s + 1) % 2],
+                                      partial_base + (size_t)(t - 1) * nb, partial_base + (size_t)t * nb,
+                                      t == 1 ? 1 : 0, c->d_err, c->st));
+      }
+    }
+    for (; t <= count; ++t)
       PICARD_CUDA(sweep(a0 + t, rsel, partial_base + (size_t)(t - 1) * nb, t == 1 ? 1 : 0));
     return PICARD_OK;
   };
@@ -298,8 +308,9 @@ namespace picard {
 namespace {
 struct SweepShape {
   int ctas, pdl, stages;
-  int res;    // 0: TMA sweep kernel; q + 1: resident sweep with CTA shape q
-  int pairs;  // TMA sweep: 1 the x-pair kernel
+  int res;     // 0: TMA sweep kernel; q + 1: resident sweep with CTA shape q
+  int pairs;   // TMA sweep: 1 the x-pair kernel
+  int fused2;  // x-pair sweeps two per launch
 };
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, SweepShape> g_tuned;
@@ -309,6 +320,7 @@ int apply_shape(picard_ctx* c, const SweepShape& sh) {
   c->G.pdl = sh.pdl;
   c->G.stages = sh.stages;
   c->G.pairs = sh.pairs;
+  c->G.fused2 = sh.fused2;
   c->G.res = 0;
   if (sh.res > 0) {
     if (!resident_plan(c->K, c->G, sh.res - 1)) return fail(PICARD_ERR_STATE, "resident sweep shape does not fit");
@@ -335,7 +347,7 @@ int set_resident(picard_ctx* c, int value) {
     return PICARD_OK;
   }
   if (!c->G.tma || !c->w[0]) return fail(PICARD_ERR_STATE, "resident sweeps need open boundaries and the F32_REFINE solver");
-  SweepShape sh{0, 0, 1, value, 0};
+  SweepShape sh{0, 0, 1, value, 0, 0};
   JacobiGeom g = c->G;
   if (!resident_plan(c->K, g, value - 1)) return fail(PICARD_ERR_STATE, "resident sweep shape does not fit the device");
   c->G.res = 0;
@@ -346,6 +358,7 @@ int set_resident(picard_ctx* c, int value) {
   sh.pdl = pdl;
   sh.stages = stages;
   sh.pairs = c->G.pairs;
+  sh.fused2 = c->G.fused2;
   return apply_shape(c, sh);
 }
 
@@ -365,7 +378,7 @@ int tune_sweep(picard_ctx* c, bool fresh) {
   if (const char* v = std::getenv("PICARD_SWEEP_TUNE"); v && v[0] == '0' && !fresh) {
     // no timing: the x-pair kernel, one CTA per tile, PDL (the 32-wide
     // kernel when the grid is at most one tile wide)
-    return apply(SweepShape{0, 1, 1, 0, c->K.nx > 32 ? 1 : 0});
+    return apply(SweepShape{0, 1, 1, 0, c->K.nx > 32 ? 1 : 0, 0});
   }
   if (!fresh) {
     SweepShape cached;
@@ -388,15 +401,17 @@ int tune_sweep(picard_ctx* c, bool fresh) {
     const int occ2 = pairs ? sweep_tma2_occupancy(c->G, 2) : sweep_tma_occupancy(c->G, 2);
     const int tiles = pairs ? sweep_tma2_tiles(c->K, c->G) : c->G.nblocks;
     for (int pdl = 1; pdl >= 0; --pdl) {
-      cand.push_back({0, pdl, 1, 0, pairs});  // one CTA per tile
+      cand.push_back({0, pdl, 1, 0, pairs, 0});  // one CTA per tile
       for (int k = 1; k <= occ2; ++k)
-        if ((long long)k * sms < tiles) cand.push_back({k * sms, pdl, 2, 0, pairs});
-      if ((long long)occ1 * sms < tiles) cand.push_back({occ1 * sms, pdl, 1, 0, pairs});
+        if ((long long)k * sms < tiles) cand.push_back({k * sms, pdl, 2, 0, pairs, 0});
+      if ((long long)occ1 * sms < tiles) cand.push_back({occ1 * sms, pdl, 1, 0, pairs, 0});
     }
   }
+  if (c->G.zc <= 8)
+    for (int pdl = 1; pdl >= 0; --pdl) cand.push_back({0, pdl, 1, 0, 1, 1});  // two sweeps per launch
   for (int q = 0; q < kResidentShapes; ++q) {
     JacobiGeom g = c->G;
-    if (resident_plan(c->K, g, q)) cand.push_back({0, 0, 1, q + 1, 0});
+    if (resident_plan(c->K, g, q)) cand.push_back({0, 0, 1, q + 1, 0, 0});
   }
   constexpr int kReps = 24;
   std::vector<float> best(cand.size(), 1e30f);
@@ -415,14 +430,18 @@ int tune_sweep(picard_ctx* c, bool fresh) {
         PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
       } else {
         auto one = [&](int s) {
+          if (c->G.fused2)  // sweeps s, s+1
+            return launch_sweep2_tma(c->K, c->G, &c->tmw3[(s - 1) % 2], &c->tmr3[0], c->w[(s + 1) % 2],
+                                     c->partials, c->partials + c->G.nblocks, 0, c->d_err, c->st);
           return c->G.pairs ? launch_sweep_tma2(c->K, c->G, &c->tmw2[(s - 1) % 2], &c->tmr2[0], c->w[s % 2],
                                                 c->partials, 0, c->d_err, c->st)
                             : launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2],
                                                c->partials, 0, c->d_err, c->st);
         };
-        for (int s = 1; s <= 2; ++s) PICARD_CUDA(one(s));
+        const int step = c->G.fused2 ? 2 : 1;
+        for (int s = 1; s <= 2 * step; s += step) PICARD_CUDA(one(s));
         PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
-        for (int s = 1; s <= kReps; ++s) PICARD_CUDA(one(s));
+        for (int s = 1; s <= kReps; s += step) PICARD_CUDA(one(s));
         PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
         PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
       }
@@ -440,9 +459,10 @@ int tune_sweep(picard_ctx* c, bool fresh) {
         std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: resident shape %d  %.3f us%s\n", c->K.nx, c->K.ny,
                      c->K.nz, c->G.zc, cand[q].res - 1, best[q] * 1e3, q == pick ? "  <- picked" : "");
       else
-        std::fprintf(stderr, "picard sweep tune %dx%dx%d zc=%d: pairs=%d ctas=%d pdl=%d stages=%d  %.3f us%s\n",
-                     c->K.nx, c->K.ny, c->K.nz, c->G.zc, cand[q].pairs, cand[q].ctas, cand[q].pdl, cand[q].stages,
-                     best[q] * 1e3, q == pick ? "  <- picked" : "");
+        std::fprintf(stderr,
+                     "picard sweep tune %dx%dx%d zc=%d: pairs=%d fused2=%d ctas=%d pdl=%d stages=%d  %.3f us%s\n",
+                     c->K.nx, c->K.ny, c->K.nz, c->G.zc, cand[q].pairs, cand[q].fused2, cand[q].ctas, cand[q].pdl,
+                     cand[q].stages, best[q] * 1e3, q == pick ? "  <- picked" : "");
     }
   }
   PICARD_TRY(apply(cand[pick]));
