@@ -293,6 +293,17 @@ PICARD_API int picard_gpu_run(picard_ctx* ctx, int32_t iter_start, int32_t iter_
 PICARD_API int picard_gpu_run_fused(picard_ctx* ctx, int32_t iter_start, int32_t iter_end,
                          int64_t* sweeps_total);
 
+/* Batched parameter sweep: iterations iter_start+1 .. iter_end of the fused
+ * loop for n independent contexts (runs) together.  Every run's particle
+ * phases are issued on its own stream before any is waited for, and the
+ * Jacobi sweeps of all runs advance in lockstep rounds with one launch per
+ * sweep over the tiles of every run (open boundaries, F32_REFINE solver;
+ * other runs solve on their own).  Each run's result is bit-identical to
+ * picard_gpu_run_fused on that run alone.  sweeps_total (may be NULL) is an
+ * array of n counters accumulating each run's Jacobi sweeps. */
+PICARD_API int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter_start, int32_t iter_end,
+                                      int64_t* sweeps_total);
+
 #ifdef __cplusplus
 }
 #endif

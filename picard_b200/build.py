@@ -30,6 +30,7 @@ UNITS = {
     "context.cu": [],
     "driver.cu": [],
     "server.cu": [],
+    "batch.cu": [],
 }
 
 

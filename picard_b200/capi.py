@@ -157,6 +157,7 @@ def lib():
         "picard_gpu_get_stream": [ctx, C.POINTER(C.c_void_p)],
         "picard_gpu_set_option": [ctx, C.c_int32, C.c_int32],
         "picard_gpu_get_option": [ctx, C.c_int32, ip],
+        "picard_batch_run_fused": [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int64)],
         "picard_server_create": [C.c_uint64, C.c_int32, C.POINTER(C.c_void_p)],
         "picard_server_submit": [C.c_void_p, C.POINTER(PicardRequest)],
         "picard_server_now_ms": [C.c_void_p, dp],

@@ -1,0 +1,434 @@
+// batch.cu -- many independent runs advanced together (the batched
+// parameter sweep): picard_batch_run_fused.
+//
+// Each run is its own picard_ctx (own memory, own stream).  Per iteration of
+// picard.f90:554-674 the driver issues every run's particle phases on the
+// runs' streams before waiting on any of them (the particle-count round trips
+// of all runs travel together), then solves every run's Poisson problem in
+// lockstep: per round each run plans its batch of sweeps from its own anchor
+// (the F32_REFINE loop of solve_f32.cuh, unchanged), and sweep t of the round
+// is ONE launch over the tiles of every run still at least t sweeps into its
+// round -- the run table (tensor maps, stencil, coefficients, output, tile
+// range) rides in the kernel parameters -- instead of one launch per run.
+// Anchors, reductions and the stop tests stay per run; runs that converge drop
+// out of later rounds.  The sweep kernel is the x-pair TMA sweep with the
+// same per-node arithmetic and per-tile partials, so every run's result is
+// bit-identical to the same run advanced alone with picard_gpu_run_fused.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "context.cuh"
+#include "grid.cuh"
+#include "kernels.cuh"
+#include "picard_gpu.h"
+#include "solve_f32.cuh"
+#include "stencil.cuh"
+
+using namespace picard;
+
+namespace picard {
+namespace {
+
+constexpr int kBatchRuns = 40;  // runs per launch (kernel parameter space)
+
+struct alignas(64) BatchRun {
+  CUtensorMap tw;  // w of the sweep's input iterate (x-pair boxes 72 x 10 x zc+2)
+  CUtensorMap tr;  // the run's live anchor residual (boxes 64 x 8 x zc)
+  Stencil S;
+  JacobiCoefF J;
+  float* wout;
+  double* partial;
+  int gx2, gx, gy, tiles, tile_base, w_zero;
+};
+
+struct BatchArgs {
+  BatchRun run[kBatchRuns];
+  int nruns;
+  int total_tiles;
+  int* err;
+};
+static_assert(sizeof(BatchArgs) < 32000, "kernel parameter space");
+
+// The x-pair sweep (grid.cu sweep_tma2_kernel) over a table of runs: CTA t
+// takes tile t - tile_base of the run whose tile range holds t.
+template <int ZC>
+__global__ void __launch_bounds__(256) sweep_batch_kernel(const __grid_constant__ BatchArgs A) {
+  constexpr int kBoxX = 72, kTile = 64, kTy = 8, kTx = 32;
+  constexpr int kW = (ZC + 2) * (kTy + 2) * kBoxX, kR = ZC * kTy * kTile;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* sw = reinterpret_cast<float*>(smem_raw);
+  float* sr = sw + kW;
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ double rows[2][kTy];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kTx * ty;
+  const int t = blockIdx.x;
+  int r = 0;
+  while (r + 1 < A.nruns && t >= A.run[r + 1].tile_base) ++r;
+  const BatchRun& R = A.run[r];
+  const int lt = t - R.tile_base;
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const int bx2 = lt % R.gx2, by = (lt / R.gx2) % R.gy, bz = lt / (R.gx2 * R.gy);
+  const int x0 = bx2 * kTile, y0 = by * kTy, z0 = bz * ZC;
+  if (tid == 0) {
+    uint32_t bytes = (uint32_t)(kR * sizeof(float));
+    if (!R.w_zero) bytes += (uint32_t)(kW * sizeof(float));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+    if (!R.w_zero)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+          ::"r"((uint32_t)__cvta_generic_to_shared(sw)), "l"((unsigned long long)&R.tw), "r"(x0), "r"(y0), "r"(z0),
+          "r"(mb)
+          : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)&R.tr), "r"(x0 + 4), "r"(y0 + 1),
+        "r"(z0 + 1), "r"(mb)
+        : "memory");
+  }
+  bool done = false;
+  for (long long it = 0; it < (1LL << 24); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(mb), "r"(0u)
+        : "memory");
+    if (ok) {
+      done = true;
+      break;
+    }
+  }
+  if (!__syncthreads_and(done ? 1 : 0)) {
+    if (tid == 0) atomicCAS(A.err, 0, int(kDevTimeout));
+    // let this CTA's copies land (bounded) before it exits
+    for (long long it = 0; it < (1LL << 24); ++it) {
+      uint32_t ok;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(ok)
+          : "r"(mb), "r"(0u)
+          : "memory");
+      if (ok) break;
+    }
+    return;
+  }
+  const Stencil& S = R.S;
+  const JacobiCoefF& J = R.J;
+  const int i0 = x0 + 2 * tx + 1, j = y0 + ty + 1;
+  const bool act0 = i0 <= S.nx && j <= S.ny, act1 = i0 + 1 <= S.nx && j <= S.ny;
+  const int kend = min(ZC, S.nz - z0);
+  const long long plane = (long long)S.fpitch * S.nyp;
+  float* out = R.wout + fidx(S, i0, j, z0 + 1);
+  auto wv = [&](int kk, int row, int col) { return sw[(kk * (kTy + 2) + row) * kBoxX + col]; };
+  float2 wm = R.w_zero ? make_float2(0.f, 0.f) : make_float2(wv(0, ty + 1, 2 * tx + 4), wv(0, ty + 1, 2 * tx + 5));
+  float2 wc = R.w_zero ? make_float2(0.f, 0.f) : make_float2(wv(1, ty + 1, 2 * tx + 4), wv(1, ty + 1, 2 * tx + 5));
+  float r2a = 0.0f, r2b = 0.0f;
+#pragma unroll
+  for (int kk = 1; kk <= ZC; ++kk) {
+    if (kk <= kend) {
+      float2 wp = make_float2(0.f, 0.f), ym = wp, yp = wp;
+      float xl = 0.f, xr = 0.f;
+      if (!R.w_zero) {
+        wp = make_float2(wv(kk + 1, ty + 1, 2 * tx + 4), wv(kk + 1, ty + 1, 2 * tx + 5));
+        ym = make_float2(wv(kk, ty, 2 * tx + 4), wv(kk, ty, 2 * tx + 5));
+        yp = make_float2(wv(kk, ty + 2, 2 * tx + 4), wv(kk, ty + 2, 2 * tx + 5));
+        xl = wv(kk, ty + 1, 2 * tx + 3);
+        xr = wv(kk, ty + 1, 2 * tx + 6);
+      }
+      const float* rr = sr + ((kk - 1) * kTy + ty) * kTile + 2 * tx;
+      const float res0 = jacobi_res_f32(J, wc.x, xl, wc.y, ym.x, yp.x, wm.x, wp.x, rr[0]);
+      const float res1 = jacobi_res_f32(J, wc.y, wc.x, xr, ym.y, yp.y, wm.y, wp.y, rr[1]);
+      r2a = acc_r2_f32(r2a, act0 ? res0 : 0.0f);
+      r2b = acc_r2_f32(r2b, act1 ? res1 : 0.0f);
+      const float n0 = jacobi_next_f32(J, wc.x, res0), n1 = jacobi_next_f32(J, wc.y, res1);
+      if (act1) {
+        *reinterpret_cast<float2*>(out) = make_float2(n0, n1);
+      } else if (act0) {
+        out[0] = n0;
+      }
+      out += plane;
+      wm = wc;
+      wc = wp;
+    }
+  }
+  // the 32-lane tree of block_sum_store for the two 32-wide tiles (lanes 0-15, 16-31)
+  double v0 = (double)r2a, v1 = (double)r2b;
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) {
+    v0 += __shfl_down_sync(0xffffffffu, v0, o);
+    v1 += __shfl_down_sync(0xffffffffu, v1, o);
+  }
+  if ((tx & 15) == 0) rows[tx >> 4][ty] = v0 + v1;
+  __syncthreads();
+  if (tid < 2) {
+    const int bx = 2 * bx2 + tid;
+    if (bx < R.gx) {
+      double sum = 0.0;
+      for (int q = 0; q < kTy; ++q) sum += rows[tid][q];
+      R.partial[bx + (long long)R.gx * (by + (long long)R.gy * bz)] = sum;
+    }
+  }
+}
+
+template <int ZC>
+cudaError_t launch_batch_zc(const BatchArgs& A, cudaStream_t st) {
+  constexpr size_t smem = sizeof(float) * ((size_t)(ZC + 2) * 10 * 72 + (size_t)ZC * 8 * 64);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(sweep_batch_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(A.total_tiles);
+  cfg.blockDim = dim3(32, 8);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, sweep_batch_kernel<ZC>, A);
+}
+
+struct RunSolve {
+  picard_ctx* c = nullptr;
+  EpotSetup e;
+  F32Solve S;
+  bool batched = false;  // the lockstep loop drives this run's solve
+  bool done = true;
+  long long sweeps = 0;
+  bool converged = true;
+};
+
+// Sweep t (1-based) of the current round for every run with m_eff >= t, in
+// launches of at most kBatchRuns runs of one tile depth.
+int launch_round_sweep(std::vector<RunSolve*>& runs, int t, int* err, cudaStream_t st) {
+  for (int zc : {4, 8}) {
+    BatchArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.err = err;
+    auto flush = [&]() -> int {
+      if (A.nruns == 0) return PICARD_OK;
+      cudaError_t e = zc == 8 ? launch_batch_zc<8>(A, st) : launch_batch_zc<4>(A, st);
+      PICARD_CUDA(e);
+      std::memset(&A, 0, sizeof(A));
+      A.err = err;
+      return PICARD_OK;
+    };
+    for (RunSolve* rs : runs) {
+      if (rs->done || !rs->batched || rs->S.m_eff < t || rs->c->G.zc != zc) continue;
+      picard_ctx* c = rs->c;
+      const long long s = rs->S.a + t;
+      BatchRun& R = A.run[A.nruns];
+      R.tw = c->tmw2[(s - 1) % 2];
+      R.tr = c->tmr2[rs->S.rcur];
+      R.S = make_stencil(c->K);
+      R.J = jacobi_coef_f(c->K);
+      R.wout = c->w[s % 2];
+      R.partial = c->partials + (size_t)(t - 1) * c->G.nblocks;
+      R.gx2 = (c->K.nx + 63) / 64;
+      R.gx = (int)c->G.grid.x;
+      R.gy = (int)c->G.grid.y;
+      R.tiles = R.gx2 * (int)c->G.grid.y * (int)c->G.grid.z;
+      R.tile_base = A.total_tiles;
+      R.w_zero = t == 1 ? 1 : 0;
+      A.total_tiles += R.tiles;
+      if (++A.nruns == kBatchRuns) PICARD_TRY(flush());
+    }
+    PICARD_TRY(flush());
+  }
+  return PICARD_OK;
+}
+
+}  // namespace
+}  // namespace picard
+
+extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter_start, int32_t iter_end,
+                                      int64_t* sweeps_total) {
+  if (!ctxs || n < 1) return fail(PICARD_ERR_BAD_ARG, "no contexts");
+  for (int r = 0; r < n; ++r) {
+    if (!ctxs[r]) return fail(PICARD_ERR_BAD_ARG, "a context is NULL");
+    for (int q = 0; q < r; ++q)
+      if (ctxs[q] == ctxs[r]) return fail(PICARD_ERR_BAD_ARG, "a context appears twice in the batch");
+  }
+  int dev = 0;
+  PICARD_CUDA(cudaGetDevice(&dev));
+  for (int r = 0; r < n; ++r)
+    if (ctxs[r]->device != dev) return fail(PICARD_ERR_BAD_ARG, "batched contexts must live on the current device");
+  cudaStream_t bst = nullptr;
+  cudaEvent_t bev = nullptr;
+  std::vector<cudaEvent_t> rev(n, nullptr);
+  auto cleanup = [&]() {
+    if (bst) cudaStreamSynchronize(bst);
+    for (int r = 0; r < n; ++r)
+      if (rev[r]) cudaEventDestroy(rev[r]);
+    if (bev) cudaEventDestroy(bev);
+    if (bst) cudaStreamDestroy(bst);
+  };
+  int rc = PICARD_OK;
+  int* berr = nullptr;  // timeout flag of the batched sweeps (run 0's error word)
+  rc = check_cuda(cudaStreamCreateWithFlags(&bst, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (rc == PICARD_OK) rc = check_cuda(cudaEventCreateWithFlags(&bev, cudaEventDisableTiming), "cudaEventCreate");
+  for (int r = 0; r < n && rc == PICARD_OK; ++r)
+    rc = check_cuda(cudaEventCreateWithFlags(&rev[r], cudaEventDisableTiming), "cudaEventCreate");
+  if (rc != PICARD_OK) {
+    cleanup();
+    return rc;
+  }
+  berr = ctxs[0]->d_err;
+  bool nc = false;
+  std::vector<RunSolve> solves(n);
+  std::vector<RunSolve*> rp(n);
+  for (int r = 0; r < n; ++r) rp[r] = &solves[r];
+
+  auto body = [&]() -> int {
+    for (int32_t it = iter_start + 1; it <= iter_end; ++it) {
+      // ---- AdvancePosition, ParticlesProduce (device count) for every run
+      for (int r = 0; r < n; ++r) {
+        picard_ctx* c = ctxs[r];
+        const KParams& K = c->K;
+        const int cells = c->prm.nx * c->prm.ny * c->prm.nz;
+        PICARD_TRY(picard_gpu_advance_position(c, c->prm.dt));
+        PICARD_CUDA(launch_produce_count(K, it, c->cell_counts, c->st));
+        PICARD_CUDA(launch_scan_int(c->cell_counts, c->cell_offsets, cells, c->cell_offsets + cells,
+                                    c->cell_offsets + cells + 2, c->st));
+        if (c->layout == PICARD_LAYOUT_F64)
+          PICARD_CUDA(launch_produce_emit_f64(K, it, c->cell_offsets, c->f64[c->cur], c->d_count + c->cur,
+                                              c->capacity, c->d_err, c->st));
+        else
+          PICARD_CUDA(launch_produce_emit_c32(K, it, c->cell_offsets, c->c32[c->cur], c->d_count + c->cur,
+                                              c->capacity, c->d_err, c->st));
+        PICARD_TRY(count_issue(c));
+      }
+      for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));
+      // ---- BCoutflow + ParticlesTransfer (compaction), BCinflow (fused)
+      for (int r = 0; r < n; ++r) {
+        picard_ctx* c = ctxs[r];
+        const KParams& K = c->K;
+        const int nxt = 1 - c->cur;
+        if (c->layout == PICARD_LAYOUT_F64)
+          PICARD_CUDA(launch_compact_outflow_f64(K, c->f64[c->cur], c->f64[nxt], c->num_local, c->blk_counts,
+                                                 c->blk_offsets, c->d_count + nxt, 1, c->st));
+        else
+          PICARD_CUDA(launch_compact_outflow_c32(K, c->c32[c->cur], c->c32[nxt], c->num_local, c->blk_counts,
+                                                 c->blk_offsets, c->d_count + nxt, 1, c->st));
+        c->cur = nxt;
+        if (c->layout == PICARD_LAYOUT_F64)
+          PICARD_CUDA(launch_inflow_fused_f64(K, c->inflow, it, c->f64[c->cur], c->d_count + c->cur, c->capacity,
+                                              c->d_err, c->st));
+        else
+          PICARD_CUDA(launch_inflow_fused_c32(K, c->inflow, it, c->c32[c->cur], c->d_count + c->cur, c->capacity,
+                                              c->d_err, c->st));
+        PICARD_TRY(count_issue(c));
+      }
+      for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));
+      // ---- ParticlesGridify, BCpotentials, b and ||b||
+      for (int r = 0; r < n; ++r) {
+        picard_ctx* c = ctxs[r];
+        PICARD_TRY(picard_gpu_particles_gridify(c));
+        PICARD_TRY(picard_gpu_bc_potentials(c));
+        PICARD_TRY(epot_rhs_issue(c));
+      }
+      // ---- CalcEpotential: lockstep rounds over the runs
+      for (int r = 0; r < n; ++r) {
+        picard_ctx* c = ctxs[r];
+        RunSolve& rs = solves[r];
+        rs = RunSolve();
+        rs.c = c;
+        PICARD_CUDA(cudaStreamSynchronize(c->st));
+        rs.e = epot_setup(c, c->prm.maxerr, c->prm.maxit);
+        rs.done = rs.e.trivial;
+        rs.sweeps = 0;
+        rs.converged = true;
+        if (rs.done) continue;
+        if (c->solver == PICARD_SOLVER_F32_REFINE && c->G.tma && c->G.zc <= 8) {
+          rs.batched = true;
+          PICARD_TRY(f32_begin(rs.S, c, rs.e.tol, rs.e.smax, rs.e.maxit, rs.e.sigma));
+        } else {
+          // not batchable (FP64 solver or periodic axes): its own solve
+          int32_t sw = 0;
+          int q = picard_gpu_calc_epotential(c, c->prm.maxerr, c->prm.maxit, &sw);
+          if (q == PICARD_ERR_NOT_CONVERGED) nc = true;
+          else if (q != PICARD_OK) return q;
+          if (sweeps_total) sweeps_total[r] += sw;
+          rs.done = true;
+          rs.batched = false;
+          rs.e.trivial = false;
+        }
+      }
+      for (;;) {
+        int M = 0;
+        for (int r = 0; r < n; ++r)
+          if (!solves[r].done && solves[r].batched) M = std::max(M, f32_plan(solves[r].S));
+        if (M == 0) break;
+        // the batch stream follows every active run's stream (anchors done)
+        for (int r = 0; r < n; ++r) {
+          if (solves[r].done || !solves[r].batched) continue;
+          PICARD_CUDA(cudaEventRecord(rev[r], ctxs[r]->st));
+          PICARD_CUDA(cudaStreamWaitEvent(bst, rev[r], 0));
+        }
+        for (int t = 1; t <= M; ++t) PICARD_TRY(launch_round_sweep(rp, t, berr, bst));
+        PICARD_CUDA(cudaEventRecord(bev, bst));
+        for (int r = 0; r < n; ++r) {
+          if (solves[r].done || !solves[r].batched) continue;
+          PICARD_CUDA(cudaStreamWaitEvent(ctxs[r]->st, bev, 0));
+          PICARD_CUDA(cudaEventRecord(ctxs[r]->ev[0], ctxs[r]->st));  // no per-run sweep timing in a batch
+          PICARD_TRY(f32_issue_tail(solves[r].S));
+        }
+        for (int r = 0; r < n; ++r) {
+          RunSolve& rs = solves[r];
+          if (rs.done || !rs.batched) continue;
+          PICARD_TRY(f32_finish(rs.S, false));
+          if (rs.S.done) {
+            rs.done = true;
+            rs.sweeps = rs.S.sweeps;
+            rs.converged = rs.S.converged;
+          }
+        }
+      }
+      for (int r = 0; r < n; ++r) {
+        RunSolve& rs = solves[r];
+        if (!rs.batched && !rs.e.trivial) continue;  // solved on its own above
+        int32_t sw = 0;
+        int q = epot_finish(ctxs[r], rs.e, rs.sweeps, rs.converged, &sw);
+        if (q == PICARD_ERR_NOT_CONVERGED) nc = true;
+        else if (q != PICARD_OK) return q;
+        if (sweeps_total) sweeps_total[r] += sw;
+      }
+      // ---- CalcEfield + BCfields, AdvanceVelocity
+      for (int r = 0; r < n; ++r) {
+        picard_ctx* c = ctxs[r];
+        PICARD_TRY(picard_gpu_calc_efield(c));
+        PICARD_TRY(picard_gpu_advance_velocity(c, c->prm.dt));
+        c->stats.steps += 1;
+        c->stats.particle_steps += c->num_local;
+      }
+    }
+    for (int r = 0; r < n; ++r) PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
+    return PICARD_OK;
+  };
+  rc = body();
+  if (rc == PICARD_OK) rc = check_cuda(cudaStreamSynchronize(bst), "batch stream");
+  cleanup();
+  if (rc != PICARD_OK) return rc;
+  if (nc) return fail(PICARD_ERR_NOT_CONVERGED, "at least one Jacobi solve hit 2*maxit+1 sweeps");
+  return PICARD_OK;
+}

@@ -256,6 +256,23 @@ int sync_count_public(picard_ctx* c) {
   PICARD_TRY(check_dev_err(c));
   return sync_count(c);
 }
+
+int count_issue(picard_ctx* c) {
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 2, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i, c->d_count + c->cur, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  c->stats.d2h_bytes += 2 * sizeof(int);
+  return PICARD_OK;
+}
+
+int count_collect(picard_ctx* c) {
+  PICARD_CUDA(cudaStreamSynchronize(c->st));
+  if (c->h_pinned_i[2] == kDevCapacity) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+    return fail(PICARD_ERR_CAPACITY, "particle capacity max_per_proc exceeded on the device");
+  }
+  c->num_local = c->h_pinned_i[0];
+  return PICARD_OK;
+}
 }  // namespace picard
 
 // ======================================================================= ABI

@@ -97,6 +97,10 @@ picard::InflowTable make_inflow_table(const picard_params& p);
 // Reads the device particle count into ctx->num_local after surfacing any
 // device-side capacity error.
 int sync_count_public(picard_ctx* c);
+// The same in two halves, so that many contexts' counts travel together:
+// count_issue queues the copies, count_collect waits for the context's stream.
+int count_issue(picard_ctx* c);
+int count_collect(picard_ctx* c);
 // Device memory owned by the context (zeroed, freed with it).
 int dev_alloc(picard_ctx* c, void** p, size_t bytes);
 // Times the launch shapes of the TMA sweep on this context's buffers and keeps

@@ -22,6 +22,7 @@
 
 #include "context.cuh"
 #include "picard_gpu.h"
+#include "solve_f32.cuh"
 
 using namespace picard;
 
@@ -136,158 +137,242 @@ int solve_f64(picard_ctx* c, double tol, long long smax, int maxit, long long* s
 }
 
 // ---------------------------------------------- FP32 increment + FP64 anchor
-int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma, long long* sweeps,
-              bool* converged) {
+//
+// The loop is a resumable state machine (F32Solve, solve_f32.cuh) so that the
+// batched driver can advance many runs' solves in lockstep, running the
+// sweeps of a round for all runs in one launch per sweep; solve_f32 drives one
+// run with its own sweep launches.
+
+}  // namespace
+
+namespace picard {
+
+// One sweep s (1-based from the anchor) of run c: reads w[(s-1)%2] and the
+// anchor residual R[rsel], writes w[s%2] and the sweep's tile partials.
+static cudaError_t single_sweep(picard_ctx* c, long long s, int rsel, double* partial, int w_zero) {
+  const KParams& K = c->K;
+  float* R[2] = {c->r, c->r + f32_elems(K)};
+  if (c->G.tma && c->G.pairs)
+    return launch_sweep_tma2(K, c->G, &c->tmw2[(s - 1) % 2], &c->tmr2[rsel], c->w[s % 2], partial, w_zero,
+                             c->d_err, c->st);
+  if (c->G.tma)
+    return launch_sweep_tma(K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[rsel], c->w[s % 2], partial, w_zero, c->d_err,
+                            c->st);
+  return launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rsel], partial, w_zero, c->st);
+}
+
+int run_sweeps_single(picard_ctx* c, long long a0, int count, int rsel, double* partial_base) {
   const KParams& K = c->K;
   const int nb = c->G.nblocks;
-  double* V[2] = {c->U, c->U1};
-  float* R[2] = {c->r, c->r + f32_elems(K)};  // anchor residuals, one per live anchor
-  // sweep s reads w[(s-1)%2] (TMA descriptor tmw[(s-1)%2]) and R[rcur] (tmr[rcur])
-  auto sweep = [&](long long s, int rsel, double* partial, int w_zero) -> cudaError_t {
-    if (c->G.tma && c->G.pairs)
-      return launch_sweep_tma2(K, c->G, &c->tmw2[(s - 1) % 2], &c->tmr2[rsel], c->w[s % 2], partial, w_zero,
-                               c->d_err, c->st);
-    if (c->G.tma)
-      return launch_sweep_tma(K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[rsel], c->w[s % 2], partial, w_zero, c->d_err,
-                              c->st);
-    return launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rsel], partial, w_zero, c->st);
-  };
-  // sweeps a0+1 .. a0+count from w = 0 (the anchor), partials of sweep a0+t at
-  // partial_base + (t-1) nb
-  auto run_sweeps = [&](long long a0, int count, int rsel, double* partial_base) -> int {
-    if (c->G.res) {
-      // one resident launch at a time on the device: its CTAs must all be
-      // resident together, which another cooperative grid could prevent
-      std::lock_guard<std::mutex> lk(g_resident_mu);
-      PICARD_CUDA(launch_sweeps_resident(K, c->G, R[rsel], nullptr, c->w[(a0 + count) % 2], c->res_faces,
-                                         c->res_bar, partial_base, count, 1, c->d_err, c->st));
-      PICARD_CUDA(cudaStreamSynchronize(c->st));
-      return PICARD_OK;
-    }
-    int t = 1;
-    if (c->G.tma && c->G.pairs && c->G.fused2) {
-      // sweeps a0+t and a0+t+1 per launch: reads w[(s-1)%2], writes w[(s+1)%2]
-      for (; t + 1 <= count; t += 2) {
-        const long long s = a0 + t;
-        PICARD_CUDA(launch_sweep2_tma(K, c->G, &c->tmw3[(s - 1) % 2], &c->tmr3[rsel], c->w[(s + 1) % 2],
-                                      partial_base + (size_t)(t - 1) * nb, partial_base + (size_t)t * nb,
-                                      t == 1 ? 1 : 0, c->d_err, c->st));
-      }
-    }
-    for (; t <= count; ++t)
-      PICARD_CUDA(sweep(a0 + t, rsel, partial_base + (size_t)(t - 1) * nb, t == 1 ? 1 : 0));
+  float* R[2] = {c->r, c->r + f32_elems(K)};
+  if (c->G.res) {
+    // one resident launch at a time on the device: its CTAs must all be
+    // resident together, which another cooperative grid could prevent
+    std::lock_guard<std::mutex> lk(g_resident_mu);
+    PICARD_CUDA(launch_sweeps_resident(K, c->G, R[rsel], nullptr, c->w[(a0 + count) % 2], c->res_faces, c->res_bar,
+                                       partial_base, count, 1, c->d_err, c->st));
+    PICARD_CUDA(cudaStreamSynchronize(c->st));
     return PICARD_OK;
-  };
-  int vcur = 0, rcur = 0;
+  }
+  int t = 1;
+  if (c->G.tma && c->G.pairs && c->G.fused2) {
+    // sweeps a0+t and a0+t+1 per launch: reads w[(s-1)%2], writes w[(s+1)%2]
+    for (; t + 1 <= count; t += 2) {
+      const long long s = a0 + t;
+      PICARD_CUDA(launch_sweep2_tma(K, c->G, &c->tmw3[(s - 1) % 2], &c->tmr3[rsel], c->w[(s + 1) % 2],
+                                    partial_base + (size_t)(t - 1) * nb, partial_base + (size_t)t * nb,
+                                    t == 1 ? 1 : 0, c->d_err, c->st));
+    }
+  }
+  for (; t <= count; ++t) PICARD_CUDA(single_sweep(c, a0 + t, rsel, partial_base + (size_t)(t - 1) * nb, t == 1 ? 1 : 0));
+  return PICARD_OK;
+}
+
+int f32_begin(F32Solve& S, picard_ctx* c, double tol, long long smax, int maxit, double sigma) {
+  const KParams& K = c->K;
+  S = F32Solve();
+  S.c = c;
+  S.tol = tol;
+  S.tol2 = tol * tol;
+  S.smax = smax;
+  S.maxit = maxit;
+  S.sigma = sigma;
+  S.V[0] = c->U;
+  S.V[1] = c->U1;
+  S.R[0] = c->r;
+  S.R[1] = c->r + f32_elems(K);
   PICARD_CUDA(cudaMemcpyAsync(c->U1, c->U, sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
   // anchor 0: r = (b - L U_0) / sigma
-  PICARD_CUDA(launch_anchor(K, c->G, V[vcur], V[1 - vcur], nullptr, c->b, R[rcur], sigma, c->partials, 1, c->st));
-  vcur = 1 - vcur;
-  long long a = 0;
-  int m = 64;
-  double r2_prev = 0.0, r2_last = 0.0;
-  const double tol2 = tol * tol;
-  for (;;) {
-    int m_eff = int(std::min<long long>(m, smax - a));
-    PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
-    PICARD_TRY(run_sweeps(a, m_eff, rcur, c->partials));
-    PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
-    // next anchor: fold w_{a+m_eff} into V, exact FP64 residual of that iterate
-    long long an = a + m_eff;
-    PICARD_CUDA(launch_anchor(K, c->G, V[vcur], V[1 - vcur], c->w[an % 2], c->b, R[1 - rcur], sigma,
-                              c->partials + (size_t)m_eff * nb, 0, c->st));
-    PICARD_CUDA(cudaEventRecord(c->ev[2], c->st));
-    PICARD_CUDA(launch_reduce_sweeps(c->partials, nb, m_eff + 1, c->r2, c->st));
-    PICARD_TRY(read_r2(c, m_eff + 1));
-    PICARD_TRY(check_timeout(c));
-    c->stats.sweep_launches += m_eff;
-    c->stats.sweep_ms += elapsed_ms(c, 0, 1);
-    c->stats.anchor_launches += 1;
-    c->stats.anchor_ms += elapsed_ms(c, 1, 2);
-    long long hit = -1;
-    // sweep a+t (t >= 2) measured iterate a+t-1 in FP32 (scaled by sigma^2);
-    // the anchor measured iterate a+m_eff in FP64
-    for (int t = 2; t <= m_eff + 1; ++t) {
-      long long d = a + t - 1;
-      double r2 = t <= m_eff ? c->h_pinned[t - 1] * sigma * sigma : c->h_pinned[m_eff];
-      r2_prev = r2_last;
-      r2_last = r2;
-      c->last_residual = std::sqrt(r2);
-      if (d >= 1 && d + 1 <= maxit && passes(r2, tol)) {
-        hit = d;
-        break;
-      }
-    }
-    if (hit >= 0) {
-      if (hit == an) {
-        // the new anchor holds the iterate
-        if (V[1 - vcur] != c->U)
-          PICARD_CUDA(cudaMemcpyAsync(c->U, V[1 - vcur], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
-      } else {
-        // replay sweeps a+1..hit from the old anchor (unchanged in V[vcur])
-        PICARD_TRY(run_sweeps(a, int(hit - a), rcur, c->partials));
-        c->stats.sweep_launches += hit - a;
-        PICARD_CUDA(launch_finalize(K, V[vcur], c->w[hit % 2], sigma, c->U, 0, c->st));
-      }
-      *sweeps = hit;
-      *converged = true;
-      return PICARD_OK;
-    }
-    vcur = 1 - vcur;
-    rcur = 1 - rcur;
-    a = an;
-    if (a >= smax) {
-      if (V[vcur] != c->U)
-        PICARD_CUDA(cudaMemcpyAsync(c->U, V[vcur], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
-      *sweeps = a;
-      *converged = false;
-      return PICARD_OK;
-    }
-    m = next_batch(r2_prev, r2_last, tol2, c->m_max);
+  PICARD_CUDA(launch_anchor(K, c->G, S.V[S.vcur], S.V[1 - S.vcur], nullptr, c->b, S.R[S.rcur], sigma, c->partials, 1,
+                            c->st));
+  S.vcur = 1 - S.vcur;
+  return PICARD_OK;
+}
+
+int f32_plan(F32Solve& S) {
+  S.m_eff = int(std::min<long long>(S.m, S.smax - S.a));
+  return S.m_eff;
+}
+
+int f32_issue_tail(F32Solve& S) {
+  picard_ctx* c = S.c;
+  const KParams& K = c->K;
+  const int nb = c->G.nblocks;
+  // next anchor: fold w_{a+m_eff} into V, exact FP64 residual of that iterate
+  const long long an = S.a + S.m_eff;
+  PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
+  PICARD_CUDA(launch_anchor(K, c->G, S.V[S.vcur], S.V[1 - S.vcur], c->w[an % 2], c->b, S.R[1 - S.rcur], S.sigma,
+                            c->partials + (size_t)S.m_eff * nb, 0, c->st));
+  PICARD_CUDA(cudaEventRecord(c->ev[2], c->st));
+  PICARD_CUDA(launch_reduce_sweeps(c->partials, nb, S.m_eff + 1, c->r2, c->st));
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->r2, sizeof(double) * (S.m_eff + 1), cudaMemcpyDeviceToHost, c->st));
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 4, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  c->stats.d2h_bytes += (int64_t)sizeof(double) * (S.m_eff + 1) + (int64_t)sizeof(int);
+  return PICARD_OK;
+}
+
+int f32_finish(F32Solve& S, bool timed_sweeps) {
+  picard_ctx* c = S.c;
+  const KParams& K = c->K;
+  PICARD_CUDA(cudaStreamSynchronize(c->st));
+  if (c->h_pinned_i[4] == kDevTimeout) {
+    PICARD_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+    return fail(PICARD_ERR_TIMEOUT, "a Jacobi sweep timed out waiting for its TMA tiles");
   }
+  c->stats.sweep_launches += S.m_eff;
+  if (timed_sweeps) c->stats.sweep_ms += elapsed_ms(c, 0, 1);
+  c->stats.anchor_launches += 1;
+  c->stats.anchor_ms += elapsed_ms(c, 1, 2);
+  const double sigma = S.sigma;
+  const long long an = S.a + S.m_eff;
+  long long hit = -1;
+  // sweep a+t (t >= 2) measured iterate a+t-1 in FP32 (scaled by sigma^2);
+  // the anchor measured iterate a+m_eff in FP64
+  for (int t = 2; t <= S.m_eff + 1; ++t) {
+    long long d = S.a + t - 1;
+    double r2 = t <= S.m_eff ? c->h_pinned[t - 1] * sigma * sigma : c->h_pinned[S.m_eff];
+    S.r2_prev = S.r2_last;
+    S.r2_last = r2;
+    c->last_residual = std::sqrt(r2);
+    if (d >= 1 && d + 1 <= S.maxit && passes(r2, S.tol)) {
+      hit = d;
+      break;
+    }
+  }
+  if (hit >= 0) {
+    if (hit == an) {
+      // the new anchor holds the iterate
+      if (S.V[1 - S.vcur] != c->U)
+        PICARD_CUDA(cudaMemcpyAsync(c->U, S.V[1 - S.vcur], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+    } else {
+      // replay sweeps a+1..hit from the old anchor (unchanged in V[vcur])
+      PICARD_TRY(run_sweeps_single(c, S.a, int(hit - S.a), S.rcur, c->partials));
+      c->stats.sweep_launches += hit - S.a;
+      PICARD_CUDA(launch_finalize(K, S.V[S.vcur], c->w[hit % 2], sigma, c->U, 0, c->st));
+    }
+    S.sweeps = hit;
+    S.converged = true;
+    S.done = true;
+    return PICARD_OK;
+  }
+  S.vcur = 1 - S.vcur;
+  S.rcur = 1 - S.rcur;
+  S.a = an;
+  if (S.a >= S.smax) {
+    if (S.V[S.vcur] != c->U)
+      PICARD_CUDA(cudaMemcpyAsync(c->U, S.V[S.vcur], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
+    S.sweeps = S.a;
+    S.converged = false;
+    S.done = true;
+    return PICARD_OK;
+  }
+  S.m = next_batch(S.r2_prev, S.r2_last, S.tol2, c->m_max);
+  return PICARD_OK;
+}
+
+}  // namespace picard
+
+namespace {
+
+int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma, long long* sweeps,
+              bool* converged) {
+  F32Solve S;
+  PICARD_TRY(f32_begin(S, c, tol, smax, maxit, sigma));
+  while (!S.done) {
+    f32_plan(S);
+    PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
+    PICARD_TRY(run_sweeps_single(c, S.a, S.m_eff, S.rcur, c->partials));
+    PICARD_TRY(f32_issue_tail(S));
+    PICARD_TRY(f32_finish(S, true));
+  }
+  *sweeps = S.sweeps;
+  *converged = S.converged;
+  return PICARD_OK;
 }
 
 }  // namespace
 
-extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t maxit, int32_t* sweeps_out) {
-  if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
-  if (maxit < 0) return fail(PICARD_ERR_BAD_ARG, "maxit must be >= 0");
-  const KParams& K = c->K;
+namespace picard {
+
+int epot_rhs_issue(picard_ctx* c) {
   // b = -C/(dV eps0) and ||b||^2 over the interior (CalcEpotential.f90:50-54)
-  PICARD_CUDA(launch_rhs(K, c->C, c->b, c->red_partial, c->red_result + 4, c->st));
-  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->red_result + 4, sizeof(double), cudaMemcpyDeviceToHost, c->st));
-  PICARD_CUDA(cudaStreamSynchronize(c->st));
+  PICARD_CUDA(launch_rhs(c->K, c->C, c->b, c->red_partial, c->red_result + 4, c->st));
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned + kPinnedB2, c->red_result + 4, sizeof(double), cudaMemcpyDeviceToHost,
+                              c->st));
   c->stats.d2h_bytes += sizeof(double);
-  const double b2 = c->h_pinned[0];
-  const double bnorm = std::sqrt(b2);
-  const double tol = maxerr * bnorm;
-  const long long smax = 2LL * maxit + 1;
-  c->last_bnorm = bnorm;
-  long long sweeps = 0;
-  bool converged = true;
+  return PICARD_OK;
+}
+
+EpotSetup epot_setup(picard_ctx* c, double maxerr, int32_t maxit) {
+  const KParams& K = c->K;
+  EpotSetup e;
+  const double b2 = c->h_pinned[kPinnedB2];
+  e.bnorm = std::sqrt(b2);
+  e.tol = maxerr * e.bnorm;
+  e.smax = 2LL * maxit + 1;
+  e.maxit = maxit;
+  c->last_bnorm = e.bnorm;
   // the check at the top of sweep 1 uses r_global = ||b||^2 (CalcEpotential.f90:55-61)
-  if (1 <= maxit && std::sqrt(b2) <= tol) {
-    sweeps = 0;
-    c->last_residual = bnorm;
-  } else if (c->solver == PICARD_SOLVER_F64) {
-    PICARD_TRY(solve_f64(c, tol, smax, maxit, &sweeps, &converged));
-  } else {
-    long long nint = (long long)K.nx * K.ny * K.nz;
-    double sigma = std::sqrt(b2 / (double)nint);
-    if (!(sigma > 0.0)) sigma = 1.0;
-    PICARD_TRY(solve_f32(c, tol, smax, maxit, sigma, &sweeps, &converged));
-  }
-  PICARD_CUDA(launch_refresh_periodic(K, c->U, c->st));
+  e.trivial = 1 <= maxit && std::sqrt(b2) <= e.tol;
+  long long nint = (long long)K.nx * K.ny * K.nz;
+  e.sigma = std::sqrt(b2 / (double)nint);
+  if (!(e.sigma > 0.0)) e.sigma = 1.0;
+  return e;
+}
+
+int epot_finish(picard_ctx* c, const EpotSetup& e, long long sweeps, bool converged, int32_t* sweeps_out) {
+  if (e.trivial) c->last_residual = e.bnorm;
+  PICARD_CUDA(launch_refresh_periodic(c->K, c->U, c->st));
   c->last_sweeps = sweeps;
   c->stats.solves += 1;
   c->stats.sweeps += sweeps;
   c->stats.last_residual = c->last_residual;
-  c->stats.last_bnorm = bnorm;
+  c->stats.last_bnorm = e.bnorm;
   if (sweeps_out) *sweeps_out = int32_t(sweeps);
   if (!converged)
     return fail(PICARD_ERR_NOT_CONVERGED,
-                "Jacobi reached 2*maxit+1 = " + std::to_string(smax) + " sweeps without meeting maxerr");
+                "Jacobi reached 2*maxit+1 = " + std::to_string(e.smax) + " sweeps without meeting maxerr");
   return PICARD_OK;
+}
+
+}  // namespace picard
+
+extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t maxit, int32_t* sweeps_out) {
+  if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
+  if (maxit < 0) return fail(PICARD_ERR_BAD_ARG, "maxit must be >= 0");
+  PICARD_TRY(epot_rhs_issue(c));
+  PICARD_CUDA(cudaStreamSynchronize(c->st));
+  const EpotSetup e = epot_setup(c, maxerr, maxit);
+  long long sweeps = 0;
+  bool converged = true;
+  if (e.trivial) {
+    sweeps = 0;
+  } else if (c->solver == PICARD_SOLVER_F64) {
+    PICARD_TRY(solve_f64(c, e.tol, e.smax, maxit, &sweeps, &converged));
+  } else {
+    PICARD_TRY(solve_f32(c, e.tol, e.smax, maxit, e.sigma, &sweeps, &converged));
+  }
+  return epot_finish(c, e, sweeps, converged, sweeps_out);
 }
 
 // ------------------------------------------------------- sweep launch tuner

@@ -202,3 +202,15 @@ class Simulation:
 
 
 LOG_NONE = capi.LOG_FN()
+
+
+def batch_run_fused(sims: "list[Simulation]", iter_start: int, iter_end: int) -> list[int]:
+    """Advance independent runs together (picard_batch_run_fused): every run's
+    particle phases issued before any is waited for, all runs' Jacobi sweeps
+    in one launch per sweep.  Returns each run's Jacobi sweeps."""
+    n = len(sims)
+    arr = (C.c_void_p * n)(*[s._h.value for s in sims])
+    sweeps = (C.c_int64 * n)()
+    capi.check(capi.lib().picard_batch_run_fused(arr, n, iter_start, iter_end, sweeps), "picard_batch_run_fused",
+               (capi.OK, capi.ERR_NOT_CONVERGED))
+    return [int(v) for v in sweeps]
