@@ -46,7 +46,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["picard", "reference"], default="picard")
-    ap.add_argument("--workload", choices=["scale", "plain32", "poisson", "serving", "precision"], default="scale")
+    ap.add_argument("--workload", choices=["scale", "plain32", "poisson", "serving", "precision", "batch"],
+                    default="scale")
+    ap.add_argument("--runs", type=int, default=64, help="batch workload: runs in the parameter sweep")
     ap.add_argument("--precision-n", type=int, default=512, help="precision workload: box edge in cells")
     ap.add_argument("--precision-sweeps", type=int, default=4001, help="precision workload: Jacobi sweeps compared")
     ap.add_argument("--requests", type=int, default=12, help="serving workload: runs in the arrival stream")
@@ -610,6 +612,92 @@ def run_precision(args, local_rank):
     print(json.dumps(out), flush=True)
 
 
+def run_batch(args, local_rank):
+    """Batched parameter sweep: --runs independent runs (cubic grids 16..96
+    cells, 8..32 ppc, drift 300..800 km/s, |B| 1..10 nT in a random direction,
+    --run-steps iterations each, CELL32 / F32_REFINE) advanced two ways:
+      plain:   one run after another through picard_gpu_run_fused;
+      batched: all runs together through picard_batch_run_fused (one sweep
+               launch per sweep for every run).
+    Both arms create, initialise, run and release every run inside the timed
+    region (the sweep launch tuner runs at creation in both).  Reports
+    particle-steps/s of each arm and checks that every run ends bit for bit
+    where it ends alone."""
+    import numpy as np
+    import torch
+
+    from picard_b200 import capi
+    from picard_b200 import params as P
+    from picard_b200.simulation import Simulation, batch_run_fused
+
+    torch.cuda.set_device(local_rank)
+    sets = P.batch_set(seed=0, count=args.runs)
+    runs = []
+    for p, steps in sets:
+        if args.run_steps != steps:
+            p = P._size_capacity(p, args.run_steps, max(1, int(p.ppc[1])))
+        runs.append(capi.params_derive(p))
+    steps = args.run_steps
+    layout, solver = capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE
+    # warm-up: kernels loaded, one small run
+    w = Simulation(runs[0], derive=False, layout=layout, solver=solver)
+    w.calc_distance()
+    w.particles_initialize()
+    w.run_fused(0, 1)
+    w.close()
+    torch.cuda.synchronize()
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = ClockSampler(int(visible.split(",")[local_rank]) if visible else local_rank)
+    clocks.start()
+    t0 = time.perf_counter()
+    plain = []
+    for p in runs:
+        g = Simulation(p, derive=False, layout=layout, solver=solver)
+        g.calc_distance()
+        g.particles_initialize()
+        sw = g.run_fused(0, steps)
+        plain.append({"sweeps": sw, "particle_steps": g.stats()["particle_steps"],
+                      "u": float(np.abs(g.field(capi.FIELD_U)).sum()), "n": g.num_local})
+        g.close()
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sims = []
+    for p in runs:
+        g = Simulation(p, derive=False, layout=layout, solver=solver)
+        g.calc_distance()
+        g.particles_initialize()
+        sims.append(g)
+    sweeps = batch_run_fused(sims, 0, steps)
+    batched = []
+    for g, sw in zip(sims, sweeps):
+        batched.append({"sweeps": sw, "particle_steps": g.stats()["particle_steps"],
+                        "u": float(np.abs(g.field(capi.FIELD_U)).sum()), "n": g.num_local})
+        g.close()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    clk = clocks.stop()
+    same = all(a["u"] == b["u"] and a["n"] == b["n"] and a["sweeps"] == b["sweeps"] for a, b in zip(plain, batched))
+    ps_plain = sum(r["particle_steps"] for r in plain)
+    ps_batch = sum(r["particle_steps"] for r in batched)
+    line = {
+        "metric": "particle-steps/s, batched vs plain", "value": ps_batch / t_batch, "unit": UNIT, "n_gpus": 1,
+        "higher_is_better": True, "impl": "picard", "workload": "batch", "vs_baseline": None,
+        "dtype": "f32 particles, f32 Jacobi sweeps with f64 anchors",
+        "data": "synthetic (seeded Philox plasma, run seeds 0..runs-1)",
+        "config": {"workload": f"batched parameter sweep: {len(runs)} runs, cubic grids 16..96 cells, 8..32 ppc, "
+                               f"drift 300..800 km/s, |B| 1..10 nT random direction, {steps} steps each",
+                   "grids": [int(p.nx) for p in runs]},
+        "batched": {"particle_steps_per_s": ps_batch / t_batch, "seconds": t_batch},
+        "plain": {"particle_steps_per_s": ps_plain / t_plain, "seconds": t_plain},
+        "batched_over_plain": (ps_batch / t_batch) / (ps_plain / t_plain),
+        "jacobi_sweeps_total": sum(r["sweeps"] for r in batched),
+        "results_identical_to_plain": same,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -638,6 +726,10 @@ def main():
         return
     if args.workload == "poisson":
         run_poisson(args, local_rank)
+        return
+    if args.workload == "batch":
+        if rank == 0:
+            run_batch(args, local_rank)
         return
     if args.workload == "precision":
         if rank == 0:
