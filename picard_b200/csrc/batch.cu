@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) sweep_batch_kernel(const __grid_constant_
 }
 
 template <int ZC>
-cudaError_t launch_batch_zc(const BatchArgs& A, cudaStream_t st) {
+cudaError_t launch_batch_zc(const BatchArgs& A, int pdl, cudaStream_t st) {
   constexpr size_t smem = sizeof(float) * ((size_t)(ZC + 2) * 10 * 72 + (size_t)ZC * 8 * 64);
   static bool attr = false;
   if (!attr) {
@@ -201,7 +201,7 @@ cudaError_t launch_batch_zc(const BatchArgs& A, cudaStream_t st) {
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
+  at[0].val.programmaticStreamSerializationAllowed = pdl;
   cfg.attrs = at;
   cfg.numAttrs = 1;
   note_launch();
@@ -219,15 +219,23 @@ struct RunSolve {
 };
 
 // Sweep t (1-based) of the current round for every run with m_eff >= t, in
-// launches of at most kBatchRuns runs of one tile depth.
+// launches of at most kBatchRuns runs of one tile depth.  The first launch of
+// a round follows event waits on the runs' streams (their anchors), which a
+// programmatic dependent launch would not cover -- griddepcontrol.wait only
+// orders a kernel after its predecessor on the same stream -- so it is a plain
+// launch; the round's later launches depend on the batch stream alone and
+// overlap their predecessors' tails.
 int launch_round_sweep(std::vector<RunSolve*>& runs, int t, int* err, cudaStream_t st) {
+  bool first = t == 1;
   for (int zc : {4, 8}) {
     BatchArgs A;
     std::memset(&A, 0, sizeof(A));
     A.err = err;
     auto flush = [&]() -> int {
       if (A.nruns == 0) return PICARD_OK;
-      cudaError_t e = zc == 8 ? launch_batch_zc<8>(A, st) : launch_batch_zc<4>(A, st);
+      const int pdl = first ? 0 : 1;
+      first = false;
+      cudaError_t e = zc == 8 ? launch_batch_zc<8>(A, pdl, st) : launch_batch_zc<4>(A, pdl, st);
       PICARD_CUDA(e);
       std::memset(&A, 0, sizeof(A));
       A.err = err;
