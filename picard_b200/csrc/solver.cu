@@ -245,6 +245,13 @@ int f32_finish(F32Solve& S, bool timed_sweeps) {
   c->stats.anchor_ms += elapsed_ms(c, 1, 2);
   const double sigma = S.sigma;
   const long long an = S.a + S.m_eff;
+  if (const char* v = std::getenv("PICARD_SOLVE_LOG"); v && *v && *v != '0') {
+    double sum = 0.0;
+    for (int t = 0; t <= S.m_eff; ++t) sum += c->h_pinned[t];
+    std::fprintf(stderr, "picard solve %dx%dx%d seed=%llu a=%lld m=%d r2[1]=%.17g r2[m]=%.17g sum=%.17g\n", c->K.nx,
+                 c->K.ny, c->K.nz, (unsigned long long)c->prm.seed, S.a, S.m_eff, S.m_eff > 1 ? c->h_pinned[1] : 0.0,
+                 c->h_pinned[S.m_eff], sum);
+  }
   long long hit = -1;
   // sweep a+t (t >= 2) measured iterate a+t-1 in FP32 (scaled by sigma^2);
   // the anchor measured iterate a+m_eff in FP64
