@@ -244,13 +244,14 @@ int launch_round_sweep(std::vector<RunSolve*>& runs, int t, int* err, cudaStream
     for (RunSolve* rs : runs) {
       if (rs->done || !rs->batched || rs->S.m_eff < t || rs->c->G.zc != zc) continue;
       picard_ctx* c = rs->c;
-      const long long s = rs->S.a + t;
+      const int in = rs->S.wcur, out = 1 - in;  // never write the buffer being read
       BatchRun& R = A.run[A.nruns];
-      R.tw = c->tmw2[(s - 1) % 2];
+      R.tw = c->tmw2[in];
       R.tr = c->tmr2[rs->S.rcur];
       R.S = make_stencil(c->K);
       R.J = jacobi_coef_f(c->K);
-      R.wout = c->w[s % 2];
+      R.wout = c->w[out];
+      rs->S.wcur = out;
       R.partial = c->partials + (size_t)(t - 1) * c->G.nblocks;
       R.gx2 = (c->K.nx + 63) / 64;
       R.gx = (int)c->G.grid.x;

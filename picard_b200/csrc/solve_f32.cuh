@@ -13,8 +13,8 @@
 //   f32_begin       anchor 0 on the context stream
 //   f32_plan        m_eff of the next round
 //   (the caller runs sweeps a+1 .. a+m_eff, partials of sweep a+t at
-//    ctx->partials + (t-1) * nblocks: run_sweeps_single, or the batched
-//    multi-run launch)
+//    ctx->partials + (t-1) * nblocks, S.wcur following the latest iterate:
+//    run_sweeps_single, or the batched multi-run launch)
 //   f32_issue_tail  anchor, reduction and the host copy, asynchronously
 //   f32_finish      after the copy: stop test, replay, next batch length
 #pragma once
@@ -31,6 +31,7 @@ struct F32Solve {
   double* V[2] = {nullptr, nullptr};
   float* R[2] = {nullptr, nullptr};
   int vcur = 0, rcur = 0;
+  int wcur = 0;  // buffer (ctx->w[wcur]) holding the latest increment
   long long a = 0;
   int m = 64, m_eff = 0;
   double r2_prev = 0.0, r2_last = 0.0;
@@ -58,7 +59,8 @@ int f32_plan(F32Solve& S);
 int f32_issue_tail(F32Solve& S);
 // timed_sweeps: the context's events ev[0] and ev[1] bracket the round's sweeps
 int f32_finish(F32Solve& S, bool timed_sweeps);
-// Sweeps a0+1 .. a0+count of one run with its own launches.
-int run_sweeps_single(picard_ctx* c, long long a0, int count, int rsel, double* partial_base);
+// count sweeps of one run with its own launches, the first from w = 0; each
+// launch reads ctx->w[*wcur] and writes the other buffer, *wcur following.
+int run_sweeps_single(picard_ctx* c, int count, int rsel, double* partial_base, int* wcur);
 
 }  // namespace picard

@@ -147,21 +147,25 @@ int solve_f64(picard_ctx* c, double tol, long long smax, int maxit, long long* s
 
 namespace picard {
 
-// One sweep s (1-based from the anchor) of run c: reads w[(s-1)%2] and the
-// anchor residual R[rsel], writes w[s%2] and the sweep's tile partials.
-static cudaError_t single_sweep(picard_ctx* c, long long s, int rsel, double* partial, int w_zero) {
+// The increment ping-pongs between c->w[0] and c->w[1]; *wcur names the
+// buffer holding the latest iterate, and every launch writes the other one --
+// a launch never writes the buffer it reads (the two-sweep kernel included:
+// its CTAs load their halos from the input while others store their tiles).
+
+// One sweep of run c: reads w[in] and the anchor residual R[rsel], writes
+// w[1 - in] and the sweep's tile partials.
+static cudaError_t single_sweep(picard_ctx* c, int in, int rsel, double* partial, int w_zero) {
   const KParams& K = c->K;
   float* R[2] = {c->r, c->r + f32_elems(K)};
+  const int out = 1 - in;
   if (c->G.tma && c->G.pairs)
-    return launch_sweep_tma2(K, c->G, &c->tmw2[(s - 1) % 2], &c->tmr2[rsel], c->w[s % 2], partial, w_zero,
-                             c->d_err, c->st);
+    return launch_sweep_tma2(K, c->G, &c->tmw2[in], &c->tmr2[rsel], c->w[out], partial, w_zero, c->d_err, c->st);
   if (c->G.tma)
-    return launch_sweep_tma(K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[rsel], c->w[s % 2], partial, w_zero, c->d_err,
-                            c->st);
-  return launch_sweep_f32(K, c->G, c->w[(s - 1) % 2], c->w[s % 2], R[rsel], partial, w_zero, c->st);
+    return launch_sweep_tma(K, c->G, &c->tmw[in], &c->tmr[rsel], c->w[out], partial, w_zero, c->d_err, c->st);
+  return launch_sweep_f32(K, c->G, c->w[in], c->w[out], R[rsel], partial, w_zero, c->st);
 }
 
-int run_sweeps_single(picard_ctx* c, long long a0, int count, int rsel, double* partial_base) {
+int run_sweeps_single(picard_ctx* c, int count, int rsel, double* partial_base, int* wcur) {
   const KParams& K = c->K;
   const int nb = c->G.nblocks;
   float* R[2] = {c->r, c->r + f32_elems(K)};
@@ -169,22 +173,28 @@ int run_sweeps_single(picard_ctx* c, long long a0, int count, int rsel, double* 
     // one resident launch at a time on the device: its CTAs must all be
     // resident together, which another cooperative grid could prevent
     std::lock_guard<std::mutex> lk(g_resident_mu);
-    PICARD_CUDA(launch_sweeps_resident(K, c->G, R[rsel], nullptr, c->w[(a0 + count) % 2], c->res_faces, c->res_bar,
-                                       partial_base, count, 1, c->d_err, c->st));
+    const int out = 1 - *wcur;
+    PICARD_CUDA(launch_sweeps_resident(K, c->G, R[rsel], nullptr, c->w[out], c->res_faces, c->res_bar, partial_base,
+                                       count, 1, c->d_err, c->st));
     PICARD_CUDA(cudaStreamSynchronize(c->st));
+    *wcur = out;
     return PICARD_OK;
   }
   int t = 1;
   if (c->G.tma && c->G.pairs && c->G.fused2) {
-    // sweeps a0+t and a0+t+1 per launch: reads w[(s-1)%2], writes w[(s+1)%2]
+    // sweeps t and t+1 per launch
     for (; t + 1 <= count; t += 2) {
-      const long long s = a0 + t;
-      PICARD_CUDA(launch_sweep2_tma(K, c->G, &c->tmw3[(s - 1) % 2], &c->tmr3[rsel], c->w[(s + 1) % 2],
+      const int out = 1 - *wcur;
+      PICARD_CUDA(launch_sweep2_tma(K, c->G, &c->tmw3[*wcur], &c->tmr3[rsel], c->w[out],
                                     partial_base + (size_t)(t - 1) * nb, partial_base + (size_t)t * nb,
                                     t == 1 ? 1 : 0, c->d_err, c->st));
+      *wcur = out;
     }
   }
-  for (; t <= count; ++t) PICARD_CUDA(single_sweep(c, a0 + t, rsel, partial_base + (size_t)(t - 1) * nb, t == 1 ? 1 : 0));
+  for (; t <= count; ++t) {
+    PICARD_CUDA(single_sweep(c, *wcur, rsel, partial_base + (size_t)(t - 1) * nb, t == 1 ? 1 : 0));
+    *wcur = 1 - *wcur;
+  }
   return PICARD_OK;
 }
 
@@ -218,10 +228,9 @@ int f32_issue_tail(F32Solve& S) {
   picard_ctx* c = S.c;
   const KParams& K = c->K;
   const int nb = c->G.nblocks;
-  // next anchor: fold w_{a+m_eff} into V, exact FP64 residual of that iterate
-  const long long an = S.a + S.m_eff;
+  // next anchor: fold w_{a+m_eff} (in w[wcur]) into V, exact FP64 residual of that iterate
   PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
-  PICARD_CUDA(launch_anchor(K, c->G, S.V[S.vcur], S.V[1 - S.vcur], c->w[an % 2], c->b, S.R[1 - S.rcur], S.sigma,
+  PICARD_CUDA(launch_anchor(K, c->G, S.V[S.vcur], S.V[1 - S.vcur], c->w[S.wcur], c->b, S.R[1 - S.rcur], S.sigma,
                             c->partials + (size_t)S.m_eff * nb, 0, c->st));
   PICARD_CUDA(cudaEventRecord(c->ev[2], c->st));
   PICARD_CUDA(launch_reduce_sweeps(c->partials, nb, S.m_eff + 1, c->r2, c->st));
@@ -273,9 +282,10 @@ int f32_finish(F32Solve& S, bool timed_sweeps) {
         PICARD_CUDA(cudaMemcpyAsync(c->U, S.V[1 - S.vcur], sizeof(double) * K.nodes, cudaMemcpyDeviceToDevice, c->st));
     } else {
       // replay sweeps a+1..hit from the old anchor (unchanged in V[vcur])
-      PICARD_TRY(run_sweeps_single(c, S.a, int(hit - S.a), S.rcur, c->partials));
+      int wr = S.wcur;
+      PICARD_TRY(run_sweeps_single(c, int(hit - S.a), S.rcur, c->partials, &wr));
       c->stats.sweep_launches += hit - S.a;
-      PICARD_CUDA(launch_finalize(K, S.V[S.vcur], c->w[hit % 2], sigma, c->U, 0, c->st));
+      PICARD_CUDA(launch_finalize(K, S.V[S.vcur], c->w[wr], sigma, c->U, 0, c->st));
     }
     S.sweeps = hit;
     S.converged = true;
@@ -308,7 +318,7 @@ int solve_f32(picard_ctx* c, double tol, long long smax, int maxit, double sigma
   while (!S.done) {
     f32_plan(S);
     PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
-    PICARD_TRY(run_sweeps_single(c, S.a, S.m_eff, S.rcur, c->partials));
+    PICARD_TRY(run_sweeps_single(c, S.m_eff, S.rcur, c->partials, &S.wcur));
     PICARD_TRY(f32_issue_tail(S));
     PICARD_TRY(f32_finish(S, true));
   }
@@ -521,19 +531,22 @@ int tune_sweep(picard_ctx* c, bool fresh) {
         PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
         PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
       } else {
+        // reads w[in], writes w[1 - in] (the launch after reads what this one wrote)
         auto one = [&](int s) {
+          const int in = (s - 1) % 2, out = 1 - in;
           if (c->G.fused2)  // sweeps s, s+1
-            return launch_sweep2_tma(c->K, c->G, &c->tmw3[(s - 1) % 2], &c->tmr3[0], c->w[(s + 1) % 2],
-                                     c->partials, c->partials + c->G.nblocks, 0, c->d_err, c->st);
-          return c->G.pairs ? launch_sweep_tma2(c->K, c->G, &c->tmw2[(s - 1) % 2], &c->tmr2[0], c->w[s % 2],
-                                                c->partials, 0, c->d_err, c->st)
-                            : launch_sweep_tma(c->K, c->G, &c->tmw[(s - 1) % 2], &c->tmr[0], c->w[s % 2],
-                                               c->partials, 0, c->d_err, c->st);
+            return launch_sweep2_tma(c->K, c->G, &c->tmw3[in], &c->tmr3[0], c->w[out], c->partials,
+                                     c->partials + c->G.nblocks, 0, c->d_err, c->st);
+          return c->G.pairs ? launch_sweep_tma2(c->K, c->G, &c->tmw2[in], &c->tmr2[0], c->w[out], c->partials, 0,
+                                                c->d_err, c->st)
+                            : launch_sweep_tma(c->K, c->G, &c->tmw[in], &c->tmr[0], c->w[out], c->partials, 0,
+                                               c->d_err, c->st);
         };
         const int step = c->G.fused2 ? 2 : 1;
-        for (int s = 1; s <= 2 * step; s += step) PICARD_CUDA(one(s));
+        int q2 = 1;
+        for (int s = 1; s <= 2 * step; s += step) PICARD_CUDA(one(q2++));
         PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
-        for (int s = 1; s <= kReps; s += step) PICARD_CUDA(one(s));
+        for (int s = 1; s <= kReps; s += step) PICARD_CUDA(one(q2++));
         PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
         PICARD_CUDA(cudaEventSynchronize(c->ev[1]));
       }
