@@ -353,7 +353,7 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
       for (int r = 0; r < n; ++r) {
         picard_ctx* c = ctxs[r];
         PICARD_TRY(picard_gpu_particles_gridify(c));
-        PICARD_TRY(picard_gpu_bc_potentials(c));
+        PICARD_TRY(bc_potentials_async(c));
         PICARD_TRY(epot_rhs_issue(c));
       }
       // ---- CalcEpotential: lockstep rounds over the runs
@@ -431,7 +431,10 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
         c->stats.particle_steps += c->num_local;
       }
     }
-    for (int r = 0; r < n; ++r) PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
+    for (int r = 0; r < n; ++r) {
+      PICARD_TRY(count_issue(ctxs[r]));  // a wait that gave up in the last step
+      PICARD_TRY(count_collect(ctxs[r]));
+    }
     return PICARD_OK;
   };
   rc = body();

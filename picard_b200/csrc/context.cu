@@ -228,6 +228,10 @@ int check_dev_err(picard_ctx* c) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
     return fail(PICARD_ERR_CAPACITY, "particle capacity max_per_proc exceeded on the device");
   }
+  if (e == kDevTimeout) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+    return fail(PICARD_ERR_TIMEOUT, "a bounded device wait gave up");
+  }
   return PICARD_OK;
 }
 
@@ -257,6 +261,25 @@ int sync_count_public(picard_ctx* c) {
   return sync_count(c);
 }
 
+int check_dev_err_public(picard_ctx* c) { return check_dev_err(c); }
+
+int bc_potentials_async(picard_ctx* c) {
+  if (c->bcpot_tensor) {
+    if (!c->tc_cs) {
+      long long cs = 0, pe = 0;
+      bcpot_tc_scratch(c->K, &cs, &pe);
+      unsigned short* csb = nullptr;
+      PICARD_TRY(dalloc(c, csb, (size_t)cs));
+      PICARD_TRY(dalloc(c, c->tc_partial, (size_t)pe));
+      c->tc_cs = csb;
+    }
+    PICARD_CUDA(launch_bc_potentials_tc(c->K, c->C, c->D, c->U, c->tc_cs, c->tc_partial, c->d_err, c->st));
+    return PICARD_OK;
+  }
+  PICARD_CUDA(launch_bc_potentials(c->K, c->C, c->D, c->U, c->st));
+  return PICARD_OK;
+}
+
 int count_issue(picard_ctx* c) {
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 2, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i, c->d_count + c->cur, sizeof(int), cudaMemcpyDeviceToHost, c->st));
@@ -269,6 +292,10 @@ int count_collect(picard_ctx* c) {
   if (c->h_pinned_i[2] == kDevCapacity) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
     return fail(PICARD_ERR_CAPACITY, "particle capacity max_per_proc exceeded on the device");
+  }
+  if (c->h_pinned_i[2] == kDevTimeout) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+    return fail(PICARD_ERR_TIMEOUT, "a bounded device wait gave up");
   }
   c->num_local = c->h_pinned_i[0];
   return PICARD_OK;
@@ -786,20 +813,8 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
 // BCpotentials.f90:1-145
 int picard_gpu_bc_potentials(picard_ctx* c) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
-  if (c->bcpot_tensor) {
-    if (!c->tc_cs) {
-      long long cs = 0, pe = 0;
-      bcpot_tc_scratch(c->K, &cs, &pe);
-      unsigned short* csb = nullptr;
-      PICARD_TRY(dalloc(c, csb, (size_t)cs));
-      PICARD_TRY(dalloc(c, c->tc_partial, (size_t)pe));
-      c->tc_cs = csb;
-    }
-    PICARD_CUDA(launch_bc_potentials_tc(c->K, c->C, c->D, c->U, c->tc_cs, c->tc_partial, c->d_err, c->st));
-    return check_dev_err_timeout(c);
-  }
-  PICARD_CUDA(launch_bc_potentials(c->K, c->C, c->D, c->U, c->st));
-  return PICARD_OK;
+  PICARD_TRY(bc_potentials_async(c));
+  return c->bcpot_tensor ? check_dev_err_timeout(c) : PICARD_OK;
 }
 
 // CalcEfield.f90:3-232

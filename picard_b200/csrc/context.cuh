@@ -100,6 +100,12 @@ int sync_count_public(picard_ctx* c);
 // The same in two halves, so that many contexts' counts travel together:
 // count_issue queues the copies, count_collect waits for the context's stream.
 int count_issue(picard_ctx* c);
+// BCpotentials without waiting for the device: a tensor-core timeout stays in
+// the context's error word, which the Jacobi solve that follows reads.
+int bc_potentials_async(picard_ctx* c);
+// Waits for the context's stream and reports a capacity overflow or a device
+// wait that gave up, recorded in the context's error word.
+int check_dev_err_public(picard_ctx* c);
 int count_collect(picard_ctx* c);
 // Device memory owned by the context (zeroed, freed with it).
 int dev_alloc(picard_ctx* c, void** p, size_t bytes);

@@ -241,7 +241,7 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
     PICARD_CUDA(cudaEventRecord(c->pev[1], c->st));
     PICARD_TRY(picard_gpu_particles_gridify(c));
     PICARD_CUDA(cudaEventRecord(c->pev[2], c->st));
-    PICARD_TRY(picard_gpu_bc_potentials(c));
+    PICARD_TRY(bc_potentials_async(c));  // a timeout surfaces through the solve's error check
     PICARD_CUDA(cudaEventRecord(c->pev[3], c->st));
     int32_t sw = 0;
     int rc = picard_gpu_calc_epotential(c, p.maxerr, p.maxit, &sw);
@@ -263,6 +263,7 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
     c->stats.particle_steps += c->num_local;
   }
   PICARD_CUDA(cudaStreamSynchronize(c->st));
+  PICARD_TRY(check_dev_err_public(c));  // a wait that gave up in the last step
   if (nc) return fail(PICARD_ERR_NOT_CONVERGED, "at least one Jacobi solve hit 2*maxit+1 sweeps");
   return PICARD_OK;
 }

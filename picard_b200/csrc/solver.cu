@@ -60,7 +60,7 @@ int check_timeout(picard_ctx* c) {
   c->stats.d2h_bytes += sizeof(int);
   if (c->h_pinned_i[4] == kDevTimeout) {
     PICARD_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
-    return fail(PICARD_ERR_TIMEOUT, "a Jacobi sweep timed out waiting for its TMA tiles");
+    return fail(PICARD_ERR_TIMEOUT, "a bounded device wait (TMA tiles, tensor-core MMAs or a grid barrier) gave up");
   }
   return PICARD_OK;
 }
@@ -246,7 +246,7 @@ int f32_finish(F32Solve& S, bool timed_sweeps) {
   PICARD_CUDA(cudaStreamSynchronize(c->st));
   if (c->h_pinned_i[4] == kDevTimeout) {
     PICARD_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
-    return fail(PICARD_ERR_TIMEOUT, "a Jacobi sweep timed out waiting for its TMA tiles");
+    return fail(PICARD_ERR_TIMEOUT, "a bounded device wait (TMA tiles, tensor-core MMAs or a grid barrier) gave up");
   }
   c->stats.sweep_launches += S.m_eff;
   if (timed_sweeps) c->stats.sweep_ms += elapsed_ms(c, 0, 1);
