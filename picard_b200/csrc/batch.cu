@@ -17,6 +17,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -308,8 +311,21 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
   std::vector<RunSolve*> rp(n);
   for (int r = 0; r < n; ++r) rp[r] = &solves[r];
 
+  // PICARD_BATCH_LOG=1: host time per phase (waits for the device included)
+  const char* logv = std::getenv("PICARD_BATCH_LOG");
+  const bool log = logv && *logv && *logv != '0';
+  double ph[6] = {0, 0, 0, 0, 0, 0};
+  long long rounds = 0, launches = 0;
+  auto now = []() { return std::chrono::steady_clock::now(); };
+  auto tick = now();
+  auto lap = [&](int k) {
+    auto t = now();
+    ph[k] += std::chrono::duration<double, std::milli>(t - tick).count();
+    tick = t;
+  };
   auto body = [&]() -> int {
     for (int32_t it = iter_start + 1; it <= iter_end; ++it) {
+      tick = now();
       // ---- AdvancePosition, ParticlesProduce (device count) for every run
       for (int r = 0; r < n; ++r) {
         picard_ctx* c = ctxs[r];
@@ -328,6 +344,7 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
         PICARD_TRY(count_issue(c));
       }
       for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));
+      lap(0);
       // ---- BCoutflow + ParticlesTransfer (compaction), BCinflow (fused)
       for (int r = 0; r < n; ++r) {
         picard_ctx* c = ctxs[r];
@@ -349,6 +366,7 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
         PICARD_TRY(count_issue(c));
       }
       for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));
+      lap(1);
       // ---- ParticlesGridify, BCpotentials, b and ||b||
       for (int r = 0; r < n; ++r) {
         picard_ctx* c = ctxs[r];
@@ -357,12 +375,13 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
         PICARD_TRY(epot_rhs_issue(c));
       }
       // ---- CalcEpotential: lockstep rounds over the runs
+      for (int r = 0; r < n; ++r) PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
+      lap(2);
       for (int r = 0; r < n; ++r) {
         picard_ctx* c = ctxs[r];
         RunSolve& rs = solves[r];
         rs = RunSolve();
         rs.c = c;
-        PICARD_CUDA(cudaStreamSynchronize(c->st));
         rs.e = epot_setup(c, c->prm.maxerr, c->prm.maxit);
         rs.done = rs.e.trivial;
         rs.sweeps = 0;
@@ -395,6 +414,8 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
           PICARD_CUDA(cudaStreamWaitEvent(bst, rev[r], 0));
         }
         for (int t = 1; t <= M; ++t) PICARD_TRY(launch_round_sweep(rp, t, berr, bst));
+        ++rounds;
+        launches += M;
         PICARD_CUDA(cudaEventRecord(bev, bst));
         for (int r = 0; r < n; ++r) {
           if (solves[r].done || !solves[r].batched) continue;
@@ -422,6 +443,7 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
         else if (q != PICARD_OK) return q;
         if (sweeps_total) sweeps_total[r] += sw;
       }
+      lap(3);
       // ---- CalcEfield + BCfields, AdvanceVelocity
       for (int r = 0; r < n; ++r) {
         picard_ctx* c = ctxs[r];
@@ -430,6 +452,7 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
         c->stats.steps += 1;
         c->stats.particle_steps += c->num_local;
       }
+      lap(4);
     }
     for (int r = 0; r < n; ++r) {
       PICARD_TRY(count_issue(ctxs[r]));  // a wait that gave up in the last step
@@ -438,6 +461,11 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
     return PICARD_OK;
   };
   rc = body();
+  if (log)
+    std::fprintf(stderr,
+                 "picard batch %d runs: particles %.1f ms, compaction+inflow %.1f ms, deposit+bcpot+rhs %.1f ms, "
+                 "jacobi %.1f ms (%lld rounds, %lld sweep steps), push %.1f ms\n",
+                 n, ph[0], ph[1], ph[2], ph[3], rounds, launches, ph[4]);
   if (rc == PICARD_OK) rc = check_cuda(cudaStreamSynchronize(bst), "batch stream");
   cleanup();
   if (rc != PICARD_OK) return rc;
