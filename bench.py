@@ -457,13 +457,19 @@ def run_serving(args, local_rank):
         reqs.append((t, capi.params_derive(p), args.run_steps))
     layout, solver = capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE
 
-    # warm-up: load the kernels, tune nothing that the timed arms reuse
+    # warm-up, untimed: load the kernels, and run the sweep launch tuner once per
+    # grid shape (cached for the process) so that neither arm pays for tuning
     w = P.config_plain_scale(seed=99, nx=16, ny=16, nz=16, ppc_ion=2)
     sim = Simulation(w, layout=layout, solver=solver)
     sim.calc_distance()
     sim.particles_initialize()
     sim.run_fused(0, 2)
     sim.close()
+    seen = set()
+    for _, p, _ in reqs:
+        if (p.nx, p.ny, p.nz) not in seen:
+            seen.add((p.nx, p.ny, p.nz))
+            Simulation(p, derive=False, layout=layout, solver=solver).close()
     torch.cuda.synchronize()
 
     visible = os.environ.get("CUDA_VISIBLE_DEVICES")
@@ -639,24 +645,35 @@ def run_batch(args, local_rank):
         runs.append(capi.params_derive(p))
     steps = args.run_steps
     layout, solver = capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE
-    # warm-up: kernels loaded, one small run
+    # warm-up, untimed: kernels loaded, and the sweep launch tuner run once per
+    # grid shape (its choices are cached for the process), so that neither
+    # arm pays for tuning
     w = Simulation(runs[0], derive=False, layout=layout, solver=solver)
     w.calc_distance()
     w.particles_initialize()
     w.run_fused(0, 1)
     w.close()
+    seen = set()
+    for p in runs:
+        if (p.nx, p.ny, p.nz) not in seen:
+            seen.add((p.nx, p.ny, p.nz))
+            Simulation(p, derive=False, layout=layout, solver=solver).close()
     torch.cuda.synchronize()
     visible = os.environ.get("CUDA_VISIBLE_DEVICES")
     clocks = ClockSampler(int(visible.split(",")[local_rank]) if visible else local_rank)
     clocks.start()
     t0 = time.perf_counter()
     plain = []
+    plain_phase = {}
     for p in runs:
         g = Simulation(p, derive=False, layout=layout, solver=solver)
         g.calc_distance()
         g.particles_initialize()
         sw = g.run_fused(0, steps)
-        plain.append({"sweeps": sw, "particle_steps": g.stats()["particle_steps"],
+        st = g.stats()
+        for k, v in st["phase_ms"].items():
+            plain_phase[k] = plain_phase.get(k, 0.0) + v
+        plain.append({"sweeps": sw, "particle_steps": st["particle_steps"],
                       "u": float(np.abs(g.field(capi.FIELD_U)).sum()), "n": g.num_local})
         g.close()
     torch.cuda.synchronize()
@@ -693,7 +710,8 @@ def run_batch(args, local_rank):
                                f"drift 300..800 km/s, |B| 1..10 nT random direction, {steps} steps each",
                    "grids": [int(p.nx) for p in runs]},
         "batched": {"particle_steps_per_s": ps_batch / t_batch, "seconds": t_batch},
-        "plain": {"particle_steps_per_s": ps_plain / t_plain, "seconds": t_plain},
+        "plain": {"particle_steps_per_s": ps_plain / t_plain, "seconds": t_plain,
+                  "phase_ms": {k: round(v, 1) for k, v in plain_phase.items()}},
         "batched_over_plain": (ps_batch / t_batch) / (ps_plain / t_plain),
         "jacobi_sweeps_total": sum(r["sweeps"] for r in batched),
         "results_identical_to_plain": same,

@@ -30,6 +30,7 @@
 #include "picard_gpu.h"
 #include "solve_f32.cuh"
 #include "stencil.cuh"
+#include "pair_tile.cuh"
 
 using namespace picard;
 
@@ -56,8 +57,9 @@ struct BatchArgs {
 };
 static_assert(sizeof(BatchArgs) < 32000, "kernel parameter space");
 
-// The x-pair sweep (grid.cu sweep_tma2_kernel) over a table of runs: CTA t
-// takes tile t - tile_base of the run whose tile range holds t.
+// The x-pair sweep (pair_tile.cuh, as in grid.cu sweep_tma2_kernel) over a
+// table of runs: CTA t takes tile t - tile_base of the run whose tile range
+// holds t.
 template <int ZC>
 __global__ void __launch_bounds__(256) sweep_batch_kernel(const __grid_constant__ BatchArgs A) {
   constexpr int kBoxX = 72, kTile = 64, kTy = 8, kTx = 32;
@@ -130,62 +132,7 @@ __global__ void __launch_bounds__(256) sweep_batch_kernel(const __grid_constant_
     }
     return;
   }
-  const Stencil& S = R.S;
-  const JacobiCoefF& J = R.J;
-  const int i0 = x0 + 2 * tx + 1, j = y0 + ty + 1;
-  const bool act0 = i0 <= S.nx && j <= S.ny, act1 = i0 + 1 <= S.nx && j <= S.ny;
-  const int kend = min(ZC, S.nz - z0);
-  const long long plane = (long long)S.fpitch * S.nyp;
-  float* out = R.wout + fidx(S, i0, j, z0 + 1);
-  auto wv = [&](int kk, int row, int col) { return sw[(kk * (kTy + 2) + row) * kBoxX + col]; };
-  float2 wm = R.w_zero ? make_float2(0.f, 0.f) : make_float2(wv(0, ty + 1, 2 * tx + 4), wv(0, ty + 1, 2 * tx + 5));
-  float2 wc = R.w_zero ? make_float2(0.f, 0.f) : make_float2(wv(1, ty + 1, 2 * tx + 4), wv(1, ty + 1, 2 * tx + 5));
-  float r2a = 0.0f, r2b = 0.0f;
-#pragma unroll
-  for (int kk = 1; kk <= ZC; ++kk) {
-    if (kk <= kend) {
-      float2 wp = make_float2(0.f, 0.f), ym = wp, yp = wp;
-      float xl = 0.f, xr = 0.f;
-      if (!R.w_zero) {
-        wp = make_float2(wv(kk + 1, ty + 1, 2 * tx + 4), wv(kk + 1, ty + 1, 2 * tx + 5));
-        ym = make_float2(wv(kk, ty, 2 * tx + 4), wv(kk, ty, 2 * tx + 5));
-        yp = make_float2(wv(kk, ty + 2, 2 * tx + 4), wv(kk, ty + 2, 2 * tx + 5));
-        xl = wv(kk, ty + 1, 2 * tx + 3);
-        xr = wv(kk, ty + 1, 2 * tx + 6);
-      }
-      const float* rr = sr + ((kk - 1) * kTy + ty) * kTile + 2 * tx;
-      const float res0 = jacobi_res_f32(J, wc.x, xl, wc.y, ym.x, yp.x, wm.x, wp.x, rr[0]);
-      const float res1 = jacobi_res_f32(J, wc.y, wc.x, xr, ym.y, yp.y, wm.y, wp.y, rr[1]);
-      r2a = acc_r2_f32(r2a, act0 ? res0 : 0.0f);
-      r2b = acc_r2_f32(r2b, act1 ? res1 : 0.0f);
-      const float n0 = jacobi_next_f32(J, wc.x, res0), n1 = jacobi_next_f32(J, wc.y, res1);
-      if (act1) {
-        *reinterpret_cast<float2*>(out) = make_float2(n0, n1);
-      } else if (act0) {
-        out[0] = n0;
-      }
-      out += plane;
-      wm = wc;
-      wc = wp;
-    }
-  }
-  // the 32-lane tree of block_sum_store for the two 32-wide tiles (lanes 0-15, 16-31)
-  double v0 = (double)r2a, v1 = (double)r2b;
-#pragma unroll
-  for (int o = 8; o > 0; o >>= 1) {
-    v0 += __shfl_down_sync(0xffffffffu, v0, o);
-    v1 += __shfl_down_sync(0xffffffffu, v1, o);
-  }
-  if ((tx & 15) == 0) rows[tx >> 4][ty] = v0 + v1;
-  __syncthreads();
-  if (tid < 2) {
-    const int bx = 2 * bx2 + tid;
-    if (bx < R.gx) {
-      double sum = 0.0;
-      for (int q = 0; q < kTy; ++q) sum += rows[tid][q];
-      R.partial[bx + (long long)R.gx * (by + (long long)R.gy * bz)] = sum;
-    }
-  }
+  pair_tile_sweep<ZC>(sw, sr, R.S, R.J, R.wout, R.partial, R.w_zero, bx2, by, bz, R.gx, R.gy, rows);
 }
 
 template <int ZC>

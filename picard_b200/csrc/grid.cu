@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "grid.cuh"
 #include "stencil.cuh"
+#include "pair_tile.cuh"
 
 namespace picard {
 
@@ -547,37 +548,6 @@ struct Tma2Stage {
   static_assert(kBytes % 128 == 0, "stage buffers stay 128-byte aligned");
 };
 
-__device__ __forceinline__ unsigned long long pk2(float lo, float hi) {
-  unsigned long long r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ float2 up2(unsigned long long v) {
-  float2 r;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
-  return r;
-}
-__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
-  unsigned long long d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
-  unsigned long long d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
-  unsigned long long d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
-  unsigned long long d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-
 template <int ZC>
 __device__ inline void tma2_issue_tile(const CUtensorMap* tw, const CUtensorMap* tr, float* stage, uint32_t mb, int t,
                                        int gx2, int gy, int w_zero) {
@@ -626,9 +596,6 @@ __global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__
   int t = blockIdx.x;
   if (t >= ntiles) return;
   if (tid == 0) tma2_issue_tile<ZC>(&tw, &tr, stages, mb0, t, gx2, gy, w_zero);
-  const long long plane = (long long)S.fpitch * S.nyp;
-  const unsigned long long m2 = pk2(-2.0f, -2.0f), ix2 = pk2(J.idx2, J.idx2), iy2 = pk2(J.idy2, J.idy2),
-                           iz2 = pk2(J.idz2, J.idz2), naf = pk2(-J.af, -J.af);
   for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
     const int st = STAGES == 2 ? (it & 1) : 0;
     const uint32_t phase = (uint32_t)(STAGES == 2 ? ((it >> 1) & 1) : (it & 1));
@@ -644,74 +611,8 @@ __global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__
       return;
     }
     const float* sw = stages + st * Tma2Stage<ZC>::kFloats;
-    const float* sr = sw + Tma2Stage<ZC>::kW;
     const int bx2 = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
-    const int i0 = bx2 * kTma2Tile + 2 * tx + 1, j = by * kTmaTy + ty + 1, z0 = bz * ZC;
-    const bool act0 = i0 <= S.nx && j <= S.ny, act1 = i0 + 1 <= S.nx && j <= S.ny;
-    const int kend = min(ZC, S.nz - z0);
-    // w rows of this thread's pair: plane kk (0 .. ZC+1), row 0 .. 9, columns 2 tx + 4, + 5
-    auto wrow = [&](int kk, int row) {
-      return *reinterpret_cast<const unsigned long long*>(sw + (kk * (kTmaTy + 2) + row) * kTma2BoxX + 2 * tx + 4);
-    };
-    auto wcol = [&](int kk, int row, int col) { return sw[(kk * (kTmaTy + 2) + row) * kTma2BoxX + col]; };
-    unsigned long long wm = w_zero ? 0ull : wrow(0, ty + 1);
-    unsigned long long wc = w_zero ? 0ull : wrow(1, ty + 1);
-    unsigned long long r2 = 0ull;  // (+0.0f, +0.0f)
-    float* out = wout + fidx(S, i0, j, z0 + 1);
-#pragma unroll
-    for (int kk = 1; kk <= ZC; ++kk) {
-      if (kk <= kend) {
-        unsigned long long wp = 0ull, ym = 0ull, yp = 0ull;
-        float xl = 0.0f, xr = 0.0f;
-        const float2 c = up2(wc);
-        if (!w_zero) {
-          wp = wrow(kk + 1, ty + 1);
-          ym = wrow(kk, ty);
-          yp = wrow(kk, ty + 2);
-          xl = wcol(kk, ty + 1, 2 * tx + 3);  // x - 1 of the pair's first node
-          xr = wcol(kk, ty + 1, 2 * tx + 6);  // x + 1 of the pair's second node
-        }
-        const unsigned long long xm = pk2(xl, c.x), xp = pk2(c.y, xr);
-        const unsigned long long rr =
-            *reinterpret_cast<const unsigned long long*>(sr + ((kk - 1) * kTmaTy + ty) * kTma2Tile + 2 * tx);
-        // jacobi_res_f32 on both lanes
-        const unsigned long long sx = add2(xp, xm), sy = add2(yp, ym), sz = add2(wp, wm);
-        unsigned long long lap = mul2(fma2(m2, wc, sx), ix2);
-        lap = fma2(fma2(m2, wc, sy), iy2, lap);
-        lap = fma2(fma2(m2, wc, sz), iz2, lap);
-        const unsigned long long res = sub2(rr, lap);
-        const float2 rf = up2(res);
-        const unsigned long long resm = pk2(act0 ? rf.x : 0.0f, act1 ? rf.y : 0.0f);
-        r2 = fma2(resm, resm, r2);
-        const float2 wn = up2(fma2(naf, res, wc));
-        if (act1) {
-          *reinterpret_cast<float2*>(out) = wn;
-        } else if (act0) {
-          out[0] = wn.x;
-        }
-        out += plane;
-        wm = wc;
-        wc = wp;
-      }
-    }
-    // partials of the two 32-wide tiles, block_sum_store's tree reproduced
-    const float2 rr2 = up2(r2);
-    double v0 = (double)rr2.x, v1 = (double)rr2.y;
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) {
-      v0 += __shfl_down_sync(0xffffffffu, v0, o);
-      v1 += __shfl_down_sync(0xffffffffu, v1, o);
-    }
-    if ((tx & 15) == 0) rows[tx >> 4][ty] = v0 + v1;
-    __syncthreads();
-    if (tid < 2) {
-      const int bx = 2 * bx2 + tid;
-      if (bx < gx) {
-        double sum = 0.0;
-        for (int q = 0; q < kTmaTy; ++q) sum += rows[tid][q];
-        partial[bx + (long long)gx * (by + (long long)gy * bz)] = sum;
-      }
-    }
+    pair_tile_sweep<ZC>(sw, sw + Tma2Stage<ZC>::kW, S, J, wout, partial, w_zero, bx2, by, bz, gx, gy, rows);
     __syncthreads();
     if (STAGES == 1 && tid == 0 && tn < ntiles) tma2_issue_tile<ZC>(&tw, &tr, stages, mb0, tn, gx2, gy, w_zero);
   }
