@@ -46,8 +46,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["picard", "reference"], default="picard")
-    ap.add_argument("--workload", choices=["scale", "plain32", "poisson", "serving", "precision", "batch"],
-                    default="scale")
+    ap.add_argument("--workload", choices=["scale", "plain32", "poisson", "serving", "precision", "batch",
+                                           "bcpot", "deposit"], default="scale")
     ap.add_argument("--runs", type=int, default=64, help="batch workload: runs in the parameter sweep")
     ap.add_argument("--precision-n", type=int, default=512, help="precision workload: box edge in cells")
     ap.add_argument("--precision-sweeps", type=int, default=4001, help="precision workload: Jacobi sweeps compared")
@@ -721,6 +721,83 @@ def run_batch(args, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_bcpot(args, local_rank):
+    """Tensor-core BCpotentials alone: one context on --poisson-dims (default
+    256,128,128) with a random charge; device time per call (3 axes)."""
+    import numpy as np
+    import torch
+
+    from picard_b200 import capi
+    from picard_b200 import params as P
+    from picard_b200.simulation import Simulation
+
+    torch.cuda.set_device(local_rank)
+    nx, ny, nz = [int(v) for v in (args.poisson_dims or "256,128,128").split(",")]
+    p = P.config_plain_32(n=8, ppc=1, capacity=1024)
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.xmin, p.xmax = -500.0 * nx, 500.0 * nx
+    p.ymin, p.ymax = -500.0 * ny, 500.0 * ny
+    p.zmin, p.zmax = -500.0 * nz, 500.0 * nz
+    sim = Simulation(p, layout=capi.LAYOUT_F64, solver=capi.SOLVER_F64)
+    sim.calc_distance()
+    rng = np.random.default_rng(0)
+    C = np.zeros((nz + 2, ny + 2, nx + 2))
+    C[1:-1, 1:-1, 1:-1] = rng.normal(size=(nz, ny, nx)) * 1e-15
+    sim.set_field(capi.FIELD_C, C)
+    sim.set_option(capi.OPT_BCPOT_TENSOR, 1)
+    ext = torch.cuda.ExternalStream(sim.stream_handle)
+    sim.bc_potentials()
+    sim.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = max(1, args.steps)
+    e0.record(ext)
+    for _ in range(reps):
+        sim.bc_potentials()
+    e1.record(ext)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    faces = 2 * (ny * nz + nx * nz + nx * ny)
+    flops = 2.0 * 6 * faces * nx * ny * nz  # six split products
+    print(json.dumps({"workload": f"bcpot {nx}x{ny}x{nz}", "bcpot_tc_ms": ms,
+                      "split_product_tflops": flops / (ms * 1e-3) / 1e12}), flush=True)
+    sim.close()
+
+
+def run_deposit(args, local_rank):
+    """CELL32 ParticlesGridify alone on the at-scale grid with --ppc ions per
+    cell (default 32), after two fused steps; device time per call."""
+    import torch
+
+    from picard_b200 import capi
+    from picard_b200 import params as P
+    from picard_b200.simulation import Simulation
+
+    torch.cuda.set_device(local_rank)
+    ppc = args.ppc or 32
+    sim = Simulation(P.config_plain_scale(seed=0, ppc_ion=ppc), layout=capi.LAYOUT_CELL32,
+                     solver=capi.SOLVER_F32_REFINE)
+    sim.calc_distance()
+    sim.particles_initialize()
+    sim.run_fused(0, 2)
+    ext = torch.cuda.ExternalStream(sim.stream_handle)
+    sim.particles_gridify()
+    sim.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = max(1, args.steps)
+    e0.record(ext)
+    for _ in range(reps):
+        sim.particles_gridify()
+    e1.record(ext)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    n = sim.num_local
+    print(json.dumps({"workload": f"deposit 256x128x128, {ppc}+{ppc} ppc", "particles": n, "gridify_ms": ms,
+                      "read_gbs": 17.0 * n / (ms * 1e-3) / 1e9}), flush=True)
+    sim.close()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -749,6 +826,10 @@ def main():
         return
     if args.workload == "poisson":
         run_poisson(args, local_rank)
+        return
+    if args.workload in ("bcpot", "deposit"):
+        if rank == 0:
+            (run_bcpot if args.workload == "bcpot" else run_deposit)(args, local_rank)
         return
     if args.workload == "batch":
         if rank == 0:
