@@ -5,13 +5,13 @@
 // picard.f90:554-674 the driver issues every run's particle phases on the
 // runs' streams before waiting on any of them (the particle-count round trips
 // of all runs travel together), then solves every run's Poisson problem in
-// lockstep: per round each run plans its batch of sweeps from its own anchor
-// (the F32_REFINE loop of solve_f32.cuh, unchanged), and sweep t of the round
-// is ONE launch over the tiles of every run still at least t sweeps into its
-// round -- the run table (tensor maps, stencil, coefficients, output, tile
-// range) rides in the kernel parameters -- instead of one launch per run.
-// Anchors, reductions and the stop tests stay per run; runs that converge drop
-// out of later rounds.  The sweep kernel is the x-pair TMA sweep with the
+// ticks: each run plans its rounds of sweeps from its own anchor (the
+// F32_REFINE loop of solve_f32.cuh, unchanged), and one tick is ONE launch
+// advancing every run that is in the middle of a round by one sweep -- the
+// run table (tensor maps, stencil, coefficients, output, tile range) rides in
+// the kernel parameters -- instead of one launch per run.  Anchors, reductions
+// and the stop tests stay per run, asynchronous to the ticks; runs that
+// converge drop out.  The sweep kernel is the x-pair TMA sweep with the
 // same per-node arithmetic and per-tile partials, so every run's result is
 // bit-identical to the same run advanced alone with picard_gpu_run_fused.
 #include <cuda_runtime.h>
@@ -38,6 +38,7 @@ namespace picard {
 namespace {
 
 constexpr int kBatchRuns = 40;  // runs per launch (kernel parameter space)
+constexpr int kTicksAhead = 6;  // batched sweep launches queued ahead of the device
 
 struct alignas(64) BatchRun {
   CUtensorMap tw;  // w of the sweep's input iterate (x-pair boxes 72 x 10 x zc+2)
@@ -162,38 +163,42 @@ struct RunSolve {
   picard_ctx* c = nullptr;
   EpotSetup e;
   F32Solve S;
-  bool batched = false;  // the lockstep loop drives this run's solve
+  bool batched = false;  // the batched loop drives this run's solve
   bool done = true;
+  int phase = 0;         // 0 round to plan, 1 sweeping, 2 anchor and stop test in flight
+  int p = 0;             // sweeps of the current round done
   long long sweeps = 0;
   bool converged = true;
 };
 
-// Sweep t (1-based) of the current round for every run with m_eff >= t, in
-// launches of at most kBatchRuns runs of one tile depth.  The first launch of
-// a round follows event waits on the runs' streams (their anchors), which a
-// programmatic dependent launch would not cover -- griddepcontrol.wait only
-// orders a kernel after its predecessor on the same stream -- so it is a plain
-// launch; the round's later launches depend on the batch stream alone and
-// overlap their predecessors' tails.
-int launch_round_sweep(std::vector<RunSolve*>& runs, int t, int* err, cudaStream_t st) {
-  bool first = t == 1;
+// One tick: the next sweep of every run in the middle of a round, in
+// launches of at most kBatchRuns runs of one tile depth.  Runs whose round is
+// complete after the tick are appended to `ended`.  pdl: the tick may overlap
+// the previous one on the batch stream (griddepcontrol.wait orders it after
+// its predecessor there); the first tick of a solve phase follows event waits
+// on the runs' streams, which PDL would not cover, so it is a plain launch.
+int launch_tick(std::vector<RunSolve*>& runs, int* err, cudaStream_t st, bool pdl, std::vector<RunSolve*>& ended,
+                long long* launches) {
+  bool first = !pdl;
   for (int zc : {4, 8}) {
     BatchArgs A;
     std::memset(&A, 0, sizeof(A));
     A.err = err;
     auto flush = [&]() -> int {
       if (A.nruns == 0) return PICARD_OK;
-      const int pdl = first ? 0 : 1;
+      const int use_pdl = first ? 0 : 1;
       first = false;
-      cudaError_t e = zc == 8 ? launch_batch_zc<8>(A, pdl, st) : launch_batch_zc<4>(A, pdl, st);
+      cudaError_t e = zc == 8 ? launch_batch_zc<8>(A, use_pdl, st) : launch_batch_zc<4>(A, use_pdl, st);
       PICARD_CUDA(e);
+      ++*launches;
       std::memset(&A, 0, sizeof(A));
       A.err = err;
       return PICARD_OK;
     };
     for (RunSolve* rs : runs) {
-      if (rs->done || !rs->batched || rs->S.m_eff < t || rs->c->G.zc != zc) continue;
+      if (rs->done || !rs->batched || rs->phase != 1 || rs->c->G.zc != zc) continue;
       picard_ctx* c = rs->c;
+      const int t = rs->p + 1;                  // sweep t of the round
       const int in = rs->S.wcur, out = 1 - in;  // never write the buffer being read
       BatchRun& R = A.run[A.nruns];
       R.tw = c->tmw2[in];
@@ -210,6 +215,8 @@ int launch_round_sweep(std::vector<RunSolve*>& runs, int t, int* err, cudaStream
       R.tile_base = A.total_tiles;
       R.w_zero = t == 1 ? 1 : 0;
       A.total_tiles += R.tiles;
+      rs->p = t;
+      if (t == rs->S.m_eff) ended.push_back(rs);
       if (++A.nruns == kBatchRuns) PICARD_TRY(flush());
     }
     PICARD_TRY(flush());
@@ -234,20 +241,29 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
     if (ctxs[r]->device != dev) return fail(PICARD_ERR_BAD_ARG, "batched contexts must live on the current device");
   cudaStream_t bst = nullptr;
   cudaEvent_t bev = nullptr;
-  std::vector<cudaEvent_t> rev(n, nullptr);
+  std::vector<cudaEvent_t> rev(n, nullptr), dev_ev(n, nullptr);
+  cudaEvent_t tick_ev[kTicksAhead] = {};
   auto cleanup = [&]() {
     if (bst) cudaStreamSynchronize(bst);
-    for (int r = 0; r < n; ++r)
+    for (int r = 0; r < n; ++r) {
       if (rev[r]) cudaEventDestroy(rev[r]);
+      if (dev_ev[r]) cudaEventDestroy(dev_ev[r]);
+    }
     if (bev) cudaEventDestroy(bev);
+    for (cudaEvent_t& e : tick_ev)
+      if (e) cudaEventDestroy(e);
     if (bst) cudaStreamDestroy(bst);
   };
   int rc = PICARD_OK;
   int* berr = nullptr;  // timeout flag of the batched sweeps (run 0's error word)
   rc = check_cuda(cudaStreamCreateWithFlags(&bst, cudaStreamNonBlocking), "cudaStreamCreate");
   if (rc == PICARD_OK) rc = check_cuda(cudaEventCreateWithFlags(&bev, cudaEventDisableTiming), "cudaEventCreate");
-  for (int r = 0; r < n && rc == PICARD_OK; ++r)
+  for (cudaEvent_t& e : tick_ev)
+    if (rc == PICARD_OK) rc = check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  for (int r = 0; r < n && rc == PICARD_OK; ++r) {
     rc = check_cuda(cudaEventCreateWithFlags(&rev[r], cudaEventDisableTiming), "cudaEventCreate");
+    if (rc == PICARD_OK) rc = check_cuda(cudaEventCreateWithFlags(&dev_ev[r], cudaEventDisableTiming), "cudaEventCreate");
+  }
   if (rc != PICARD_OK) {
     cleanup();
     return rc;
@@ -349,36 +365,73 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
           rs.e.trivial = false;
         }
       }
-      for (;;) {
-        int M = 0;
-        for (int r = 0; r < n; ++r)
-          if (!solves[r].done && solves[r].batched) M = std::max(M, f32_plan(solves[r].S));
-        if (M == 0) break;
-        // the batch stream follows every active run's stream (anchors done)
-        for (int r = 0; r < n; ++r) {
-          if (solves[r].done || !solves[r].batched) continue;
-          PICARD_CUDA(cudaEventRecord(rev[r], ctxs[r]->st));
+      // Rounds are asynchronous across runs: every tick advances each run in
+      // the middle of a round by one sweep; a run whose round ends gets its
+      // anchor, reduction and stop test on its own stream while the ticks go
+      // on for the others, and starts its next round once the host has its
+      // decision (its anchor then is complete, so later ticks need no wait).
+      for (int r = 0; r < n; ++r)
+        if (solves[r].batched && !solves[r].done) {
+          PICARD_CUDA(cudaEventRecord(rev[r], ctxs[r]->st));  // anchor 0
           PICARD_CUDA(cudaStreamWaitEvent(bst, rev[r], 0));
         }
-        for (int t = 1; t <= M; ++t) PICARD_TRY(launch_round_sweep(rp, t, berr, bst));
-        ++rounds;
-        launches += M;
-        PICARD_CUDA(cudaEventRecord(bev, bst));
-        for (int r = 0; r < n; ++r) {
-          if (solves[r].done || !solves[r].batched) continue;
-          PICARD_CUDA(cudaStreamWaitEvent(ctxs[r]->st, bev, 0));
-          PICARD_CUDA(cudaEventRecord(ctxs[r]->ev[0], ctxs[r]->st));  // no per-run sweep timing in a batch
-          PICARD_TRY(f32_issue_tail(solves[r].S));
-        }
+      bool first_tick = true;
+      std::vector<RunSolve*> ended;
+      long long issued = 0, retired = 0;  // ticks queued / known complete
+      for (;;) {
+        int sweeping = 0, waiting = 0;
         for (int r = 0; r < n; ++r) {
           RunSolve& rs = solves[r];
           if (rs.done || !rs.batched) continue;
+          if (rs.phase == 0) {
+            f32_plan(rs.S);
+            rs.phase = 1;
+            rs.p = 0;
+            ++rounds;
+          }
+          sweeping += rs.phase == 1;
+          waiting += rs.phase == 2;
+        }
+        if (sweeping == 0 && waiting == 0) break;
+        if (sweeping > 0) {
+          // keep at most kTicksAhead ticks queued, so that a run whose stop
+          // test the host has just read joins the ticks right away instead of
+          // behind a long queue
+          if (issued - retired == kTicksAhead) {
+            PICARD_CUDA(cudaEventSynchronize(tick_ev[retired % kTicksAhead]));
+            ++retired;
+          }
+          ended.clear();
+          PICARD_TRY(launch_tick(rp, berr, bst, !first_tick, ended, &launches));
+          first_tick = false;
+          PICARD_CUDA(cudaEventRecord(tick_ev[issued % kTicksAhead], bst));
+          ++issued;
+          for (RunSolve* rs : ended) {
+            const int r = int(rs - solves.data());
+            PICARD_CUDA(cudaEventRecord(rev[r], bst));
+            PICARD_CUDA(cudaStreamWaitEvent(ctxs[r]->st, rev[r], 0));
+            PICARD_CUDA(cudaEventRecord(ctxs[r]->ev[0], ctxs[r]->st));  // no per-run sweep timing in a batch
+            PICARD_TRY(f32_issue_tail(rs->S));
+            PICARD_CUDA(cudaEventRecord(dev_ev[r], ctxs[r]->st));
+            rs->phase = 2;
+          }
+        }
+        // collect the stop tests that have landed (block when nothing else can move)
+        for (int r = 0; r < n; ++r) {
+          RunSolve& rs = solves[r];
+          if (rs.done || !rs.batched || rs.phase != 2) continue;
+          cudaError_t q = sweeping > 0 ? cudaEventQuery(dev_ev[r]) : cudaEventSynchronize(dev_ev[r]);
+          if (q == cudaErrorNotReady) continue;
+          PICARD_CUDA(q);
           PICARD_TRY(f32_finish(rs.S, false));
           if (rs.S.done) {
             rs.done = true;
             rs.sweeps = rs.S.sweeps;
             rs.converged = rs.S.converged;
+          } else {
+            rs.phase = 0;
           }
+          if (sweeping == 0) break;  // one at a time while blocking: replan at once
         }
       }
       for (int r = 0; r < n; ++r) {
