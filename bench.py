@@ -55,6 +55,10 @@ def parse_args():
     ap.add_argument("--rate", type=float, default=20.0, help="serving workload: mean arrivals per second")
     ap.add_argument("--run-steps", type=int, default=200, help="serving workload: iterations per run")
     ap.add_argument("--slots", type=int, default=8, help="serving workload: runs in flight at once")
+    ap.add_argument("--batch-slots", type=int, default=24,
+                    help="serving workload, continuous batching: runs in the cohort at once")
+    ap.add_argument("--preparers", type=int, default=3,
+                    help="serving workload, continuous batching: threads preparing admitted runs")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving workload: HBM budget of admitted runs")
     ap.add_argument("--poisson-n", type=int, default=256)
     ap.add_argument("--poisson-dims", type=str, default=None, help="poisson workload: nx,ny,nz (default n^3)")
@@ -430,14 +434,17 @@ def run_poisson(args, local_rank):
 def run_serving(args, local_rank):
     """Serving workload: a Poisson stream of parameter-sweep runs (cubic grids
     of 24..128 cells, 8..64 ppc, Haser Q log-uniform in [1e25, 1e28] s^-1,
-    --run-steps iterations each) served two ways on one GPU.
+    --run-steps iterations each) served three ways on one GPU.
       plain:  one run after another through picard_gpu_run (the per-subroutine
               call sequence of picard.f90), the arrival stream replayed against
               the measured service times;
       served: the picard_server request loop -- admission under the HBM
               budget, --slots runs in flight on their own streams, requests
               submitted at their arrival times.
-    Both arms create, initialise, run and release every run inside the timed
+      batched: the continuous-batching request loop -- the same admission, up
+              to --batch-slots runs advanced together one iteration at a time,
+              all their Jacobi sweeps in one launch per sweep.
+    All arms create, initialise, run and release every run inside the timed
     region.  Throughput = particle-steps of all runs / (last finish - first
     arrival); latency = finish - arrival."""
     import numpy as np
@@ -495,7 +502,7 @@ def run_serving(args, local_rank):
         plain_lat.append(clock - t)
     plain_makespan = clock - reqs[0][0]
 
-    with Server(int(args.budget_gb * 1e9), args.slots) as srv:
+    def serve(srv):
         base = srv.now_ms()
         for i, (t, p, steps) in enumerate(reqs):
             wait = base + t * 1e3 - srv.now_ms()
@@ -503,21 +510,33 @@ def run_serving(args, local_rank):
                 time.sleep(wait * 1e-3)
             srv.submit(i, p, steps, layout=layout, solver=solver, arrival_ms=base + t * 1e3)
         res = sorted(srv.poll(wait_all=True), key=lambda r: r["id"])
+        makespan = (max(r["finish_ms"] for r in res) - (base + reqs[0][0] * 1e3)) * 1e-3
+        return res, makespan
+
+    with Server(int(args.budget_gb * 1e9), args.slots) as srv:
+        res, served_makespan = serve(srv)
+    with Server(int(args.budget_gb * 1e9), args.batch_slots, batched=True, preparers=args.preparers) as srv:
+        bres, batched_makespan = serve(srv)
     clk = clocks.stop()
-    bad = [r for r in res if r["status"] != capi.OK]
+    bad = [r for r in res + bres if r["status"] != capi.OK]
     served_lat = [(r["finish_ms"] - r["arrival_ms"]) * 1e-3 for r in res]
-    served_makespan = (max(r["finish_ms"] for r in res) - (base + reqs[0][0] * 1e3)) * 1e-3
+    batched_lat = [(r["finish_ms"] - r["arrival_ms"]) * 1e-3 for r in bres]
     ps_served = sum(r["particle_steps"] for r in res)
+    ps_batched = sum(r["particle_steps"] for r in bres)
     ps_plain = sum(r["particle_steps"] for r in plain)
     u_diff = max(abs(r["u_sum"] - q["u_sum"]) / max(abs(q["u_sum"]), 1e-300) for r, q in zip(res, plain))
+    b_mismatch = sum(1 for r, q in zip(bres, res)
+                     if (r["u_sum"], r["u_abs_sum"], r["num_local"], r["sweeps"]) !=
+                     (q["u_sum"], q["u_abs_sum"], q["num_local"], q["sweeps"]))
 
     def pct(v, q):
         return float(np.percentile(np.asarray(v), q))
 
     served_tput = ps_served / served_makespan
+    batched_tput = ps_batched / batched_makespan
     plain_tput = ps_plain / plain_makespan
     line = {
-        "metric": "particle-steps/s & run p50/p99 latency, served vs plain", "value": served_tput,
+        "metric": "particle-steps/s & run p50/p99 latency, served vs plain", "value": max(served_tput, batched_tput),
         "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "impl": "picard",
         "workload": "serving", "vs_baseline": None,
         "dtype": "f32 particles, f32 Jacobi sweeps with f64 anchors",
@@ -525,14 +544,19 @@ def run_serving(args, local_rank):
         "config": {"workload": f"serving stream: {len(reqs)} runs, Poisson arrivals {args.rate}/s, cubic grids "
                                f"24..128 cells, 8..64 ppc, Haser Q log-uniform [1e25, 1e28] s^-1, "
                                f"{args.run_steps} steps each",
-                   "grids": [int(p.nx) for _, p, _ in reqs], "budget_gb": args.budget_gb, "slots": args.slots},
+                   "grids": [int(p.nx) for _, p, _ in reqs], "budget_gb": args.budget_gb, "slots": args.slots,
+                   "batch_slots": args.batch_slots, "preparers": args.preparers},
         "served": {"particle_steps_per_s": served_tput, "makespan_s": served_makespan,
                    "p50_latency_s": pct(served_lat, 50), "p99_latency_s": pct(served_lat, 99),
                    "failed": len(bad)},
+        "batched_served": {"particle_steps_per_s": batched_tput, "makespan_s": batched_makespan,
+                           "p50_latency_s": pct(batched_lat, 50), "p99_latency_s": pct(batched_lat, 99),
+                           "results_differing_from_stream_mode": b_mismatch},
         "plain": {"particle_steps_per_s": plain_tput, "makespan_s": plain_makespan,
                   "p50_latency_s": pct(plain_lat, 50), "p99_latency_s": pct(plain_lat, 99),
                   "busy_s": sum(r["service_s"] for r in plain)},
         "served_over_plain": served_tput / plain_tput,
+        "batched_served_over_plain": batched_tput / plain_tput,
         "offered_load": {"arrivals_per_s": args.rate,
                          "plain_service_rate_per_s": len(reqs) / sum(r["service_s"] for r in plain)},
         "u_sum_max_rel_diff_served_vs_plain": u_diff,
@@ -625,7 +649,10 @@ def run_batch(args, local_rank):
       plain:   one run after another through picard_gpu_run_fused;
       batched: all runs together through picard_batch_run_fused (one sweep
                launch per sweep for every run).
-    Both arms create, initialise, run and release every run inside the timed
+      batched: the continuous-batching request loop -- the same admission, up
+              to --batch-slots runs advanced together one iteration at a time,
+              all their Jacobi sweeps in one launch per sweep.
+    All arms create, initialise, run and release every run inside the timed
     region (the sweep launch tuner runs at creation in both).  Reports
     particle-steps/s of each arm and checks that every run ends bit for bit
     where it ends alone."""

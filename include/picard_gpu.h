@@ -303,6 +303,10 @@ PICARD_API int picard_gpu_run_fused(picard_ctx* ctx, int32_t iter_start, int32_t
  * array of n counters accumulating each run's Jacobi sweeps. */
 PICARD_API int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter_start, int32_t iter_end,
                                       int64_t* sweeps_total);
+/* One iteration of every run of a batch whose runs are at different points:
+ * run r takes iteration iterations[r] (the continuous-batching step of the
+ * serving loop, where runs join and leave between steps). */
+PICARD_API int picard_batch_step(picard_ctx** ctxs, int32_t n, const int32_t* iterations, int64_t* sweeps_total);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,14 @@ typedef struct picard_result {
  * max_slots: runs in flight at once (one host worker thread and one CUDA
  * stream each).  The server uses the calling thread's current device. */
 PICARD_API int picard_server_create(uint64_t hbm_budget_bytes, int32_t max_slots, picard_server** out);
+/* Continuous batching on the current device: at most max_runs runs admitted at
+ * once (same admission rule), prepared (context, CalcDistance,
+ * ParticlesInitialize) by `preparers` threads, and advanced together one
+ * iteration at a time by picard_batch_step -- every run's Jacobi sweeps in
+ * one launch per sweep -- joining and leaving the cohort between steps.  Each
+ * run's result is bit-identical to the same run alone. */
+PICARD_API int picard_server_create_batched(uint64_t hbm_budget_bytes, int32_t max_runs, int32_t preparers,
+                                            picard_server** out);
 /* Queues a run.  PICARD_ERR_CAPACITY if its footprint exceeds the whole budget
  * (it could never be admitted), PICARD_ERR_BAD_ARG for invalid params. */
 PICARD_API int picard_server_submit(picard_server* s, const picard_request* rq);

@@ -158,7 +158,9 @@ def lib():
         "picard_gpu_set_option": [ctx, C.c_int32, C.c_int32],
         "picard_gpu_get_option": [ctx, C.c_int32, ip],
         "picard_batch_run_fused": [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int64)],
+        "picard_batch_step": [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64)],
         "picard_server_create": [C.c_uint64, C.c_int32, C.POINTER(C.c_void_p)],
+        "picard_server_create_batched": [C.c_uint64, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)],
         "picard_server_submit": [C.c_void_p, C.POINTER(PicardRequest)],
         "picard_server_now_ms": [C.c_void_p, dp],
         "picard_server_poll": [C.c_void_p, C.POINTER(PicardResult), C.c_int32, ip, C.c_int32],

@@ -227,8 +227,10 @@ int launch_tick(std::vector<RunSolve*>& runs, int* err, cudaStream_t st, bool pd
 }  // namespace
 }  // namespace picard
 
-extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter_start, int32_t iter_end,
-                                      int64_t* sweeps_total) {
+namespace {
+
+// nsteps iterations of every run; run r takes iterations it0[r]+1 .. it0[r]+nsteps.
+int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nsteps, int64_t* sweeps_total) {
   if (!ctxs || n < 1) return fail(PICARD_ERR_BAD_ARG, "no contexts");
   for (int r = 0; r < n; ++r) {
     if (!ctxs[r]) return fail(PICARD_ERR_BAD_ARG, "a context is NULL");
@@ -287,7 +289,7 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
     tick = t;
   };
   auto body = [&]() -> int {
-    for (int32_t it = iter_start + 1; it <= iter_end; ++it) {
+    for (int32_t step = 1; step <= nsteps; ++step) {
       tick = now();
       // ---- AdvancePosition, ParticlesProduce (device count) for every run
       for (int r = 0; r < n; ++r) {
@@ -295,6 +297,7 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
         const KParams& K = c->K;
         const int cells = c->prm.nx * c->prm.ny * c->prm.nz;
         PICARD_TRY(picard_gpu_advance_position(c, c->prm.dt));
+        const int32_t it = it0[r] + step;
         PICARD_CUDA(launch_produce_count(K, it, c->cell_counts, c->st));
         PICARD_CUDA(launch_scan_int(c->cell_counts, c->cell_offsets, cells, c->cell_offsets + cells,
                                     c->cell_offsets + cells + 2, c->st));
@@ -312,6 +315,7 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
       for (int r = 0; r < n; ++r) {
         picard_ctx* c = ctxs[r];
         const KParams& K = c->K;
+        const int32_t it = it0[r] + step;
         const int nxt = 1 - c->cur;
         if (c->layout == PICARD_LAYOUT_F64)
           PICARD_CUDA(launch_compact_outflow_f64(K, c->f64[c->cur], c->f64[nxt], c->num_local, c->blk_counts,
@@ -471,4 +475,21 @@ extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter
   if (rc != PICARD_OK) return rc;
   if (nc) return fail(PICARD_ERR_NOT_CONVERGED, "at least one Jacobi solve hit 2*maxit+1 sweeps");
   return PICARD_OK;
+}
+
+}  // namespace
+
+extern "C" int picard_batch_run_fused(picard_ctx** ctxs, int32_t n, int32_t iter_start, int32_t iter_end,
+                                      int64_t* sweeps_total) {
+  if (n < 1 || n > (1 << 20)) return fail(PICARD_ERR_BAD_ARG, "bad run count");
+  if (iter_end < iter_start) return fail(PICARD_ERR_BAD_ARG, "iter_end < iter_start");
+  std::vector<int32_t> it0((size_t)n, iter_start);
+  return batch_run_impl(ctxs, n, it0.data(), iter_end - iter_start, sweeps_total);
+}
+
+extern "C" int picard_batch_step(picard_ctx** ctxs, int32_t n, const int32_t* iterations, int64_t* sweeps_total) {
+  if (!iterations || n < 1 || n > (1 << 20)) return fail(PICARD_ERR_BAD_ARG, "bad arguments");
+  std::vector<int32_t> it0((size_t)n);
+  for (int r = 0; r < n; ++r) it0[(size_t)r] = iterations[r] - 1;
+  return batch_run_impl(ctxs, n, it0.data(), 1, sweeps_total);
 }

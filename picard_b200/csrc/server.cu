@@ -38,14 +38,25 @@ struct picard_server {
   int max_slots = 1;
   int running = 0;
   bool stopping = false;
+  bool batched = false;  // continuous batching: one cohort advanced by picard_batch_step
   std::deque<std::pair<picard_request, uint64_t>> queue;  // request, footprint
   std::vector<picard_result> done;
   std::mutex mu;
   std::condition_variable cv_work;  // a worker may be able to start a request
   std::condition_variable cv_done;  // a request finished
+  std::condition_variable cv_ready;  // batched mode: a prepared run can join the cohort
   std::vector<std::thread> workers;
   std::chrono::steady_clock::time_point t0;
   int64_t submitted = 0, finished = 0;
+  // batched mode
+  struct Prepared {
+    picard_ctx* c;
+    picard_request rq;
+    uint64_t fp;
+    picard_result r;
+  };
+  std::deque<std::pair<picard_request, uint64_t>> admitted;  // waiting for a preparer
+  std::vector<Prepared> ready;                               // prepared, waiting for a step boundary
 };
 
 namespace {
@@ -54,34 +65,53 @@ double now_ms(const picard_server* s) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s->t0).count();
 }
 
-int run_request(const picard_request& rq, picard_result* out) {
+// Context creation, CalcDistance and ParticlesInitialize of a request.
+int prepare_run(const picard_request& rq, picard_ctx** out) {
   picard_ctx* c = nullptr;
   PICARD_TRY(picard_gpu_create(&rq.params, rq.layout, rq.solver, &c));
   int rc = picard_gpu_calc_distance(c);
   if (rc == PICARD_OK) rc = picard_gpu_particles_initialize(c);
-  int64_t sweeps = 0;
-  if (rc == PICARD_OK) {
-    rc = picard_gpu_run_fused(c, 0, rq.steps, &sweeps);
-    if (rc == PICARD_ERR_NOT_CONVERGED) rc = PICARD_OK;  // the reference carries on too
+  if (rc == PICARD_OK) rc = check_cuda(cudaStreamSynchronize(c->st), "prepare");
+  if (rc != PICARD_OK) {
+    picard_gpu_destroy(c);
+    return rc;
   }
-  if (rc == PICARD_OK) rc = picard_gpu_energy(c, out->energy, &out->num_local);
+  *out = c;
+  return PICARD_OK;
+}
+
+// Energies, particle count and checksums of the final potential; releases the context.
+int finish_run(picard_ctx* c, picard_result* out) {
+  int rc = picard_gpu_energy(c, out->energy, &out->num_local);
   picard_stats st;
   if (rc == PICARD_OK) rc = picard_gpu_get_stats(c, &st);
   if (rc == PICARD_OK) {
-    out->sweeps = sweeps;
+    out->sweeps = st.sweeps;
     out->particle_steps = st.particle_steps;
-    // checksum of the final potential (sum over all nodes, FP64)
     const long long nn = c->K.nodes;
     std::vector<double> h((size_t)nn);
     rc = check_cuda(cudaMemcpyAsync(h.data(), c->U, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st), "U");
     if (rc == PICARD_OK) rc = check_cuda(cudaStreamSynchronize(c->st), "sync");
-    double s = 0.0, a = 0.0;
-    for (long long g = 0; g < nn; ++g) s += h[(size_t)g], a += std::fabs(h[(size_t)g]);
-    out->u_sum = s;
-    out->u_abs_sum = a;
+    double sm = 0.0, ab = 0.0;
+    for (long long g = 0; g < nn; ++g) sm += h[(size_t)g], ab += std::fabs(h[(size_t)g]);
+    out->u_sum = sm;
+    out->u_abs_sum = ab;
   }
   picard_gpu_destroy(c);
   return rc;
+}
+
+int run_request(const picard_request& rq, picard_result* out) {
+  picard_ctx* c = nullptr;
+  PICARD_TRY(prepare_run(rq, &c));
+  int64_t sweeps = 0;
+  int rc = picard_gpu_run_fused(c, 0, rq.steps, &sweeps);
+  if (rc == PICARD_ERR_NOT_CONVERGED) rc = PICARD_OK;  // the reference carries on too
+  if (rc != PICARD_OK) {
+    picard_gpu_destroy(c);
+    return rc;
+  }
+  return finish_run(c, out);
 }
 
 void worker_main(picard_server* s) {
@@ -120,6 +150,115 @@ void worker_main(picard_server* s) {
   }
 }
 
+// ------------------------------------------------ continuous batching
+//
+// Admission as in the stream mode (arrival order, slots and HBM budget).
+// Admitted requests are prepared (context, CalcDistance, ParticlesInitialize)
+// by preparer threads; a prepared run joins the cohort at the next step
+// boundary.  The scheduler advances the whole cohort one iteration at a time
+// with picard_batch_step -- all runs' Jacobi sweeps in one launch per tick --
+// and retires each run after its last step.  A run's result is bit-identical
+// to the same run alone: the batched step is.
+
+// In this mode `running` counts the admitted runs that have not finished.
+void admit_locked(picard_server* s) {
+  while (s->running < s->max_slots && !s->queue.empty() && s->queue.front().second <= s->budget - s->in_use) {
+    s->in_use += s->queue.front().second;
+    s->running += 1;
+    s->admitted.push_back(s->queue.front());
+    s->queue.pop_front();
+  }
+}
+
+void post_result(picard_server* s, const picard_result& r, uint64_t fp) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->in_use -= fp;
+  s->running -= 1;
+  s->finished += 1;
+  s->done.push_back(r);
+  admit_locked(s);
+  s->cv_work.notify_all();
+  s->cv_done.notify_all();
+}
+
+void preparer_main(picard_server* s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    std::pair<picard_request, uint64_t> job;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] { return !s->admitted.empty() || (s->stopping && s->queue.empty()); });
+      if (s->admitted.empty()) return;
+      job = s->admitted.front();
+      s->admitted.pop_front();
+    }
+    picard_result r;
+    std::memset(&r, 0, sizeof(r));
+    r.id = job.first.id;
+    r.arrival_ms = job.first.arrival_ms;
+    r.start_ms = now_ms(s);
+    picard_ctx* c = nullptr;
+    int rc = prepare_run(job.first, &c);
+    if (rc != PICARD_OK) {
+      r.status = rc;
+      r.finish_ms = now_ms(s);
+      post_result(s, r, job.second);
+      continue;
+    }
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->ready.push_back({c, job.first, job.second, r});
+    }
+    s->cv_ready.notify_all();
+  }
+}
+
+void scheduler_main(picard_server* s) {
+  cudaSetDevice(s->device);
+  struct Active {
+    picard_ctx* c;
+    picard_request rq;
+    uint64_t fp;
+    picard_result r;
+    int32_t iter;  // iterations done
+  };
+  std::vector<Active> act;
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_ready.wait(lk, [&] {
+        return !s->ready.empty() || !act.empty() ||
+               (s->stopping && s->queue.empty() && s->running == 0);
+      });
+      for (auto& p : s->ready) act.push_back({p.c, p.rq, p.fp, p.r, 0});
+      s->ready.clear();
+      if (act.empty()) return;  // stopping and nothing left
+    }
+    std::vector<picard_ctx*> ctxs;
+    std::vector<int32_t> its;
+    for (auto& a : act) {
+      ctxs.push_back(a.c);
+      its.push_back(a.iter + 1);
+    }
+    int rc = picard_batch_step(ctxs.data(), int32_t(ctxs.size()), its.data(), nullptr);
+    if (rc == PICARD_ERR_NOT_CONVERGED) rc = PICARD_OK;  // the reference carries on too
+    std::vector<Active> keep;
+    for (auto& a : act) {
+      a.iter += 1;
+      if (rc != PICARD_OK || a.iter >= a.rq.steps) {
+        picard_result r = a.r;
+        r.status = rc != PICARD_OK ? rc : finish_run(a.c, &r);
+        if (rc != PICARD_OK) picard_gpu_destroy(a.c);
+        r.finish_ms = now_ms(s);
+        post_result(s, r, a.fp);
+      } else {
+        keep.push_back(a);
+      }
+    }
+    act.swap(keep);
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -145,8 +284,33 @@ int picard_server_create(uint64_t hbm_budget_bytes, int32_t max_slots, picard_se
   return PICARD_OK;
 }
 
+int picard_server_create_batched(uint64_t hbm_budget_bytes, int32_t max_runs, int32_t preparers,
+                                 picard_server** out) {
+  if (!out || max_runs < 1 || preparers < 1 || hbm_budget_bytes == 0)
+    return fail(PICARD_ERR_BAD_ARG, "bad server arguments");
+  picard_server* s = new picard_server();
+  s->budget = hbm_budget_bytes;
+  s->max_slots = max_runs;
+  s->batched = true;
+  s->t0 = std::chrono::steady_clock::now();
+  if (cudaGetDevice(&s->device) != cudaSuccess) {
+    delete s;
+    return fail(PICARD_ERR_CUDA, "no CUDA device");
+  }
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+    uint64_t keep = hbm_budget_bytes;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  for (int i = 0; i < preparers; ++i) s->workers.emplace_back(preparer_main, s);
+  s->workers.emplace_back(scheduler_main, s);
+  *out = s;
+  return PICARD_OK;
+}
+
 int picard_server_submit(picard_server* s, const picard_request* rq) {
   if (!s || !rq) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  if (rq->steps < 1) return fail(PICARD_ERR_BAD_ARG, "steps < 1");
   uint64_t fp = 0;
   PICARD_TRY(picard_gpu_footprint(&rq->params, rq->layout, rq->solver, &fp));
   if (fp > s->budget)
@@ -158,6 +322,7 @@ int picard_server_submit(picard_server* s, const picard_request* rq) {
     if (copy.arrival_ms < 0) copy.arrival_ms = now_ms(s);
     s->queue.emplace_back(copy, fp);
     s->submitted += 1;
+    if (s->batched) admit_locked(s);
   }
   s->cv_work.notify_all();
   return PICARD_OK;
@@ -198,6 +363,15 @@ int picard_server_destroy(picard_server* s) {
     s->stopping = true;
   }
   s->cv_work.notify_all();
+  s->cv_ready.notify_all();
+  if (s->batched) {
+    // the queue drains first: wait for every submitted run
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_done.wait(lk, [&] { return s->finished == s->submitted; });
+    lk.unlock();
+    s->cv_work.notify_all();
+    s->cv_ready.notify_all();
+  }
   for (auto& t : s->workers) t.join();
   delete s;
   return PICARD_OK;

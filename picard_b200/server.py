@@ -16,13 +16,24 @@ from .params import PicardParams
 
 
 class Server:
-    def __init__(self, hbm_budget_bytes: int, slots: int):
+    """``batched=False``: one worker thread and CUDA stream per slot, each run
+    driven alone (picard_server_create).  ``batched=True``: continuous
+    batching (picard_server_create_batched) -- up to ``slots`` admitted runs
+    advanced together one iteration at a time, all their Jacobi sweeps in one
+    launch per sweep, ``preparers`` threads building newly admitted runs."""
+
+    def __init__(self, hbm_budget_bytes: int, slots: int, batched: bool = False, preparers: int = 2):
         self._lib = capi.lib()
         self._h = C.c_void_p()
-        capi.check(self._lib.picard_server_create(int(hbm_budget_bytes), int(slots), C.byref(self._h)),
-                   "picard_server_create")
+        if batched:
+            capi.check(self._lib.picard_server_create_batched(int(hbm_budget_bytes), int(slots), int(preparers),
+                                                              C.byref(self._h)), "picard_server_create_batched")
+        else:
+            capi.check(self._lib.picard_server_create(int(hbm_budget_bytes), int(slots), C.byref(self._h)),
+                       "picard_server_create")
         self.budget = int(hbm_budget_bytes)
         self.slots = int(slots)
+        self.batched = bool(batched)
 
     def submit(self, rid: int, params: PicardParams, steps: int, layout: int = capi.LAYOUT_CELL32,
                solver: int = capi.SOLVER_F32_REFINE, arrival_ms: float = -1.0) -> None:

@@ -214,3 +214,16 @@ def batch_run_fused(sims: "list[Simulation]", iter_start: int, iter_end: int) ->
     capi.check(capi.lib().picard_batch_run_fused(arr, n, iter_start, iter_end, sweeps), "picard_batch_run_fused",
                (capi.OK, capi.ERR_NOT_CONVERGED))
     return [int(v) for v in sweeps]
+
+
+def batch_step(sims: "list[Simulation]", iterations: "list[int]") -> list[int]:
+    """One main-loop iteration of each run together (picard_batch_step); run r
+    takes iteration ``iterations[r]`` (1-based), so runs at different points of
+    their loops share the step.  Returns each run's Jacobi sweeps."""
+    n = len(sims)
+    arr = (C.c_void_p * n)(*[s._h.value for s in sims])
+    its = (C.c_int32 * n)(*[int(i) for i in iterations])
+    sweeps = (C.c_int64 * n)()
+    capi.check(capi.lib().picard_batch_step(arr, n, its, sweeps), "picard_batch_step",
+               (capi.OK, capi.ERR_NOT_CONVERGED))
+    return [int(v) for v in sweeps]

@@ -12,7 +12,7 @@ import pytest
 
 from picard_b200 import capi
 from picard_b200 import params as P
-from picard_b200.simulation import Simulation, batch_run_fused
+from picard_b200.simulation import Simulation, batch_run_fused, batch_step
 
 pytestmark = pytest.mark.gpu
 
@@ -68,3 +68,34 @@ def test_batch_rejects_duplicates():
         batch_run_fused([g, g], 0, 1)
     assert e.value.code == capi.ERR_BAD_ARG
     g.close()
+
+
+def test_staggered_steps_equal_each_run_alone():
+    """picard_batch_step: runs at different iterations of their loops share a
+    step (continuous batching) and still end bit for bit where they end alone."""
+    steps = 4
+    params = _runs()[:3]
+    offsets = [0, 2, 1]  # iterations each run took alone before joining
+    alone = []
+    for p in params:
+        g = _start(p)
+        g.run_fused(0, steps)
+        alone.append((g.num_local, g.field(capi.FIELD_U), g.field(capi.FIELD_N)))
+        g.close()
+    sims = [_start(p) for p in params]
+    done = list(offsets)
+    for g, k in zip(sims, offsets):
+        if k:
+            g.run_fused(0, k)
+    while any(d < steps for d in done):
+        live = [i for i in range(len(sims)) if done[i] < steps]
+        batch_step([sims[i] for i in live], [done[i] + 1 for i in live])
+        for i in live:
+            done[i] += 1
+    for k, g in enumerate(sims):
+        n, U, N = alone[k]
+        assert g.num_local == n, k
+        np.testing.assert_array_equal(g.field(capi.FIELD_U), U, err_msg=f"run {k}")
+        np.testing.assert_array_equal(g.field(capi.FIELD_N), N, err_msg=f"run {k}")
+    for g in sims:
+        g.close()

@@ -99,3 +99,29 @@ def test_admission_keeps_within_the_budget():
         with pytest.raises(capi.PicardError) as e:
             s.submit(0, reqs[big], steps)
         assert e.value.code == capi.ERR_CAPACITY
+
+
+def test_batched_server_result_is_the_same_alone_and_in_the_mix():
+    """Continuous batching: runs join and leave the cohort between steps (the
+    step counts differ), and each result equals the run served alone and the
+    run served by the stream-mode server."""
+    reqs = _serving_requests(14, 5, 8)
+    steps = [3, 5, 2, 4, 6]
+    target = 3
+    with Server(8 * GB, 1, batched=True) as s:
+        s.submit(target, reqs[target], steps[target])
+        alone = s.poll(wait_all=True)
+    assert len(alone) == 1 and alone[0]["status"] == capi.OK
+    with Server(8 * GB, 1) as s:
+        s.submit(target, reqs[target], steps[target])
+        streamed = s.poll(wait_all=True)[0]
+    with Server(8 * GB, 3, batched=True, preparers=2) as s:
+        for i, p in enumerate(reqs):
+            s.submit(i, p, steps[i])
+        mix = {r["id"]: r for r in s.poll(wait_all=True)}
+    assert sorted(mix) == list(range(len(reqs)))
+    assert all(r["status"] == capi.OK for r in mix.values())
+    spans = sorted((r["start_ms"], r["finish_ms"]) for r in mix.values())
+    assert any(spans[k + 1][0] < spans[k][1] for k in range(len(spans) - 1))
+    _same(alone[0], mix[target])
+    _same(streamed, mix[target])
