@@ -281,7 +281,10 @@ def run_picard(args, rank, world, local_rank):
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "launch_ms": sweep_avg_ms,
-                         "traffic": None},
+                         "traffic": SWEEP_DRAM_BYTES.get((p.nx, p.ny, p.nz, solver)),
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of "
+                                           "the sweep kernel on this grid (caches flushed by the replay; in the "
+                                           "live loop the 52 MB working set stays in L2)"},
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -292,6 +295,11 @@ def run_picard(args, rank, world, local_rank):
 
 
 # ----------------------------------------------------------- CPU baseline
+
+# DRAM bytes of one Jacobi sweep launch, from an ncu capture of that launch
+# (dram__bytes_read.sum + dram__bytes_write.sum), keyed by (nx, ny, nz, solver)
+SWEEP_DRAM_BYTES = {(256, 128, 128, 1): 35.27e6}
+
 
 def cpu_baseline(args, sweeps_per_step=None, steps: int = 1) -> dict:
     """Bounded samples of full-size iterations on the CPU oracle with every
@@ -646,16 +654,18 @@ def run_batch(args, local_rank):
     """Batched parameter sweep: --runs independent runs (cubic grids 16..96
     cells, 8..32 ppc, drift 300..800 km/s, |B| 1..10 nT in a random direction,
     --run-steps iterations each, CELL32 / F32_REFINE) advanced two ways:
-      plain:   one run after another through picard_gpu_run_fused;
+      plain:   one run after another through picard_gpu_run, the
+               per-subroutine call sequence of picard.f90 (the drop-in loop);
+      fused:   one run after another through picard_gpu_run_fused (the
+               single-run loop the batch and the server build on);
       batched: all runs together through picard_batch_run_fused (one sweep
                launch per sweep for every run).
-      batched: the continuous-batching request loop -- the same admission, up
-              to --batch-slots runs advanced together one iteration at a time,
-              all their Jacobi sweeps in one launch per sweep.
-    All arms create, initialise, run and release every run inside the timed
-    region (the sweep launch tuner runs at creation in both).  Reports
-    particle-steps/s of each arm and checks that every run ends bit for bit
-    where it ends alone."""
+    Every arm creates, initialises, runs and releases every run inside its
+    timed region (the sweep launch tuner runs at creation).  Reports
+    particle-steps/s of each arm and checks that every batched run ends bit
+    for bit where the fused loop ends it alone (the per-subroutine loop plans
+    its FP32 rounds differently, so its potentials agree to the solver's
+    tolerance, not bit for bit)."""
     import numpy as np
     import torch
 
@@ -689,6 +699,17 @@ def run_batch(args, local_rank):
     visible = os.environ.get("CUDA_VISIBLE_DEVICES")
     clocks = ClockSampler(int(visible.split(",")[local_rank]) if visible else local_rank)
     clocks.start()
+    t0 = time.perf_counter()
+    sub = []
+    for p in runs:
+        g = Simulation(p, derive=False, layout=layout, solver=solver)
+        g.calc_distance()
+        g.particles_initialize()
+        g.run(0, steps)
+        sub.append({"particle_steps": g.stats()["particle_steps"], "u": float(np.abs(g.field(capi.FIELD_U)).sum())})
+        g.close()
+    torch.cuda.synchronize()
+    t_sub = time.perf_counter() - t0
     t0 = time.perf_counter()
     plain = []
     plain_phase = {}
@@ -728,6 +749,7 @@ def run_batch(args, local_rank):
     same = not mism
     ps_plain = sum(r["particle_steps"] for r in plain)
     ps_batch = sum(r["particle_steps"] for r in batched)
+    ps_sub = sum(r["particle_steps"] for r in sub)
     line = {
         "metric": "particle-steps/s, batched vs plain", "value": ps_batch / t_batch, "unit": UNIT, "n_gpus": 1,
         "higher_is_better": True, "impl": "picard", "workload": "batch", "vs_baseline": None,
@@ -737,11 +759,18 @@ def run_batch(args, local_rank):
                                f"drift 300..800 km/s, |B| 1..10 nT random direction, {steps} steps each",
                    "grids": [int(p.nx) for p in runs]},
         "batched": {"particle_steps_per_s": ps_batch / t_batch, "seconds": t_batch},
-        "plain": {"particle_steps_per_s": ps_plain / t_plain, "seconds": t_plain,
-                  "phase_ms": {k: round(v, 1) for k, v in plain_phase.items()}},
-        "batched_over_plain": (ps_batch / t_batch) / (ps_plain / t_plain),
+        "plain": {"particle_steps_per_s": ps_sub / t_sub, "seconds": t_sub,
+                  "loop": "picard_gpu_run (per-subroutine calls)",
+                  "u_abs_sum_max_rel_diff_vs_batched": max(abs(a["u"] - b["u"]) / max(abs(b["u"]), 1e-300)
+                                                            for a, b in zip(sub, batched))},
+        "fused": {"particle_steps_per_s": ps_plain / t_plain, "seconds": t_plain,
+                  "loop": "picard_gpu_run_fused", "phase_ms": {k: round(v, 1) for k, v in plain_phase.items()}},
+        "batched_over_plain": (ps_batch / t_batch) / (ps_sub / t_sub),
+        "batched_over_fused": (ps_batch / t_batch) / (ps_plain / t_plain),
         "jacobi_sweeps_total": sum(r["sweeps"] for r in batched),
-        "results_identical_to_plain": same,
+        "jacobi_node_sweeps": sum(r["sweeps"] * int(p.nx) * int(p.ny) * int(p.nz) for r, p in zip(batched, runs)),
+        "jacobi_sweeps_per_run": [r["sweeps"] for r in batched],
+        "results_identical_to_fused": same,
         "mismatches": mism[:8],
         "clocks": clk,
     }

@@ -39,6 +39,11 @@ namespace {
 
 constexpr int kBatchRuns = 40;  // runs per launch (kernel parameter space)
 constexpr int kTicksAhead = 6;  // batched sweep launches queued ahead of the device
+// Working set (w in, w out, the anchor residual: 12 B a node) of the runs that
+// sweep together.  Kept within the L2 (126 MB) so that consecutive ticks find
+// their tiles there instead of streaming every run from HBM on every sweep;
+// the other runs wait, and join as runs of the set converge.
+constexpr double kTickSetBytes = 80e6;
 
 struct alignas(64) BatchRun {
   CUtensorMap tw;  // w of the sweep's input iterate (x-pair boxes 72 x 10 x zc+2)
@@ -164,6 +169,7 @@ struct RunSolve {
   EpotSetup e;
   F32Solve S;
   bool batched = false;  // the batched loop drives this run's solve
+  bool active = false;   // in the set of runs that sweep together
   bool done = true;
   int phase = 0;         // 0 round to plan, 1 sweeping, 2 anchor and stop test in flight
   int p = 0;             // sweeps of the current round done
@@ -276,6 +282,9 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
   std::vector<RunSolve*> rp(n);
   for (int r = 0; r < n; ++r) rp[r] = &solves[r];
 
+  // PICARD_BATCH_SET_MB: working-set budget of the runs that sweep together
+  const char* setv = std::getenv("PICARD_BATCH_SET_MB");
+  const double tick_set_bytes = setv && *setv ? std::atof(setv) * 1e6 : kTickSetBytes;
   // PICARD_BATCH_LOG=1: host time per phase (waits for the device included)
   const char* logv = std::getenv("PICARD_BATCH_LOG");
   const bool log = logv && *logv && *logv != '0';
@@ -382,11 +391,34 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
       bool first_tick = true;
       std::vector<RunSolve*> ended;
       long long issued = 0, retired = 0;  // ticks queued / known complete
+      // runs join the sweeping set largest first (they need the most sweeps),
+      // within the working-set budget
+      std::vector<int> order;
+      for (int r = 0; r < n; ++r)
+        if (solves[r].batched && !solves[r].done) order.push_back(r);
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int a, int b) { return ctxs[a]->K.nodes > ctxs[b]->K.nodes; });
+      size_t next_join = 0;
+      double set_bytes = 0.0;
       for (;;) {
+        for (int r = 0; r < n; ++r) {
+          RunSolve& rs = solves[r];
+          if (rs.active && rs.done) {
+            rs.active = false;
+            set_bytes -= 12.0 * double(ctxs[r]->K.nodes);
+          }
+        }
+        while (next_join < order.size()) {
+          const double b = 12.0 * double(ctxs[order[next_join]]->K.nodes);
+          if (set_bytes > 0.0 && set_bytes + b > tick_set_bytes) break;
+          solves[order[next_join]].active = true;
+          set_bytes += b;
+          ++next_join;
+        }
         int sweeping = 0, waiting = 0;
         for (int r = 0; r < n; ++r) {
           RunSolve& rs = solves[r];
-          if (rs.done || !rs.batched) continue;
+          if (rs.done || !rs.batched || !rs.active) continue;
           if (rs.phase == 0) {
             f32_plan(rs.S);
             rs.phase = 1;
@@ -396,7 +428,7 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
           sweeping += rs.phase == 1;
           waiting += rs.phase == 2;
         }
-        if (sweeping == 0 && waiting == 0) break;
+        if (sweeping == 0 && waiting == 0 && next_join == order.size()) break;
         if (sweeping > 0) {
           // keep at most kTicksAhead ticks queued, so that a run whose stop
           // test the host has just read joins the ticks right away instead of
@@ -423,7 +455,7 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
         // collect the stop tests that have landed (block when nothing else can move)
         for (int r = 0; r < n; ++r) {
           RunSolve& rs = solves[r];
-          if (rs.done || !rs.batched || rs.phase != 2) continue;
+          if (rs.done || !rs.batched || !rs.active || rs.phase != 2) continue;
           cudaError_t q = sweeping > 0 ? cudaEventQuery(dev_ev[r]) : cudaEventSynchronize(dev_ev[r]);
           if (q == cudaErrorNotReady) continue;
           PICARD_CUDA(q);

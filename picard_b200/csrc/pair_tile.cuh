@@ -56,17 +56,21 @@ constexpr int kPairBoxX = 72, kPairTile = 64, kPairTy = 8;
 
 // rows: [2][8] shared doubles (row sums of the two 32-wide tiles).  Ends with
 // the CTA's threads past a barrier; the caller separates tiles by another.
-template <int ZC>
-__device__ __forceinline__ void pair_tile_sweep(const float* sw, const float* sr, const Stencil& S,
-                                                const JacobiCoefF& J, float* wout, double* partial, int w_zero,
-                                                int bx2, int by, int bz, int gx, int gy, double (*rows)[kPairTy]) {
+// FULL: the tile lies wholly inside the interior (pair_tile_full), so no lane
+// is masked and every plane is swept -- the same arithmetic without the
+// bounds selects.
+template <int ZC, bool FULL>
+__device__ __forceinline__ void pair_tile_sweep_body(const float* sw, const float* sr, const Stencil& S,
+                                                     const JacobiCoefF& J, float* wout, double* partial, int w_zero,
+                                                     int bx2, int by, int bz, int gx, int gy,
+                                                     double (*rows)[kPairTy]) {
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
   const long long plane = (long long)S.fpitch * S.nyp;
   const unsigned long long m2 = pk2(-2.0f, -2.0f), ix2 = pk2(J.idx2, J.idx2), iy2 = pk2(J.idy2, J.idy2),
                            iz2 = pk2(J.idz2, J.idz2), naf = pk2(-J.af, -J.af);
   const int i0 = bx2 * kPairTile + 2 * tx + 1, j = by * kPairTy + ty + 1, z0 = bz * ZC;
-  const bool act0 = i0 <= S.nx && j <= S.ny, act1 = i0 + 1 <= S.nx && j <= S.ny;
-  const int kend = min(ZC, S.nz - z0);
+  const bool act0 = FULL || (i0 <= S.nx && j <= S.ny), act1 = FULL || (i0 + 1 <= S.nx && j <= S.ny);
+  const int kend = FULL ? ZC : min(ZC, S.nz - z0);
   // w rows of this thread's pair: plane kk (0 .. ZC+1), row 0 .. 9, columns 2 tx + 4, + 5
   auto wrow = [&](int kk, int row) {
     return *reinterpret_cast<const unsigned long long*>(sw + (kk * (kPairTy + 2) + row) * kPairBoxX + 2 * tx + 4);
@@ -78,7 +82,7 @@ __device__ __forceinline__ void pair_tile_sweep(const float* sw, const float* sr
   float* out = wout + fidx(S, i0, j, z0 + 1);
 #pragma unroll
   for (int kk = 1; kk <= ZC; ++kk) {
-    if (kk <= kend) {
+    if (FULL || kk <= kend) {
       unsigned long long wp = 0ull, ym = 0ull, yp = 0ull;
       float xl = 0.0f, xr = 0.0f;
       const float2 c = up2(wc);
@@ -99,10 +103,10 @@ __device__ __forceinline__ void pair_tile_sweep(const float* sw, const float* sr
       lap = fma2(fma2(m2, wc, sz), iz2, lap);
       const unsigned long long res = sub2(rr, lap);
       const float2 rf = up2(res);
-      const unsigned long long resm = pk2(act0 ? rf.x : 0.0f, act1 ? rf.y : 0.0f);
+      const unsigned long long resm = FULL ? res : pk2(act0 ? rf.x : 0.0f, act1 ? rf.y : 0.0f);
       r2 = fma2(resm, resm, r2);
       const float2 wn = up2(fma2(naf, res, wc));
-      if (act1) {
+      if (FULL || act1) {
         *reinterpret_cast<float2*>(out) = wn;
       } else if (act0) {
         out[0] = wn.x;
@@ -130,6 +134,21 @@ __device__ __forceinline__ void pair_tile_sweep(const float* sw, const float* sr
       partial[bx + (long long)gx * (by + (long long)gy * bz)] = sum;
     }
   }
+}
+
+// The tile (bx2, by, bz) lies wholly inside the nx x ny x nz interior.
+__device__ __forceinline__ bool pair_tile_full(const Stencil& S, int bx2, int by, int z0, int zc) {
+  return (bx2 + 1) * kPairTile <= S.nx && (by + 1) * kPairTy <= S.ny && z0 + zc <= S.nz;
+}
+
+template <int ZC>
+__device__ __forceinline__ void pair_tile_sweep(const float* sw, const float* sr, const Stencil& S,
+                                                const JacobiCoefF& J, float* wout, double* partial, int w_zero,
+                                                int bx2, int by, int bz, int gx, int gy, double (*rows)[kPairTy]) {
+  if (pair_tile_full(S, bx2, by, bz * ZC, ZC))
+    pair_tile_sweep_body<ZC, true>(sw, sr, S, J, wout, partial, w_zero, bx2, by, bz, gx, gy, rows);
+  else
+    pair_tile_sweep_body<ZC, false>(sw, sr, S, J, wout, partial, w_zero, bx2, by, bz, gx, gy, rows);
 }
 
 }  // namespace picard
