@@ -49,6 +49,10 @@ typedef struct picard_result {
   double energy[3];        /* kinetic, electric, magnetic (picard.f90:667-671) */
   double u_sum;            /* sum of the final potential over all nodes      */
   double u_abs_sum;        /* sum of its absolute values                     */
+  uint32_t warnings;       /* WriteWarnings.f90 mask of the request's params
+                              (picard_io.h picard_warning); the reference only
+                              warns, so a run with warnings still runs       */
+  int32_t reserved;
 } picard_result;
 
 /* hbm_budget_bytes: device memory the admitted runs may hold together.

@@ -89,6 +89,8 @@ class PicardResult(C.Structure):
         ("energy", C.c_double * 3),
         ("u_sum", C.c_double),
         ("u_abs_sum", C.c_double),
+        ("warnings", C.c_uint32),
+        ("reserved", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -96,6 +98,39 @@ class PicardResult(C.Structure):
         d["energy"] = tuple(self.energy)
         return d
 
+
+class PicardPlasma(C.Structure):
+    """include/picard_io.h picard_plasma."""
+    _fields_ = [
+        ("wp", C.c_double * 3), ("wc", C.c_double * 3), ("va", C.c_double), ("vc", C.c_double * 3),
+        ("Ld", C.c_double * 3), ("rL", C.c_double * 3), ("rPU", C.c_double * 3), ("Li", C.c_double * 3),
+        ("sd", C.c_double), ("rM", C.c_double * 3), ("cfl", C.c_double), ("freq", C.c_double),
+        ("dt_c", C.c_double), ("dt_opt_part", C.c_double), ("dt_opt_wave", C.c_double), ("dt_opt", C.c_double),
+        ("dt_rec", C.c_double), ("vth", C.c_double * 8), ("warnings", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            out[k] = tuple(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class PicardIO(C.Structure):
+    """include/picard_io.h picard_io."""
+    _fields_ = [
+        ("write_fields", C.c_int32),
+        ("write_particles", C.c_int32),
+        ("fields_interval", C.c_double),
+        ("particles_interval", C.c_double),
+        ("fields_iteration", C.c_int32),
+        ("particles_iteration", C.c_int32),
+        ("root", C.c_char * 512),
+    ]
+
+
+WARN_COUNT = 17
 
 LOG_FN = C.CFUNCTYPE(None, C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_void_p)
 
@@ -168,6 +203,13 @@ def lib():
         "picard_server_destroy": [C.c_void_p],
         "picard_gpu_particles_gridify_noalloc": [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                                  C.c_void_p, C.c_void_p, C.c_void_p],
+        "picard_format_e": [C.c_double, C.c_int32, C.c_int32, C.c_char_p],
+        "picard_gpu_dump_particles": [ctx, C.c_char_p, ip],
+        "picard_gpu_dump_fields": [ctx, C.c_char_p, ip],
+        "picard_params_plasma": [P, C.POINTER(PicardPlasma)],
+        "picard_write_parameters": [P, C.c_char_p, C.POINTER(C.c_uint32)],
+        "picard_gpu_run_io": [ctx, C.c_int32, C.c_int32, C.c_int32, LOG_FN, C.c_void_p, C.POINTER(PicardIO),
+                              C.POINTER(C.c_int64)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -175,6 +217,8 @@ def lib():
         f.restype = C.c_int
     L.picard_gpu_last_error.argtypes = []
     L.picard_gpu_last_error.restype = C.c_char_p
+    L.picard_warning_text.argtypes = [C.c_int32]
+    L.picard_warning_text.restype = C.c_char_p
     _lib = L
     return L
 
@@ -205,3 +249,28 @@ def footprint(p: PicardParams, layout: int, solver: int) -> int:
     b = C.c_uint64(0)
     check(lib().picard_gpu_footprint(C.byref(p), layout, solver, C.byref(b)), "picard_gpu_footprint")
     return int(b.value)
+
+
+def format_e(value: float, w: int = 10, d: int = 4) -> str:
+    """Fortran Ew.d of value (picard_format_e)."""
+    buf = C.create_string_buffer(w + 1)
+    check(lib().picard_format_e(float(value), w, d, buf), "picard_format_e")
+    return buf.value.decode()
+
+
+def plasma(p) -> dict:
+    """WriteWarnings.f90's plasma quantities and warning mask of derived params."""
+    out = PicardPlasma()
+    check(lib().picard_params_plasma(C.byref(p), C.byref(out)), "picard_params_plasma")
+    return out.as_dict()
+
+
+def warning_texts(mask: int) -> list[str]:
+    return [lib().picard_warning_text(k).decode() for k in range(WARN_COUNT) if mask >> k & 1]
+
+
+def write_parameters(p, root: str) -> int:
+    """<root>/parameters.dat and <root>/warnings.dat; returns the warning mask."""
+    m = C.c_uint32(0)
+    check(lib().picard_write_parameters(C.byref(p), root.encode(), C.byref(m)), "picard_write_parameters")
+    return int(m.value)

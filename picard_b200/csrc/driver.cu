@@ -9,6 +9,7 @@
 
 #include "context.cuh"
 #include "picard_gpu.h"
+#include "picard_io.h"
 
 using namespace picard;
 
@@ -160,10 +161,24 @@ static int log_energy(picard_ctx* c, int32_t it, double time, picard_log_fn fn, 
   return PICARD_OK;
 }
 
-// picard.f90:554-674, writeFields = writeParticles = .false.
-int picard_gpu_run(picard_ctx* c, int32_t iter_start, int32_t iter_end, int32_t log_interval, picard_log_fn log_fn,
-                   void* user, int64_t* sweeps_total) {
-  if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
+// The end of a step on a write step (picard.f90:602-621): the velocity push
+// split around the dumps.
+static int write_step(picard_ctx* c, double time, picard_io* io) {
+  const picard_params& p = c->prm;
+  const bool wp = io->write_particles && std::fmod(time, io->particles_interval) < p.dt;
+  const bool wf = io->write_fields && std::fmod(time, io->fields_interval) < p.dt;
+  PICARD_TRY(picard_gpu_advance_velocity_imp(c, 0.5 * p.dt, p.dt));
+  if (wp) PICARD_TRY(picard_gpu_dump_particles(c, io->root, &io->particles_iteration));
+  if (wf) {
+    PICARD_TRY(picard_gpu_particles_gridify_all(c));
+    PICARD_TRY(picard_gpu_dump_fields(c, io->root, &io->fields_iteration));
+  }
+  return picard_gpu_advance_velocity_exp(c, 0.5 * p.dt, p.dt);
+}
+
+// picard.f90:554-674; io == NULL: writeFields = writeParticles = .false.
+static int run_loop(picard_ctx* c, int32_t iter_start, int32_t iter_end, int32_t log_interval, picard_log_fn log_fn,
+                    void* user, picard_io* io, int64_t* sweeps_total) {
   const picard_params& p = c->prm;
   double time = (double)iter_start * p.dt;
   bool nc = false;
@@ -187,7 +202,13 @@ int picard_gpu_run(picard_ctx* c, int32_t iter_start, int32_t iter_end, int32_t 
     PICARD_TRY(picard_gpu_calc_efield(c));
     PICARD_TRY(picard_gpu_bc_fields(c));
     // ParticlesModifyImp(): empty (ParticlesModify.f90:9-14)
-    PICARD_TRY(picard_gpu_advance_velocity(c, p.dt));
+    const bool writing = io && (io->write_fields || io->write_particles) &&
+                         ((io->write_fields && std::fmod(time, io->fields_interval) < p.dt) ||
+                          (io->write_particles && std::fmod(time, io->particles_interval) < p.dt));
+    if (writing)
+      PICARD_TRY(write_step(c, time, io));
+    else
+      PICARD_TRY(picard_gpu_advance_velocity(c, p.dt));
     c->stats.steps += 1;
     c->stats.particle_steps += c->num_local;
     if (log_interval > 0 && it % log_interval == 0) PICARD_TRY(log_energy(c, it, time, log_fn, user));
@@ -195,6 +216,21 @@ int picard_gpu_run(picard_ctx* c, int32_t iter_start, int32_t iter_end, int32_t 
   PICARD_CUDA(cudaStreamSynchronize(c->st));
   if (nc) return fail(PICARD_ERR_NOT_CONVERGED, "at least one Jacobi solve hit 2*maxit+1 sweeps");
   return PICARD_OK;
+}
+
+int picard_gpu_run(picard_ctx* c, int32_t iter_start, int32_t iter_end, int32_t log_interval, picard_log_fn log_fn,
+                   void* user, int64_t* sweeps_total) {
+  if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
+  return run_loop(c, iter_start, iter_end, log_interval, log_fn, user, nullptr, sweeps_total);
+}
+
+int picard_gpu_run_io(picard_ctx* c, int32_t iter_start, int32_t iter_end, int32_t log_interval, picard_log_fn log_fn,
+                      void* user, picard_io* io, int64_t* sweeps_total) {
+  if (!c || !io) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  if ((io->write_fields && !(io->fields_interval > 0.0)) ||
+      (io->write_particles && !(io->particles_interval > 0.0)))
+    return fail(PICARD_ERR_BAD_ARG, "write interval must be positive");
+  return run_loop(c, iter_start, iter_end, log_interval, log_fn, user, io, sweeps_total);
 }
 
 // The same iterations with the inflow candidates generated, advanced and

@@ -27,6 +27,7 @@
 
 #include "context.cuh"
 #include "picard_gpu.h"
+#include "picard_io.h"
 #include "picard_server.h"
 
 using namespace picard;
@@ -114,6 +115,12 @@ int run_request(const picard_request& rq, picard_result* out) {
   return finish_run(c, out);
 }
 
+// WriteWarnings.f90's mask of a request's parameters (0 if it cannot be formed).
+uint32_t request_warnings(const picard_request& rq) {
+  picard_plasma q;
+  return picard_params_plasma(&rq.params, &q) == PICARD_OK ? q.warnings : 0u;
+}
+
 void worker_main(picard_server* s) {
   cudaSetDevice(s->device);
   for (;;) {
@@ -134,6 +141,7 @@ void worker_main(picard_server* s) {
     picard_result r;
     std::memset(&r, 0, sizeof(r));
     r.id = job.first.id;
+    r.warnings = request_warnings(job.first);
     r.start_ms = now_ms(s);
     r.status = run_request(job.first, &r);
     r.finish_ms = now_ms(s);
@@ -195,6 +203,7 @@ void preparer_main(picard_server* s) {
     picard_result r;
     std::memset(&r, 0, sizeof(r));
     r.id = job.first.id;
+    r.warnings = request_warnings(job.first);
     r.arrival_ms = job.first.arrival_ms;
     r.start_ms = now_ms(s);
     picard_ctx* c = nullptr;

@@ -194,6 +194,38 @@ class Simulation:
                    allow=(capi.OK, capi.ERR_NOT_CONVERGED))
         return total.value
 
+    def run_io(self, iter_start: int, iter_end: int, root: str, write_fields: bool = True,
+               write_particles: bool = True, fields_interval: float | None = None,
+               particles_interval: float | None = None, fields_iteration: int = 0, particles_iteration: int = 0,
+               log_interval: int = 0, log=None) -> tuple[int, int, int]:
+        """picard.f90:554-674 with the write-step branch (602-627) and the dumps
+        of Write.f90 under ``root`` (the reference's ``save``).  Intervals are
+        seconds (reference defaults 100 dt for fields, 1000 dt for particles).
+        Returns (sweeps, next fields file number, next particles file number)."""
+        io = capi.PicardIO()
+        io.write_fields = 1 if write_fields else 0
+        io.write_particles = 1 if write_particles else 0
+        io.fields_interval = float(100.0 * self.p.dt if fields_interval is None else fields_interval)
+        io.particles_interval = float(1000.0 * self.p.dt if particles_interval is None else particles_interval)
+        io.fields_iteration = int(fields_iteration)
+        io.particles_iteration = int(particles_iteration)
+        io.root = root.encode()
+        total = C.c_int64(0)
+        cb = LOG_NONE if log is None else capi.LOG_FN(lambda it, t, n, up, ue, ub, _u: log(it, t, n, up, ue, ub))
+        self._call("picard_gpu_run_io", iter_start, iter_end, log_interval, cb, None, C.byref(io), C.byref(total),
+                   allow=(capi.OK, capi.ERR_NOT_CONVERGED))
+        return total.value, io.fields_iteration, io.particles_iteration
+
+    def dump_particles(self, root: str, write_iteration: int) -> int:   # Write.f90:1-31
+        it = C.c_int32(write_iteration)
+        self._call("picard_gpu_dump_particles", root.encode(), C.byref(it))
+        return it.value
+
+    def dump_fields(self, root: str, write_iteration: int) -> int:      # Write.f90:34-523
+        it = C.c_int32(write_iteration)
+        self._call("picard_gpu_dump_fields", root.encode(), C.byref(it))
+        return it.value
+
     def run_fused(self, iter_start: int, iter_end: int) -> int:
         total = C.c_int64(0)
         self._call("picard_gpu_run_fused", iter_start, iter_end, C.byref(total),

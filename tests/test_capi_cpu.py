@@ -97,14 +97,20 @@ _LAYOUT_PROBE = r"""
 #include <stddef.h>
 #include <stdio.h>
 #include "picard_server.h"
+#include "picard_io.h"
 #define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m))
 int main(void) {
+  printf("picard_plasma %zu\n", sizeof(picard_plasma));
+  printf("picard_io %zu\n", sizeof(picard_io));
+  F(picard_plasma, va); F(picard_plasma, sd); F(picard_plasma, cfl); F(picard_plasma, dt_rec);
+  F(picard_plasma, vth); F(picard_plasma, warnings);
+  F(picard_io, fields_interval); F(picard_io, fields_iteration); F(picard_io, root);
   printf("picard_params %zu\n", sizeof(picard_params));
   printf("picard_stats %zu\n", sizeof(picard_stats));
   printf("picard_request %zu\n", sizeof(picard_request));
   printf("picard_result %zu\n", sizeof(picard_result));
   F(picard_request, params); F(picard_request, layout); F(picard_request, steps); F(picard_request, arrival_ms);
-  F(picard_result, status); F(picard_result, sweeps); F(picard_result, energy); F(picard_result, u_abs_sum);
+  F(picard_result, status); F(picard_result, sweeps); F(picard_result, energy); F(picard_result, u_abs_sum); F(picard_result, warnings);
   F(picard_stats, phase_ms); F(picard_params, u0);
   return 0;
 }
@@ -124,12 +130,15 @@ def test_ctypes_structs_match_the_c_compiler(tmp_path):
     assert int(got["picard_stats"]) == C.sizeof(capi.PicardStats)
     assert int(got["picard_request"]) == C.sizeof(capi.PicardRequest)
     assert int(got["picard_result"]) == C.sizeof(capi.PicardResult)
+    assert int(got["picard_plasma"]) == C.sizeof(capi.PicardPlasma)
+    assert int(got["picard_io"]) == C.sizeof(capi.PicardIO)
     for key, val in got.items():
         if "." not in key:
             continue
         sname, field = key.split(".")
         cls = {"picard_request": capi.PicardRequest, "picard_result": capi.PicardResult,
-               "picard_stats": capi.PicardStats, "picard_params": P.PicardParams}[sname]
+               "picard_stats": capi.PicardStats, "picard_params": P.PicardParams,
+               "picard_plasma": capi.PicardPlasma, "picard_io": capi.PicardIO}[sname]
         assert getattr(cls, field).offset == int(val), key
 
 

@@ -73,6 +73,7 @@ def test_served_run_equals_the_direct_fused_loop():
         s.submit(0, p, steps)
         r = s.poll(wait_all=True)[0]
     assert r["status"] == capi.OK
+    assert r["warnings"] == capi.plasma(p)["warnings"]  # WriteWarnings.f90 on the request
     assert r["num_local"] == n
     assert r["u_sum"] == pytest.approx(float(U.sum()), rel=1e-12, abs=0)
     np.testing.assert_allclose(r["energy"], e, rtol=1e-12)
