@@ -11,9 +11,10 @@
 // run table (tensor maps, stencil, coefficients, output, tile range) rides in
 // the kernel parameters -- instead of one launch per run.  Anchors, reductions
 // and the stop tests stay per run, asynchronous to the ticks; runs that
-// converge drop out.  The sweep kernel is the x-pair TMA sweep with the
-// same per-node arithmetic and per-tile partials, so every run's result is
-// bit-identical to the same run advanced alone with picard_gpu_run_fused.
+// converge drop out.  The sweep kernels are the x-pair TMA sweep and, on
+// request, the 32-wide one, with the same per-node arithmetic and per-tile
+// partials as the single-run kernels, so every run's result is bit-identical
+// to the same run advanced alone with picard_gpu_run_fused.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,6 +32,7 @@
 #include "solve_f32.cuh"
 #include "stencil.cuh"
 #include "pair_tile.cuh"
+#include "tile32.cuh"
 
 using namespace picard;
 
@@ -44,10 +46,11 @@ constexpr int kTicksAhead = 6;  // batched sweep launches queued ahead of the de
 // their tiles there instead of streaming every run from HBM on every sweep;
 // the other runs wait, and join as runs of the set converge.
 constexpr double kTickSetBytes = 80e6;
+long long g_batch_ctas = 0;  // CTAs launched by batched sweeps (PICARD_BATCH_LOG)
 
 struct alignas(64) BatchRun {
-  CUtensorMap tw;  // w of the sweep's input iterate (x-pair boxes 72 x 10 x zc+2)
-  CUtensorMap tr;  // the run's live anchor residual (boxes 64 x 8 x zc)
+  CUtensorMap tw;  // w of the sweep's input iterate (boxes 72 x 10 x zc+2; 32-wide tiles 40 x 10 x zc+2)
+  CUtensorMap tr;  // the run's live anchor residual (boxes 64 x 8 x zc; 32-wide tiles 32 x 8 x zc)
   Stencil S;
   JacobiCoefF J;
   float* wout;
@@ -141,6 +144,106 @@ __global__ void __launch_bounds__(256) sweep_batch_kernel(const __grid_constant_
   pair_tile_sweep<ZC>(sw, sr, R.S, R.J, R.wout, R.partial, R.w_zero, bx2, by, bz, R.gx, R.gy, rows);
 }
 
+// The 32-wide tile body (tile32.cuh, as in grid.cu sweep_tma_kernel) over a
+// table of runs, for runs whose x extent would leave half of a 64-wide tile
+// empty.
+template <int ZC>
+__global__ void __launch_bounds__(256) sweep_batch32_kernel(const __grid_constant__ BatchArgs A) {
+  constexpr int kW = (ZC + 2) * (kT32Ty + 2) * kT32BoxX, kR = ZC * kT32Ty * kT32Tx;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* sw = reinterpret_cast<float*>(smem_raw);
+  float* sr = sw + kW;
+  __shared__ __align__(8) unsigned long long mbar;
+  const int tid = threadIdx.x + kT32Tx * threadIdx.y;
+  const int t = blockIdx.x;
+  int r = 0;
+  while (r + 1 < A.nruns && t >= A.run[r + 1].tile_base) ++r;
+  const BatchRun& R = A.run[r];
+  const int lt = t - R.tile_base;
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const int bx = lt % R.gx, by = (lt / R.gx) % R.gy, bz = lt / (R.gx * R.gy);
+  const int x0 = bx * kT32Tx, y0 = by * kT32Ty, z0 = bz * ZC;
+  if (tid == 0) {
+    uint32_t bytes = (uint32_t)(kR * sizeof(float));
+    if (!R.w_zero) bytes += (uint32_t)(kW * sizeof(float));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+    if (!R.w_zero)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+          ::"r"((uint32_t)__cvta_generic_to_shared(sw)), "l"((unsigned long long)&R.tw), "r"(x0), "r"(y0), "r"(z0),
+          "r"(mb)
+          : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)&R.tr), "r"(x0 + 4), "r"(y0 + 1),
+        "r"(z0 + 1), "r"(mb)
+        : "memory");
+  }
+  bool done = false;
+  for (long long it = 0; it < (1LL << 24); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(mb), "r"(0u)
+        : "memory");
+    if (ok) {
+      done = true;
+      break;
+    }
+  }
+  if (!__syncthreads_and(done ? 1 : 0)) {
+    if (tid == 0) atomicCAS(A.err, 0, int(kDevTimeout));
+    for (long long it = 0; it < (1LL << 24); ++it) {
+      uint32_t ok;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(ok)
+          : "r"(mb), "r"(0u)
+          : "memory");
+      if (ok) break;
+    }
+    return;
+  }
+  tile32_sweep<ZC>(sw, sr, R.S, R.J, R.wout, R.partial + (bx + (long long)R.gx * (by + (long long)R.gy * bz)),
+                   R.w_zero, bx, by, bz);
+}
+
+template <int ZC>
+cudaError_t launch_batch32_zc(const BatchArgs& A, int pdl, cudaStream_t st) {
+  constexpr size_t smem = sizeof(float) * ((size_t)(ZC + 2) * 10 * 40 + (size_t)ZC * 8 * 32);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e =
+        cudaFuncSetAttribute(sweep_batch32_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(A.total_tiles);
+  cfg.blockDim = dim3(32, 8);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, sweep_batch32_kernel<ZC>, A);
+}
+
 template <int ZC>
 cudaError_t launch_batch_zc(const BatchArgs& A, int pdl, cudaStream_t st) {
   constexpr size_t smem = sizeof(float) * ((size_t)(ZC + 2) * 10 * 72 + (size_t)ZC * 8 * 64);
@@ -170,6 +273,7 @@ struct RunSolve {
   F32Solve S;
   bool batched = false;  // the batched loop drives this run's solve
   bool active = false;   // in the set of runs that sweep together
+  bool w32 = false;      // 32-wide tiles (tile32.cuh) instead of 64-wide x pairs
   bool done = true;
   int phase = 0;         // 0 round to plan, 1 sweeping, 2 anchor and stop test in flight
   int p = 0;             // sweeps of the current round done
@@ -186,7 +290,9 @@ struct RunSolve {
 int launch_tick(std::vector<RunSolve*>& runs, int* err, cudaStream_t st, bool pdl, std::vector<RunSolve*>& ended,
                 long long* launches) {
   bool first = !pdl;
-  for (int zc : {4, 8}) {
+  for (int cls = 0; cls < 4; ++cls) {
+    const int zc = cls & 1 ? 8 : 4;
+    const bool w32 = cls >= 2;
     BatchArgs A;
     std::memset(&A, 0, sizeof(A));
     A.err = err;
@@ -194,21 +300,23 @@ int launch_tick(std::vector<RunSolve*>& runs, int* err, cudaStream_t st, bool pd
       if (A.nruns == 0) return PICARD_OK;
       const int use_pdl = first ? 0 : 1;
       first = false;
-      cudaError_t e = zc == 8 ? launch_batch_zc<8>(A, use_pdl, st) : launch_batch_zc<4>(A, use_pdl, st);
+      cudaError_t e = w32 ? (zc == 8 ? launch_batch32_zc<8>(A, use_pdl, st) : launch_batch32_zc<4>(A, use_pdl, st))
+                          : (zc == 8 ? launch_batch_zc<8>(A, use_pdl, st) : launch_batch_zc<4>(A, use_pdl, st));
       PICARD_CUDA(e);
       ++*launches;
+      g_batch_ctas += A.total_tiles;
       std::memset(&A, 0, sizeof(A));
       A.err = err;
       return PICARD_OK;
     };
     for (RunSolve* rs : runs) {
-      if (rs->done || !rs->batched || rs->phase != 1 || rs->c->G.zc != zc) continue;
+      if (rs->done || !rs->batched || rs->phase != 1 || rs->c->G.zc != zc || rs->w32 != w32) continue;
       picard_ctx* c = rs->c;
       const int t = rs->p + 1;                  // sweep t of the round
       const int in = rs->S.wcur, out = 1 - in;  // never write the buffer being read
       BatchRun& R = A.run[A.nruns];
-      R.tw = c->tmw2[in];
-      R.tr = c->tmr2[rs->S.rcur];
+      R.tw = w32 ? c->tmw[in] : c->tmw2[in];
+      R.tr = w32 ? c->tmr[rs->S.rcur] : c->tmr2[rs->S.rcur];
       R.S = make_stencil(c->K);
       R.J = jacobi_coef_f(c->K);
       R.wout = c->w[out];
@@ -217,7 +325,7 @@ int launch_tick(std::vector<RunSolve*>& runs, int* err, cudaStream_t st, bool pd
       R.gx2 = (c->K.nx + 63) / 64;
       R.gx = (int)c->G.grid.x;
       R.gy = (int)c->G.grid.y;
-      R.tiles = R.gx2 * (int)c->G.grid.y * (int)c->G.grid.z;
+      R.tiles = (w32 ? R.gx : R.gx2) * (int)c->G.grid.y * (int)c->G.grid.z;
       R.tile_base = A.total_tiles;
       R.w_zero = t == 1 ? 1 : 0;
       A.total_tiles += R.tiles;
@@ -282,6 +390,12 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
   std::vector<RunSolve*> rp(n);
   for (int r = 0; r < n; ++r) rp[r] = &solves[r];
 
+  // PICARD_BATCH_W32=1: 32-wide tiles for runs whose x extent leaves half of a
+  // 64-wide tile empty.  Off by default: the sweep's cost follows the bytes a
+  // tile moves through L2, not the lanes it keeps busy, and the extra launch
+  // class per tick cancels the lanes saved (measured on the 64-run set).
+  const char* w32v = std::getenv("PICARD_BATCH_W32");
+  const bool tile_w32 = w32v && *w32v == '1';
   // PICARD_BATCH_SET_MB: working-set budget of the runs that sweep together
   const char* setv = std::getenv("PICARD_BATCH_SET_MB");
   const double tick_set_bytes = setv && *setv ? std::atof(setv) * 1e6 : kTickSetBytes;
@@ -289,7 +403,8 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
   const char* logv = std::getenv("PICARD_BATCH_LOG");
   const bool log = logv && *logv && *logv != '0';
   double ph[6] = {0, 0, 0, 0, 0, 0};
-  long long rounds = 0, launches = 0;
+  long long rounds = 0, launches = 0, ticks = 0;
+  g_batch_ctas = 0;
   auto now = []() { return std::chrono::steady_clock::now(); };
   auto tick = now();
   auto lap = [&](int k) {
@@ -365,6 +480,8 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
         if (rs.done) continue;
         if (c->solver == PICARD_SOLVER_F32_REFINE && c->G.tma && c->G.zc <= 8) {
           rs.batched = true;
+          // 32-wide tiles when 64-wide ones would leave a 32-column half empty
+          rs.w32 = tile_w32 && ((c->K.nx + 31) / 32) % 2 == 1;
           PICARD_TRY(f32_begin(rs.S, c, rs.e.tol, rs.e.smax, rs.e.maxit, rs.e.sigma));
         } else {
           // not batchable (FP64 solver or periodic axes): its own solve
@@ -439,6 +556,7 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
           }
           ended.clear();
           PICARD_TRY(launch_tick(rp, berr, bst, !first_tick, ended, &launches));
+          ++ticks;
           first_tick = false;
           PICARD_CUDA(cudaEventRecord(tick_ev[issued % kTicksAhead], bst));
           ++issued;
@@ -500,8 +618,8 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
   if (log)
     std::fprintf(stderr,
                  "picard batch %d runs: particles %.1f ms, compaction+inflow %.1f ms, deposit+bcpot+rhs %.1f ms, "
-                 "jacobi %.1f ms (%lld rounds, %lld sweep steps), push %.1f ms\n",
-                 n, ph[0], ph[1], ph[2], ph[3], rounds, launches, ph[4]);
+                 "jacobi %.1f ms (%lld rounds, %lld ticks, %lld launches, %lld CTAs), push %.1f ms\n",
+                 n, ph[0], ph[1], ph[2], ph[3], rounds, ticks, launches, g_batch_ctas, ph[4]);
   if (rc == PICARD_OK) rc = check_cuda(cudaStreamSynchronize(bst), "batch stream");
   cleanup();
   if (rc != PICARD_OK) return rc;

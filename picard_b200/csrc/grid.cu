@@ -27,6 +27,7 @@
 #include "grid.cuh"
 #include "stencil.cuh"
 #include "pair_tile.cuh"
+#include "tile32.cuh"
 
 namespace picard {
 
@@ -208,20 +209,6 @@ __device__ inline void neighbours(const Stencil& S, int i, int j, int k, long lo
   yp = (long long)i + (long long)S.nxp * ((long long)jp + (long long)S.nyp * k);
   zm = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * km);
   zp = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * kp);
-}
-
-__device__ inline void block_sum_store(double v, double* out) {
-  __shared__ double sh[32];
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  int t = threadIdx.x + blockDim.x * threadIdx.y;
-  if ((t & 31) == 0) sh[t >> 5] = v;
-  __syncthreads();
-  if (t == 0) {
-    double s = 0.0;
-    int nw = (blockDim.x * blockDim.y) >> 5;
-    for (int w = 0; w < nw; ++w) s += sh[w];
-    *out = s;
-  }
 }
 
 // b = -C / (dV eps0) everywhere; block partials of b^2 over the interior.
@@ -462,7 +449,6 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
   int t = blockIdx.x;
   if (t >= ntiles) return;
   if (tid == 0) tma_issue_tile<ZC>(&tw, &tr, stages, mb0, t, gx, gy, w_zero);
-  const long long plane = (long long)S.fpitch * S.nyp;
   for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
     const int st = STAGES == 2 ? (it & 1) : 0;
     const uint32_t phase = (uint32_t)(STAGES == 2 ? ((it >> 1) & 1) : (it & 1));
@@ -481,37 +467,8 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
       return;
     }
     const float* sw = stages + st * TmaStage<ZC>::kFloats;
-    const float* sr = sw + TmaStage<ZC>::kW;
     const int bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
-    const int x0 = bx * kTmaTx, y0 = by * kTmaTy, z0 = bz * ZC;
-    const int i = x0 + tx + 1, j = y0 + ty + 1;
-    float r2 = 0.0f;
-    if (i <= S.nx && j <= S.ny) {
-      const int kend = min(ZC, S.nz - z0);
-      long long c = fidx(S, i, j, z0 + 1);
-      const int col = tx + 4;  // smem column of node i
-      if (w_zero) {
-        for (int kk = 1; kk <= kend; ++kk, c += plane) {
-          float res = sr[((kk - 1) * kTmaTy + ty) * kTmaTx + tx];
-          r2 = acc_r2_f32(r2, res);
-          wout[c] = jacobi_next_f32(J, 0.0f, res);
-        }
-      } else {
-        auto W = [&](int kk, int row, int cc) { return sw[(kk * (kTmaTy + 2) + row) * kTmaBoxX + cc]; };
-        float wm = W(0, ty + 1, col);
-        float wc = W(1, ty + 1, col);
-        for (int kk = 1; kk <= kend; ++kk, c += plane) {
-          float wp = W(kk + 1, ty + 1, col);
-          float res = jacobi_res_f32(J, wc, W(kk, ty + 1, col - 1), W(kk, ty + 1, col + 1), W(kk, ty, col),
-                                     W(kk, ty + 2, col), wm, wp, sr[((kk - 1) * kTmaTy + ty) * kTmaTx + tx]);
-          r2 = acc_r2_f32(r2, res);
-          wout[c] = jacobi_next_f32(J, wc, res);
-          wm = wc;
-          wc = wp;
-        }
-      }
-    }
-    block_sum_store((double)r2, partial + t);
+    tile32_sweep<ZC>(sw, sw + TmaStage<ZC>::kW, S, J, wout, partial + t, w_zero, bx, by, bz);
     // every thread is done with this stage (and thread 0 with the reduction
     // scratch) before the stage is refilled
     __syncthreads();

@@ -39,7 +39,9 @@ def _start(p):
     return g
 
 
-def test_batch_equals_each_run_alone():
+@pytest.mark.parametrize("w32", ["0", "1"])
+def test_batch_equals_each_run_alone(w32, monkeypatch):
+    monkeypatch.setenv("PICARD_BATCH_W32", w32)  # 32-wide tiles for the 24^3 and 16^3 runs when "1"
     steps = 4
     params = _runs()
     alone = []
