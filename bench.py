@@ -55,7 +55,7 @@ def parse_args():
     ap.add_argument("--rate", type=float, default=20.0, help="serving workload: mean arrivals per second")
     ap.add_argument("--run-steps", type=int, default=200, help="serving workload: iterations per run")
     ap.add_argument("--slots", type=int, default=8, help="serving workload: runs in flight at once")
-    ap.add_argument("--batch-slots", type=int, default=24,
+    ap.add_argument("--batch-slots", type=int, default=8,
                     help="serving workload, continuous batching: runs in the cohort at once")
     ap.add_argument("--preparers", type=int, default=3,
                     help="serving workload, continuous batching: threads preparing admitted runs")
