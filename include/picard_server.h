@@ -52,7 +52,7 @@ typedef struct picard_result {
   uint32_t warnings;       /* WriteWarnings.f90 mask of the request's params
                               (picard_io.h picard_warning); the reference only
                               warns, so a run with warnings still runs       */
-  int32_t reserved;
+  int32_t shard;           /* index into the device list of picard_server_create_multi (0 otherwise) */
 } picard_result;
 
 /* hbm_budget_bytes: device memory the admitted runs may hold together.
@@ -67,6 +67,17 @@ PICARD_API int picard_server_create(uint64_t hbm_budget_bytes, int32_t max_slots
  * run's result is bit-identical to the same run alone. */
 PICARD_API int picard_server_create_batched(uint64_t hbm_budget_bytes, int32_t max_runs, int32_t preparers,
                                             picard_server** out);
+/* Run placement over several devices: one server per entry of devices[ndev]
+ * (stream mode, or continuous batching when `batched`), each with its own HBM
+ * budget and slots.  A request goes to the shard whose admitted and queued
+ * footprint is the smallest fraction of its budget (the first on ties); runs
+ * are independent, so nothing crosses between devices.  submit, poll (results
+ * of every shard, in finish order, tagged with their shard), load (summed) and
+ * destroy work on the whole set.  An ordinal may appear more than once: two
+ * shards then share that device. */
+PICARD_API int picard_server_create_multi(const int32_t* devices, int32_t ndev, uint64_t hbm_budget_per_device,
+                                          int32_t slots_per_device, int32_t batched, int32_t preparers,
+                                          picard_server** out);
 /* Queues a run.  PICARD_ERR_CAPACITY if its footprint exceeds the whole budget
  * (it could never be admitted), PICARD_ERR_BAD_ARG for invalid params. */
 PICARD_API int picard_server_submit(picard_server* s, const picard_request* rq);

@@ -90,7 +90,7 @@ class PicardResult(C.Structure):
         ("u_sum", C.c_double),
         ("u_abs_sum", C.c_double),
         ("warnings", C.c_uint32),
-        ("reserved", C.c_int32),
+        ("shard", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -196,6 +196,8 @@ def lib():
         "picard_batch_step": [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64)],
         "picard_server_create": [C.c_uint64, C.c_int32, C.POINTER(C.c_void_p)],
         "picard_server_create_batched": [C.c_uint64, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)],
+        "picard_server_create_multi": [C.POINTER(C.c_int32), C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
+                                       C.POINTER(C.c_void_p)],
         "picard_server_submit": [C.c_void_p, C.POINTER(PicardRequest)],
         "picard_server_now_ms": [C.c_void_p, dp],
         "picard_server_poll": [C.c_void_p, C.POINTER(PicardResult), C.c_int32, ip, C.c_int32],

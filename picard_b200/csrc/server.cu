@@ -15,6 +15,7 @@
 // synchronise the device.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -40,6 +41,8 @@ struct picard_server {
   int running = 0;
   bool stopping = false;
   bool batched = false;  // continuous batching: one cohort advanced by picard_batch_step
+  int shard = 0;         // index of this server among the shards of a multi-device server
+  std::vector<picard_server*> shards;  // multi-device server: one server per device
   std::deque<std::pair<picard_request, uint64_t>> queue;  // request, footprint
   std::vector<picard_result> done;
   std::mutex mu;
@@ -142,6 +145,7 @@ void worker_main(picard_server* s) {
     std::memset(&r, 0, sizeof(r));
     r.id = job.first.id;
     r.warnings = request_warnings(job.first);
+    r.shard = s->shard;
     r.start_ms = now_ms(s);
     r.status = run_request(job.first, &r);
     r.finish_ms = now_ms(s);
@@ -204,6 +208,7 @@ void preparer_main(picard_server* s) {
     std::memset(&r, 0, sizeof(r));
     r.id = job.first.id;
     r.warnings = request_warnings(job.first);
+    r.shard = s->shard;
     r.arrival_ms = job.first.arrival_ms;
     r.start_ms = now_ms(s);
     picard_ctx* c = nullptr;
@@ -268,28 +273,49 @@ void scheduler_main(picard_server* s) {
   }
 }
 
+// A server on `device` (its worker threads make it current), results timed
+// from t0, reporting `shard` as the shard index.
+picard_server* open_server(uint64_t budget, int slots, bool batched, int preparers, int device, int shard,
+                           std::chrono::steady_clock::time_point t0) {
+  picard_server* s = new picard_server();
+  s->budget = budget;
+  s->max_slots = slots;
+  s->batched = batched;
+  s->device = device;
+  s->shard = shard;
+  s->t0 = t0;
+  // keep freed context memory in the pool between runs
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = budget;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  if (batched) {
+    for (int i = 0; i < preparers; ++i) s->workers.emplace_back(preparer_main, s);
+    s->workers.emplace_back(scheduler_main, s);
+  } else {
+    for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker_main, s);
+  }
+  return s;
+}
+
+// Footprint a shard holds or has queued, relative to its budget.
+double shard_load(picard_server* s) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  uint64_t q = s->in_use;
+  for (const auto& e : s->queue) q += e.second;
+  return (double)q / (double)s->budget;
+}
+
 }  // namespace
 
 extern "C" {
 
 int picard_server_create(uint64_t hbm_budget_bytes, int32_t max_slots, picard_server** out) {
   if (!out || max_slots < 1 || hbm_budget_bytes == 0) return fail(PICARD_ERR_BAD_ARG, "bad server arguments");
-  picard_server* s = new picard_server();
-  s->budget = hbm_budget_bytes;
-  s->max_slots = max_slots;
-  s->t0 = std::chrono::steady_clock::now();
-  if (cudaGetDevice(&s->device) != cudaSuccess) {
-    delete s;
-    return fail(PICARD_ERR_CUDA, "no CUDA device");
-  }
-  // keep freed context memory in the pool between runs
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
-    uint64_t keep = hbm_budget_bytes;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  }
-  for (int i = 0; i < max_slots; ++i) s->workers.emplace_back(worker_main, s);
-  *out = s;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(PICARD_ERR_CUDA, "no CUDA device");
+  *out = open_server(hbm_budget_bytes, max_slots, false, 0, dev, 0, std::chrono::steady_clock::now());
   return PICARD_OK;
 }
 
@@ -297,29 +323,48 @@ int picard_server_create_batched(uint64_t hbm_budget_bytes, int32_t max_runs, in
                                  picard_server** out) {
   if (!out || max_runs < 1 || preparers < 1 || hbm_budget_bytes == 0)
     return fail(PICARD_ERR_BAD_ARG, "bad server arguments");
-  picard_server* s = new picard_server();
-  s->budget = hbm_budget_bytes;
-  s->max_slots = max_runs;
-  s->batched = true;
-  s->t0 = std::chrono::steady_clock::now();
-  if (cudaGetDevice(&s->device) != cudaSuccess) {
-    delete s;
-    return fail(PICARD_ERR_CUDA, "no CUDA device");
-  }
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
-    uint64_t keep = hbm_budget_bytes;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  }
-  for (int i = 0; i < preparers; ++i) s->workers.emplace_back(preparer_main, s);
-  s->workers.emplace_back(scheduler_main, s);
-  *out = s;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(PICARD_ERR_CUDA, "no CUDA device");
+  *out = open_server(hbm_budget_bytes, max_runs, true, preparers, dev, 0, std::chrono::steady_clock::now());
+  return PICARD_OK;
+}
+
+int picard_server_create_multi(const int32_t* devices, int32_t ndev, uint64_t hbm_budget_per_device,
+                               int32_t slots_per_device, int32_t batched, int32_t preparers, picard_server** out) {
+  if (!out || !devices || ndev < 1 || ndev > 64 || slots_per_device < 1 || hbm_budget_per_device == 0 ||
+      (batched && preparers < 1))
+    return fail(PICARD_ERR_BAD_ARG, "bad server arguments");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) return fail(PICARD_ERR_CUDA, "no CUDA device");
+  for (int k = 0; k < ndev; ++k)
+    if (devices[k] < 0 || devices[k] >= count) return fail(PICARD_ERR_BAD_ARG, "device ordinal out of range");
+  picard_server* m = new picard_server();
+  m->budget = hbm_budget_per_device;
+  m->max_slots = slots_per_device;
+  m->batched = batched != 0;
+  m->t0 = std::chrono::steady_clock::now();
+  for (int k = 0; k < ndev; ++k)
+    m->shards.push_back(open_server(hbm_budget_per_device, slots_per_device, batched != 0, preparers, devices[k], k,
+                                    m->t0));
+  *out = m;
   return PICARD_OK;
 }
 
 int picard_server_submit(picard_server* s, const picard_request* rq) {
   if (!s || !rq) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
   if (rq->steps < 1) return fail(PICARD_ERR_BAD_ARG, "steps < 1");
+  if (!s->shards.empty()) {
+    // the least loaded shard (footprint held and queued over budget), the first on ties
+    size_t best = 0;
+    double lb = shard_load(s->shards[0]);
+    for (size_t k = 1; k < s->shards.size(); ++k) {
+      const double l = shard_load(s->shards[k]);
+      if (l < lb) best = k, lb = l;
+    }
+    picard_request copy = *rq;
+    if (copy.arrival_ms < 0) copy.arrival_ms = now_ms(s);
+    return picard_server_submit(s->shards[best], &copy);
+  }
   uint64_t fp = 0;
   PICARD_TRY(picard_gpu_footprint(&rq->params, rq->layout, rq->solver, &fp));
   if (fp > s->budget)
@@ -345,6 +390,17 @@ int picard_server_now_ms(picard_server* s, double* ms) {
 
 int picard_server_poll(picard_server* s, picard_result* out, int32_t max, int32_t* n, int32_t wait_all) {
   if (!s || !n) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  if (!s->shards.empty()) {
+    int32_t k = 0;
+    for (picard_server* sh : s->shards) {
+      int32_t got = 0;
+      PICARD_TRY(picard_server_poll(sh, out + k, max - k, &got, wait_all));
+      k += got;
+    }
+    std::stable_sort(out, out + k, [](const picard_result& a, const picard_result& b) { return a.finish_ms < b.finish_ms; });
+    *n = k;
+    return PICARD_OK;
+  }
   std::unique_lock<std::mutex> lk(s->mu);
   if (wait_all) s->cv_done.wait(lk, [&] { return s->finished == s->submitted; });
   int32_t k = 0;
@@ -358,6 +414,20 @@ int picard_server_poll(picard_server* s, picard_result* out, int32_t max, int32_
 
 int picard_server_load(picard_server* s, int32_t* running, int32_t* queued, uint64_t* bytes_in_use) {
   if (!s) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
+  if (!s->shards.empty()) {
+    int32_t r = 0, q = 0;
+    uint64_t b = 0;
+    for (picard_server* sh : s->shards) {
+      int32_t r1 = 0, q1 = 0;
+      uint64_t b1 = 0;
+      PICARD_TRY(picard_server_load(sh, &r1, &q1, &b1));
+      r += r1, q += q1, b += b1;
+    }
+    if (running) *running = r;
+    if (queued) *queued = q;
+    if (bytes_in_use) *bytes_in_use = b;
+    return PICARD_OK;
+  }
   std::lock_guard<std::mutex> lk(s->mu);
   if (running) *running = s->running;
   if (queued) *queued = int32_t(s->queue.size());
@@ -367,6 +437,15 @@ int picard_server_load(picard_server* s, int32_t* running, int32_t* queued, uint
 
 int picard_server_destroy(picard_server* s) {
   if (!s) return PICARD_OK;
+  if (!s->shards.empty()) {
+    int rc = PICARD_OK;
+    for (picard_server* sh : s->shards) {
+      const int q = picard_server_destroy(sh);
+      if (rc == PICARD_OK) rc = q;
+    }
+    delete s;
+    return rc;
+  }
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stopping = true;

@@ -22,10 +22,19 @@ class Server:
     advanced together one iteration at a time, all their Jacobi sweeps in one
     launch per sweep, ``preparers`` threads building newly admitted runs."""
 
-    def __init__(self, hbm_budget_bytes: int, slots: int, batched: bool = False, preparers: int = 2):
+    def __init__(self, hbm_budget_bytes: int, slots: int, batched: bool = False, preparers: int = 2,
+                 devices: "list[int] | None" = None):
+        """``devices``: place runs over these device ordinals (one shard each,
+        ``hbm_budget_bytes`` and ``slots`` per shard; picard_server_create_multi);
+        None: the current device only."""
         self._lib = capi.lib()
         self._h = C.c_void_p()
-        if batched:
+        if devices is not None:
+            arr = (C.c_int32 * len(devices))(*[int(d) for d in devices])
+            capi.check(self._lib.picard_server_create_multi(arr, len(devices), int(hbm_budget_bytes), int(slots),
+                                                            1 if batched else 0, int(preparers), C.byref(self._h)),
+                       "picard_server_create_multi")
+        elif batched:
             capi.check(self._lib.picard_server_create_batched(int(hbm_budget_bytes), int(slots), int(preparers),
                                                               C.byref(self._h)), "picard_server_create_batched")
         else:

@@ -110,7 +110,7 @@ int main(void) {
   printf("picard_request %zu\n", sizeof(picard_request));
   printf("picard_result %zu\n", sizeof(picard_result));
   F(picard_request, params); F(picard_request, layout); F(picard_request, steps); F(picard_request, arrival_ms);
-  F(picard_result, status); F(picard_result, sweeps); F(picard_result, energy); F(picard_result, u_abs_sum); F(picard_result, warnings);
+  F(picard_result, status); F(picard_result, sweeps); F(picard_result, energy); F(picard_result, u_abs_sum); F(picard_result, warnings); F(picard_result, shard);
   F(picard_stats, phase_ms); F(picard_params, u0);
   return 0;
 }
@@ -147,5 +147,9 @@ def test_server_rejects_bad_arguments_without_a_device():
     out = C.c_void_p()
     assert L.picard_server_create(0, 2, C.byref(out)) == capi.ERR_BAD_ARG
     assert L.picard_server_create(1 << 30, 0, C.byref(out)) == capi.ERR_BAD_ARG
+    devs = (C.c_int32 * 2)(0, 0)
+    assert L.picard_server_create_multi(devs, 0, 1 << 30, 2, 0, 1, C.byref(out)) == capi.ERR_BAD_ARG
+    assert L.picard_server_create_multi(devs, 2, 1 << 30, 0, 0, 1, C.byref(out)) == capi.ERR_BAD_ARG
+    assert L.picard_server_create_multi(None, 2, 1 << 30, 2, 0, 1, C.byref(out)) == capi.ERR_BAD_ARG
     assert L.picard_server_submit(None, None) == capi.ERR_BAD_ARG
     assert L.picard_server_destroy(None) == capi.OK

@@ -126,3 +126,24 @@ def test_batched_server_result_is_the_same_alone_and_in_the_mix():
     assert any(spans[k + 1][0] < spans[k][1] for k in range(len(spans) - 1))
     _same(alone[0], mix[target])
     _same(streamed, mix[target])
+
+
+@pytest.mark.parametrize("batched", [False, True])
+def test_multi_device_placement_spreads_runs_and_keeps_results(batched):
+    """picard_server_create_multi with the device list [0, 0]: two shards on
+    one GPU (the only one a test box has).  Runs go to both shards, and each
+    result equals the same run served by a single-device server."""
+    reqs = _serving_requests(15, 4, 3)
+    with Server(8 * GB, 2) as s:
+        for i, p in enumerate(reqs):
+            s.submit(i, p, 3)
+        single = {r["id"]: r for r in s.poll(wait_all=True)}
+    with Server(8 * GB, 2, batched=batched, preparers=1, devices=[0, 0]) as s:
+        for i, p in enumerate(reqs):
+            s.submit(i, p, 3)
+        multi = {r["id"]: r for r in s.poll(wait_all=True)}
+        assert s.load()[:2] == (0, 0)
+    assert sorted(multi) == list(range(len(reqs)))
+    assert {r["shard"] for r in multi.values()} == {0, 1}
+    for i in range(len(reqs)):
+        _same(single[i], multi[i])
