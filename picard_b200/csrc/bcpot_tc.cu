@@ -7,14 +7,16 @@
 // where f = 0, 1 are the two faces of the axis (they differ only in the normal
 // offset of D).  For a fixed plane q and row shift d = q1 - p1 this is a GEMM
 //   U_f(p1, :) += C(q, p1 + d, :) . T_{q,d,f},  T[q2, p2] = D_f(q, d, q2 - p2)
-// (T is Toeplitz).  A CTA owns one face of a 128 x 128 output tile -- 128
-// rows p1 by 128 columns p2 -- and accumulates it in tensor memory over a
-// slice of the (q, d) pairs (split-K over all SMs).
+// (T is Toeplitz).  A CTA owns one face of a 128 x N output tile -- 128
+// rows p1 by N columns p2, N = 64, 96 or 128 (the smallest that holds a face
+// of up to 128 columns, so that narrow faces are not padded to 128) -- and
+// accumulates it in tensor memory over a slice of the (q, d) pairs (split-K
+// over all SMs).
 //
 // Precision: every FP64 operand is split into three BF16 parts
 // (x = x1 + x2 + x3, 24 significant bits) and each K-step issues the six
 // products x_i y_j with i + j <= 4.  Each FP32 MMA accumulation spans one
-// step (128 K-values); the steps are summed in tensor memory with Kahan
+// step (N K-values); the steps are summed in tensor memory with Kahan
 // compensation, and the CTA's result goes out once as FP64.  A reduction
 // kernel sums the per-CTA partials in a fixed order.
 //
@@ -38,16 +40,14 @@ namespace picard {
 namespace {
 
 constexpr int kTcM = 128;          // rows p1 per tile
-constexpr int kTcHalfN = 128;      // columns p2 per face
-constexpr int kTcN = 2 * kTcHalfN; // both faces
-constexpr int kTcKC = 128;         // K (q2) per chunk
 constexpr int kTcThreads = 128;
 constexpr long long kTcSpin = 1LL << 26;
 
 struct TcAxis {
   int axis;        // normal axis
   int n1, n2, nn;  // in-plane extents (p1, p2) and normal extent
-  int n2pad;       // n2 rounded up to kTcKC
+  int n2pad;       // n2 rounded up to the K chunk
+  int N;           // columns p2 per face of a tile, also the K chunk: 64, 96 or 128
   int mtiles, ntiles, splits;
 };
 
@@ -142,22 +142,32 @@ __device__ inline long long d_index(const KParams& P, const TcAxis& X, int f, in
 // partial (sum - compensation) once at the end.
 constexpr int kDB = 64;             // shifts served by one T buffer
 constexpr int kRT = 193;            // T rows (>= kDB + 127; odd multiple of 16 B keeps cp.async conflict-free)
-constexpr int kKB = kTcKC / 8;      // K blocks per chunk
-constexpr int kZN = 128 + kTcKC - 8;  // Z entries per split: n' + 8 floor(k/8) <= 127 + kTcKC - 8
-constexpr int kWUsed = kZN + 7;     // window values used (255)
-constexpr int kWL = kWUsed + 1;
-constexpr size_t kTSplit = (size_t)kKB * kRT * 16;   // bytes of one split of T
-constexpr size_t kZS = (size_t)kZN * 16;             // bytes of one split of Z
-constexpr size_t kSmemT = 3 * kTSplit;
-constexpr size_t kSmemZ = 2 * 3 * kZS;               // [buf][split]
-constexpr size_t kSmemW = (size_t)3 * kWL * 2;       // [split][kWL] bf16
-constexpr size_t kTcSmem = kSmemT + kSmemZ + kSmemW;
+// Tile shape for N columns p2 per face and K chunks of N q2 values (N = 64,
+// 96, 128: narrow faces pad less).
+template <int N>
+struct TcShape {
+  static constexpr int kHalfN = N;                  // columns p2 per face
+  static constexpr int kFullN = 2 * N;              // both faces (partial row)
+  static constexpr int kKC = N;                     // K (q2) per chunk
+  static constexpr int kKB = kKC / 8;               // K blocks per chunk
+  static constexpr int kZN = N + kKC - 8;           // Z entries per split: n' + 8 floor(k/8) <= N - 1 + kKC - 8
+  static constexpr int kWUsed = kZN + 7;            // window values used
+  static constexpr int kWL = kWUsed + 1;
+  static constexpr size_t kTSplit = (size_t)kKB * kRT * 16;  // bytes of one split of T
+  static constexpr size_t kZS = (size_t)kZN * 16;            // bytes of one split of Z
+  static constexpr size_t kSmemT = 3 * kTSplit;
+  static constexpr size_t kSmemZ = 2 * 3 * kZS;              // [buf][split]
+  static constexpr size_t kSmemW = (size_t)3 * kWL * 2;      // [split][kWL] bf16
+  static constexpr size_t kSmem = kSmemT + kSmemZ + kSmemW;
+  // kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
+  // K-major, M = 128, N.
+  static constexpr uint32_t kIdesc =
+      (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+  static_assert(N % 16 == 0 && N >= 64 && N <= 128, "MMA shape with M = 128");
+  static_assert(kWUsed <= 2 * 128, "window within the prefetch of 128 threads x 2");
+};
 constexpr uint32_t kColAcc = 0, kColSum = 256, kColComp = 384;
-// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
-// K-major, M = 128, N = 128.
-constexpr uint32_t kIdescFace = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcHalfN >> 3) << 17) |
-                                ((uint32_t)(kTcM >> 4) << 24);
-constexpr int kPrefetch = 2;  // D values per thread per step (255 <= 2 * 128)
+constexpr int kPrefetch = 2;  // D values per thread per step (the window <= 2 * 128)
 
 __device__ inline void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
   asm volatile(
@@ -175,9 +185,15 @@ __device__ inline void tmem_st16(uint32_t addr, const uint32_t (&r)[16]) {
       : "memory");
 }
 
+template <int N>
 __global__ void __launch_bounds__(kTcThreads, 1)
     bcpot_tc_kernel(KParams P, TcAxis X, const __nv_bfloat16* __restrict__ Cs, const double* __restrict__ D,
                     double* partial, int* err) {
+  using Sh = TcShape<N>;
+  constexpr int kTcHalfN = Sh::kHalfN, kTcN = Sh::kFullN, kTcKC = Sh::kKC, kKB = Sh::kKB, kZN = Sh::kZN,
+                kWUsed = Sh::kWUsed, kWL = Sh::kWL;
+  constexpr size_t kTSplit = Sh::kTSplit, kZS = Sh::kZS, kSmemT = Sh::kSmemT, kSmemZ = Sh::kSmemZ;
+  constexpr uint32_t kIdescFace = Sh::kIdesc;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* sT = smem;                   // [3][kKB][kRT][16 B]
   unsigned char* sZ = smem + kSmemT;          // [2][3][kZN][16 B]
@@ -422,6 +438,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // U on both faces of the axis = (sum over splits of the partial tiles) / (4 pi eps0).
 __global__ void bcpot_reduce_kernel(KParams P, TcAxis X, const double* partial, double* U) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int kTcHalfN = X.N, kTcN = 2 * X.N;
   long long total = (long long)X.mtiles * X.ntiles * kTcM * kTcN;
   if (t >= total) return;
   int col = int(t % kTcN);
@@ -449,9 +466,10 @@ TcAxis tc_axis(const KParams& P, int axis, int sms) {
   if (axis == 0) X.n1 = P.ny, X.n2 = P.nz, X.nn = P.nx;
   else if (axis == 1) X.n1 = P.nx, X.n2 = P.nz, X.nn = P.ny;
   else X.n1 = P.nx, X.n2 = P.ny, X.nn = P.nz;
-  X.n2pad = (X.n2 + kTcKC - 1) / kTcKC * kTcKC;
+  X.N = X.n2 <= 64 ? 64 : (X.n2 <= 96 ? 96 : 128);
+  X.n2pad = (X.n2 + X.N - 1) / X.N * X.N;
   X.mtiles = (X.n1 + kTcM - 1) / kTcM;
-  X.ntiles = (X.n2 + kTcHalfN - 1) / kTcHalfN;
+  X.ntiles = (X.n2 + X.N - 1) / X.N;
   int tiles = X.mtiles * X.ntiles * 2;  // one CTA per face of a tile
   X.splits = sms / tiles;
   if (X.splits < 1) X.splits = 1;
@@ -461,8 +479,13 @@ TcAxis tc_axis(const KParams& P, int axis, int sms) {
 }  // namespace
 
 size_t bcpot_tc_smem_bytes(const KParams& P) {
-  (void)P;
-  return kTcSmem;
+  size_t m = 0;
+  for (int axis = 0; axis < 3; ++axis) {
+    const int N = tc_axis(P, axis, 148).N;
+    const size_t b = N == 64 ? TcShape<64>::kSmem : (N == 96 ? TcShape<96>::kSmem : TcShape<128>::kSmem);
+    m = b > m ? b : m;
+  }
+  return m;
 }
 
 void bcpot_tc_scratch(const KParams& P, long long* cs_elems, long long* partial_elems) {
@@ -470,7 +493,7 @@ void bcpot_tc_scratch(const KParams& P, long long* cs_elems, long long* partial_
   for (int axis = 0; axis < 3; ++axis) {
     TcAxis X = tc_axis(P, axis, 148);
     long long c = 3LL * X.nn * X.n1 * X.n2pad;
-    long long p = (long long)X.mtiles * X.ntiles * X.splits * kTcM * kTcN;
+    long long p = (long long)X.mtiles * X.ntiles * X.splits * kTcM * (2LL * X.N);
     cs = c > cs ? c : cs;
     pe = p > pe ? p : pe;
   }
@@ -482,12 +505,17 @@ cudaError_t launch_bc_potentials_tc(const KParams& P, const double* C, const dou
                                     double* partial, int* err, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(U, 0, sizeof(double) * P.nodes, st);
   if (e != cudaSuccess) return e;
-  const size_t smem = bcpot_tc_smem_bytes(P);
-  static size_t attr = 0;
-  if (attr < smem) {
-    e = cudaFuncSetAttribute(bcpot_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static bool attr = false;
+  if (!attr) {
+    e = cudaFuncSetAttribute(bcpot_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcShape<64>::kSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(bcpot_tc_kernel<96>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)TcShape<96>::kSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(bcpot_tc_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)TcShape<128>::kSmem);
     if (e != cudaSuccess) return e;
-    attr = smem;
+    attr = true;
   }
   const int flows[3] = {P.xflow, P.yflow, P.zflow};
   __nv_bfloat16* Cs = static_cast<__nv_bfloat16*>(cs_buf);
@@ -498,8 +526,14 @@ cudaError_t launch_bc_potentials_tc(const KParams& P, const double* C, const dou
     note_launch();
     split_charge_kernel<<<(unsigned)((per + 255) / 256), 256, 0, st>>>(P, X, C, Cs);
     note_launch();
-    bcpot_tc_kernel<<<X.mtiles * X.ntiles * 2 * X.splits, kTcThreads, smem, st>>>(P, X, Cs, D, partial, err);
-    long long outs = (long long)X.mtiles * X.ntiles * kTcM * kTcN;
+    const unsigned grid = (unsigned)(X.mtiles * X.ntiles * 2 * X.splits);
+    if (X.N == 64)
+      bcpot_tc_kernel<64><<<grid, kTcThreads, TcShape<64>::kSmem, st>>>(P, X, Cs, D, partial, err);
+    else if (X.N == 96)
+      bcpot_tc_kernel<96><<<grid, kTcThreads, TcShape<96>::kSmem, st>>>(P, X, Cs, D, partial, err);
+    else
+      bcpot_tc_kernel<128><<<grid, kTcThreads, TcShape<128>::kSmem, st>>>(P, X, Cs, D, partial, err);
+    long long outs = (long long)X.mtiles * X.ntiles * kTcM * (2LL * X.N);
     note_launch();
     bcpot_reduce_kernel<<<(unsigned)((outs + 255) / 256), 256, 0, st>>>(P, X, partial, U);
     e = cudaGetLastError();

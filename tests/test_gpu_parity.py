@@ -127,11 +127,13 @@ def test_bc_potentials_matches_oracle():
     assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-12
 
 
-@pytest.mark.parametrize("dims", [(16, 16, 16), (160, 24, 20), (40, 136, 12)])
+@pytest.mark.parametrize("dims", [(16, 16, 16), (160, 24, 20), (40, 136, 12), (72, 66, 70)])
 def test_bc_potentials_tensor_cores_vs_fp64(dims):
-    # three-way BF16 split, one FP32 MMA accumulation per 128 K-values, the
-    # steps summed with Kahan compensation in tensor memory: the face
-    # potentials agree with the FP64 sum within the north-star 1e-6 relative
+    # three-way BF16 split, one FP32 MMA accumulation per K chunk, the steps
+    # summed with Kahan compensation in tensor memory: the face potentials
+    # agree with the FP64 sum within the north-star 1e-6 relative.  The faces
+    # cover every tile width: <= 64 columns (16^3, 160x24x20, 40x136x12),
+    # 65..96 (72x66x70) and > 96 (the 136-row axis of 40x136x12)
     nx, ny, nz = dims
     p = small_plasma(n=8, ppc=2, seed=23)
     p.nx, p.ny, p.nz = nx, ny, nz
