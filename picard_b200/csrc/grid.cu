@@ -313,18 +313,21 @@ __global__ void __launch_bounds__(256) anchor_kernel(Stencil S, JacobiCoef J, co
   double r2 = 0.0;
   if (i <= S.nx && j <= S.ny) {
     int k1 = min(k0 + zc - 1, S.nz);
+    const int im = (S.px && i == 1) ? S.nx : i - 1, ip = (S.px && i == S.nx) ? 1 : i + 1;
+    const int jm = (S.py && j == 1) ? S.ny : j - 1, jp = (S.py && j == S.ny) ? 1 : j + 1;
     for (int k = k0; k <= k1; ++k) {
-      long long c = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * k);
-      long long xm, xp, ym, yp, zm, zp;
-      neighbours(S, i, j, k, xm, xp, ym, yp, zm, zp);
-      // FP32 index of a node given its FP64 index (same (i, j, k))
-      auto fof = [&](long long g) {
-        long long ii = g % S.nxp, rest = g / S.nxp;
-        return (ii + 3) + (long long)S.fpitch * rest;
+      const int km = (S.pz && k == 1) ? S.nz : k - 1, kp = (S.pz && k == S.nz) ? 1 : k + 1;
+      // U = V + sigma w at node (ii, jj, kk): the FP64 array is (nxp, nyp, ..), the
+      // FP32 one has rows of fpitch with node ii at column ii + 3
+      auto val = [&](int ii, int jj, int kk) {
+        const long long rest = (long long)jj + (long long)S.nyp * kk;
+        const long long g = (long long)ii + (long long)S.nxp * rest;
+        return w_zero ? Vin[g] : Vin[g] + sigma * (double)w[(long long)(ii + 3) + (long long)S.fpitch * rest];
       };
-      auto val = [&](long long g) { return w_zero ? Vin[g] : Vin[g] + sigma * (double)w[fof(g)]; };
-      double u = val(c);
-      double sx = val(xp) + val(xm), sy = val(yp) + val(ym), sz = val(zp) + val(zm);
+      const long long c = (long long)i + (long long)S.nxp * ((long long)j + (long long)S.nyp * k);
+      double u = val(i, j, k);
+      double sx = val(ip, j, k) + val(im, j, k), sy = val(i, jp, k) + val(i, jm, k),
+             sz = val(i, j, kp) + val(i, j, km);
       double bc = b[c];
       double res = bc - ((sx - 2.0 * u) / J.dx2 + (sy - 2.0 * u) / J.dy2 + (sz - 2.0 * u) / J.dz2);
       r2 += res * res;
