@@ -242,10 +242,11 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
   const KParams& K = c->K;
   const int cells = p.nx * p.ny * p.nz;
   bool nc = false;
+  bool advanced = false;  // the previous step's push already advanced the positions
   for (int32_t it = iter_start + 1; it <= iter_end; ++it) {
     PICARD_CUDA(cudaEventRecord(c->pev[0], c->st));
     // AdvancePosition on the particles present before BCinflow
-    PICARD_TRY(picard_gpu_advance_position(c, p.dt));
+    if (!advanced) PICARD_TRY(picard_gpu_advance_position(c, p.dt));
     // ParticlesProduce, appended behind them (device-side count)
     PICARD_CUDA(launch_produce_count(K, it, c->cell_counts, c->st));
     PICARD_CUDA(launch_scan_int(c->cell_counts, c->cell_offsets, cells, c->cell_offsets + cells,
@@ -288,7 +289,13 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
     if (sweeps_total) *sweeps_total += sw;
     PICARD_CUDA(cudaEventRecord(c->pev[4], c->st));
     PICARD_TRY(picard_gpu_calc_efield(c));
-    PICARD_TRY(picard_gpu_advance_velocity(c, p.dt));
+    // AdvanceVelocity; in the CELL32 layout, when another step follows, fused
+    // with that step's AdvancePosition (one pass over the particles)
+    advanced = c->layout == PICARD_LAYOUT_CELL32 && it < iter_end;
+    if (advanced)
+      PICARD_CUDA(launch_push_advance_c32(K, c->c32[c->cur], c->num_local, c->E32, p.dt, c->st));
+    else
+      PICARD_TRY(picard_gpu_advance_velocity(c, p.dt));
     PICARD_CUDA(cudaEventRecord(c->pev[5], c->st));
     PICARD_CUDA(cudaEventSynchronize(c->pev[5]));
     for (int ph = 0; ph < 5; ++ph) {

@@ -66,6 +66,9 @@ cudaError_t launch_cell_indices_f64(const KParams& P, PartF64 a, long long n, in
 
 // ------------------------------------------------------------ CELL32 unit
 cudaError_t launch_advance_position_c32(const KParams& P, PartC32 a, long long n, double dt, cudaStream_t st);
+// AdvanceVelocity (dt) then the next step's AdvancePosition (dt) in one pass; bit-identical to the two launches.
+cudaError_t launch_push_advance_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
+                                    cudaStream_t st);
 cudaError_t launch_transfer_c32(const KParams& P, PartC32 a, long long n, cudaStream_t st);
 cudaError_t launch_compact_outflow_c32(const KParams& P, PartC32 in, PartC32 out, long long n, int* block_counts,
                                        int* block_offsets, int* new_count, int wrap, cudaStream_t st);

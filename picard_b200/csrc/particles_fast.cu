@@ -332,6 +332,31 @@ __global__ void advance_velocity_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, 
   }
 }
 
+// AdvanceVelocity of one step followed by AdvancePosition of the next, in one
+// pass over the particles: the same operations as advance_velocity_c32_kernel
+// (mode 0) then advance_position_c32_kernel, so the same bits, with one read
+// and one write of each particle instead of two.
+__global__ void push_advance_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, long long n, const float4* E,
+                                        float dtdx, float dtdy, float dtdz) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    C32 c = load_pos(a, p);
+    float Ep[3];
+    gather_c32(P, c, E, Ep);
+    float v[3] = {a.vx[p], a.vy[p], a.vz[p]};
+    boris_c32(P, S, a.sp[p], 0, Ep, v);
+    a.vx[p] = v[0];
+    a.vy[p] = v[1];
+    a.vz[p] = v[2];
+    move_axis(c.i, c.f[0], v[0] * dtdx, P.nx, P.xflow);
+    move_axis(c.j, c.f[1], v[1] * dtdy, P.ny, P.yflow);
+    move_axis(c.k, c.f[2], v[2] * dtdz, P.nz, P.zflow);
+    a.cell[p] = pack_cell(c.i, c.j, c.k);
+    a.fx[p] = c.f[0];
+    a.fy[p] = c.f[1];
+    a.fz[p] = c.f[2];
+  }
+}
+
 __device__ inline int fold_index(int i, int n, int open) {
   if (open) return i < 1 ? 1 : (i > n ? n : i);
   while (i < 1) i += n;
@@ -636,6 +661,16 @@ cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n
   SpeciesF32 S = species_f32(P, dt, deltat, mode);
   note_launch();
   advance_velocity_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, S, a, n, E, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_push_advance_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
+                                    cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  SpeciesF32 S = species_f32(P, dt, 0.0, 0);
+  note_launch();
+  push_advance_c32_kernel<<<persistent_grid(n), kThreads, 0, st>>>(P, S, a, n, E, float(dt / P.dx), float(dt / P.dy),
+                                                                   float(dt / P.dz));
   return cudaGetLastError();
 }
 
