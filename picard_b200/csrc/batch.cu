@@ -426,34 +426,21 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
         PICARD_CUDA(launch_scan_int(c->cell_counts, c->cell_offsets, cells, c->cell_offsets + cells,
                                     c->cell_offsets + cells + 2, c->st));
         if (c->layout == PICARD_LAYOUT_F64)
-          PICARD_CUDA(launch_produce_emit_f64(K, it, c->cell_offsets, c->f64[c->cur], c->d_count + c->cur,
+          PICARD_CUDA(launch_produce_emit_f64(K, it, c->cell_offsets, c->f64, c->d_count,
                                               c->capacity, c->d_err, c->st));
         else
-          PICARD_CUDA(launch_produce_emit_c32(K, it, c->cell_offsets, c->c32[c->cur], c->d_count + c->cur,
+          PICARD_CUDA(launch_produce_emit_c32(K, it, c->cell_offsets, c->c32, c->d_count,
                                               c->capacity, c->d_err, c->st));
         PICARD_TRY(count_issue(c));
       }
       for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));
       lap(0);
-      // ---- BCoutflow + ParticlesTransfer (compaction), BCinflow (fused)
+      // ---- BCoutflow + ParticlesTransfer (in place), BCinflow (fused)
       for (int r = 0; r < n; ++r) {
         picard_ctx* c = ctxs[r];
-        const KParams& K = c->K;
         const int32_t it = it0[r] + step;
-        const int nxt = 1 - c->cur;
-        if (c->layout == PICARD_LAYOUT_F64)
-          PICARD_CUDA(launch_compact_outflow_f64(K, c->f64[c->cur], c->f64[nxt], c->num_local, c->blk_counts,
-                                                 c->blk_offsets, c->d_count + nxt, 1, c->st));
-        else
-          PICARD_CUDA(launch_compact_outflow_c32(K, c->c32[c->cur], c->c32[nxt], c->num_local, c->blk_counts,
-                                                 c->blk_offsets, c->d_count + nxt, 1, c->st));
-        c->cur = nxt;
-        if (c->layout == PICARD_LAYOUT_F64)
-          PICARD_CUDA(launch_inflow_fused_f64(K, c->inflow, it, c->f64[c->cur], c->d_count + c->cur, c->capacity,
-                                              c->d_err, c->st));
-        else
-          PICARD_CUDA(launch_inflow_fused_c32(K, c->inflow, it, c->c32[c->cur], c->d_count + c->cur, c->capacity,
-                                              c->d_err, c->st));
+        PICARD_CUDA(launch_outflow(c, 1));
+        PICARD_CUDA(launch_inflow_fused(c, it));
         PICARD_TRY(count_issue(c));
       }
       for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));

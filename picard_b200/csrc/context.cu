@@ -172,7 +172,7 @@ namespace {
 
 struct Sizes {
   long long cap, nodes, cells, dsize;
-  int species, nb_compact, nb_jacobi;
+  int species, nb_compact, nb_jacobi, nb_inflow;
 };
 
 Sizes sizes_of(const picard_params& p) {
@@ -183,6 +183,8 @@ Sizes sizes_of(const picard_params& p) {
   s.dsize = (long long)(2 * p.nx + 1) * (2 * p.ny + 1) * (2 * p.nz + 1);
   s.species = p.species;
   s.nb_compact = compact_blocks(s.cap) + 1;
+  const InflowTable T = make_inflow_table(p);
+  s.nb_inflow = T.cells * T.per_cell > 0 ? inflow_blocks(T.cells * T.per_cell) : 0;
   KParams K = make_kparams(p);
   s.nb_jacobi = jacobi_geom(K).nblocks;
   return s;
@@ -204,7 +206,7 @@ int validate(const picard_params* p, int layout, int solver) {
 }
 
 int sync_count(picard_ctx* c) {
-  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i, c->d_count + c->cur, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i, c->d_count, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
   c->stats.d2h_bytes += sizeof(int);
   c->num_local = c->h_pinned_i[0];
@@ -213,7 +215,7 @@ int sync_count(picard_ctx* c) {
 
 int push_count(picard_ctx* c) {
   c->h_pinned_i[1] = int(c->num_local);
-  PICARD_CUDA(cudaMemcpyAsync(c->d_count + c->cur, c->h_pinned_i + 1, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  PICARD_CUDA(cudaMemcpyAsync(c->d_count, c->h_pinned_i + 1, sizeof(int), cudaMemcpyHostToDevice, c->st));
   PICARD_CUDA(cudaStreamSynchronize(c->st));
   c->stats.h2d_bytes += sizeof(int);
   return PICARD_OK;
@@ -280,9 +282,25 @@ int bc_potentials_async(picard_ctx* c) {
   return PICARD_OK;
 }
 
+cudaError_t launch_outflow(picard_ctx* c, int wrap) {
+  if (c->layout == PICARD_LAYOUT_F64)
+    return launch_outflow_f64(c->K, c->f64, c->num_local, c->out_words, c->blk_counts, c->blk_offsets, c->d_count,
+                              wrap, c->d_err, c->st);
+  return launch_outflow_c32(c->K, c->c32, c->num_local, c->out_words, c->blk_counts, c->blk_offsets, c->d_count, wrap,
+                            c->d_err, c->st);
+}
+
+cudaError_t launch_inflow_fused(picard_ctx* c, int iteration) {
+  if (c->layout == PICARD_LAYOUT_F64)
+    return launch_inflow_fused_f64(c->K, c->inflow, iteration, c->f64, c->d_count, c->capacity, c->inflow_counts,
+                                   c->inflow_offsets, c->d_err, c->st);
+  return launch_inflow_fused_c32(c->K, c->inflow, iteration, c->c32, c->d_count, c->capacity, c->inflow_counts,
+                                 c->inflow_offsets, c->d_err, c->st);
+}
+
 int count_issue(picard_ctx* c) {
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 2, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i, c->d_count + c->cur, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i, c->d_count, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   c->stats.d2h_bytes += 2 * sizeof(int);
   return PICARD_OK;
 }
@@ -313,14 +331,15 @@ int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver,
   if (!bytes) return fail(PICARD_ERR_BAD_ARG, "bytes is NULL");
   Sizes s = sizes_of(*p);
   double per_particle = layout == PICARD_LAYOUT_F64 ? 49.0 : 29.0;
-  double b = 2.0 * per_particle * (double)s.cap;
+  double b = per_particle * (double)s.cap;
   b += (double)s.nodes * (8.0 * s.species /*Nacc*/ + 8.0 * s.species /*N*/ + 8 * 3 /*C,U,b*/ + 24 /*E*/ + 8 /*U1*/);
   if (layout == PICARD_LAYOUT_CELL32) b += 16.0 * s.nodes;
   if (solver == PICARD_SOLVER_F64) b += 8.0 * s.nodes;
   else b += 16.0 * (double)f32_elems(make_kparams(*p));
   b += 8.0 * (double)s.dsize;
   b += 8.0 * (double)s.cells;                // produce counts + offsets
-  b += 8.0 * (double)s.nb_compact * 3;       // compaction scratch
+  b += 8.0 * (double)s.nb_compact * (3 + kOutflowWordsPerBlock);  // BCoutflow scratch
+  b += 8.0 * (double)s.nb_inflow * 2;        // fused BCinflow scan
   b += 8.0 * 1025.0 * s.nb_jacobi;           // sweep partials
   if (layout == PICARD_LAYOUT_CELL32) {      // tensor-core BCpotentials scratch
     long long cs = 0, pe = 0;
@@ -352,23 +371,22 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
   if ((rc = check_cuda(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking), "cudaStreamCreate"))) return bail(rc);
   Sizes s = sizes_of(*p);
   const long long cap = s.cap;
-  for (int b = 0; b < 2; ++b) {
-    if (layout == PICARD_LAYOUT_F64) {
-      PartF64& a = c->f64[b];
-      if ((rc = dalloc(c, a.x, cap)) || (rc = dalloc(c, a.y, cap)) || (rc = dalloc(c, a.z, cap)) ||
-          (rc = dalloc(c, a.vx, cap)) || (rc = dalloc(c, a.vy, cap)) || (rc = dalloc(c, a.vz, cap)) ||
-          (rc = dalloc(c, a.sp, cap)))
-        return bail(rc);
-    } else {
-      PartC32& a = c->c32[b];
-      if ((rc = dalloc(c, a.cell, cap)) || (rc = dalloc(c, a.fx, cap)) || (rc = dalloc(c, a.fy, cap)) ||
-          (rc = dalloc(c, a.fz, cap)) || (rc = dalloc(c, a.vx, cap)) || (rc = dalloc(c, a.vy, cap)) ||
-          (rc = dalloc(c, a.vz, cap)) || (rc = dalloc(c, a.sp, cap)))
-        return bail(rc);
-    }
+  // one particle buffer: BCoutflow removes in place
+  if (layout == PICARD_LAYOUT_F64) {
+    PartF64& a = c->f64;
+    if ((rc = dalloc(c, a.x, cap)) || (rc = dalloc(c, a.y, cap)) || (rc = dalloc(c, a.z, cap)) ||
+        (rc = dalloc(c, a.vx, cap)) || (rc = dalloc(c, a.vy, cap)) || (rc = dalloc(c, a.vz, cap)) ||
+        (rc = dalloc(c, a.sp, cap)))
+      return bail(rc);
+  } else {
+    PartC32& a = c->c32;
+    if ((rc = dalloc(c, a.cell, cap)) || (rc = dalloc(c, a.fx, cap)) || (rc = dalloc(c, a.fy, cap)) ||
+        (rc = dalloc(c, a.fz, cap)) || (rc = dalloc(c, a.vx, cap)) || (rc = dalloc(c, a.vy, cap)) ||
+        (rc = dalloc(c, a.vz, cap)) || (rc = dalloc(c, a.sp, cap)))
+      return bail(rc);
   }
   const long long nn = s.nodes;
-  if ((rc = dalloc(c, c->d_count, 2)) || (rc = dalloc(c, c->d_err, 1)) ||
+  if ((rc = dalloc(c, c->d_count, 1)) || (rc = dalloc(c, c->d_err, 1)) ||
       (rc = dalloc(c, c->Nacc, nn * s.species)) || (rc = dalloc(c, c->N, nn * s.species)) ||
       (rc = dalloc(c, c->C, nn)) || (rc = dalloc(c, c->U, nn)) || (rc = dalloc(c, c->E, 3 * nn)) ||
       (rc = dalloc(c, c->D, s.dsize)) || (rc = dalloc(c, c->b, nn)) || (rc = dalloc(c, c->U1, nn)))
@@ -403,7 +421,12 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
     return bail(rc);
   int scan_extra = scan_scratch_ints(s.nb_compact) + 4;
   if ((rc = dalloc(c, c->blk_counts, s.nb_compact)) ||
-      (rc = dalloc(c, c->blk_offsets, 2 * (size_t)s.nb_compact + 2 + scan_extra)))
+      (rc = dalloc(c, c->blk_offsets, 2 * (size_t)s.nb_compact + 2 + scan_extra)) ||
+      (rc = dalloc(c, c->out_words, (size_t)kOutflowWordsPerBlock * s.nb_compact)))
+    return bail(rc);
+  if (s.nb_inflow > 0 &&
+      ((rc = dalloc(c, c->inflow_counts, s.nb_inflow)) ||
+       (rc = dalloc(c, c->inflow_offsets, (size_t)s.nb_inflow + 2 + scan_scratch_ints(s.nb_inflow) + 4))))
     return bail(rc);
   int cells = int(s.cells);
   if ((rc = dalloc(c, c->cell_counts, cells)) ||
@@ -489,7 +512,7 @@ int picard_gpu_set_particles(picard_ctx* c, const double* rp, const int32_t* ip,
   PartF64 dst;
   std::vector<void*> tmp;
   if (c->layout == PICARD_LAYOUT_F64) {
-    dst = c->f64[c->cur];
+    dst = c->f64;
   } else {
     double* buf = nullptr;
     int8_t* sb = nullptr;
@@ -508,7 +531,7 @@ int picard_gpu_set_particles(picard_ctx* c, const double* rp, const int32_t* ip,
   for (int q = 0; q < 6; ++q)
     PICARD_CUDA(cudaMemcpyAsync(cols[q], soa.data() + (size_t)q * n, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
   PICARD_CUDA(cudaMemcpyAsync(dst.sp, sp.data(), n, cudaMemcpyHostToDevice, c->st));
-  if (c->layout == PICARD_LAYOUT_CELL32) PICARD_CUDA(launch_f64_to_c32(c->K, dst, n, c->c32[c->cur], c->st));
+  if (c->layout == PICARD_LAYOUT_CELL32) PICARD_CUDA(launch_f64_to_c32(c->K, dst, n, c->c32, c->st));
   for (void* q : tmp) cudaFreeAsync(q, c->st);
   PICARD_CUDA(cudaStreamSynchronize(c->st));
   c->stats.h2d_bytes += (int64_t)n * 49;
@@ -525,7 +548,7 @@ int picard_gpu_get_particles(picard_ctx* c, double* rp, int32_t* ip, int32_t cap
   PartF64 src;
   std::vector<void*> tmp;
   if (c->layout == PICARD_LAYOUT_F64) {
-    src = c->f64[c->cur];
+    src = c->f64;
   } else {
     double* buf = nullptr;
     int8_t* sb = nullptr;
@@ -539,7 +562,7 @@ int picard_gpu_get_particles(picard_ctx* c, double* rp, int32_t* ip, int32_t cap
     src.vy = buf + 4 * n;
     src.vz = buf + 5 * n;
     src.sp = sb;
-    PICARD_CUDA(launch_c32_to_f64(c->K, c->c32[c->cur], n, src, c->st));
+    PICARD_CUDA(launch_c32_to_f64(c->K, c->c32, n, src, c->st));
   }
   std::vector<double> soa((size_t)6 * n);
   std::vector<int8_t> sp(n);
@@ -645,9 +668,9 @@ int picard_gpu_particles_initialize(picard_ctx* c) {
   long long total = (long long)c->prm.nx * c->prm.ny * c->prm.nz * per_cell;
   PICARD_TRY(ensure_capacity(c, total));
   if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_init_f64(c->K, c->f64[c->cur], c->num_local, c->st));
+    PICARD_CUDA(launch_init_f64(c->K, c->f64, c->num_local, c->st));
   else
-    PICARD_CUDA(launch_init_c32(c->K, c->c32[c->cur], c->num_local, c->st));
+    PICARD_CUDA(launch_init_c32(c->K, c->c32, c->num_local, c->st));
   c->num_local += total;
   return push_count(c);
 }
@@ -658,9 +681,9 @@ int picard_gpu_bc_inflow(picard_ctx* c, int32_t iteration) {
   long long total = c->inflow.cells * c->inflow.per_cell;
   PICARD_TRY(ensure_capacity(c, total));
   if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_inflow_f64(c->K, c->inflow, iteration, c->f64[c->cur], c->num_local, c->st));
+    PICARD_CUDA(launch_inflow_f64(c->K, c->inflow, iteration, c->f64, c->num_local, c->st));
   else
-    PICARD_CUDA(launch_inflow_c32(c->K, c->inflow, iteration, c->c32[c->cur], c->num_local, c->st));
+    PICARD_CUDA(launch_inflow_c32(c->K, c->inflow, iteration, c->c32, c->num_local, c->st));
   c->num_local += total;
   return push_count(c);
 }
@@ -669,9 +692,9 @@ int picard_gpu_bc_inflow(picard_ctx* c, int32_t iteration) {
 int picard_gpu_advance_position(picard_ctx* c, double dt) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
   if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_advance_position_f64(c->K, c->f64[c->cur], c->num_local, dt, c->st));
+    PICARD_CUDA(launch_advance_position_f64(c->K, c->f64, c->num_local, dt, c->st));
   else
-    PICARD_CUDA(launch_advance_position_c32(c->K, c->c32[c->cur], c->num_local, dt, c->st));
+    PICARD_CUDA(launch_advance_position_c32(c->K, c->c32, c->num_local, dt, c->st));
   return PICARD_OK;
 }
 
@@ -689,26 +712,20 @@ int picard_gpu_particles_produce(picard_ctx* c, int32_t iteration) {
   if (add == 0) return PICARD_OK;
   PICARD_TRY(ensure_capacity(c, add));
   if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_produce_emit_f64(c->K, iteration, c->cell_offsets, c->f64[c->cur], c->d_count + c->cur,
+    PICARD_CUDA(launch_produce_emit_f64(c->K, iteration, c->cell_offsets, c->f64, c->d_count,
                                         c->capacity, c->d_err, c->st));
   else
-    PICARD_CUDA(launch_produce_emit_c32(c->K, iteration, c->cell_offsets, c->c32[c->cur], c->d_count + c->cur,
+    PICARD_CUDA(launch_produce_emit_c32(c->K, iteration, c->cell_offsets, c->c32, c->d_count,
                                         c->capacity, c->d_err, c->st));
   PICARD_TRY(check_dev_err(c));
   return sync_count(c);
 }
 
-// BCoutflow.f90:5-87 (order-preserving compaction instead of swap-with-last)
+// BCoutflow.f90:5-87, in place and in the reference's order (outflow.cuh)
 int picard_gpu_bc_outflow(picard_ctx* c) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
-  int nxt = 1 - c->cur;
-  if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_compact_outflow_f64(c->K, c->f64[c->cur], c->f64[nxt], c->num_local, c->blk_counts,
-                                           c->blk_offsets, c->d_count + nxt, 0, c->st));
-  else
-    PICARD_CUDA(launch_compact_outflow_c32(c->K, c->c32[c->cur], c->c32[nxt], c->num_local, c->blk_counts,
-                                           c->blk_offsets, c->d_count + nxt, 0, c->st));
-  c->cur = nxt;
+  PICARD_CUDA(launch_outflow(c, 0));
+  PICARD_TRY(check_dev_err(c));
   return sync_count(c);
 }
 
@@ -716,9 +733,9 @@ int picard_gpu_bc_outflow(picard_ctx* c) {
 int picard_gpu_particles_transfer(picard_ctx* c) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
   if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_transfer_f64(c->K, c->f64[c->cur], c->num_local, c->st));
+    PICARD_CUDA(launch_transfer_f64(c->K, c->f64, c->num_local, c->st));
   else
-    PICARD_CUDA(launch_transfer_c32(c->K, c->c32[c->cur], c->num_local, c->st));
+    PICARD_CUDA(launch_transfer_c32(c->K, c->c32, c->num_local, c->st));
   return PICARD_OK;
 }
 
@@ -734,9 +751,9 @@ static int deposit(picard_ctx* c, bool with_flux) {
     PICARD_CUDA(cudaMemsetAsync(Facc, 0, sizeof(unsigned long long) * nn * S * 3, c->st));
   }
   if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_deposit_f64(c->K, c->f64[c->cur], c->num_local, c->Nacc, Facc, c->st));
+    PICARD_CUDA(launch_deposit_f64(c->K, c->f64, c->num_local, c->Nacc, Facc, c->st));
   else
-    PICARD_CUDA(launch_deposit_c32(c->K, c->c32[c->cur], c->num_local, c->Nacc, Facc, c->st));
+    PICARD_CUDA(launch_deposit_c32(c->K, c->c32, c->num_local, c->Nacc, Facc, c->st));
   PICARD_CUDA(launch_finish_deposit(c->K, c->Nacc, c->N, c->C, c->st));
   if (with_flux) PICARD_CUDA(launch_finish_flux(c->K, Facc, c->F, c->st));
   return PICARD_OK;
@@ -837,9 +854,9 @@ static int advance_velocity(picard_ctx* c, double dt, double deltat, int mode) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
   if (!(dt != 0.0)) return fail(PICARD_ERR_BAD_ARG, "dt must be nonzero");
   if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_advance_velocity_f64(c->K, c->f64[c->cur], c->num_local, c->E, dt, deltat, mode, c->st));
+    PICARD_CUDA(launch_advance_velocity_f64(c->K, c->f64, c->num_local, c->E, dt, deltat, mode, c->st));
   else
-    PICARD_CUDA(launch_advance_velocity_c32(c->K, c->c32[c->cur], c->num_local, c->E32, dt, deltat, mode, c->st));
+    PICARD_CUDA(launch_advance_velocity_c32(c->K, c->c32, c->num_local, c->E32, dt, deltat, mode, c->st));
   return PICARD_OK;
 }
 
@@ -859,9 +876,9 @@ int picard_gpu_energy(picard_ctx* c, double out[3], int32_t* num) {
   if (!c || !out) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
   ReduceBuf rb{c->red_partial, c->red_result, c->red_blocks};
   if (c->layout == PICARD_LAYOUT_F64)
-    PICARD_CUDA(launch_energy_particles_f64(c->K, c->f64[c->cur], c->num_local, rb, c->st));
+    PICARD_CUDA(launch_energy_particles_f64(c->K, c->f64, c->num_local, rb, c->st));
   else
-    PICARD_CUDA(launch_energy_particles_c32(c->K, c->c32[c->cur], c->num_local, rb, c->st));
+    PICARD_CUDA(launch_energy_particles_c32(c->K, c->c32, c->num_local, rb, c->st));
   ReduceBuf rf{c->red_partial, c->red_result + 1, c->red_blocks};
   PICARD_CUDA(launch_energy_field(c->K, c->E, rf.partial, rf.result, c->st));
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, c->red_result, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));

@@ -17,12 +17,11 @@ struct picard_ctx {
   long long capacity = 0;
 
   // particles: two buffers of each layout's arrays (compaction ping-pong)
-  picard::PartF64 f64[2] = {};
-  picard::PartC32 c32[2] = {};
-  int cur = 0;
-  int* d_count = nullptr;  // [2] live counts of the two buffers
+  picard::PartF64 f64 = {};  // the particles (one layout allocated)
+  picard::PartC32 c32 = {};
+  int* d_count = nullptr;    // live particle count
   int* d_err = nullptr;
-  long long num_local = 0;  // host mirror of d_count[cur]
+  long long num_local = 0;   // host mirror of *d_count
 
   // node arrays (plane-major, see common.cuh)
   unsigned long long* Nacc = nullptr;  // [species][nodes] fixed point
@@ -53,8 +52,11 @@ struct picard_ctx {
   long long last_sweeps = 0;
 
   // scratch
-  int* blk_counts = nullptr;
+  int* blk_counts = nullptr;     // BCoutflow block counts and offsets
   int* blk_offsets = nullptr;
+  uint2* out_words = nullptr;    // BCoutflow keep words (outflow.cuh)
+  int* inflow_counts = nullptr;  // fused BCinflow block counts and offsets
+  int* inflow_offsets = nullptr;
   int* cell_counts = nullptr;
   int* cell_offsets = nullptr;
   double* red_partial = nullptr;
@@ -72,12 +74,6 @@ struct picard_ctx {
   int bcpot_tensor = 0;
   void* tc_cs = nullptr;
   double* tc_partial = nullptr;
-
-  // fused-path scratch
-  int* tile_state = nullptr;
-  int* tile_ticket = nullptr;
-  double* up_partial = nullptr;
-  long long tile_cap = 0;
 
   picard::InflowTable inflow;
   std::vector<void*> allocs;
@@ -107,6 +103,13 @@ int bc_potentials_async(picard_ctx* c);
 // wait that gave up, recorded in the context's error word.
 int check_dev_err_public(picard_ctx* c);
 int count_collect(picard_ctx* c);
+// BCoutflow in place on the context's particles (wrap != 0: with the
+// ParticlesTransfer periodic wrap); *d_count receives the survivors.  Does not
+// synchronise.
+cudaError_t launch_outflow(picard_ctx* c, int wrap);
+// The fused BCinflow of `iteration`, appended at *d_count in candidate order.
+// Does not synchronise.
+cudaError_t launch_inflow_fused(picard_ctx* c, int iteration);
 // Device memory owned by the context (zeroed, freed with it).
 int dev_alloc(picard_ctx* c, void** p, size_t bytes);
 // Times the launch shapes of the TMA sweep on this context's buffers and keeps

@@ -252,28 +252,16 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
     PICARD_CUDA(launch_scan_int(c->cell_counts, c->cell_offsets, cells, c->cell_offsets + cells,
                                 c->cell_offsets + cells + 2, c->st));
     if (c->layout == PICARD_LAYOUT_F64)
-      PICARD_CUDA(launch_produce_emit_f64(K, it, c->cell_offsets, c->f64[c->cur], c->d_count + c->cur, c->capacity,
+      PICARD_CUDA(launch_produce_emit_f64(K, it, c->cell_offsets, c->f64, c->d_count, c->capacity,
                                           c->d_err, c->st));
     else
-      PICARD_CUDA(launch_produce_emit_c32(K, it, c->cell_offsets, c->c32[c->cur], c->d_count + c->cur, c->capacity,
+      PICARD_CUDA(launch_produce_emit_c32(K, it, c->cell_offsets, c->c32, c->d_count, c->capacity,
                                           c->d_err, c->st));
     PICARD_TRY(sync_count_public(c));
-    // BCoutflow + ParticlesTransfer in one order-preserving compaction
-    int nxt = 1 - c->cur;
-    if (c->layout == PICARD_LAYOUT_F64)
-      PICARD_CUDA(launch_compact_outflow_f64(K, c->f64[c->cur], c->f64[nxt], c->num_local, c->blk_counts,
-                                             c->blk_offsets, c->d_count + nxt, 1, c->st));
-    else
-      PICARD_CUDA(launch_compact_outflow_c32(K, c->c32[c->cur], c->c32[nxt], c->num_local, c->blk_counts,
-                                             c->blk_offsets, c->d_count + nxt, 1, c->st));
-    c->cur = nxt;
+    // BCoutflow + ParticlesTransfer in place, in the reference's order
+    PICARD_CUDA(launch_outflow(c, 1));
     // BCinflow + AdvancePosition + BCoutflow + ParticlesTransfer of the new particles
-    if (c->layout == PICARD_LAYOUT_F64)
-      PICARD_CUDA(launch_inflow_fused_f64(K, c->inflow, it, c->f64[c->cur], c->d_count + c->cur, c->capacity,
-                                          c->d_err, c->st));
-    else
-      PICARD_CUDA(launch_inflow_fused_c32(K, c->inflow, it, c->c32[c->cur], c->d_count + c->cur, c->capacity,
-                                          c->d_err, c->st));
+    PICARD_CUDA(launch_inflow_fused(c, it));
     PICARD_TRY(sync_count_public(c));
     PICARD_CUDA(cudaEventRecord(c->pev[1], c->st));
     PICARD_TRY(picard_gpu_particles_gridify(c));
@@ -293,7 +281,7 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
     // with that step's AdvancePosition (one pass over the particles)
     advanced = c->layout == PICARD_LAYOUT_CELL32 && it < iter_end;
     if (advanced)
-      PICARD_CUDA(launch_push_advance_c32(K, c->c32[c->cur], c->num_local, c->E32, p.dt, c->st));
+      PICARD_CUDA(launch_push_advance_c32(K, c->c32, c->num_local, c->E32, p.dt, c->st));
     else
       PICARD_TRY(picard_gpu_advance_velocity(c, p.dt));
     PICARD_CUDA(cudaEventRecord(c->pev[5], c->st));

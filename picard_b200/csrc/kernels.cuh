@@ -40,11 +40,16 @@ cudaError_t launch_inflow_f64(const KParams& P, const InflowTable& T, int iterat
 cudaError_t launch_inflow_c32(const KParams& P, const InflowTable& T, int iteration, PartC32 out, long long start,
                               cudaStream_t st);
 // Fused inflow (fast path): candidates are generated, advanced by dt and kept
-// only if BCoutflow would keep them; survivors are appended at *count.
+// only if BCoutflow would keep them; survivors are appended at *count in
+// candidate order.  block_counts holds inflow_blocks(candidates) ints,
+// block_offsets that many + 2 + scan_scratch_ints(that many).
 cudaError_t launch_inflow_fused_c32(const KParams& P, const InflowTable& T, int iteration, PartC32 out, int* count,
-                                    long long capacity, int* err, cudaStream_t st);
+                                    long long capacity, int* block_counts, int* block_offsets, int* err,
+                                    cudaStream_t st);
 cudaError_t launch_inflow_fused_f64(const KParams& P, const InflowTable& T, int iteration, PartF64 out, int* count,
-                                    long long capacity, int* err, cudaStream_t st);
+                                    long long capacity, int* block_counts, int* block_offsets, int* err,
+                                    cudaStream_t st);
+int inflow_blocks(long long candidates);
 // ParticlesProduce: per-cell counts, then emission at offsets[].
 cudaError_t launch_produce_count(const KParams& P, int iteration, int* counts, cudaStream_t st);
 // Appends at *count (device); offsets[cells] holds the total, added to *count.
@@ -54,9 +59,15 @@ cudaError_t launch_produce_emit_c32(const KParams& P, int iteration, const int* 
                                     long long capacity, int* err, cudaStream_t st);
 cudaError_t launch_advance_position_f64(const KParams& P, PartF64 a, long long n, double dt, cudaStream_t st);
 cudaError_t launch_transfer_f64(const KParams& P, PartF64 a, long long n, cudaStream_t st);
-// wrap != 0 also applies the ParticlesTransfer periodic wrap to survivors.
-cudaError_t launch_compact_outflow_f64(const KParams& P, PartF64 in, PartF64 out, long long n, int* block_counts,
-                                       int* block_offsets, int* new_count, int wrap, cudaStream_t st);
+// Keep words per 2048-particle BCoutflow block (one per 32 particles).
+constexpr int kOutflowWordsPerBlock = 64;
+// BCoutflow in place, leaving the particles in the reference's order
+// (outflow.cuh); *count receives the survivors.  wrap != 0 also applies the
+// ParticlesTransfer periodic wrap to them.  words: 64 compact_blocks(n)
+// entries; block_counts / block_offsets as for launch_scan_int over
+// compact_blocks(n) counts.
+cudaError_t launch_outflow_f64(const KParams& P, PartF64 a, long long n, uint2* words, int* block_counts,
+                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st);
 cudaError_t launch_advance_velocity_f64(const KParams& P, PartF64 a, long long n, const double* E, double dt,
                                         double deltat, int mode, cudaStream_t st);
 cudaError_t launch_deposit_f64(const KParams& P, PartF64 a, long long n, unsigned long long* Nacc,
@@ -70,8 +81,8 @@ cudaError_t launch_advance_position_c32(const KParams& P, PartC32 a, long long n
 cudaError_t launch_push_advance_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
                                     cudaStream_t st);
 cudaError_t launch_transfer_c32(const KParams& P, PartC32 a, long long n, cudaStream_t st);
-cudaError_t launch_compact_outflow_c32(const KParams& P, PartC32 in, PartC32 out, long long n, int* block_counts,
-                                       int* block_offsets, int* new_count, int wrap, cudaStream_t st);
+cudaError_t launch_outflow_c32(const KParams& P, PartC32 a, long long n, uint2* words, int* block_counts,
+                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st);
 cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
                                         double deltat, int mode, cudaStream_t st);
 cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
@@ -79,13 +90,6 @@ cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigne
 cudaError_t launch_energy_particles_c32(const KParams& P, PartC32 a, long long n, ReduceBuf rb, cudaStream_t st);
 cudaError_t launch_c32_to_f64(const KParams& P, PartC32 a, long long n, PartF64 out, cudaStream_t st);
 cudaError_t launch_f64_to_c32(const KParams& P, PartF64 a, long long n, PartC32 out, cudaStream_t st);
-// Fused step kernel: optional Boris push with E (mode >= 0), position
-// advance, outflow and periodic wrap, deterministic order-preserving
-// compaction into `out` starting at out_base.
-cudaError_t launch_push_fused_c32(const KParams& P, PartC32 in, PartC32 out, const int* n_in, int* n_out,
-                                  const float4* E, int push, int* tile_state, int* tile_ticket, long long capacity,
-                                  double* up_partial, int* err, cudaStream_t st);
-
 // ------------------------------------------------------------ scans
 // Exclusive scan of n int32 counts into offsets; *total receives the sum.
 cudaError_t launch_scan_int(const int* in, int* out, int n, int* total, int* scratch, cudaStream_t st);

@@ -12,6 +12,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "outflow.cuh"
 
 namespace picard {
 
@@ -272,45 +273,25 @@ __device__ inline void transfer_wrap(const KParams& P, double& x, double& y, dou
 }
 
 // Fast-path inflow: BCinflow + AdvancePosition + BCoutflow + ParticlesTransfer
-// for the new candidates only.  Survivors are appended with a warp-aggregated
-// atomic (order among survivors is not the reference's; the set is).
-template <class Store>
-__global__ void inflow_fused_kernel(KParams P, InflowTable T, int iteration, long long total, int* count,
-                                    long long capacity, int* err, Store store) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bool keep = false;
-  double x[3], v[3];
-  int sp = 0;
-  if (t < total) {
-    long long g = t / T.per_cell;
-    int local = int(t - g * T.per_cell);
-    int ii, jj, kk;
-    double x0, y0, z0;
-    inflow_cell(P, T, g, ii, jj, kk, x0, y0, z0);
-    uint32_t a = uint32_t(node_index(P, ii - 1, jj - 1, kk - 1));
-    int ss, pp, m;
-    decode_group(P, T.group_prefix, local, ss, pp, m);
-    gen_member(P, kTagInflow, uint32_t(iteration), a, ss, pp, m, x0, y0, z0, x, v, sp);
-    x[0] = x[0] + v[0] * P.dt;
-    x[1] = x[1] + v[1] * P.dt;
-    x[2] = x[2] + v[2] * P.dt;
-    keep = outflow_keep(P, x[0], x[1], x[2]);
-    if (keep) transfer_wrap(P, x[0], x[1], x[2]);
-  }
-  unsigned mask = __ballot_sync(0xffffffffu, keep);
-  if (mask == 0) return;
-  int lane = threadIdx.x & 31;
-  int leader = __ffs(mask) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(count, __popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (keep) {
-    long long slot = base + __popc(mask & ((1u << lane) - 1u));
-    if (slot < capacity)
-      store(slot, x, v, sp);
-    else
-      atomicCAS(err, 0, int(kDevCapacity));
-  }
+// for the new candidates only.  Candidate t is generated, advanced by dt,
+// tested and wrapped; true = it survives.
+__device__ inline bool inflow_candidate(const KParams& P, const InflowTable& T, int iteration, long long t,
+                                        double x[3], double v[3], int& sp) {
+  long long g = t / T.per_cell;
+  int local = int(t - g * T.per_cell);
+  int ii, jj, kk;
+  double x0, y0, z0;
+  inflow_cell(P, T, g, ii, jj, kk, x0, y0, z0);
+  uint32_t a = uint32_t(node_index(P, ii - 1, jj - 1, kk - 1));
+  int ss, pp, m;
+  decode_group(P, T.group_prefix, local, ss, pp, m);
+  gen_member(P, kTagInflow, uint32_t(iteration), a, ss, pp, m, x0, y0, z0, x, v, sp);
+  x[0] = x[0] + v[0] * P.dt;
+  x[1] = x[1] + v[1] * P.dt;
+  x[2] = x[2] + v[2] * P.dt;
+  if (!outflow_keep(P, x[0], x[1], x[2])) return false;
+  transfer_wrap(P, x[0], x[1], x[2]);
+  return true;
 }
 
 // ------------------------------------------------------------- produce
@@ -443,12 +424,7 @@ __global__ void transfer_f64_kernel(KParams P, PartF64 a, long long n) {
   }
 }
 
-// Deterministic, order-preserving compaction in two passes: per-block
-// survivor counts, an exclusive scan of the counts, then a scatter.
-constexpr int kCompactThreads = 256;
-constexpr int kCompactItems = 8;  // particles per thread
-constexpr int kCompactTile = kCompactThreads * kCompactItems;
-
+// Exclusive scan of one int per thread over the block; total = the block's sum.
 __device__ inline int block_exclusive_scan(int v, int* smem_warp, int& total) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int x = v;
@@ -475,47 +451,69 @@ __device__ inline int block_exclusive_scan(int v, int* smem_warp, int& total) {
   return warp_prefix + x - v;
 }
 
-__global__ void outflow_count_f64(KParams P, PartF64 a, long long n, int* block_counts) {
-  __shared__ int warp_sums[32];
-  long long base = (long long)blockIdx.x * kCompactTile + (long long)threadIdx.x * kCompactItems;
-  int c = 0;
-  for (int q = 0; q < kCompactItems; ++q) {
-    long long p = base + q;
-    if (p < n && outflow_keep(P, a.x[p], a.y[p], a.z[p])) ++c;
+// BCoutflow.f90:28-66 and ParticlesTransfer.f90:494-519 on the FP64 layout,
+// for the in-place removal of outflow.cuh.
+struct OutflowF64 {
+  KParams P;
+  PartF64 a;
+  __device__ bool keep_wrap(long long p, int wrap) const {
+    const double x = a.x[p], y = a.y[p], z = a.z[p];
+    if (!outflow_keep(P, x, y, z)) return false;
+    if (wrap) {
+      double wx = x, wy = y, wz = z;
+      transfer_wrap(P, wx, wy, wz);
+      if (wx != x || wy != y || wz != z) {
+        a.x[p] = wx;
+        a.y[p] = wy;
+        a.z[p] = wz;
+      }
+    }
+    return true;
   }
-  int total;
-  block_exclusive_scan(c, warp_sums, total);
-  if (threadIdx.x == 0) block_counts[blockIdx.x] = total;
+  __device__ void move(long long d, long long s) const {
+    a.x[d] = a.x[s];
+    a.y[d] = a.y[s];
+    a.z[d] = a.z[s];
+    a.vx[d] = a.vx[s];
+    a.vy[d] = a.vy[s];
+    a.vz[d] = a.vz[s];
+    a.sp[d] = a.sp[s];
+  }
+};
+
+// The fused inflow in two passes, so that survivors land in candidate order
+// (deterministic): per-block survivor counts, an exclusive scan, then every
+// block regenerates its candidates and stores the survivors at *count + its
+// offset + their rank in the block.
+__global__ void __launch_bounds__(kThreads) inflow_count_kernel(KParams P, InflowTable T, int iteration,
+                                                                long long total, int* block_counts) {
+  __shared__ int warp_sums[32];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double x[3], v[3];
+  int sp = 0;
+  const bool keep = t < total && inflow_candidate(P, T, iteration, t, x, v, sp);
+  int sum;
+  block_exclusive_scan(keep ? 1 : 0, warp_sums, sum);
+  if (threadIdx.x == 0) block_counts[blockIdx.x] = sum;
 }
 
-__global__ void outflow_scatter_f64(KParams P, PartF64 a, PartF64 o, long long n, const int* block_offsets, int wrap) {
+template <class Store>
+__global__ void __launch_bounds__(kThreads) inflow_emit_kernel(KParams P, InflowTable T, int iteration,
+                                                               long long total, const int* offsets, const int* count,
+                                                               long long capacity, int* err, Store store) {
   __shared__ int warp_sums[32];
-  long long base = (long long)blockIdx.x * kCompactTile + (long long)threadIdx.x * kCompactItems;
-  unsigned keepbits = 0;
-  int c = 0;
-  for (int q = 0; q < kCompactItems; ++q) {
-    long long p = base + q;
-    if (p < n && outflow_keep(P, a.x[p], a.y[p], a.z[p])) {
-      keepbits |= 1u << q;
-      ++c;
-    }
-  }
-  int total;
-  int off = block_exclusive_scan(c, warp_sums, total) + block_offsets[blockIdx.x];
-  for (int q = 0; q < kCompactItems; ++q) {
-    if (keepbits & (1u << q)) {
-      long long p = base + q;
-      double x = a.x[p], y = a.y[p], z = a.z[p];
-      if (wrap) transfer_wrap(P, x, y, z);
-      o.x[off] = x;
-      o.y[off] = y;
-      o.z[off] = z;
-      o.vx[off] = a.vx[p];
-      o.vy[off] = a.vy[p];
-      o.vz[off] = a.vz[p];
-      o.sp[off] = a.sp[p];
-      ++off;
-    }
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double x[3], v[3];
+  int sp = 0;
+  const bool keep = t < total && inflow_candidate(P, T, iteration, t, x, v, sp);
+  int sum;
+  const int rank = block_exclusive_scan(keep ? 1 : 0, warp_sums, sum);
+  if (keep) {
+    const long long slot = (long long)*count + offsets[blockIdx.x] + rank;
+    if (slot < capacity)
+      store(slot, x, v, sp);
+    else
+      atomicCAS(err, 0, int(kDevCapacity));
   }
 }
 
@@ -825,7 +823,9 @@ __global__ void f64_to_c32_kernel(KParams P, PartF64 a, long long n, PartC32 o) 
 
 }  // namespace
 
-int compact_blocks(long long n) { return int((n + kCompactTile - 1) / kCompactTile); }
+int compact_blocks(long long n) { return int((n + kOutflowTile - 1) / kOutflowTile); }
+
+int inflow_blocks(long long candidates) { return grid_for(candidates); }
 
 cudaError_t launch_calc_distance(const KParams& P, double* D, cudaStream_t st) {
   long long total = (long long)(P.nx + 1) * (P.ny + 1) * (P.nz + 1);
@@ -870,26 +870,6 @@ cudaError_t launch_inflow_c32(const KParams& P, const InflowTable& T, int iterat
   return cudaGetLastError();
 }
 
-cudaError_t launch_inflow_fused_c32(const KParams& P, const InflowTable& T, int iteration, PartC32 out, int* count,
-                                    long long capacity, int* err, cudaStream_t st) {
-  long long total = T.cells * T.per_cell;
-  if (total == 0) return cudaSuccess;
-  note_launch();
-  inflow_fused_kernel<<<grid_for(total), kThreads, 0, st>>>(P, T, iteration, total, count, capacity, err,
-                                                            StoreC32{P, out});
-  return cudaGetLastError();
-}
-
-cudaError_t launch_inflow_fused_f64(const KParams& P, const InflowTable& T, int iteration, PartF64 out, int* count,
-                                    long long capacity, int* err, cudaStream_t st) {
-  long long total = T.cells * T.per_cell;
-  if (total == 0) return cudaSuccess;
-  note_launch();
-  inflow_fused_kernel<<<grid_for(total), kThreads, 0, st>>>(P, T, iteration, total, count, capacity, err,
-                                                            StoreF64{out});
-  return cudaGetLastError();
-}
-
 cudaError_t launch_produce_count(const KParams& P, int iteration, int* counts, cudaStream_t st) {
   long long cells = (long long)P.nx * P.ny * P.nz;
   note_launch();
@@ -900,6 +880,35 @@ cudaError_t launch_produce_count(const KParams& P, int iteration, int* counts, c
 __global__ void add_count_kernel(int* count, const int* add, long long capacity) {
   long long v = (long long)*count + *add;
   *count = int(v < capacity ? v : capacity);
+}
+
+template <class Store>
+static cudaError_t inflow_fused(const KParams& P, const InflowTable& T, int iteration, Store store, int* count,
+                                long long capacity, int* block_counts, int* block_offsets, int* err, cudaStream_t st) {
+  const long long total = T.cells * T.per_cell;
+  if (total == 0) return cudaSuccess;
+  const int nb = inflow_blocks(total);
+  note_launch();
+  inflow_count_kernel<<<nb, kThreads, 0, st>>>(P, T, iteration, total, block_counts);
+  cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, block_offsets + nb, block_offsets + nb + 1, st);
+  if (e != cudaSuccess) return e;
+  note_launch();
+  inflow_emit_kernel<<<nb, kThreads, 0, st>>>(P, T, iteration, total, block_offsets, count, capacity, err, store);
+  note_launch();
+  add_count_kernel<<<1, 1, 0, st>>>(count, block_offsets + nb, capacity);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inflow_fused_c32(const KParams& P, const InflowTable& T, int iteration, PartC32 out, int* count,
+                                    long long capacity, int* block_counts, int* block_offsets, int* err,
+                                    cudaStream_t st) {
+  return inflow_fused(P, T, iteration, StoreC32{P, out}, count, capacity, block_counts, block_offsets, err, st);
+}
+
+cudaError_t launch_inflow_fused_f64(const KParams& P, const InflowTable& T, int iteration, PartF64 out, int* count,
+                                    long long capacity, int* block_counts, int* block_offsets, int* err,
+                                    cudaStream_t st) {
+  return inflow_fused(P, T, iteration, StoreF64{out}, count, capacity, block_counts, block_offsets, err, st);
 }
 
 cudaError_t launch_produce_emit_f64(const KParams& P, int iteration, const int* offsets, PartF64 out, int* count,
@@ -944,17 +953,9 @@ cudaError_t launch_transfer_f64(const KParams& P, PartF64 a, long long n, cudaSt
   return cudaGetLastError();
 }
 
-cudaError_t launch_compact_outflow_f64(const KParams& P, PartF64 in, PartF64 out, long long n, int* block_counts,
-                                       int* block_offsets, int* new_count, int wrap, cudaStream_t st) {
-  int nb = compact_blocks(n);
-  if (n <= 0) return cudaMemsetAsync(new_count, 0, sizeof(int), st);
-  note_launch();
-  outflow_count_f64<<<nb, kCompactThreads, 0, st>>>(P, in, n, block_counts);
-  cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, new_count, block_offsets + nb + 1, st);
-  if (e != cudaSuccess) return e;
-  note_launch();
-  outflow_scatter_f64<<<nb, kCompactThreads, 0, st>>>(P, in, out, n, block_offsets, wrap);
-  return cudaGetLastError();
+cudaError_t launch_outflow_f64(const KParams& P, PartF64 a, long long n, uint2* words, int* block_counts,
+                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st) {
+  return launch_outflow_inplace(OutflowF64{P, a}, n, words, block_counts, block_offsets, count, wrap, err, st);
 }
 
 cudaError_t launch_advance_velocity_f64(const KParams& P, PartF64 a, long long n, const double* E, double dt,

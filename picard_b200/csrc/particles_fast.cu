@@ -14,6 +14,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "outflow.cuh"
 
 namespace picard {
 
@@ -173,64 +174,39 @@ __global__ void transfer_c32_kernel(KParams P, PartC32 a, long long n) {
   }
 }
 
-constexpr int kCompactThreads = 256;
-constexpr int kCompactItems = 8;
-constexpr int kCompactTile = kCompactThreads * kCompactItems;
-
-__global__ void outflow_count_c32(KParams P, PartC32 a, long long n, int* block_counts) {
-  long long base = (long long)blockIdx.x * kCompactTile;
-  int c = 0;
-  for (int q = 0; q < kCompactItems; ++q) {
-    long long p = base + (long long)q * kCompactThreads + threadIdx.x;
-    if (p < n && keep_c32(P, load_pos(a, p))) ++c;
-  }
-  int total;
-  block_scan_excl(c, total);
-  if (threadIdx.x == 0) block_counts[blockIdx.x] = total;
-}
-
-// Order-preserving scatter: item q of thread t is particle base + q*256 + t;
-// survivors keep their order inside the tile (warp ballots per item row).
-__global__ void outflow_scatter_c32(KParams P, PartC32 a, PartC32 o, long long n, const int* block_offsets, int wrap) {
-  __shared__ int row_count[kCompactItems][kCompactThreads / 32];
-  long long base = (long long)blockIdx.x * kCompactTile;
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  bool keep[kCompactItems];
-  for (int q = 0; q < kCompactItems; ++q) {
-    long long p = base + (long long)q * kCompactThreads + threadIdx.x;
-    keep[q] = p < n && keep_c32(P, load_pos(a, p));
-    unsigned m = __ballot_sync(0xffffffffu, keep[q]);
-    if (lane == 0) row_count[q][warp] = __popc(m);
-  }
-  __syncthreads();
-  // prefix over (row, warp) in row-major order = particle order
-  int off = block_offsets[blockIdx.x];
-  for (int q = 0; q < kCompactItems; ++q) {
-    long long p = base + (long long)q * kCompactThreads + threadIdx.x;
-    int before = 0;
-    for (int r = 0; r < q; ++r)
-      for (int w = 0; w < kCompactThreads / 32; ++w) before += row_count[r][w];
-    for (int w = 0; w < warp; ++w) before += row_count[q][w];
-    unsigned m = __ballot_sync(0xffffffffu, keep[q]);
-    if (keep[q]) {
-      long long d = off + before + __popc(m & ((1u << lane) - 1u));
-      uint32_t cell = a.cell[p];
-      if (wrap) {
-        C32 c = load_pos(a, p);
-        wrap_c32(P, c);
-        cell = pack_cell(c.i, c.j, c.k);
-      }
-      o.cell[d] = cell;
-      o.fx[d] = a.fx[p];
-      o.fy[d] = a.fy[p];
-      o.fz[d] = a.fz[p];
-      o.vx[d] = a.vx[p];
-      o.vy[d] = a.vy[p];
-      o.vz[d] = a.vz[p];
-      o.sp[d] = a.sp[p];
+// BCoutflow.f90:28-53 and ParticlesTransfer.f90:494-519 on the CELL32
+// layout, for the in-place removal of outflow.cuh.  An in-cell offset decides
+// an axis only when the cell index is 0 or n there (below / above), so the
+// offsets are read only for those particles.
+struct OutflowC32 {
+  KParams P;
+  PartC32 a;
+  __device__ bool keep_wrap(long long p, int wrap) const {
+    const uint32_t cell = a.cell[p];
+    C32 c;
+    unpack_cell(cell, c.i, c.j, c.k);
+    c.f[0] = (c.i == 0 || c.i == P.nx) ? a.fx[p] : 0.5f;
+    c.f[1] = (c.j == 0 || c.j == P.ny) ? a.fy[p] : 0.5f;
+    c.f[2] = (c.k == 0 || c.k == P.nz) ? a.fz[p] : 0.5f;
+    if (!keep_c32(P, c)) return false;
+    if (wrap) {
+      wrap_c32(P, c);
+      const uint32_t moved = pack_cell(c.i, c.j, c.k);
+      if (moved != cell) a.cell[p] = moved;
     }
+    return true;
   }
-}
+  __device__ void move(long long d, long long s) const {
+    a.cell[d] = a.cell[s];
+    a.fx[d] = a.fx[s];
+    a.fy[d] = a.fy[s];
+    a.fz[d] = a.fz[s];
+    a.vx[d] = a.vx[s];
+    a.vy[d] = a.vy[s];
+    a.vz[d] = a.vz[s];
+    a.sp[d] = a.sp[s];
+  }
+};
 
 // Per-species push constants in FP32.
 struct SpeciesF32 {
@@ -642,17 +618,9 @@ cudaError_t launch_transfer_c32(const KParams& P, PartC32 a, long long n, cudaSt
   return cudaGetLastError();
 }
 
-cudaError_t launch_compact_outflow_c32(const KParams& P, PartC32 in, PartC32 out, long long n, int* block_counts,
-                                       int* block_offsets, int* new_count, int wrap, cudaStream_t st) {
-  if (n <= 0) return cudaMemsetAsync(new_count, 0, sizeof(int), st);
-  int nb = int((n + kCompactTile - 1) / kCompactTile);
-  note_launch();
-  outflow_count_c32<<<nb, kCompactThreads, 0, st>>>(P, in, n, block_counts);
-  cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, new_count, block_offsets + nb + 1, st);
-  if (e != cudaSuccess) return e;
-  note_launch();
-  outflow_scatter_c32<<<nb, kCompactThreads, 0, st>>>(P, in, out, n, block_offsets, wrap);
-  return cudaGetLastError();
+cudaError_t launch_outflow_c32(const KParams& P, PartC32 a, long long n, uint2* words, int* block_counts,
+                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st) {
+  return launch_outflow_inplace(OutflowC32{P, a}, n, words, block_counts, block_offsets, count, wrap, err, st);
 }
 
 cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,

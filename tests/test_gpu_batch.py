@@ -5,8 +5,9 @@ with picard_gpu_run_fused ends -- potential, density, particle count and
 Jacobi sweeps (the batched sweep launch computes each node and each tile
 partial exactly as the single-run kernels) -- with a mix of grid sizes, both
 tile depths (nz < 64 and nz >= 64) and one run with a periodic axis, which
-solves on its own inside the batch.  Energies agree within 1e-12 (particle
-order under concurrent appends is not deterministic)."""
+solves on its own inside the batch.  The particles too: inflow survivors are
+appended in candidate order and BCoutflow fills holes in a fixed order, so
+the particle arrays and the energies summed over them match bit for bit."""
 import numpy as np
 import pytest
 
@@ -48,17 +49,20 @@ def test_batch_equals_each_run_alone(w32, monkeypatch):
     for p in params:
         g = _start(p)
         sw = g.run_fused(0, steps)
-        alone.append((sw, g.num_local, g.field(capi.FIELD_U), g.field(capi.FIELD_N), g.energy()))
+        alone.append((sw, g.num_local, g.field(capi.FIELD_U), g.field(capi.FIELD_N), g.energy(), g.particles()))
         g.close()
     sims = [_start(p) for p in params]
     sweeps = batch_run_fused(sims, 0, steps)
     for k, g in enumerate(sims):
-        sw, n, U, N, e = alone[k]
+        sw, n, U, N, e, (rp, ip) = alone[k]
         assert sweeps[k] == sw, k
         assert g.num_local == n, k
         np.testing.assert_array_equal(g.field(capi.FIELD_U), U, err_msg=f"run {k}")
         np.testing.assert_array_equal(g.field(capi.FIELD_N), N, err_msg=f"run {k}")
-        np.testing.assert_allclose(g.energy(), e, rtol=1e-12)
+        np.testing.assert_array_equal(g.energy(), e, err_msg=f"run {k}")
+        rg, ig = g.particles()
+        np.testing.assert_array_equal(ig, ip, err_msg=f"run {k}")
+        np.testing.assert_array_equal(rg, rp, err_msg=f"run {k}")
     for g in sims:
         g.close()
 
