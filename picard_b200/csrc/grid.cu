@@ -461,6 +461,8 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
     // read in iteration it-1 (ended at a barrier)
     if (STAGES == 2 && tid == 0 && tn < ntiles)
       tma_issue_tile<ZC>(&tw, &tr, stages + (st ^ 1) * TmaStage<ZC>::kFloats, st ? mb0 : mb1, tn, gx, gy, w_zero);
+    // tile coordinates before the wait: the divisions overlap the copies
+    const int bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
     const bool ok = __syncthreads_and(mbar_wait(mb, phase, kMbarSpin) ? 1 : 0);
     if (!ok) {
       if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
@@ -470,7 +472,6 @@ __global__ void __launch_bounds__(256) sweep_tma_kernel(const __grid_constant__ 
       return;
     }
     const float* sw = stages + st * TmaStage<ZC>::kFloats;
-    const int bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
     tile32_sweep<ZC>(sw, sw + TmaStage<ZC>::kW, S, J, wout, partial + t, w_zero, bx, by, bz);
     // every thread is done with this stage (and thread 0 with the reduction
     // scratch) before the stage is refilled
@@ -530,11 +531,18 @@ __device__ inline void tma2_issue_tile(const CUtensorMap* tw, const CUtensorMap*
       : "memory");
 }
 
-template <int ZC, int STAGES>
+// W_ZERO: the first sweep after an anchor (zero iterate, no w box), a
+// separate instantiation so that the common sweep carries no run-time flag.
+// LOOP = false: one CTA per tile (the grid covers every tile), without the
+// persistent loop: 42 instead of 54 registers, so shared memory, not
+// registers, sets the CTAs per SM (7.6 instead of 8.0 us per sweep at
+// 256 x 128 x 128).
+template <int ZC, int STAGES, bool W_ZERO, bool LOOP>
 __global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__ CUtensorMap tw,
                                                          const __grid_constant__ CUtensorMap tr, Stencil S,
                                                          JacobiCoefF J, float* __restrict__ wout, double* partial,
-                                                         int w_zero, int gx2, int gx, int gy, int ntiles, int* err) {
+                                                         int gx2, int gx, int gy, int ntiles, int* err) {
+  constexpr int w_zero = W_ZERO ? 1 : 0;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float* stages = reinterpret_cast<float*>(smem_raw);  // [STAGES][Tma2Stage<ZC>::kFloats]
   __shared__ __align__(8) unsigned long long mbar[2];
@@ -543,6 +551,27 @@ __global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__
   const int tid = tx + kTmaTx * ty;
   const uint32_t mb0 = (uint32_t)__cvta_generic_to_shared(&mbar[0]);
   const uint32_t mb1 = (uint32_t)__cvta_generic_to_shared(&mbar[1]);
+  if (!LOOP) {
+    if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const int bx2 = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
+    if (tid == 0) tma2_issue_tile<ZC>(&tw, &tr, stages, mb0, t, gx2, gy, w_zero);
+    if (!__syncthreads_and(mbar_wait(mb0, 0, kMbarSpin) ? 1 : 0)) {
+      if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+      mbar_wait(mb0, 0, kMbarSpin);
+      return;
+    }
+    pair_tile_sweep_wz<ZC, W_ZERO>(stages, stages + Tma2Stage<ZC>::kW, S, J, wout, partial, bx2, by, bz, gx, gy,
+                                   rows);
+    return;
+  }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1) : "memory");
@@ -563,6 +592,10 @@ __global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__
     const int tn = t + gridDim.x;
     if (STAGES == 2 && tid == 0 && tn < ntiles)
       tma2_issue_tile<ZC>(&tw, &tr, stages + (st ^ 1) * Tma2Stage<ZC>::kFloats, st ? mb0 : mb1, tn, gx2, gy, w_zero);
+    // tile coordinates before the wait: computed after it, the three divisions
+    // sat between the copies landing and the sweep and cost ~1.5 us per sweep
+    // at 256 x 128 x 128 (9.1 instead of 7.6 us)
+    const int bx2 = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
     const bool ok = __syncthreads_and(mbar_wait(mb, phase, kMbarSpin) ? 1 : 0);
     if (!ok) {
       if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
@@ -571,8 +604,7 @@ __global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__
       return;
     }
     const float* sw = stages + st * Tma2Stage<ZC>::kFloats;
-    const int bx2 = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
-    pair_tile_sweep<ZC>(sw, sw + Tma2Stage<ZC>::kW, S, J, wout, partial, w_zero, bx2, by, bz, gx, gy, rows);
+    pair_tile_sweep_wz<ZC, W_ZERO>(sw, sw + Tma2Stage<ZC>::kW, S, J, wout, partial, bx2, by, bz, gx, gy, rows);
     __syncthreads();
     if (STAGES == 1 && tid == 0 && tn < ntiles) tma2_issue_tile<ZC>(&tw, &tr, stages, mb0, tn, gx2, gy, w_zero);
   }
@@ -1107,8 +1139,10 @@ static cudaError_t launch_tma2_zs(const KParams& P, const JacobiGeom& G, const C
   const size_t smem = STAGES * Tma2Stage<ZC>::kBytes;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e =
-        cudaFuncSetAttribute(sweep_tma2_kernel<ZC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaSuccess;
+    for (auto k : {sweep_tma2_kernel<ZC, STAGES, false, true>, sweep_tma2_kernel<ZC, STAGES, true, true>,
+                   sweep_tma2_kernel<ZC, STAGES, false, false>, sweep_tma2_kernel<ZC, STAGES, true, false>})
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -1126,8 +1160,12 @@ static cudaError_t launch_tma2_zs(const KParams& P, const JacobiGeom& G, const C
   cfg.attrs = at;
   cfg.numAttrs = 1;
   note_launch();
-  return cudaLaunchKernelEx(&cfg, sweep_tma2_kernel<ZC, STAGES>, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout,
-                            partial, w_zero, gx2, (int)G.grid.x, (int)G.grid.y, ntiles, err);
+  // one CTA per tile with one stage: the loop-free instantiation
+  const bool loop = STAGES == 2 || ctas < ntiles;
+  auto kern = w_zero ? (loop ? sweep_tma2_kernel<ZC, STAGES, true, true> : sweep_tma2_kernel<ZC, STAGES, true, false>)
+                     : (loop ? sweep_tma2_kernel<ZC, STAGES, false, true> : sweep_tma2_kernel<ZC, STAGES, false, false>);
+  return cudaLaunchKernelEx(&cfg, kern, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout, partial, gx2,
+                            (int)G.grid.x, (int)G.grid.y, ntiles, err);
 }
 
 template <int ZC>
@@ -1140,11 +1178,12 @@ static cudaError_t launch_tma2_zc(const KParams& P, const JacobiGeom& G, const C
 template <int ZC, int STAGES>
 static int occupancy2_zs() {
   const size_t smem = STAGES * Tma2Stage<ZC>::kBytes;
-  if (cudaFuncSetAttribute(sweep_tma2_kernel<ZC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-      cudaSuccess)
+  if (cudaFuncSetAttribute(sweep_tma2_kernel<ZC, STAGES, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
     return 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_tma2_kernel<ZC, STAGES>, kTmaTx * kTmaTy, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_tma2_kernel<ZC, STAGES, false, true>, kTmaTx * kTmaTy,
+                                                    smem) !=
       cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
