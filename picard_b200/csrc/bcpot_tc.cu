@@ -40,7 +40,10 @@ namespace picard {
 namespace {
 
 constexpr int kTcM = 128;          // rows p1 per tile
-constexpr int kTcThreads = 128;
+// Two warpgroups: warps w and w + 4 share TMEM lanes 32 (w % 4) .. + 31 and
+// split the accumulator columns, so folding a step and building the next
+// B window take half as long between MMA batches.
+constexpr int kTcThreads = 256;
 constexpr long long kTcSpin = 1LL << 26;
 
 struct TcAxis {
@@ -164,10 +167,10 @@ struct TcShape {
   static constexpr uint32_t kIdesc =
       (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
   static_assert(N % 16 == 0 && N >= 64 && N <= 128, "MMA shape with M = 128");
-  static_assert(kWUsed <= 2 * 128, "window within the prefetch of 128 threads x 2");
+  static_assert(kWUsed <= 2 * 128, "window within the prefetch");
 };
 constexpr uint32_t kColAcc = 0, kColSum = 256, kColComp = 384;
-constexpr int kPrefetch = 2;  // D values per thread per step (the window <= 2 * 128)
+constexpr int kPrefetch = (2 * 128 + kTcThreads - 1) / kTcThreads;  // D values per thread per step (window <= 256)
 
 __device__ inline void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
   asm volatile(
@@ -201,6 +204,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __shared__ __align__(8) unsigned long long mbar[2];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quad = warp & 3;                        // TMEM lane quadrant of this warp
+  const int c0 = (warp >> 2) * (N / 2), c1 = c0 + N / 2;  // this warpgroup's accumulator columns
 
   // CTA -> (tile, face, split)
   const int split = blockIdx.x % X.splits;
@@ -235,7 +240,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's 32 TMEM lanes
+  const uint32_t lanebase = tmem + ((uint32_t)(32 * quad) << 16);  // this warp's 32 TMEM lanes
   uint32_t phase[2] = {0, 0};
   bool pending[2] = {false, false};  // MMAs committed on mbar[b], not yet waited for
   bool unfolded[2] = {false, false};  // accumulator b holds a step not yet folded
@@ -246,7 +251,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint32_t z[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) z[j] = 0u;
-    for (int col = 0; col < kTcHalfN; col += 16) {
+    for (int col = c0; col < c1; col += 16) {
       tmem_st16(lanebase + kColSum + col, z);
       tmem_st16(lanebase + kColComp + col, z);
     }
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   // Kahan: y = a - c; t = s + y; c = (t - s) - y; s = t
   auto fold = [&](int b) {
     if (!unfolded[b]) return;
-    for (int col = 0; col < kTcHalfN; col += 16) {
+    for (int col = c0; col < c1; col += 16) {
       uint32_t a[16], sm[16], cp[16];
       tmem_ld16(lanebase + kColAcc + (uint32_t)(b * kTcHalfN + col), a);
       tmem_ld16(lanebase + kColSum + col, sm);
@@ -354,6 +359,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
       }
       if (tid < 3) sWin[tid * kWL + kWUsed] = __float2bfloat16_rn(0.0f);
+      // D values of the next step: issued now, so that their latency overlaps
+      // the Z build and the MMA issue of this step
+      {
+        long long npr = pr + 1;
+        int nkc = kc;
+        if (npr >= pend) {
+          npr = pbeg;
+          ++nkc;
+        }
+        if (nkc < nchunks) prefetch(int(npr / nd) + 1, dlo + int(npr % nd), nkc);
+      }
       __syncthreads();
       // Z[b][s][u] = w_s[u .. u+7]
       unsigned char* zb = sZ + (size_t)b * 3 * kZS;
@@ -373,14 +389,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint32_t zs = (uint32_t)__cvta_generic_to_shared(zb);
         const uint32_t acc_cols = tmem + kColAcc + (uint32_t)(b * kTcHalfN);
         const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
+        // descriptors of this step's first A and B blocks; every other block
+        // is a multiple of 16 bytes further in, which adds to the start
+        // address field (address / 16, below 2^14 for any shared-memory
+        // address) without carrying into the offset fields
+        const uint64_t adesc0 = smem_desc(tb, kRT * 16, 128);
+        const uint64_t bdesc0 = smem_desc(zs, 128, 128);
 #pragma unroll
         for (int ks = 0; ks < kTcKC / 16; ++ks) {
 #pragma unroll
           for (int t = 0; t < 6; ++t) {
-            const uint32_t a_addr = tb + (uint32_t)(pa[t] * kTSplit + (size_t)(2 * ks) * kRT * 16);
-            const uint32_t b_addr = zs + (uint32_t)(pb[t] * kZS + ks * 256);
-            const uint64_t adesc = smem_desc(a_addr, kRT * 16, 128);
-            const uint64_t bdesc = smem_desc(b_addr, 128, 128);
+            const uint64_t adesc = adesc0 + (uint64_t)((pa[t] * kTSplit + (size_t)(2 * ks) * kRT * 16) >> 4);
+            const uint64_t bdesc = bdesc0 + (uint64_t)((pb[t] * kZS + (size_t)ks * 256) >> 4);
             const uint32_t acc = (ks == 0 && t == 0) ? 0u : 1u;
             asm volatile(
                 "{\n\t.reg .pred p;\n\t"
@@ -396,16 +416,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       pending[b] = true;
       unfolded[b] = true;
       ++step;
-      // D values of the next step
-      {
-        long long npr = pr + 1;
-        int nkc = kc;
-        if (npr >= pend) {
-          npr = pbeg;
-          ++nkc;
-        }
-        if (nkc < nchunks) prefetch(int(npr / nd) + 1, dlo + int(npr % nd), nkc);
-      }
     }
   }
   if (ok && !__syncthreads_and(drain() ? 1 : 0)) ok = false;
@@ -413,8 +423,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     fold(step & 1);        // the older of the two outstanding steps first
     fold((step + 1) & 1);
     // partial = sum - compensation, this thread's row
-    double* row = part + (long long)(32 * warp + lane) * kTcN;
-    for (int col = 0; col < kTcHalfN; col += 16) {
+    double* row = part + (long long)(32 * quad + lane) * kTcN;
+    for (int col = c0; col < c1; col += 16) {
       uint32_t sm[16], cp[16];
       tmem_ld16(lanebase + kColSum + col, sm);
       tmem_ld16(lanebase + kColComp + col, cp);
