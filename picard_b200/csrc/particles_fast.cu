@@ -428,32 +428,36 @@ __global__ void deposit_c32_kernel(KParams P, PartC32 a, long long n, unsigned l
 constexpr int kDepChunk = 1024;          // particles per CTA iteration (4 per thread)
 constexpr int kDepTile = 8192;           // tile entries (two u32 halves each: 64 KB)
 
-__device__ inline int block_min_max(int v, bool want_max, int* red) {
-  for (int o = 16; o > 0; o >>= 1) {
-    int u = __shfl_xor_sync(0xffffffffu, v, o);
-    v = want_max ? max(v, u) : min(v, u);
-  }
+// Block-wide minima of 8 values at once (maxima enter negated): warp minima
+// into red8[warp][8], a barrier, every thread reads the 8 warps', and a
+// barrier so that red8 can be written again (two barriers instead of three
+// per value).
+__device__ inline void block_min8(int (&v)[8], int (*red8)[8]) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    for (int o = 16; o > 0; o >>= 1) v[q] = min(v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  if (w == 0) {
-    v = l < (int)(blockDim.x >> 5) ? red[l] : (want_max ? INT_MIN : INT_MAX);
-    for (int o = 16; o > 0; o >>= 1) {
-      int u = __shfl_xor_sync(0xffffffffu, v, o);
-      v = want_max ? max(v, u) : min(v, u);
-    }
-    if (l == 0) red[32] = v;
+  if (l < 8) {
+    int x = v[0];
+#pragma unroll
+    for (int q = 1; q < 8; ++q)
+      if (l == q) x = v[q];
+    red8[w][l] = x;
   }
   __syncthreads();
-  v = red[32];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    int m = red8[0][q];
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) m = min(m, red8[ww][q]);
+    v[q] = m;
+  }
   __syncthreads();
-  return v;
 }
 
 __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC32 a, long long n,
                                                                unsigned long long* Nacc) {
   extern __shared__ unsigned int dep_tile[];  // [2][kDepTile]: low and high 20-bit halves
-  __shared__ int red[33];
+  __shared__ int red8[8][8];
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
   unsigned int* lo = dep_tile;
   unsigned int* hi = dep_tile + kDepTile;
@@ -477,14 +481,14 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
         smin = min(smin, sp[m]), smax = max(smax, sp[m]);
       }
     }
-    imin = block_min_max(imin, false, red);
-    imax = block_min_max(imax, true, red);
-    jmin = block_min_max(jmin, false, red);
-    jmax = block_min_max(jmax, true, red);
-    kmin = block_min_max(kmin, false, red);
-    kmax = block_min_max(kmax, true, red);
-    smin = block_min_max(smin, false, red);
-    smax = block_min_max(smax, true, red);
+    {
+      // the bounding box of the chunk (INT_MIN maxima of idle threads negate
+      // to INT_MAX + 1: clamp them first)
+      int v[8] = {imin, -max(imax, -INT_MAX), jmin, -max(jmax, -INT_MAX),
+                  kmin, -max(kmax, -INT_MAX), smin, -max(smax, -INT_MAX)};
+      block_min8(v, red8);
+      imin = v[0], imax = -v[1], jmin = v[2], jmax = -v[3], kmin = v[4], kmax = -v[5], smin = v[6], smax = -v[7];
+    }
     const long long bi = (long long)imax - imin + 2, bj = (long long)jmax - jmin + 2, bk = (long long)kmax - kmin + 2,
                     bs = (long long)smax - smin + 1;
     const long long vol = bi * bj * bk * bs;
