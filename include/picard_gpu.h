@@ -155,6 +155,8 @@ PICARD_API int picard_gpu_particles_initialize(picard_ctx* ctx);                
 PICARD_API int picard_gpu_bc_inflow(picard_ctx* ctx, int32_t iteration);        /* BCinflow.f90:2-476           */
 PICARD_API int picard_gpu_advance_position(picard_ctx* ctx, double dt);         /* AdvancePosition.f90:4-19     */
 PICARD_API int picard_gpu_particles_produce(picard_ctx* ctx, int32_t iteration);/* ParticlesProduce.f90:1-113   */
+/* BCoutflow removes in place and leaves the particles in the order of the
+ * reference's loop (each removed particle replaced by the current last one). */
 PICARD_API int picard_gpu_bc_outflow(picard_ctx* ctx);                          /* BCoutflow.f90:5-87           */
 PICARD_API int picard_gpu_particles_transfer(picard_ctx* ctx);                  /* ParticlesTransfer.f90:2-614  */
 PICARD_API int picard_gpu_particles_gridify(picard_ctx* ctx);                   /* ParticlesGridify.f90:1-296   */
@@ -285,11 +287,14 @@ typedef void (*picard_log_fn)(int32_t iteration, double time, int32_t num_local,
 PICARD_API int picard_gpu_run(picard_ctx* ctx, int32_t iter_start, int32_t iter_end, int32_t log_interval,
                    picard_log_fn log_fn, void* user, int64_t* sweeps_total);
 
-/* The same iterations through the fused device path: one particle pass per
- * step (velocity push of the previous step, position advance, outflow and
- * periodic wrap, compaction), inflow candidates generated, advanced and
- * filtered in one kernel, no host round trip inside a step.  Results equal
- * picard_gpu_run's within the parity tolerances. */
+/* The same iterations through the fused device path: the velocity push of one
+ * step and the position advance of the next in one particle pass, BCoutflow
+ * with the periodic wrap in place, inflow candidates generated, advanced and
+ * filtered on the device and appended after BCoutflow in candidate order.
+ * Results equal picard_gpu_run's within the parity tolerances (the same
+ * particles; the inflow ones sit at the end instead of before the produced
+ * ones), and the particle order is deterministic: two runs from the same state
+ * hold the same particles in the same slots. */
 PICARD_API int picard_gpu_run_fused(picard_ctx* ctx, int32_t iter_start, int32_t iter_end,
                          int64_t* sweeps_total);
 
