@@ -66,6 +66,21 @@ struct BatchArgs {
 };
 static_assert(sizeof(BatchArgs) < 32000, "kernel parameter space");
 
+// The run whose tile range holds CTA t: the last r with tile_base <= t (the
+// bases are cumulative, so non-decreasing).  A binary search: the lookup sits
+// before the tile's TMA issue, on every tile's critical path.
+__device__ __forceinline__ int batch_run_of(const BatchArgs& A, int t) {
+  int lo = 0, hi = A.nruns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (A.run[mid].tile_base <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
 // The x-pair sweep (pair_tile.cuh, as in grid.cu sweep_tma2_kernel) over a
 // table of runs: CTA t takes tile t - tile_base of the run whose tile range
 // holds t.
@@ -80,8 +95,7 @@ __global__ void __launch_bounds__(256) sweep_batch_kernel(const __grid_constant_
   __shared__ double rows[2][kTy];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kTx * ty;
   const int t = blockIdx.x;
-  int r = 0;
-  while (r + 1 < A.nruns && t >= A.run[r + 1].tile_base) ++r;
+  const int r = batch_run_of(A, t);
   const BatchRun& R = A.run[r];
   const int lt = t - R.tile_base;
   const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
@@ -156,8 +170,7 @@ __global__ void __launch_bounds__(256) sweep_batch32_kernel(const __grid_constan
   __shared__ __align__(8) unsigned long long mbar;
   const int tid = threadIdx.x + kT32Tx * threadIdx.y;
   const int t = blockIdx.x;
-  int r = 0;
-  while (r + 1 < A.nruns && t >= A.run[r + 1].tile_base) ++r;
+  const int r = batch_run_of(A, t);
   const BatchRun& R = A.run[r];
   const int lt = t - R.tile_base;
   const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
