@@ -107,6 +107,18 @@ __device__ inline C32 load_pos(const PartC32& a, long long p) {
   return r;
 }
 
+// The same with streaming (evict-first) loads: for the passes that read every
+// particle once, so that the 7.8 GB particle stream does not push the E table
+// or the density accumulators out of L2.
+__device__ inline C32 load_pos_cs(const PartC32& a, long long p) {
+  C32 r;
+  unpack_cell(__ldcs(a.cell + p), r.i, r.j, r.k);
+  r.f[0] = __ldcs(a.fx + p);
+  r.f[1] = __ldcs(a.fy + p);
+  r.f[2] = __ldcs(a.fz + p);
+  return r;
+}
+
 // Move one axis by d cells (in cell units) and renormalise to [0, 1).
 // Open axes pin far-out particles at the outer guard node (they are outside
 // the domain and BCoutflow removes them); periodic axes shift by whole
@@ -323,21 +335,21 @@ __global__ void __launch_bounds__(256, 8) push_advance_c32_kernel(KParams P, Spe
                                                                   const float4* E, float dtdx, float dtdy,
                                                                   float dtdz) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    C32 c = load_pos(a, p);
+    C32 c = load_pos_cs(a, p);
     float Ep[3];
     gather_c32(P, c, E, Ep);
-    float v[3] = {a.vx[p], a.vy[p], a.vz[p]};
-    boris_c32(P, S, a.sp[p], 0, Ep, v);
-    a.vx[p] = v[0];
-    a.vy[p] = v[1];
-    a.vz[p] = v[2];
+    float v[3] = {__ldcs(a.vx + p), __ldcs(a.vy + p), __ldcs(a.vz + p)};
+    boris_c32(P, S, __ldcs(a.sp + p), 0, Ep, v);
+    __stcs(a.vx + p, v[0]);
+    __stcs(a.vy + p, v[1]);
+    __stcs(a.vz + p, v[2]);
     move_axis(c.i, c.f[0], v[0] * dtdx, P.nx, P.xflow);
     move_axis(c.j, c.f[1], v[1] * dtdy, P.ny, P.yflow);
     move_axis(c.k, c.f[2], v[2] * dtdz, P.nz, P.zflow);
-    a.cell[p] = pack_cell(c.i, c.j, c.k);
-    a.fx[p] = c.f[0];
-    a.fy[p] = c.f[1];
-    a.fz[p] = c.f[2];
+    __stcs(a.cell + p, pack_cell(c.i, c.j, c.k));
+    __stcs(a.fx + p, c.f[0]);
+    __stcs(a.fy + p, c.f[1]);
+    __stcs(a.fz + p, c.f[2]);
   }
 }
 
@@ -473,8 +485,8 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
       const long long p = base + threadIdx.x + 256 * m;
       act[m] = p < n;
       if (act[m]) {
-        c[m] = load_pos(a, p);
-        sp[m] = a.sp[p];
+        c[m] = load_pos_cs(a, p);
+        sp[m] = __ldcs(a.sp + p);
         imin = min(imin, c[m].i), imax = max(imax, c[m].i);
         jmin = min(jmin, c[m].j), jmax = max(jmax, c[m].j);
         kmin = min(kmin, c[m].k), kmax = max(kmax, c[m].k);
