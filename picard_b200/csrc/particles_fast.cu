@@ -178,11 +178,20 @@ __global__ void advance_position_c32_kernel(KParams P, PartC32 a, long long n, f
   }
 }
 
+// Only a particle whose cell index is 0 or n on some axis (or beyond) can
+// wrap, so interior cells are decided from the cell word alone, the in-cell
+// offsets are read only for the rest, and a cell word is written only when it
+// changes.
 __global__ void transfer_c32_kernel(KParams P, PartC32 a, long long n) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const uint32_t cell = a.cell[p];
+    const uint32_t cx = cell & kCellMaskX, cy = (cell >> kCellBitsX) & kCellMaskY,
+                   cz = cell >> (kCellBitsX + kCellBitsY);
+    if (cx - 2u < uint32_t(P.nx - 1) && cy - 2u < uint32_t(P.ny - 1) && cz - 2u < uint32_t(P.nz - 1)) continue;
     C32 c = load_pos(a, p);
     wrap_c32(P, c);
-    a.cell[p] = pack_cell(c.i, c.j, c.k);
+    const uint32_t moved = pack_cell(c.i, c.j, c.k);
+    if (moved != cell) a.cell[p] = moved;
   }
 }
 
