@@ -77,10 +77,35 @@ __device__ __forceinline__ long long kept_through(const int* block_offsets, long
   return (long long)block_offsets[q / kOutflowTile] + (long long)w.y + __popc(upto);
 }
 
+// The first survivor above s, or -1: the rest of s's keep word, then the
+// following words, skipping whole blocks that have no survivor.
+__device__ __forceinline__ long long next_survivor(const uint2* words, const int* block_counts, long long s, int nb) {
+  const long long nwords = (long long)nb * kOutflowWords;
+  long long wi = s >> 5;
+  const int sh = int(s & 31);
+  unsigned bits = sh == 31 ? 0u : (words[wi].x & (0xffffffffu << (sh + 1)));
+  while (bits == 0u) {
+    if (++wi >= nwords) return -1;
+    if ((wi & (kOutflowWords - 1)) == 0) {
+      long long b = wi / kOutflowWords;
+      while (b < nb && block_counts[b] == 0) ++b;
+      if (b >= nb) return -1;
+      wi = b * kOutflowWords;
+    }
+    bits = words[wi].x;
+  }
+  return (wi << 5) + (__ffs(bits) - 1);
+}
+
+// Between q and the next survivor g above it, S is constant, so the chain
+// steps q, q + S, q + 2S, ... until it first reaches g or beyond: the kernel
+// jumps there directly (with survivors dense, that is the single hop
+// q + S(q)).  A pathological pattern -- say only the last particle survives --
+// then takes one jump instead of a walk over every position.
 template <class L>
 __global__ void __launch_bounds__(kOutflowThreads)
-    outflow_fill_kernel(L lay, long long n, const uint2* words, const int* block_offsets, const int* survivors,
-                        int* err) {
+    outflow_fill_kernel(L lay, long long n, const uint2* words, const int* block_counts, int nb,
+                        const int* block_offsets, const int* survivors, int* err) {
   const long long np = *survivors;
   const long long base = (long long)blockIdx.x * kOutflowTile;
   if (base >= np) return;
@@ -91,11 +116,15 @@ __global__ void __launch_bounds__(kOutflowThreads)
     if ((w.x >> (p & 31)) & 1u) continue;  // a survivor below n' stays where it is
     long long s = p;
     bool found = false;
-    // the chain rises strictly and stays below n, so n hops always suffice
+    // the chain rises strictly and stays below n, so n jumps always suffice
     for (long long hop = 0; hop < n; ++hop) {
       const long long above = np - kept_through(block_offsets, s, w);
-      if (above < 1 || s + above >= n) break;  // not reachable from a hole below n'
-      s += above;
+      if (above < 1) break;  // not reachable from a hole below n'
+      const long long g = next_survivor(words, block_counts, s, nb);
+      if (g < 0) break;
+      const long long t = s + (g - s + above - 1) / above * above;
+      if (t >= n) break;
+      s = t;
       w = words[s >> 5];
       if ((w.x >> (s & 31)) & 1u) {
         found = true;
@@ -122,7 +151,7 @@ cudaError_t launch_outflow_inplace(const L& lay, long long n, uint2* words, int*
   cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, count, block_offsets + nb + 1, st);
   if (e != cudaSuccess) return e;
   note_launch();
-  outflow_fill_kernel<<<nb, kOutflowThreads, 0, st>>>(lay, n, words, block_offsets, count, err);
+  outflow_fill_kernel<<<nb, kOutflowThreads, 0, st>>>(lay, n, words, block_counts, nb, block_offsets, count, err);
   return cudaGetLastError();
 }
 

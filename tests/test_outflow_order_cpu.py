@@ -2,8 +2,10 @@
 
 The kernels (picard_b200/csrc/outflow.cuh) fill every hole p below the
 survivor count n' with the particle reached from p by q -> q + S(q), S(q) the
-survivors above q.  This file models that rule with numpy (the same keep
-words, block offsets and chase) and checks it against the oracle's literal
+survivors above q, jumping in one step over the stretch where S stays
+constant (up to the first point at or beyond the next survivor).  This file
+models that rule with numpy (the same keep words, block offsets, block counts
+and jumps) and checks it against the oracle's literal
 BCoutflow loop (BCoutflow.f90:24-83: walk from the end, move the current last
 particle into each hole) on random and structured keep patterns.  Each
 particle carries its original index in vz, so the order is compared exactly.
@@ -37,6 +39,24 @@ def chase_model(keep: np.ndarray) -> np.ndarray:
         upto = w & ((1 << ((q & 31) + 1)) - 1)
         return int(block_offsets[q // TILE]) + int(word_before[q >> 5]) + bin(upto).count("1")
 
+    nwords = nb * (TILE // 32)
+
+    def next_survivor(s: int) -> int:
+        wi = s >> 5
+        sh = s & 31
+        b = 0 if sh == 31 else int(bits[wi]) & (0xFFFFFFFF << (sh + 1)) & 0xFFFFFFFF
+        while b == 0:
+            wi += 1
+            assert wi < nwords
+            if wi % (TILE // 32) == 0:  # skip blocks without survivors
+                blk = wi // (TILE // 32)
+                while blk < nb and block_counts[blk] == 0:
+                    blk += 1
+                assert blk < nb
+                wi = blk * (TILE // 32)
+            b = int(bits[wi])
+        return (wi << 5) + ((b & -b).bit_length() - 1)
+
     out = np.arange(np_)
     for p in range(np_):
         if keep[p]:
@@ -44,8 +64,11 @@ def chase_model(keep: np.ndarray) -> np.ndarray:
         s = p
         for _ in range(n):
             above = np_ - kept_through(s)
-            assert 1 <= above and s + above < n
-            s += above
+            assert above >= 1
+            g = next_survivor(s)
+            t = s + (g - s + above - 1) // above * above
+            assert t < n
+            s = t
             if keep[s]:
                 break
         else:
@@ -92,6 +115,13 @@ def patterns():
     out.append(k)
     k = np.zeros(6000, bool)
     k[::997] = True
+    out.append(k)
+    # a long removed stretch spanning empty blocks before the only survivor
+    k = np.zeros(3 * TILE + 17, bool)
+    k[-1] = True
+    out.append(k)
+    k = np.ones(5 * TILE, bool)
+    k[TILE // 2: 4 * TILE] = False
     out.append(k)
     return out
 
