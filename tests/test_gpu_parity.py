@@ -4,7 +4,7 @@ Bars: integer and index results (cell indices, removed / wrapped particle
 sets, species, particle counts, D) bit-exact; FP64-layout positions bit-exact
 and velocities within 1e-13 relative (libm log/sin differ from CUDA's by an
 ulp); fixed-point deposits within 1e-10 relative L2; potential and field
-within 1e-6 relative L2 of the FP64 oracle (the
+within 1e-6 relative L2 of the FP64 oracle (the tolerance for the potential; the
 FP64 solver meets 1e-10).  CELL32 (FP32 particles) is held to tolerances
 written beside each check.
 """
@@ -194,7 +194,7 @@ def test_bc_potentials_matches_oracle():
 def test_bc_potentials_tensor_cores_vs_fp64(dims):
     # three-way BF16 split, one FP32 MMA accumulation per K chunk, the steps
     # summed with Kahan compensation in tensor memory: the face potentials
-    # agree with the FP64 sum within the north-star 1e-6 relative.  The faces
+    # agree with the FP64 sum within 1e-6 relative, the potential's tolerance.  The faces
     # cover every tile width: <= 64 columns (16^3, 160x24x20, 40x136x12),
     # 65..96 (72x66x70) and > 96 (the 136-row axis of 40x136x12)
     nx, ny, nz = dims
@@ -399,7 +399,7 @@ def test_one_step_parity_cell32_layout():
         np.testing.assert_allclose(rg[:, :3], ro[:, :3], rtol=0, atol=1e-5 * d.min())
         mism = np.any(cell_indices(p, rg) != cell_indices(p, ro), axis=1)
         assert mism.sum() <= 2
-    # fields: N within 1e-6, U and E within the north-star 1e-6 relative L2
+    # fields: N within 1e-6, U and E within the 1e-6 relative L2 tolerance of the potential
     assert rel_l2(g.field(capi.FIELD_N), o.N) < 1e-6
     assert rel_l2(g.field(capi.FIELD_U), o.U) < 1e-6
     assert rel_l2(g.field(capi.FIELD_E), o.E) < 1e-5
