@@ -1,7 +1,7 @@
 /*
  * picard_oracle.c -- CPU FP64 restatement of Picard's per-timestep PIC loop.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker the CUDA path is compared
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle the CUDA path is compared
  * against, and the CPU baseline that bench.py times.  Nothing in the product
  * (picard_b200/) links, loads or calls it.
  *

@@ -2,7 +2,7 @@
 // parameter sweep): picard_batch_run_fused.
 //
 // Each run is its own picard_ctx (own memory, own stream).  Per iteration of
-// picard.f90:554-674 the driver issues every run's particle phases on the
+// picard.f90:554-674 the batched loop issues every run's particle phases on the
 // runs' streams before waiting on any of them (the particle-count round trips
 // of all runs travel together), then solves every run's Poisson problem in
 // ticks: each run plans its rounds of sweeps from its own anchor (the

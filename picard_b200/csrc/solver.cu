@@ -139,7 +139,7 @@ int solve_f64(picard_ctx* c, double tol, long long smax, int maxit, long long* s
 // ---------------------------------------------- FP32 increment + FP64 anchor
 //
 // The loop is a resumable state machine (F32Solve, solve_f32.cuh) so that the
-// batched driver can advance many runs' solves in lockstep, running the
+// batched loop (batch.cu) can advance many runs' solves in lockstep, running the
 // sweeps of a round for all runs in one launch per sweep; solve_f32 drives one
 // run with its own sweep launches.
 
