@@ -1,7 +1,7 @@
 """ctypes bindings of the FP64 CPU oracle (liboracle.so built from picard_oracle.c).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as the
-checker and by bench.py's CPU-baseline leg.  The product never imports it.
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() to
+compare against, and by bench.py's CPU-baseline leg.  The product never imports it.
 PARITY UNPINNED: the reference (Fortran 90 + MPI) cannot be built here and
 ships no golden vectors; the restatement is pinned by physics known-answer
 tests and the published Philox4x32-10 vectors instead.
