@@ -77,35 +77,17 @@ __device__ __forceinline__ long long kept_through(const int* block_offsets, long
   return (long long)block_offsets[q / kOutflowTile] + (long long)w.y + __popc(upto);
 }
 
-// The first survivor above s, or -1: the rest of s's keep word, then the
-// following words, skipping whole blocks that have no survivor.
-__device__ __forceinline__ long long next_survivor(const uint2* words, const int* block_counts, long long s, int nb) {
-  const long long nwords = (long long)nb * kOutflowWords;
-  long long wi = s >> 5;
-  const int sh = int(s & 31);
-  unsigned bits = sh == 31 ? 0u : (words[wi].x & (0xffffffffu << (sh + 1)));
-  while (bits == 0u) {
-    if (++wi >= nwords) return -1;
-    if ((wi & (kOutflowWords - 1)) == 0) {
-      long long b = wi / kOutflowWords;
-      while (b < nb && block_counts[b] == 0) ++b;
-      if (b >= nb) return -1;
-      wi = b * kOutflowWords;
-    }
-    bits = words[wi].x;
-  }
-  return (wi << 5) + (__ffs(bits) - 1);
-}
-
-// Between q and the next survivor g above it, S is constant, so the chain
-// steps q, q + S, q + 2S, ... until it first reaches g or beyond: the kernel
-// jumps there directly (with survivors dense, that is the single hop
-// q + S(q)).  A pathological pattern -- say only the last particle survives --
-// then takes one jump instead of a walk over every position.
+// Between q and the next survivor above it S is constant, so the chain steps
+// q, q + S, q + 2S, ... until it first passes that survivor.  The step count k
+// is the smallest k >= 1 with a survivor in (q, q + kS], found by galloping
+// and bisection on kept_through (O(1) per probe).  With survivors dense the
+// first probe succeeds and the jump is the single hop q + S(q); a
+// pathological pattern -- say only the last particle survives -- takes a few
+// dozen probes instead of a walk over every position.
 template <class L>
 __global__ void __launch_bounds__(kOutflowThreads)
-    outflow_fill_kernel(L lay, long long n, const uint2* words, const int* block_counts, int nb,
-                        const int* block_offsets, const int* survivors, int* err) {
+    outflow_fill_kernel(L lay, long long n, const uint2* words, const int* block_offsets, const int* survivors,
+                        int* err) {
   const long long np = *survivors;
   const long long base = (long long)blockIdx.x * kOutflowTile;
   if (base >= np) return;
@@ -118,14 +100,43 @@ __global__ void __launch_bounds__(kOutflowThreads)
     bool found = false;
     // the chain rises strictly and stays below n, so n jumps always suffice
     for (long long hop = 0; hop < n; ++hop) {
-      const long long above = np - kept_through(block_offsets, s, w);
-      if (above < 1) break;  // not reachable from a hole below n'
-      const long long g = next_survivor(words, block_counts, s, nb);
-      if (g < 0) break;
-      const long long t = s + (g - s + above - 1) / above * above;
-      if (t >= n) break;
-      s = t;
-      w = words[s >> 5];
+      const long long kept = kept_through(block_offsets, s, w);
+      const long long above = np - kept;
+      if (above < 1) break;                    // not reachable from a hole below n'
+      const long long kmax = (n - 1 - s) / above;  // s + k * above stays below n
+      if (kmax < 1) break;
+      long long k = 1;
+      uint2 wt = words[(s + above) >> 5];
+      if (kept_through(block_offsets, s + above, wt) == kept) {
+        // no survivor within one hop: kept_through(s + lo S) == kept, find hi
+        long long lo = 1, hi = 2;
+        bool bracketed = false;
+        for (int g = 0; g < 64; ++g) {
+          const long long h = hi < kmax ? hi : kmax;
+          const long long t = s + h * above;
+          if (kept_through(block_offsets, t, words[t >> 5]) > kept) {
+            hi = h;
+            bracketed = true;
+            break;
+          }
+          if (h >= kmax) break;
+          lo = h;
+          hi = 2 * hi;
+        }
+        if (!bracketed) break;
+        while (hi - lo > 1) {
+          const long long mid = lo + (hi - lo) / 2;
+          const long long t = s + mid * above;
+          if (kept_through(block_offsets, t, words[t >> 5]) > kept)
+            hi = mid;
+          else
+            lo = mid;
+        }
+        k = hi;
+        wt = words[(s + k * above) >> 5];
+      }
+      s += k * above;
+      w = wt;
       if ((w.x >> (s & 31)) & 1u) {
         found = true;
         break;
@@ -151,7 +162,7 @@ cudaError_t launch_outflow_inplace(const L& lay, long long n, uint2* words, int*
   cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, count, block_offsets + nb + 1, st);
   if (e != cudaSuccess) return e;
   note_launch();
-  outflow_fill_kernel<<<nb, kOutflowThreads, 0, st>>>(lay, n, words, block_counts, nb, block_offsets, count, err);
+  outflow_fill_kernel<<<nb, kOutflowThreads, 0, st>>>(lay, n, words, block_offsets, count, err);
   return cudaGetLastError();
 }
 

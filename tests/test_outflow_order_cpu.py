@@ -3,9 +3,10 @@
 The kernels (picard_b200/csrc/outflow.cuh) fill every hole p below the
 survivor count n' with the particle reached from p by q -> q + S(q), S(q) the
 survivors above q, jumping in one step over the stretch where S stays
-constant (up to the first point at or beyond the next survivor).  This file
-models that rule with numpy (the same keep words, block offsets, block counts
-and jumps) and checks it against the oracle's literal
+constant (to the first point q + kS past the next survivor, k found by
+galloping and bisection on the survivor counts).  This file models that rule
+with numpy (the same keep words, block offsets and probes) and checks it
+against the oracle's literal
 BCoutflow loop (BCoutflow.f90:24-83: walk from the end, move the current last
 particle into each hole) on random and structured keep patterns.  Each
 particle carries its original index in vz, so the order is compared exactly.
@@ -39,36 +40,35 @@ def chase_model(keep: np.ndarray) -> np.ndarray:
         upto = w & ((1 << ((q & 31) + 1)) - 1)
         return int(block_offsets[q // TILE]) + int(word_before[q >> 5]) + bin(upto).count("1")
 
-    nwords = nb * (TILE // 32)
-
-    def next_survivor(s: int) -> int:
-        wi = s >> 5
-        sh = s & 31
-        b = 0 if sh == 31 else int(bits[wi]) & (0xFFFFFFFF << (sh + 1)) & 0xFFFFFFFF
-        while b == 0:
-            wi += 1
-            assert wi < nwords
-            if wi % (TILE // 32) == 0:  # skip blocks without survivors
-                blk = wi // (TILE // 32)
-                while blk < nb and block_counts[blk] == 0:
-                    blk += 1
-                assert blk < nb
-                wi = blk * (TILE // 32)
-            b = int(bits[wi])
-        return (wi << 5) + ((b & -b).bit_length() - 1)
-
     out = np.arange(np_)
     for p in range(np_):
         if keep[p]:
             continue
         s = p
         for _ in range(n):
-            above = np_ - kept_through(s)
+            kept = kept_through(s)
+            above = np_ - kept
             assert above >= 1
-            g = next_survivor(s)
-            t = s + (g - s + above - 1) // above * above
-            assert t < n
-            s = t
+            kmax = (n - 1 - s) // above
+            assert kmax >= 1
+            k = 1
+            if kept_through(s + above) == kept:
+                lo, hi = 1, 2
+                while True:
+                    h = min(hi, kmax)
+                    if kept_through(s + h * above) > kept:
+                        hi = h
+                        break
+                    assert h < kmax
+                    lo, hi = h, 2 * hi
+                while hi - lo > 1:
+                    mid = lo + (hi - lo) // 2
+                    if kept_through(s + mid * above) > kept:
+                        hi = mid
+                    else:
+                        lo = mid
+                k = hi
+            s += k * above
             if keep[s]:
                 break
         else:
