@@ -123,6 +123,12 @@ def patterns():
     k = np.ones(5 * TILE, bool)
     k[TILE // 2: 4 * TILE] = False
     out.append(k)
+    # the per-subroutine loop's shape: a bulk with a few per cent outflowing,
+    # then appended inflow candidates face by face, some faces removed almost
+    # entirely (long removed stretches far above the holes of the bulk)
+    bulk = rng.random(20000) > 0.03
+    faces = [rng.random(1500) > f for f in (0.1, 0.995, 0.5, 1.0, 0.98, 0.3)]
+    out.append(np.concatenate([bulk] + faces))
     return out
 
 
