@@ -78,9 +78,11 @@ def chase_model(keep: np.ndarray) -> np.ndarray:
 
 
 def oracle_order(keep: np.ndarray) -> np.ndarray:
-    p = O.derive(small_plasma(n=4, ppc=1, seed=1))
-    assert p.xflow
     n = len(keep)
+    p0 = small_plasma(n=4, ppc=1, seed=1)
+    p0.max_per_proc = max(p0.max_per_proc, n + 1)
+    p = O.derive(p0)
+    assert p.xflow
     rp = np.zeros((n, 8))
     rp[:, 0] = 0.5 * (p.xmin + p.xmax)
     rp[:, 1] = 0.5 * (p.ymin + p.ymax)
