@@ -32,6 +32,7 @@ UNITS = {
     "server.cu": [],
     "batch.cu": [],
     "output.cu": [],
+    "f90.cu": [],
 }
 
 
@@ -46,7 +47,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     headers = [os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith(".cuh")]
-    headers += [os.path.join(ROOT, "include", h) for h in ("picard_gpu.h", "picard_server.h", "picard_io.h")]
+    headers += [os.path.join(ROOT, "include", h) for h in ("picard_gpu.h", "picard_server.h", "picard_io.h", "picard_f90.h")]
     objs = []
     for unit, extra in UNITS.items():
         src = os.path.join(SRC, unit)
