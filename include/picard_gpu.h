@@ -188,14 +188,19 @@ PICARD_API int picard_gpu_advance_velocity_imp(picard_ctx* ctx, double deltat,
  * positions x, y, z and the 1-based species numbers (int_particles) of
  * num_local particles, and device outputs N (species x (Nx+2)(Ny+2)(Nz+2),
  * species fastest, as ParticlesGridify's N) and C ((Nx+2)(Ny+2)(Nz+2)); the
- * work is queued on `stream` (a cudaStream_t, NULL for the default stream).
+ * work is queued on `stream` (a cudaStream_t of the current device, NULL for
+ * its default stream; a stream of another device is not supported).
+ * Particles are expected where the reference deposits them, after BCoutflow
+ * and ParticlesTransfer: inside [min, max] on every axis.  A particle farther
+ * than half a cell outside the domain on some axis (NaN included), or whose
+ * species number is outside 1..species, is not deposited.
  * Scratch is one fixed array of PICARD_NOALLOC_MAX_WORDS int64 words that
  * every device holds from the first use of the library until exit; larger
- * grids are rejected with PICARD_ERR_BAD_ARG.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress), so make that
- * first call before any stream capture.  All calls share the array: calls
- * that overlap on the GPU race and must be ordered by the caller.  Particles
- * whose species number is outside 1..species are not deposited. */
+ * grids are rejected with PICARD_ERR_BAD_ARG.  Each call looks up the array's
+ * address on the current device (cudaGetSymbolAddress); the first call on a
+ * device also loads the library's device code there, so make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be ordered by the caller. */
 PICARD_API int picard_gpu_particles_gridify_noalloc(const picard_params* p, const double* x, const double* y,
                                                     const double* z, const int32_t* int_particles,
                                                     int32_t num_local, double* N, double* C, void* stream);
@@ -230,6 +235,7 @@ typedef struct picard_stats {
    * (advance, produce, outflow, wrap, inflow), deposit, BCpotentials, Jacobi
    * solve, E-field + velocity push */
   double phase_ms[5];
+  int64_t last_sweeps;     /* Jacobi iterations of the most recent solve     */
 } picard_stats;
 
 PICARD_API int picard_gpu_get_stats(picard_ctx* ctx, picard_stats* out);
@@ -268,7 +274,14 @@ typedef enum picard_option {
   /* 1: x-pair sweeps two at a time (one launch computes sweeps s and s+1 of
    * a tile, the intermediate iterate in shared memory); 0 one per launch.
    * Never changes a result bit. */
-  PICARD_OPT_SWEEP_FUSED = 6
+  PICARD_OPT_SWEEP_FUSED = 6,
+  /* Test of the bounded device waits.  1: the grid barrier of the
+   * register-resident sweep (PICARD_OPT_SWEEP_RESIDENT) waits for one
+   * arrival more than its grid makes, with a poll limit of 2^14 polls, so
+   * every CTA's wait runs out and returns; the solve then fails with
+   * PICARD_ERR_TIMEOUT and the context stays usable.  0 (the default): off.
+   * Nothing else uses it. */
+  PICARD_OPT_WAIT_TEST = 7
 } picard_option;
 /* Reads an option's current value (SWEEP_CTAS: 0 means one CTA per tile). */
 PICARD_API int picard_gpu_get_option(picard_ctx* ctx, int32_t option, int32_t* value);

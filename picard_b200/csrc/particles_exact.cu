@@ -632,9 +632,15 @@ __global__ void advance_velocity_f64_kernel(KParams P, PartF64 a, long long n, c
 // periodic axes fold them onto the opposite interior node (ibid. 167-170).
 __device__ inline int fold_index(int i, int n, int open) {
   if (open) return i < 1 ? 1 : (i > n ? n : i);
-  while (i < 1) i += n;
-  while (i > n) i -= n;
-  return i;
+  // periodic: the interior node congruent to i modulo n -- one period for
+  // the ghost layers, a closed-form remainder for anything farther out
+  if (i < 1)
+    i += n;
+  else if (i > n)
+    i -= n;
+  if (i >= 1 && i <= n) return i;
+  long long r = ((long long)i - 1) % n;
+  return int(r < 0 ? r + n : r) + 1;
 }
 
 // Warp-aggregated fixed-point deposit of 8 weights (each in [0, 2^40]) at
@@ -1020,7 +1026,6 @@ cudaError_t launch_f64_to_c32(const KParams& P, PartF64 a, long long n, PartC32 
 // particle arrays and the output grids from the caller and keeps its only
 // scratch -- the int64 fixed-point accumulators -- in the file-scope array
 // below, so it calls no cudaMalloc, cudaFree or allocating library routine.
-#include <mutex>
 #include <string>
 
 namespace picard {
@@ -1033,13 +1038,19 @@ namespace {
 // process exits.  All calls share it, so calls that overlap on the GPU race.
 static __device__ __align__(256) unsigned long long g_noalloc_acc[PICARD_NOALLOC_MAX_WORDS];
 
-// Device address of g_noalloc_acc, looked up once per device.
-std::mutex g_noalloc_mutex;
-constexpr int kNoAllocMaxDevices = 64;
-unsigned long long* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+// True when x lies within half a cell of [L_min, L_max] (NaN: false).  There
+// the CIC base node is 0 .. n and both stencil nodes lie inside the
+// ghost-padded box, with non-negative weights.  The reference deposits after
+// BCoutflow and ParticlesTransfer, which leave every particle inside
+// [min, max], so its particles always pass.
+__device__ inline bool within_half_cell(double x, double lo, double hi, double d) {
+  return x >= lo - 0.5 * d && x < hi + 0.5 * d;
+}
 
 // ParticlesGridify.f90:65-123 for caller-owned FP64 arrays; int_particles
-// holds the reference's 1-based species numbers, others are not deposited.
+// holds the reference's 1-based species numbers.  Particles of another
+// species number, or farther than half a cell outside the domain on some
+// axis, are not deposited.
 __global__ void deposit_noalloc_kernel(KParams P, const double* __restrict__ x, const double* __restrict__ y,
                                        const double* __restrict__ z, const int32_t* __restrict__ sp1, long long n,
                                        unsigned long long* acc) {
@@ -1048,11 +1059,19 @@ __global__ void deposit_noalloc_kernel(KParams P, const double* __restrict__ x, 
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n_round; p += stride) {
     int s = (p < n) ? sp1[p] - 1 : -1;
     bool active = s >= 0 && s < P.species;
+    double xp = 0.0, yp = 0.0, zp = 0.0;
+    if (active) {
+      xp = x[p];
+      yp = y[p];
+      zp = z[p];
+      active = within_half_cell(xp, P.Lx_min, P.Lx_max, P.dx) && within_half_cell(yp, P.Ly_min, P.Ly_max, P.dy) &&
+               within_half_cell(zp, P.Lz_min, P.Lz_max, P.dz);
+    }
     long long w[8] = {0, 0, 0, 0, 0, 0, 0, 0}, nodes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     unsigned long long key = ~0ull;
     if (active) {
       Cic64 c;
-      cic64(P, x[p], y[p], z[p], c);
+      cic64(P, xp, yp, zp, c);
       for (int q = 0; q < 8; ++q) {
         w[q] = __double2ll_rn(c.F[q] / P.dV * kDepositScale);
         int i = fold_index(c.i + kOff[q][0], P.nx, P.xflow), j = fold_index(c.j + kOff[q][1], P.ny, P.yflow),
@@ -1109,23 +1128,15 @@ extern "C" int picard_gpu_particles_gridify_noalloc(const picard_params* p, cons
   if (num_local < 0) return fail(PICARD_ERR_BAD_ARG, "num_local must be >= 0");
   if (num_local > 0 && (!x || !y || !z || !int_particles)) return fail(PICARD_ERR_BAD_ARG, "particle array is NULL");
   if (!N || !C) return fail(PICARD_ERR_BAD_ARG, "output array is NULL");
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return fail(PICARD_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(PICARD_ERR_BAD_ARG, "device ordinal out of range");
-  unsigned long long* acc = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-      // the host-side name of the array is not a device address: look the
-      // address up on this device (once), with this device current
-      void* q = nullptr;
-      e = cudaGetSymbolAddress(&q, g_noalloc_acc);
-      if (e != cudaSuccess) return fail(PICARD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      g_noalloc_ptr[dev] = static_cast<unsigned long long*>(q);
-    }
-    acc = g_noalloc_ptr[dev];
-  }
+  // The array's host-side name is not a device address.  Its address on the
+  // current device is looked up on every call (a table lookup once the
+  // library's device code is loaded), so nothing cached outlives a
+  // cudaDeviceReset.  The first call on a device loads that code: make it
+  // before any stream capture.
+  void* q = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&q, g_noalloc_acc);
+  if (e != cudaSuccess) return fail(PICARD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  unsigned long long* acc = static_cast<unsigned long long*>(q);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const KParams K = make_kparams(*p);
   // the array keeps the previous call's sums: clear the part this call uses

@@ -136,9 +136,10 @@ __device__ inline void move_axis(int& i, float& f, float d, int n, int open) {
   if (open) {
     if (i < -1) i = -1, t = 0.0f;
     if (i > n + 1) i = n + 1, t = 0.5f;
-  } else {
-    while (i < -1) i += n;
-    while (i > n + 1) i -= n;
+  } else if (i < -1) {  // whole periods up to the first index >= -1
+    i = int((long long)i + (long long)n * ((-1LL - i + n - 1) / n));
+  } else if (i > n + 1) {  // whole periods down to the first index <= n + 1
+    i = int((long long)i - (long long)n * (((long long)i - n - 1 + n - 1) / n));
   }
   f = t;
 }
@@ -364,9 +365,15 @@ __global__ void __launch_bounds__(256, 8) push_advance_c32_kernel(KParams P, Spe
 
 __device__ inline int fold_index(int i, int n, int open) {
   if (open) return i < 1 ? 1 : (i > n ? n : i);
-  while (i < 1) i += n;
-  while (i > n) i -= n;
-  return i;
+  // periodic: the interior node congruent to i modulo n -- one period for
+  // the ghost layers, a closed-form remainder for anything farther out
+  if (i < 1)
+    i += n;
+  else if (i > n)
+    i -= n;
+  if (i >= 1 && i <= n) return i;
+  long long r = ((long long)i - 1) % n;
+  return int(r < 0 ? r + n : r) + 1;
 }
 
 __device__ inline unsigned long long stencil_key(int i, int j, int k, int s) {

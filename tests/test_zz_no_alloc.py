@@ -53,8 +53,10 @@ def _reference_deposit(p, rp, ip):
     return out
 
 
-def test_noalloc_deposit_matches_context_deposit_twice():
-    p = O.derive(small_plasma(n=12, ppc=4, seed=17, yflow=0))
+@pytest.mark.parametrize("periodic", [None, "x", "y"])
+def test_noalloc_deposit_matches_context_deposit_twice(periodic):
+    kw = {} if periodic is None else {periodic + "flow": 0}
+    p = O.derive(small_plasma(n=12, ppc=4, seed=17, **kw))
     o = O.OracleState(p)
     o.calc_distance()
     o.initialize()
@@ -71,6 +73,38 @@ def test_noalloc_deposit_matches_context_deposit_twice():
         assert rel_l2(N, N_ref) < 1e-10
         scale = max(abs(p.charge[s]) * np.abs(N_ref[..., s]).max() for s in range(p.species))
         assert np.abs(Cg - C_ref).max() < 1e-10 * scale
+        # and against the oracle's own ParticlesGridify on the same arrays
+        o2 = O.OracleState(p)
+        o2.set_particles(rp, ip)
+        o2.gridify()
+        assert rel_l2(N, o2.N) < 1e-10
+        assert np.abs(Cg - o2.C).max() < 1e-10 * scale
+
+
+def test_noalloc_skips_foreign_species_and_far_out_particles():
+    # Particles of species number 0 or species+1, and particles farther than
+    # half a cell outside the domain on an axis (a periodic one included, and
+    # NaN), leave N and C exactly as the deposit of the others.
+    p = O.derive(small_plasma(n=10, ppc=3, seed=23, xflow=0))
+    o = O.OracleState(p)
+    o.calc_distance()
+    o.initialize()
+    o.step(1)
+    rp, ip = o.particles()
+    N0, C0 = _noalloc(p, rp, ip)
+    extra_r = np.repeat(rp[:1], 7, axis=0).copy()
+    extra_i = np.array([0, p.species + 1, 1, 2, 1, 2, 1], np.int32)
+    d = p.dxyz[0]
+    extra_r[2, 0] = p.Lx_max + 3.0 * d          # periodic x, three cells out
+    extra_r[3, 0] = p.Lx_min - 0.75 * d         # periodic x, below half a cell
+    extra_r[4, 1] = p.Ly_max + 1e30             # open y, far out
+    extra_r[5, 2] = float("nan")
+    extra_r[6, 0] = -1e300                      # periodic x, far beyond any period count
+    rp2 = np.concatenate([extra_r[:4], rp, extra_r[4:]])
+    ip2 = np.concatenate([extra_i[:4], ip, extra_i[4:]])
+    N1, C1 = _noalloc(p, rp2, ip2)
+    np.testing.assert_array_equal(N1, N0)
+    np.testing.assert_array_equal(C1, C0)
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
