@@ -36,6 +36,7 @@ OPT_SWEEP_STAGES = 3
 OPT_SWEEP_RESIDENT = 4
 OPT_SWEEP_PAIRS = 5
 OPT_SWEEP_FUSED = 6
+OPT_WAIT_TEST = 7
 
 class PicardStats(C.Structure):
     _fields_ = [
@@ -53,6 +54,7 @@ class PicardStats(C.Structure):
         ("h2d_bytes", C.c_int64),
         ("d2h_bytes", C.c_int64),
         ("phase_ms", C.c_double * 5),
+        ("last_sweeps", C.c_int64),
     ]
 
     PHASES = ("particles", "deposit", "bc_potentials", "jacobi", "field_push")

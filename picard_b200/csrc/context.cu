@@ -475,6 +475,7 @@ int picard_gpu_get_stats(picard_ctx* c, picard_stats* out) {
   if (!c || !out) return fail(PICARD_ERR_BAD_ARG, "NULL argument");
   *out = c->stats;
   out->kernel_launches = launches_so_far() - c->launches_at_reset;
+  out->last_sweeps = c->last_sweeps;
   return PICARD_OK;
 }
 
@@ -810,6 +811,11 @@ int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
     c->G.stages = value;
     return PICARD_OK;
   }
+  if (option == PICARD_OPT_WAIT_TEST) {
+    if (value != 0 && value != 1) return fail(PICARD_ERR_BAD_ARG, "WAIT_TEST must be 0 or 1");
+    c->wait_test = value;
+    return PICARD_OK;
+  }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");
 }
 
@@ -823,6 +829,7 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
     case PICARD_OPT_SWEEP_PAIRS: *value = c->G.pairs; return PICARD_OK;
     case PICARD_OPT_SWEEP_FUSED: *value = c->G.fused2; return PICARD_OK;
     case PICARD_OPT_SWEEP_RESIDENT: *value = resident_option_value(c); return PICARD_OK;
+    case PICARD_OPT_WAIT_TEST: *value = c->wait_test; return PICARD_OK;
   }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");
 }

@@ -70,6 +70,7 @@ struct picard_ctx {
   unsigned int* res_bar = nullptr;
   long long res_faces_cap = 0;  // floats
 
+  int wait_test = 0;  // PICARD_OPT_WAIT_TEST
   // tensor-core BCpotentials (bcpot_tc.cu)
   int bcpot_tensor = 0;
   void* tc_cs = nullptr;

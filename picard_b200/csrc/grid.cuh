@@ -46,7 +46,7 @@ long long resident_face_floats(const JacobiGeom& G);
 // sweep to wout.  bar: one counter, zeroed here.
 cudaError_t launch_sweeps_resident(const KParams& P, const JacobiGeom& G, const float* r, const float* win,
                                    float* wout, float* faces, unsigned int* bar, double* partial, int m, int w_zero,
-                                   int* err, cudaStream_t st);
+                                   int* err, cudaStream_t st, int wait_test = 0);
 // The x-pair TMA sweep (64-wide tiles; w boxes 72 x 10 x zc+2, r boxes 64 x
 // 8 x zc): launch, occupancy and tile count.  Writes the same partials (in
 // the 32-wide tile layout) as launch_sweep_tma.

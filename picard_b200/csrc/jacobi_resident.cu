@@ -25,6 +25,8 @@
 // that each CTA's elected thread increments and then polls with acquire
 // loads.  The poll is bounded: past the limit the CTA records kDevTimeout in
 // *err and returns; the other CTAs then give up at their own next barrier.
+// The wait test (PICARD_OPT_WAIT_TEST) makes every CTA's first wait run out
+// on purpose, with a short limit, so that the timeout path can be tested.
 // All CTAs are co-resident by construction of the cooperative launch.
 #include <cuda_runtime.h>
 
@@ -40,6 +42,10 @@ namespace {
 
 constexpr int kResG = 4;                 // planes per shared-memory exchange group
 constexpr long long kBarSpin = 1LL << 22;
+// Poll limit of the wait test (PICARD_OPT_WAIT_TEST): the barrier then waits
+// for one arrival more than the grid makes, so every CTA gives up after this
+// many polls and returns.
+constexpr long long kBarSpinTest = 1LL << 14;
 
 template <int BY, int NZ, int ZC>
 struct ResLayout {
@@ -68,6 +74,8 @@ struct ResArgs {
   unsigned int* bar;   // grid barrier counter, zero at launch
   double* partial;     // [m][ntiles]
   int* err;
+  unsigned int bar_extra;  // arrivals the barrier waits for beyond the grid's (0; 1 only in the wait test)
+  long long spin;          // poll limit of one barrier wait
   int m, w_zero;
   int gx, gy, gz, ntiles;  // tile grid of the TMA sweep kernel
   int cgx, cgy, cgz;       // CTA grid
@@ -81,13 +89,13 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
 
 // Every CTA of the grid arrives; returns false (uniformly over the CTA) when
 // the wait gave up.
-__device__ bool grid_barrier(unsigned int* bar, unsigned int target, int* err, int* s_abort) {
+__device__ bool grid_barrier(unsigned int* bar, unsigned int target, long long spin, int* err, int* s_abort) {
   __syncthreads();
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     __threadfence();
     atomicAdd(bar, 1u);
     bool ok = false;
-    for (long long it = 0; it < kBarSpin; ++it) {
+    for (long long it = 0; it < spin; ++it) {
       if (ld_acquire(bar) >= target) {
         ok = true;
         break;
@@ -275,7 +283,7 @@ __global__ void __launch_bounds__(32 * BY, 1) jacobi_resident_kernel(ResArgs a) 
 
     // ---- every CTA finished this sweep (after the last one too: the final
     // store below may overwrite the array the first sweep read halos from)
-    if (!grid_barrier(a.bar, (unsigned int)(s + 1) * gridDim.x, a.err, &s_abort)) return;
+    if (!grid_barrier(a.bar, (unsigned int)(s + 1) * gridDim.x + a.bar_extra, a.spin, a.err, &s_abort)) return;
     if (s + 1 < a.m) stage_from_faces<BY, NZ, ZC>(a, s, xh, yh, zlo, zhi);
   }
 
@@ -356,7 +364,7 @@ long long resident_face_floats(const JacobiGeom& G) {
 
 cudaError_t launch_sweeps_resident(const KParams& P, const JacobiGeom& G, const float* r, const float* win,
                                    float* wout, float* faces, unsigned int* bar, double* partial, int m, int w_zero,
-                                   int* err, cudaStream_t st) {
+                                   int* err, cudaStream_t st, int wait_test) {
   if (!G.res || m < 1) return cudaErrorInvalidValue;
   const ResKernel k = pick_kernel(G.res_by, G.res_nz, G.zc);
   if (!k.fn) return cudaErrorInvalidValue;
@@ -372,6 +380,8 @@ cudaError_t launch_sweeps_resident(const KParams& P, const JacobiGeom& G, const 
   a.bar = bar;
   a.partial = partial;
   a.err = err;
+  a.bar_extra = wait_test ? 1u : 0u;
+  a.spin = wait_test ? kBarSpinTest : kBarSpin;
   a.m = m;
   a.w_zero = w_zero;
   a.gx = (int)G.grid.x;

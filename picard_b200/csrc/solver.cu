@@ -175,7 +175,7 @@ int run_sweeps_single(picard_ctx* c, int count, int rsel, double* partial_base, 
     std::lock_guard<std::mutex> lk(g_resident_mu);
     const int out = 1 - *wcur;
     PICARD_CUDA(launch_sweeps_resident(K, c->G, R[rsel], nullptr, c->w[out], c->res_faces, c->res_bar, partial_base,
-                                       count, 1, c->d_err, c->st));
+                                       count, 1, c->d_err, c->st, c->wait_test));
     PICARD_CUDA(cudaStreamSynchronize(c->st));
     *wcur = out;
     return PICARD_OK;

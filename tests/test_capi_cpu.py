@@ -113,7 +113,8 @@ int main(void) {
   printf("picard_result %zu\n", sizeof(picard_result));
   F(picard_request, params); F(picard_request, layout); F(picard_request, steps); F(picard_request, arrival_ms);
   F(picard_result, status); F(picard_result, sweeps); F(picard_result, energy); F(picard_result, u_abs_sum); F(picard_result, warnings); F(picard_result, shard);
-  F(picard_stats, phase_ms); F(picard_params, u0);
+  F(picard_stats, phase_ms); F(picard_stats, last_sweeps);
+  PARAMS_FIELDS
   return 0;
 }
 """
@@ -123,7 +124,10 @@ def test_ctypes_structs_match_the_c_compiler(tmp_path):
     """Every struct that crosses the C ABI has the size and field offsets gcc
     gives it from the headers."""
     src = tmp_path / "probe.c"
-    src.write_text(_LAYOUT_PROBE)
+    # every field of picard_params: the Fortran derived type of the
+    # integration module mirrors this block field for field
+    fields = " ".join(f"F(picard_params, {name});" for name, _ in P.PicardParams._fields_)
+    src.write_text(_LAYOUT_PROBE.replace("PARAMS_FIELDS", fields))
     exe = tmp_path / "probe"
     subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
