@@ -66,6 +66,13 @@ def parse_args():
     ap.add_argument("--layout", choices=["cell32", "f64"], default="cell32")
     ap.add_argument("--solver", choices=["refine", "f64"], default="refine")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-phi", action="store_true", help="skip the FP64 check of the timed run's potential")
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served and batched blocks of the default (N=1) line")
+    ap.add_argument("--served-requests", type=int, default=16, help="default line: runs in the serving stream")
+    ap.add_argument("--served-steps", type=int, default=200, help="default line: iterations per served run")
+    ap.add_argument("--batched-runs", type=int, default=64, help="default line: runs of the batched sweep")
+    ap.add_argument("--batched-steps", type=int, default=20, help="default line: iterations per batched run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=25.0, help="rough budget of the CPU baseline sample")
     ap.add_argument("--ppc", type=int, default=None,
@@ -79,11 +86,12 @@ def workload(name: str, seed: int, ppc: int | None = None):
     if name == "scale":
         p = P.config_plain_scale(seed=seed) if ppc is None else P.config_plain_scale(seed=seed, ppc_ion=ppc)
         desc = {"workload": "plain-at-scale 256x128x128 cells, 64 ppc (32 H+ + 32 e-), Haser source Q=1e27/s",
-                "grid": [256, 128, 128], "ppc_total": 64, "species": 3}
+                "grid": [256, 128, 128], "ppc_total": 64, "species": 3,
+                "l2": "particle arrays (7.8 GB) exceed L2; the Jacobi working set (52 MB) is L2-resident"}
     else:
         p = P.config_plain_32(seed=seed)
         desc = {"workload": "plain 32^3 cells, 16 ppc per species (H+, e-)", "grid": [32, 32, 32],
-                "ppc_total": 32, "species": 2}
+                "ppc_total": 32, "species": 2, "l2": "every working set fits in L2"}
     return p, desc
 
 
@@ -216,9 +224,13 @@ def run_picard(args, rank, world, local_rank):
     alg_bytes = bytes_per_node * cells
     achieved = alg_bytes / (sweep_avg_ms * 1e-3) / 1e9 if sweep_avg_ms > 0 else 0.0
     num_final = sim.num_local
+    phi = None
+    if not args.no_phi:
+        phi = phi_check(sim, p, desc)
     sim.close()
     del sim
     torch.cuda.synchronize()
+    l2_gbs = l2_copy_gbs(torch)
 
     # end to end through the reference-facing entry points (picard_gpu_run:
     # the per-subroutine call sequence of picard.f90), from the host-side
@@ -263,6 +275,12 @@ def run_picard(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, sweeps_per_step=sweeps_per_step)
+    served = batched = None
+    if rank == 0 and world == 1 and not args.no_served and args.workload == "scale":
+        # the headline comparison on one GPU: the same runs served, batched
+        # and run one after another through the per-subroutine loop
+        served = serving_measure(args, local_rank, args.served_requests, args.served_steps)
+        batched = batch_measure(args, local_rank, args.batched_runs, args.batched_steps)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -271,10 +289,9 @@ def run_picard(args, rank, world, local_rank):
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 particles, f32 Jacobi sweeps with f64 anchors" if args.layout == "cell32" else "f64",
             "data": "synthetic (seeded Philox plasma, seed = rank)",
-            "config": dict(desc, layout=args.layout, solver=args.solver, runs_per_gpu=1,
-                           l2="particle arrays (7.8 GB) exceed L2; the Jacobi working set (52 MB) is L2-resident",
-                           parallelism=f"independent runs x{world}"),
+            "config": line_config(desc, world),
             "impl": "picard",
+            "layout": args.layout, "solver": args.solver,
             "gpu_launches": st["kernel_launches"],
             "jacobi_sweeps_per_step": sweeps_per_step,
             "phase_ms_per_step": {k: round(v / K, 3) for k, v in st["phase_ms"].items()},
@@ -290,14 +307,90 @@ def run_picard(args, rank, world, local_rank):
                                            "the sweep kernel on this grid (caches flushed by the replay; in the "
                                            "live loop the 52 MB working set stays in L2)",
                          "note": "the sweep's working set is L2-resident, so achieved algorithmic bytes can "
-                                 "exceed the HBM copy rate (frac > 1)"},
+                                 "exceed the HBM copy rate (frac > 1); l2_frac is the same achieved rate over a "
+                                 "device copy whose buffers stay in L2, measured in this run",
+                         "l2_copy_gbs": l2_gbs, "l2_frac": achieved / l2_gbs if l2_gbs else None},
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "phi_check": phi,
         }
+        if served is not None:
+            line["served"] = compact_serving(served)
+        if batched is not None:
+            line["batched"] = compact_batch(batched)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
+
+
+def phi_check(sim, p, desc) -> dict:
+    """The timed run's last potential against an all-FP64 solve of the same
+    charge density: FP64 BCpotentials (direct sum) and FP64 Jacobi sweeps
+    (SOLVER_F64, whose sweeps and stopping rule equal the oracle's) from the
+    run's C, with the reference's tolerance maxerr.  The bar is 1e-6 relative
+    L2 (the potential's tolerance)."""
+    import numpy as np
+
+    from picard_b200 import capi
+    from picard_b200.simulation import Simulation
+
+    U = sim.field(capi.FIELD_U)
+    Cd = sim.field(capi.FIELD_C)
+    sweeps_run = sim.stats()["last_sweeps"]
+    q = p.copy()
+    q.max_per_proc = 1024
+    ref = Simulation(q, layout=capi.LAYOUT_F64, solver=capi.SOLVER_F64)
+    ref.calc_distance()
+    ref.set_field(capi.FIELD_C, Cd)
+    ref.set_option(capi.OPT_BCPOT_TENSOR, 0)
+    t0 = time.perf_counter()
+    ref.bc_potentials()
+    sweeps64 = ref.calc_epotential()
+    ref.synchronize()
+    t64 = time.perf_counter() - t0
+    U64 = ref.field(capi.FIELD_U)
+    ref.close()
+    d = U - U64
+    rel = float(np.linalg.norm(d.ravel()) / np.linalg.norm(U64.ravel()))
+    return {"rel_l2": rel, "max_rel": float(np.abs(d).max() / np.abs(U64).max()), "bar": 1e-6, "ok": rel <= 1e-6,
+            "sweeps_fp64": sweeps64, "sweeps_timed_run_last_solve": sweeps_run, "fp64_solve_s": round(t64, 3),
+            "what": "U after the last timed iteration (tensor-core BCpotentials, FP32 sweeps with FP64 anchors) vs "
+                    "FP64 BCpotentials + FP64 Jacobi (SOLVER_F64) from the same C"}
+
+
+def l2_copy_gbs(torch) -> float:
+    """Device copy rate with both buffers resident in L2 (2 x 24 MiB, copied
+    back and forth): read + write bytes over CUDA-event time.  The ceiling
+    of a kernel whose working set stays in L2."""
+    n = 24 * 2 ** 20 // 4
+    a = torch.ones(n, dtype=torch.float32, device="cuda")
+    b = torch.zeros_like(a)
+    for _ in range(20):
+        b.copy_(a)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 400
+    e0.record()
+    for i in range(reps):
+        (b if i % 2 == 0 else a).copy_(a if i % 2 == 0 else b)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    del a, b
+    return 2.0 * n * 4 * reps / (ms * 1e-3) / 1e9
+
+
+def compact_serving(d: dict) -> dict:
+    keys = ("config", "served", "batched_served", "plain", "served_over_plain", "batched_served_over_plain",
+            "offered_load", "u_sum_max_rel_diff_served_vs_plain", "clocks")
+    return {k: d[k] for k in keys if k in d}
+
+
+def compact_batch(d: dict) -> dict:
+    keys = ("config", "batched", "plain", "fused", "batched_over_plain", "batched_over_fused",
+            "results_identical_to_fused", "jacobi_sweeps_total", "clocks")
+    return {k: d[k] for k in keys if k in d}
 
 
 # ----------------------------------------------------------- CPU baseline
@@ -446,9 +539,14 @@ def run_poisson(args, local_rank):
 
 
 def run_serving(args, local_rank):
-    """Serving workload: a Poisson stream of parameter-sweep runs (cubic grids
-    of 24..128 cells, 8..64 ppc, Haser Q log-uniform in [1e25, 1e28] s^-1,
-    --run-steps iterations each) served three ways on one GPU.
+    print(json.dumps(serving_measure(args, local_rank, args.requests, args.run_steps)), flush=True)
+
+
+def serving_measure(args, local_rank, requests: int, run_steps: int) -> dict:
+    """Serving workload: a Poisson stream of `requests` parameter-sweep runs
+    (cubic grids of 24..128 cells, 8..64 ppc, Haser Q log-uniform in
+    [1e25, 1e28] s^-1, `run_steps` iterations each) served three ways on one
+    GPU.
       plain:  one run after another through picard_gpu_run (the per-subroutine
               call sequence of picard.f90), the arrival stream replayed against
               the measured service times;
@@ -470,12 +568,12 @@ def run_serving(args, local_rank):
     from picard_b200.simulation import Simulation
 
     torch.cuda.set_device(local_rank)
-    stream = P.serving_stream(seed=0, count=args.requests, rate_per_s=args.rate)
+    stream = P.serving_stream(seed=0, count=requests, rate_per_s=args.rate)
     reqs = []
     for t, p, steps in stream:
-        if args.run_steps != steps:
-            p = P._size_capacity(p, args.run_steps, max(1, int(p.ppc[1])))
-        reqs.append((t, capi.params_derive(p), args.run_steps))
+        if run_steps != steps:
+            p = P._size_capacity(p, run_steps, max(1, int(p.ppc[1])))
+        reqs.append((t, capi.params_derive(p), run_steps))
     layout, solver = capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE
 
     # warm-up, untimed: load the kernels, and run the sweep launch tuner once per
@@ -557,7 +655,7 @@ def run_serving(args, local_rank):
         "data": "synthetic (seeded Philox plasma, run seeds 0..requests-1)",
         "config": {"workload": f"serving stream: {len(reqs)} runs, Poisson arrivals {args.rate}/s, cubic grids "
                                f"24..128 cells, 8..64 ppc, Haser Q log-uniform [1e25, 1e28] s^-1, "
-                               f"{args.run_steps} steps each",
+                               f"{run_steps} steps each",
                    "grids": [int(p.nx) for _, p, _ in reqs], "budget_gb": args.budget_gb, "slots": args.slots,
                    "batch_slots": args.batch_slots, "preparers": args.preparers},
         "served": {"particle_steps_per_s": served_tput, "makespan_s": served_makespan,
@@ -576,7 +674,7 @@ def run_serving(args, local_rank):
         "u_sum_max_rel_diff_served_vs_plain": u_diff,
         "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_precision(args, local_rank):
@@ -657,9 +755,13 @@ def run_precision(args, local_rank):
 
 
 def run_batch(args, local_rank):
-    """Batched parameter sweep: --runs independent runs (cubic grids 16..96
+    print(json.dumps(batch_measure(args, local_rank, args.runs, args.run_steps)), flush=True)
+
+
+def batch_measure(args, local_rank, nruns: int, run_steps: int) -> dict:
+    """Batched parameter sweep: `nruns` independent runs (cubic grids 16..96
     cells, 8..32 ppc, drift 300..800 km/s, |B| 1..10 nT in a random direction,
-    --run-steps iterations each, CELL32 / F32_REFINE) advanced two ways:
+    `run_steps` iterations each, CELL32 / F32_REFINE) advanced two ways:
       plain:   one run after another through picard_gpu_run, the
                per-subroutine call sequence of picard.f90 (the drop-in loop);
       fused:   one run after another through picard_gpu_run_fused (the
@@ -680,13 +782,13 @@ def run_batch(args, local_rank):
     from picard_b200.simulation import Simulation, batch_run_fused
 
     torch.cuda.set_device(local_rank)
-    sets = P.batch_set(seed=0, count=args.runs)
+    sets = P.batch_set(seed=0, count=nruns)
     runs = []
     for p, steps in sets:
-        if args.run_steps != steps:
-            p = P._size_capacity(p, args.run_steps, max(1, int(p.ppc[1])))
+        if run_steps != steps:
+            p = P._size_capacity(p, run_steps, max(1, int(p.ppc[1])))
         runs.append(capi.params_derive(p))
-    steps = args.run_steps
+    steps = run_steps
     layout, solver = capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE
     # warm-up, untimed: kernels loaded, and the sweep launch tuner run once per
     # grid shape (its choices are cached for the process), so that neither
@@ -780,7 +882,7 @@ def run_batch(args, local_rank):
         "mismatches": mism[:8],
         "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_bcpot(args, local_rank):
@@ -861,23 +963,75 @@ def run_deposit(args, local_rank):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: one complete full-size iteration of the loop
+    (picard.f90:554-674) on the FP64 CPU oracle with every host thread --
+    every phase in full (BCpotentials over every face node, Jacobi to the
+    reference's stopping rule), nothing sampled or extrapolated.  The untimed
+    warm-up is the oracle's setup (CalcDistance, ParticlesInitialize).  The
+    K timed steps together perform that one iteration (each step is 1/K of
+    its work), so ms_per_step = T/K and value = particles x 1 iteration / T.
+    Under torchrun only rank 0 runs."""
     if rank != 0:
         return
+    from oracle import oracle as O
+
     W, K = args.warmup, args.steps
-    # every timed step is a full-size sampled iteration; at most 3 keep the run
-    # within a few minutes (the oracle's setup of 268M particles is untimed)
-    c = cpu_baseline(args, steps=max(1, min(K, 3)))
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
     p, desc = workload(args.workload, seed=0)
+    p = O.derive(p)
+    s = O.OracleState(p)
+    t0 = time.perf_counter()
+    s.calc_distance()
+    s.initialize()
+    setup_s = time.perf_counter() - t0
+    it = 1
+    ph = {}
+
+    def timed(name, fn):
+        a = time.perf_counter()
+        r = fn()
+        ph[name] = time.perf_counter() - a
+        return r
+
+    timed("inflow", lambda: s.bc_inflow(it))
+    timed("advance", lambda: s.advance_position())
+    timed("produce", lambda: s.produce(it))
+    timed("outflow", lambda: s.bc_outflow())
+    timed("transfer", lambda: s.transfer())
+    timed("gridify", lambda: s.gridify())
+    timed("bcpot", lambda: s.bc_potentials())
+    sweeps, conv, _ = timed("jacobi", lambda: s.calc_epotential())
+    timed("efield", lambda: (s.calc_efield(), s.bc_fields()))
+    timed("velocity", lambda: s.advance_velocity())
+    total = sum(ph.values())
+    particle_steps = s.num_local
+    value = particle_steps / total
+    sample = (f"one complete full-size iteration (iteration 1 after ParticlesInitialize, {particle_steps} "
+              f"particles) on the FP64 oracle with {threads} threads: every phase in full, BCpotentials over all "
+              f"face nodes, Jacobi {sweeps} sweeps to the reference's stopping rule (converged: {conv}); the "
+              f"{K} timed steps together are that iteration (each 1/{K} of its work); warm-up = the oracle's "
+              f"setup ({setup_s:.1f} s, untimed)")
+    cpu = {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+           "seconds_per_iteration": total, "phase_seconds": {k: round(v, 4) for k, v in ph.items()},
+           "jacobi_sweeps": sweeps}
     line = {
-        "metric": METRIC, "value": c["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-        "ms_per_step": c["seconds_per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": total * 1e3 / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox plasma, seed 0)",
-        "config": dict(desc, layout="f64", solver="f64", parallelism="host threads"),
+        "config": line_config(desc, world),
         "impl": "reference",
-        "cpu_baseline": c,
-        "e2e": {"value": c["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "arithmetic": "FP64 particles (reference layout), FP64 BCpotentials and Jacobi",
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def line_config(desc: dict, world: int) -> dict:
+    """The workload named in both arms' lines (implementation choices such as
+    the particle layout and the solver precision are reported beside it)."""
+    return dict(desc, runs_per_gpu=1, parallelism=f"independent runs x{world}")
 
 
 def main():

@@ -40,3 +40,29 @@ def cell_indices(p: P.PicardParams, rp: np.ndarray) -> np.ndarray:
     lo = np.array([p.Lx_min, p.Ly_min, p.Lz_min])
     d = np.array(list(p.dxyz))
     return 1 + ((rp[:, :3] - lo) / d + 0.5).astype(np.int64)
+
+
+
+def unmatched_particles(ra: np.ndarray, ia: np.ndarray, rb: np.ndarray, ib: np.ndarray, pos_atol: float,
+                        vel_atol: float) -> int:
+    """Particles of either set without a partner in the other.  Partners have
+    the same species, are each other's nearest neighbour in (position /
+    pos_atol, velocity / vel_atol) space, and lie within ``pos_atol`` of each
+    other on every position axis and within ``vel_atol`` on every velocity
+    axis."""
+    from scipy.spatial import cKDTree
+
+    miss = 0
+    for s in np.union1d(np.unique(ia), np.unique(ib)):
+        a = ra[ia == s, :6] / np.array([pos_atol] * 3 + [vel_atol] * 3)
+        b = rb[ib == s, :6] / np.array([pos_atol] * 3 + [vel_atol] * 3)
+        if len(a) == 0 or len(b) == 0:
+            miss += len(a) + len(b)
+            continue
+        _, ab = cKDTree(b).query(a)
+        _, ba = cKDTree(a).query(b)
+        mutual = ba[ab] == np.arange(len(a))
+        close = np.all(np.abs(a - b[ab]) <= 1.0, axis=1)
+        matched = int(np.count_nonzero(mutual & close))
+        miss += (len(a) - matched) + (len(b) - matched)
+    return miss
