@@ -128,11 +128,21 @@ struct PartF64 {
   double *x, *y, *z, *vx, *vy, *vz;
   int8_t* sp;
 };
+// CELL32 particles: packed base node, in-cell offsets as 32-bit fixed point
+// (f / 2^32 in [0, 1) of a cell), FP32 velocities, species.
 struct PartC32 {
   uint32_t* cell;
-  float *fx, *fy, *fz, *vx, *vy, *vz;
+  uint32_t *fx, *fy, *fz;
+  float *vx, *vy, *vz;
   int8_t* sp;
 };
+
+// In-cell offset 1/2 (the cell centre of the reference's node spacing).
+constexpr uint32_t kOffHalf = 0x80000000u;
+
+// An in-cell offset as FP64 (exact) and as FP32 (its leading 23 bits).
+__host__ __device__ inline double off_f64(uint32_t f) { return (double)f * (1.0 / 4294967296.0); }
+__device__ inline float off_f32(uint32_t f) { return __uint_as_float((f >> 9) | 0x3F800000u) - 1.0f; }
 
 // Process-wide count of kernels launched by this library (every launch
 // wrapper calls it once per launch); reported by picard_gpu_get_stats.

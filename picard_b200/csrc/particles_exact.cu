@@ -112,30 +112,36 @@ __device__ inline void store_f64(PartF64 o, long long slot, const double x[3], c
 }
 
 // Base node (floor) and in-cell fraction of one coordinate, for CELL32.
-__device__ inline void to_cell(double x, double lmin, double d, int nmax, int& i, float& f) {
+// Position x on an axis -> CIC base node i and the 32-bit fixed-point offset
+// f = round((t - floor t) 2^32) of t = (x - lmin)/d + 1/2 (a carry moves to
+// the next node).  Far-out positions are pinned one node beyond the guard
+// layer, where BCoutflow removes them.
+__device__ inline void to_cell(double x, double lmin, double d, int nmax, int& i, uint32_t& f) {
   double t = (x - lmin) / d + 0.5;
+  if (!(t > -2.0)) t = -2.0;  // NaN too
+  if (t > nmax + 3.0) t = nmax + 3.0;
   double fl = floor(t);
   i = int(fl);
-  float ff = float(t - fl);
-  if (ff >= 1.0f) {
-    ff = 0.0f;
+  unsigned long long q = (unsigned long long)__double2ull_rn((t - fl) * 4294967296.0);
+  if (q >> 32) {
+    q = 0;
     i += 1;
   }
+  f = uint32_t(q);
   if (i < -1) {
     i = -1;
-    ff = 0.0f;
+    f = 0u;
   }
   if (i > nmax + 1) {
     i = nmax + 1;
-    ff = 0.999999940f;
+    f = 0xFFFFFFFFu;
   }
-  f = ff;
 }
 
 __device__ inline void store_c32(const KParams& P, PartC32 o, long long slot, const double x[3], const double v[3],
                                  int sp) {
   int i, j, k;
-  float fx, fy, fz;
+  uint32_t fx, fy, fz;
   to_cell(x[0], P.Lx_min, P.dx, P.nx, i, fx);
   to_cell(x[1], P.Ly_min, P.dy, P.ny, j, fy);
   to_cell(x[2], P.Lz_min, P.dz, P.nz, k, fz);
@@ -804,14 +810,14 @@ __global__ void calc_distance_kernel(KParams P, double* D) {
   D[at(ni, nj, nk)] = t0;
 }
 
-// CELL32 -> FP64 positions: x = Lx_min + (i + f - 0.5) dx.
+// CELL32 -> FP64 positions: x = Lx_min + (i + f/2^32 - 0.5) dx.
 __global__ void c32_to_f64_kernel(KParams P, PartC32 a, long long n, PartF64 o) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
     int i, j, k;
     unpack_cell(a.cell[p], i, j, k);
-    o.x[p] = P.Lx_min + ((double)i + (double)a.fx[p] - 0.5) * P.dx;
-    o.y[p] = P.Ly_min + ((double)j + (double)a.fy[p] - 0.5) * P.dy;
-    o.z[p] = P.Lz_min + ((double)k + (double)a.fz[p] - 0.5) * P.dz;
+    o.x[p] = P.Lx_min + ((double)i + off_f64(a.fx[p]) - 0.5) * P.dx;
+    o.y[p] = P.Ly_min + ((double)j + off_f64(a.fy[p]) - 0.5) * P.dy;
+    o.z[p] = P.Lz_min + ((double)k + off_f64(a.fz[p]) - 0.5) * P.dz;
     o.vx[p] = a.vx[p];
     o.vy[p] = a.vy[p];
     o.vz[p] = a.vz[p];

@@ -95,7 +95,7 @@ __global__ void scan_add_kernel(int* out, int n, const int* tile_offsets) {
 
 struct C32 {
   int i, j, k;
-  float f[3];
+  uint32_t f[3];  // in-cell offsets, 32-bit fixed point
 };
 
 __device__ inline C32 load_pos(const PartC32& a, long long p) {
@@ -119,23 +119,20 @@ __device__ inline C32 load_pos_cs(const PartC32& a, long long p) {
   return r;
 }
 
-// Move one axis by d cells (in cell units) and renormalise to [0, 1).
+// Move one axis by d cells (FP32, in cell units) in 32-bit fixed point: d is
+// scaled to 2^-32 cells (exact when |d| >= 2^-9, else rounded to the nearest
+// 2^-32), added to the offset, and the whole cells of the sum move the index.
 // Open axes pin far-out particles at the outer guard node (they are outside
 // the domain and BCoutflow removes them); periodic axes shift by whole
 // periods so the index stays representable.
-__device__ inline void move_axis(int& i, float& f, float d, int n, int open) {
-  float t = f + d;
-  float fl = floorf(t);
-  int di = int(fl);
-  t = t - fl;
-  if (t >= 1.0f) {
-    t = 0.0f;
-    di += 1;
-  }
-  i += di;
+__device__ inline void move_axis(int& i, uint32_t& f, float d, int n, int open) {
+  d = fminf(fmaxf(d, -1073741824.0f), 1073741824.0f);  // |d| <= 2^30 cells (NaN: -2^30)
+  const long long t = (long long)f + __float2ll_rn(d * 4294967296.0f);
+  f = uint32_t(t);             // t modulo 2^32: the offset in [0, 1)
+  i += int(t >> 32);           // floor(t / 2^32): whole cells
   if (open) {
-    if (i < -1) i = -1, t = 0.0f;
-    if (i > n + 1) i = n + 1, t = 0.5f;
+    if (i < -1) i = -1, f = 0u;
+    if (i > n + 1) i = n + 1, f = kOffHalf;
   } else if (i < -1) {  // whole periods up to the first index >= -1
     i = int((long long)i + (long long)n * ((-1LL - i + n - 1) / n));
   } else if (i > n + 1) {  // whole periods down to the first index <= n + 1
@@ -145,8 +142,8 @@ __device__ inline void move_axis(int& i, float& f, float d, int n, int open) {
 }
 
 // x < min  <=>  i + f < 1/2;  x > max  <=>  i + f > n + 1/2.
-__device__ inline bool below(int i, float f) { return i < 0 || (i == 0 && f < 0.5f); }
-__device__ inline bool above(int i, float f, int n) { return i > n || (i == n && f > 0.5f); }
+__device__ inline bool below(int i, uint32_t f) { return i < 0 || (i == 0 && f < kOffHalf); }
+__device__ inline bool above(int i, uint32_t f, int n) { return i > n || (i == n && f > kOffHalf); }
 
 // BCoutflow.f90:28-53 in cell coordinates (true = keep).
 __device__ inline bool keep_c32(const KParams& P, const C32& c) {
@@ -211,9 +208,9 @@ struct OutflowC32 {
     if (cx - 2u < uint32_t(P.nx - 1) && cy - 2u < uint32_t(P.ny - 1) && cz - 2u < uint32_t(P.nz - 1)) return true;
     C32 c;
     unpack_cell(cell, c.i, c.j, c.k);
-    c.f[0] = (c.i == 0 || c.i == P.nx) ? a.fx[p] : 0.5f;
-    c.f[1] = (c.j == 0 || c.j == P.ny) ? a.fy[p] : 0.5f;
-    c.f[2] = (c.k == 0 || c.k == P.nz) ? a.fz[p] : 0.5f;
+    c.f[0] = (c.i == 0 || c.i == P.nx) ? a.fx[p] : kOffHalf;
+    c.f[1] = (c.j == 0 || c.j == P.ny) ? a.fy[p] : kOffHalf;
+    c.f[2] = (c.k == 0 || c.k == P.nz) ? a.fz[p] : kOffHalf;
     if (!keep_c32(P, c)) return false;
     if (wrap) {
       wrap_c32(P, c);
@@ -242,7 +239,8 @@ struct SpeciesF32 {
 };
 
 __device__ inline void gather_c32(const KParams& P, const C32& c, const float4* __restrict__ E, float Ep[3]) {
-  float wx[2] = {1.0f - c.f[0], c.f[0]}, wy[2] = {1.0f - c.f[1], c.f[1]}, wz[2] = {1.0f - c.f[2], c.f[2]};
+  const float fx = off_f32(c.f[0]), fy = off_f32(c.f[1]), fz = off_f32(c.f[2]);
+  float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
   int i0 = min(max(c.i, 0), P.nx + 1), j0 = min(max(c.j, 0), P.ny + 1), k0 = min(max(c.k, 0), P.nz + 1);
   int i1 = min(max(c.i + 1, 0), P.nx + 1), j1 = min(max(c.j + 1, 0), P.ny + 1), k1 = min(max(c.k + 1, 0), P.nz + 1);
   Ep[0] = Ep[1] = Ep[2] = 0.0f;
@@ -381,6 +379,22 @@ __device__ inline unsigned long long stencil_key(int i, int j, int k, int s) {
   return (c(i) | (c(j) << 20) | (c(k) << 40)) << 4 | (unsigned long long)s;
 }
 
+// Corner q of the CIC stencil (ParticlesGridify.f90:70-88, F1..F8 order).
+__constant__ int kCorner[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+
+// CIC weights of a CELL32 particle: products in FP64 of the offsets (exact in
+// FP64), each rounded once to the deposit's 2^-40 fixed point.  Every CELL32
+// deposit kernel takes its weights from here, so their sums agree bit for bit.
+__device__ inline void cic_fixed_c32(const C32& c, long long w[8], double F[8]) {
+  const double fx = off_f64(c.f[0]), fy = off_f64(c.f[1]), fz = off_f64(c.f[2]);
+  const double wx[2] = {1.0 - fx, fx}, wy[2] = {1.0 - fy, fy}, wz[2] = {1.0 - fz, fz};
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    F[q] = (wx[kCorner[q][0]] * wy[kCorner[q][1]]) * wz[kCorner[q][2]];
+    w[q] = __double2ll_rn(F[q] * kDepositScale);
+  }
+}
+
 // Warp-aggregated fixed-point deposit (see particles_exact.cu deposit8).
 __device__ inline void deposit8(unsigned long long key, bool active, const long long w[8], const long long nodes[8],
                                 unsigned long long* plane) {
@@ -403,40 +417,37 @@ __device__ inline void deposit8(unsigned long long key, bool active, const long 
   }
 }
 
-// ParticlesGridify.f90:65-123 with FP32 weights rounded to 2^-40 and ghost
+// ParticlesGridify.f90:65-123 with FP64 weights rounded to 2^-40 and ghost
 // folds applied to the node indices.
 __global__ void deposit_c32_kernel(KParams P, PartC32 a, long long n, unsigned long long* Nacc,
                                    unsigned long long* Facc) {
   long long stride = (long long)gridDim.x * blockDim.x;
   long long n_round = ((n + 31) / 32) * 32;
-  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n_round; p += stride) {
     bool active = p < n;
     long long w[8] = {0, 0, 0, 0, 0, 0, 0, 0}, nodes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    float Fw[8];
+    double Fw[8];
     int s = 0;
     unsigned long long key = ~0ull;
     if (active) {
       C32 c = load_pos(a, p);
       s = a.sp[p];
-      float wx[2] = {1.0f - c.f[0], c.f[0]}, wy[2] = {1.0f - c.f[1], c.f[1]}, wz[2] = {1.0f - c.f[2], c.f[2]};
+      cic_fixed_c32(c, w, Fw);
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        Fw[q] = wx[off[q][0]] * wy[off[q][1]] * wz[off[q][2]];
-        w[q] = __float2ll_rn(Fw[q] * float(kDepositScale));
-        int i = fold_index(c.i + off[q][0], P.nx, P.xflow), j = fold_index(c.j + off[q][1], P.ny, P.yflow),
-            k = fold_index(c.k + off[q][2], P.nz, P.zflow);
+        int i = fold_index(c.i + kCorner[q][0], P.nx, P.xflow), j = fold_index(c.j + kCorner[q][1], P.ny, P.yflow),
+            k = fold_index(c.k + kCorner[q][2], P.nz, P.zflow);
         nodes[q] = node_index(P, i, j, k);
       }
       key = stencil_key(c.i, c.j, c.k, s);
     }
     deposit8(key, active, w, nodes, Nacc + (long long)s * P.nodes);
     if (Facc && active) {
-      float vel[3] = {a.vx[p], a.vy[p], a.vz[p]};
+      double vel[3] = {a.vx[p], a.vy[p], a.vz[p]};
       for (int c = 0; c < 3; ++c)
         for (int q = 0; q < 8; ++q)
           atomicAdd(Facc + ((long long)s * 3 + c) * P.nodes + nodes[q],
-                    (unsigned long long)__double2ll_rn((double)Fw[q] * (double)vel[c] * kFluxScale));
+                    (unsigned long long)__double2ll_rn(Fw[q] * vel[c] * kFluxScale));
     }
   }
 }
@@ -486,7 +497,6 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
                                                                unsigned long long* Nacc) {
   extern __shared__ unsigned int dep_tile[];  // [2][kDepTile]: low and high 20-bit halves
   __shared__ int red8[8][8];
-  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
   unsigned int* lo = dep_tile;
   unsigned int* hi = dep_tile + kDepTile;
   constexpr int kPer = kDepChunk / 256;
@@ -527,17 +537,17 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
 #pragma unroll
       for (int m = 0; m < kPer; ++m) {
         if (!act[m]) continue;
-        const float wx[2] = {1.0f - c[m].f[0], c[m].f[0]}, wy[2] = {1.0f - c[m].f[1], c[m].f[1]},
-                    wz[2] = {1.0f - c[m].f[2], c[m].f[2]};
+        long long w[8];
+        double F[8];
+        cic_fixed_c32(c[m], w, F);
         const int b0 = (((sp[m] - smin) * int(bk) + (c[m].k - kmin)) * int(bj) + (c[m].j - jmin)) * int(bi) +
                        (c[m].i - imin);
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const float F = wx[off[q][0]] * wy[off[q][1]] * wz[off[q][2]];
-          const unsigned long long w = (unsigned long long)__float2ll_rn(F * float(kDepositScale));
-          const int e = b0 + (off[q][2] * int(bj) + off[q][1]) * int(bi) + off[q][0];
-          atomicAdd(lo + e, unsigned(w & 0xFFFFFu));
-          atomicAdd(hi + e, unsigned(w >> 20));
+          const unsigned long long wq = (unsigned long long)w[q];
+          const int e = b0 + (kCorner[q][2] * int(bj) + kCorner[q][1]) * int(bi) + kCorner[q][0];
+          atomicAdd(lo + e, unsigned(wq & 0xFFFFFu));
+          atomicAdd(hi + e, unsigned(wq >> 20));
         }
       }
       __syncthreads();
@@ -561,16 +571,16 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
 #pragma unroll
       for (int m = 0; m < kPer; ++m) {
         if (!act[m]) continue;
-        const float wx[2] = {1.0f - c[m].f[0], c[m].f[0]}, wy[2] = {1.0f - c[m].f[1], c[m].f[1]},
-                    wz[2] = {1.0f - c[m].f[2], c[m].f[2]};
+        long long w[8];
+        double F[8];
+        cic_fixed_c32(c[m], w, F);
         unsigned long long* plane = Nacc + (long long)sp[m] * P.nodes;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const float F = wx[off[q][0]] * wy[off[q][1]] * wz[off[q][2]];
-          const unsigned long long w = (unsigned long long)__float2ll_rn(F * float(kDepositScale));
-          const int i = fold_index(c[m].i + off[q][0], P.nx, P.xflow), j = fold_index(c[m].j + off[q][1], P.ny, P.yflow),
-                    k = fold_index(c[m].k + off[q][2], P.nz, P.zflow);
-          atomicAdd(plane + node_index(P, i, j, k), w);
+          const int i = fold_index(c[m].i + kCorner[q][0], P.nx, P.xflow),
+                    j = fold_index(c[m].j + kCorner[q][1], P.ny, P.yflow),
+                    k = fold_index(c[m].k + kCorner[q][2], P.nz, P.zflow);
+          atomicAdd(plane + node_index(P, i, j, k), (unsigned long long)w[q]);
         }
       }
     }
