@@ -143,6 +143,18 @@ constexpr uint32_t kOffHalf = 0x80000000u;
 // An in-cell offset as FP64 (exact) and as FP32 (its leading 23 bits).
 __host__ __device__ inline double off_f64(uint32_t f) { return (double)f * (1.0 / 4294967296.0); }
 __device__ inline float off_f32(uint32_t f) { return __uint_as_float((f >> 9) | 0x3F800000u) - 1.0f; }
+// 1 + f / 2^32 as FP64, exactly, built from the bits (the 32 offset bits are
+// the top of the 52-bit mantissa): no conversion instruction.  For x in
+// [1, 2), 2 - x and x - 1 are exact.
+__device__ inline double off_one_plus(uint32_t f) {
+  return __hiloint2double(int(0x3FF00000u | (f >> 12)), int(f << 20));
+}
+// round(F * 2^40) to nearest, ties to even (the rounding of __double2ll_rn),
+// for F in [0, 2^11): one FMA against 1.5 * 2^52 leaves the integer in the
+// low mantissa bits.
+__device__ inline long long fixed40_rn(double F) {
+  return __double_as_longlong(fma(F, 1099511627776.0, 6755399441055744.0)) - 0x4338000000000000LL;
+}
 
 // Process-wide count of kernels launched by this library (every launch
 // wrapper calls it once per launch); reported by picard_gpu_get_stats.
