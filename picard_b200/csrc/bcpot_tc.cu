@@ -388,7 +388,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint32_t tb = (uint32_t)__cvta_generic_to_shared(sT) + (uint32_t)(d - TdA) * 16u;
         const uint32_t zs = (uint32_t)__cvta_generic_to_shared(zb);
         const uint32_t acc_cols = tmem + kColAcc + (uint32_t)(b * kTcHalfN);
-        const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
+        // the five correction products first, the leading product x1 y1
+        // last: an FP32 MMA accumulation loses up to an ulp of the running
+        // sum per update, so the 5 (K / 16) updates of the small products
+        // happen while the sum is small, and only the K / 16 updates of the
+        // leading product see it at full size
+        const int pa[6] = {2, 1, 0, 1, 0, 0}, pb[6] = {0, 1, 2, 0, 1, 0};
         // descriptors of this step's first A and B blocks; every other block
         // is a multiple of 16 bytes further in, which adds to the start
         // address field (address / 16, below 2^14 for any shared-memory
@@ -396,9 +401,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint64_t adesc0 = smem_desc(tb, kRT * 16, 128);
         const uint64_t bdesc0 = smem_desc(zs, 128, 128);
 #pragma unroll
-        for (int ks = 0; ks < kTcKC / 16; ++ks) {
+        for (int t = 0; t < 6; ++t) {
 #pragma unroll
-          for (int t = 0; t < 6; ++t) {
+          for (int ks = 0; ks < kTcKC / 16; ++ks) {
             const uint64_t adesc = adesc0 + (uint64_t)((pa[t] * kTSplit + (size_t)(2 * ks) * kRT * 16) >> 4);
             const uint64_t bdesc = bdesc0 + (uint64_t)((pb[t] * kZS + (size_t)ks * 256) >> 4);
             const uint32_t acc = (ks == 0 && t == 0) ? 0u : 1u;
