@@ -281,7 +281,11 @@ typedef enum picard_option {
    * every CTA's wait runs out and returns; the solve then fails with
    * PICARD_ERR_TIMEOUT and the context stays usable.  0 (the default): off.
    * Nothing else uses it. */
-  PICARD_OPT_WAIT_TEST = 7
+  PICARD_OPT_WAIT_TEST = 7,
+  /* 1: the x-pair sweep reads r from global memory and stages only the w box
+   * (with one CTA per tile and one stage; otherwise ignored); 0 r box by TMA.
+   * Never changes a result bit. */
+  PICARD_OPT_SWEEP_R_GLOBAL = 8
 } picard_option;
 /* Reads an option's current value (SWEEP_CTAS: 0 means one CTA per tile). */
 PICARD_API int picard_gpu_get_option(picard_ctx* ctx, int32_t option, int32_t* value);

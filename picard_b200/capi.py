@@ -37,6 +37,7 @@ OPT_SWEEP_RESIDENT = 4
 OPT_SWEEP_PAIRS = 5
 OPT_SWEEP_FUSED = 6
 OPT_WAIT_TEST = 7
+OPT_SWEEP_R_GLOBAL = 8
 
 class PicardStats(C.Structure):
     _fields_ = [

@@ -811,6 +811,11 @@ int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
     c->G.stages = value;
     return PICARD_OK;
   }
+  if (option == PICARD_OPT_SWEEP_R_GLOBAL) {
+    c->G.rglobal = value != 0;
+    if (c->G.rglobal) c->G.pairs = 1, c->G.fused2 = 0;
+    return PICARD_OK;
+  }
   if (option == PICARD_OPT_WAIT_TEST) {
     if (value != 0 && value != 1) return fail(PICARD_ERR_BAD_ARG, "WAIT_TEST must be 0 or 1");
     c->wait_test = value;
@@ -830,6 +835,7 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
     case PICARD_OPT_SWEEP_FUSED: *value = c->G.fused2; return PICARD_OK;
     case PICARD_OPT_SWEEP_RESIDENT: *value = resident_option_value(c); return PICARD_OK;
     case PICARD_OPT_WAIT_TEST: *value = c->wait_test; return PICARD_OK;
+    case PICARD_OPT_SWEEP_R_GLOBAL: *value = c->G.rglobal; return PICARD_OK;
   }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");
 }

@@ -610,6 +610,53 @@ __global__ void __launch_bounds__(256) sweep_tma2_kernel(const __grid_constant__
   }
 }
 
+// The x-pair sweep with r read from global memory: only the w box goes
+// through shared memory (28.8 KB at zc = 8 instead of 45 KB), so more tiles
+// are in flight per SM: with 32 registers (the launch bound asks for 7 CTAs
+// of 256 threads per SM) 7 tiles fit, so the 1,024 tiles of a 256 x 128 x 128
+// sweep run in one wave on 148 SMs.  One CTA per tile, one stage; every node
+// and every partial is computed by the same pair_tile body, so the results
+// are bit-identical to sweep_tma2_kernel's.
+template <int ZC, bool W_ZERO>
+__global__ void __launch_bounds__(256, 7) sweep_tma2r_kernel(const __grid_constant__ CUtensorMap tw,
+                                                          const float* __restrict__ r, Stencil S, JacobiCoefF J,
+                                                          float* __restrict__ wout, double* partial, int gx2, int gx,
+                                                          int gy, int ntiles, int* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* sw = reinterpret_cast<float*>(smem_raw);  // [ZC+2][10][72]
+  __shared__ __align__(8) unsigned long long mbar[1];
+  __shared__ double rows[2][kTmaTy];
+  const int tid = threadIdx.x + kTmaTx * threadIdx.y;
+  const uint32_t mb0 = (uint32_t)__cvta_generic_to_shared(&mbar[0]);
+  if (!W_ZERO && tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const int t = blockIdx.x;
+  if (t >= ntiles) return;
+  const int bx2 = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
+  if (!W_ZERO) {
+    if (tid == 0) {
+      const uint32_t bytes = (uint32_t)(Tma2Stage<ZC>::kW * sizeof(float));
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb0), "r"(bytes) : "memory");
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+          ::"r"((uint32_t)__cvta_generic_to_shared(sw)), "l"((unsigned long long)&tw), "r"(bx2 * kTma2Tile),
+          "r"(by * kTmaTy), "r"(bz * ZC), "r"(mb0)
+          : "memory");
+    }
+    if (!__syncthreads_and(mbar_wait(mb0, 0, kMbarSpin) ? 1 : 0)) {
+      if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+      mbar_wait(mb0, 0, kMbarSpin);
+      return;
+    }
+  }
+  pair_tile_sweep_wz<ZC, W_ZERO, true>(sw, nullptr, S, J, wout, partial, bx2, by, bz, gx, gy, rows, r);
+}
+
 // ---------------------------------- two sweeps per launch (temporal blocking)
 //
 // Sweeps s and s+1 of the x-pair kernel in one launch.  Per 64 x 8 x ZC tile
@@ -1135,7 +1182,8 @@ int sweep_tma_occupancy(const JacobiGeom& G, int stages) {
 
 template <int ZC, int STAGES>
 static cudaError_t launch_tma2_zs(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
-                                  float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
+                                  const float* r, float* wout, double* partial, int w_zero, int* err,
+                                  cudaStream_t st) {
   const size_t smem = STAGES * Tma2Stage<ZC>::kBytes;
   static bool attr = false;
   if (!attr) {
@@ -1162,6 +1210,14 @@ static cudaError_t launch_tma2_zs(const KParams& P, const JacobiGeom& G, const C
   note_launch();
   // one CTA per tile with one stage: the loop-free instantiation
   const bool loop = STAGES == 2 || ctas < ntiles;
+  if (G.rglobal && !loop && r) {
+    // r from global memory: the w box alone in shared memory (below the
+    // 48 KB default, no attribute needed)
+    cfg.dynamicSmemBytes = Tma2Stage<ZC>::kW * sizeof(float);
+    auto kr = w_zero ? sweep_tma2r_kernel<ZC, true> : sweep_tma2r_kernel<ZC, false>;
+    return cudaLaunchKernelEx(&cfg, kr, *tw, r, make_stencil(P), jacobi_coef_f(P), wout, partial, gx2,
+                              (int)G.grid.x, (int)G.grid.y, ntiles, err);
+  }
   auto kern = w_zero ? (loop ? sweep_tma2_kernel<ZC, STAGES, true, true> : sweep_tma2_kernel<ZC, STAGES, true, false>)
                      : (loop ? sweep_tma2_kernel<ZC, STAGES, false, true> : sweep_tma2_kernel<ZC, STAGES, false, false>);
   return cudaLaunchKernelEx(&cfg, kern, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout, partial, gx2,
@@ -1170,9 +1226,10 @@ static cudaError_t launch_tma2_zs(const KParams& P, const JacobiGeom& G, const C
 
 template <int ZC>
 static cudaError_t launch_tma2_zc(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
-                                  float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
-  return G.stages == 2 ? launch_tma2_zs<ZC, 2>(P, G, tw, tr, wout, partial, w_zero, err, st)
-                       : launch_tma2_zs<ZC, 1>(P, G, tw, tr, wout, partial, w_zero, err, st);
+                                  const float* r, float* wout, double* partial, int w_zero, int* err,
+                                  cudaStream_t st) {
+  return G.stages == 2 ? launch_tma2_zs<ZC, 2>(P, G, tw, tr, r, wout, partial, w_zero, err, st)
+                       : launch_tma2_zs<ZC, 1>(P, G, tw, tr, r, wout, partial, w_zero, err, st);
 }
 
 template <int ZC, int STAGES>
@@ -1206,11 +1263,11 @@ int sweep_tma2_tiles(const KParams& P, const JacobiGeom& G) {
 }
 
 cudaError_t launch_sweep_tma2(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
-                              float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
+                              const float* r, float* wout, double* partial, int w_zero, int* err, cudaStream_t st) {
   switch (G.zc) {
-    case 4: return launch_tma2_zc<4>(P, G, tw, tr, wout, partial, w_zero, err, st);
-    case 8: return launch_tma2_zc<8>(P, G, tw, tr, wout, partial, w_zero, err, st);
-    case 16: return launch_tma2_zc<16>(P, G, tw, tr, wout, partial, w_zero, err, st);
+    case 4: return launch_tma2_zc<4>(P, G, tw, tr, r, wout, partial, w_zero, err, st);
+    case 8: return launch_tma2_zc<8>(P, G, tw, tr, r, wout, partial, w_zero, err, st);
+    case 16: return launch_tma2_zc<16>(P, G, tw, tr, r, wout, partial, w_zero, err, st);
   }
   return cudaErrorInvalidValue;
 }

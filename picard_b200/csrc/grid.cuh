@@ -29,6 +29,7 @@ struct JacobiGeom {
   int stages = 1;  // shared-memory stages per CTA (2: the next tile is prefetched)
   int pairs = 0;   // 1: the x-pair kernel (64-wide tiles)
   int fused2 = 0;  // 1 (with pairs): two sweeps per launch where a batch allows
+  int rglobal = 0; // 1 (with pairs, one CTA per tile, one stage): r read from global memory
   // register-resident sweeps (jacobi_resident.cu): one cooperative launch per
   // batch of sweeps over CTAs of 32 x res_by x res_nz nodes
   int res = 0;
@@ -49,9 +50,11 @@ cudaError_t launch_sweeps_resident(const KParams& P, const JacobiGeom& G, const 
                                    int* err, cudaStream_t st, int wait_test = 0);
 // The x-pair TMA sweep (64-wide tiles; w boxes 72 x 10 x zc+2, r boxes 64 x
 // 8 x zc): launch, occupancy and tile count.  Writes the same partials (in
-// the 32-wide tile layout) as launch_sweep_tma.
+// the 32-wide tile layout) as launch_sweep_tma.  With G.rglobal, one CTA per
+// tile and one stage, r is read from global memory (r, the padded array tr
+// describes) and only the w box is staged.
 cudaError_t launch_sweep_tma2(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
-                              float* wout, double* partial, int w_zero, int* err, cudaStream_t st);
+                              const float* r, float* wout, double* partial, int w_zero, int* err, cudaStream_t st);
 int sweep_tma2_occupancy(const JacobiGeom& G, int stages);
 // Sweeps s and s+1 in one launch (x pairs, temporal blocking; zc 4 or 8):
 // reads w_{s-1} through tw (boxes 72 x 12 x zc+4) and r through tr (boxes 72 x

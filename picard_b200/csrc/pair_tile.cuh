@@ -62,11 +62,14 @@ constexpr int kPairBoxX = 72, kPairTile = 64, kPairTy = 8;
 // W_ZERO: the iterate entering the sweep is zero (the first sweep after an
 // anchor), so the w box is not read.  A compile-time flag: with a run-time one
 // every plane's loads sat behind a branch and the sweep ran ~15 % slower.
-template <int ZC, bool FULL, bool W_ZERO>
+// R_GLOBAL: r is read from global memory (rg, the padded array; 8-byte pair
+// loads) instead of the shared-memory r box sr, so a tile needs only the w box
+// in shared memory.
+template <int ZC, bool FULL, bool W_ZERO, bool R_GLOBAL = false>
 __device__ __forceinline__ void pair_tile_sweep_body(const float* sw, const float* sr, const Stencil& S,
                                                      const JacobiCoefF& J, float* wout, double* partial,
                                                      int bx2, int by, int bz, int gx, int gy,
-                                                     double (*rows)[kPairTy]) {
+                                                     double (*rows)[kPairTy], const float* rg = nullptr) {
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
   const long long plane = (long long)S.fpitch * S.nyp;
   const unsigned long long m2 = pk2(-2.0f, -2.0f), ix2 = pk2(J.idx2, J.idx2), iy2 = pk2(J.idy2, J.idy2),
@@ -83,6 +86,7 @@ __device__ __forceinline__ void pair_tile_sweep_body(const float* sw, const floa
   unsigned long long wc = W_ZERO ? 0ull : wrow(1, ty + 1);
   unsigned long long r2 = 0ull;  // (+0.0f, +0.0f)
   float* out = wout + fidx(S, i0, j, z0 + 1);
+  const float* rin = R_GLOBAL ? rg + fidx(S, i0, j, z0 + 1) : nullptr;
 #pragma unroll
   for (int kk = 1; kk <= ZC; ++kk) {
     if (FULL || kk <= kend) {
@@ -97,8 +101,18 @@ __device__ __forceinline__ void pair_tile_sweep_body(const float* sw, const floa
         xr = wcol(kk, ty + 1, 2 * tx + 6);  // x + 1 of the pair's second node
       }
       const unsigned long long xm = pk2(xl, c.x), xp = pk2(c.y, xr);
-      const unsigned long long rr =
-          *reinterpret_cast<const unsigned long long*>(sr + ((kk - 1) * kPairTy + ty) * kPairTile + 2 * tx);
+      unsigned long long rr;
+      if (R_GLOBAL) {
+        // the pair (i0, i0 + 1) starts at an even float (fidx adds 3 to an odd
+        // i0, rows are 8-float aligned); lanes past the interior load nothing
+        if (FULL || act1)
+          rr = __ldg(reinterpret_cast<const unsigned long long*>(rin));
+        else
+          rr = pk2(act0 ? __ldg(rin) : 0.0f, 0.0f);
+        rin += plane;
+      } else {
+        rr = *reinterpret_cast<const unsigned long long*>(sr + ((kk - 1) * kPairTy + ty) * kPairTile + 2 * tx);
+      }
       // jacobi_res_f32 on both lanes
       const unsigned long long sx = add2(xp, xm), sy = add2(yp, ym), sz = add2(wp, wm);
       unsigned long long lap = mul2(fma2(m2, wc, sx), ix2);
@@ -144,14 +158,15 @@ __device__ __forceinline__ bool pair_tile_full(const Stencil& S, int bx2, int by
   return (bx2 + 1) * kPairTile <= S.nx && (by + 1) * kPairTy <= S.ny && z0 + zc <= S.nz;
 }
 
-template <int ZC, bool W_ZERO>
+template <int ZC, bool W_ZERO, bool R_GLOBAL = false>
 __device__ __forceinline__ void pair_tile_sweep_wz(const float* sw, const float* sr, const Stencil& S,
                                                    const JacobiCoefF& J, float* wout, double* partial, int bx2,
-                                                   int by, int bz, int gx, int gy, double (*rows)[kPairTy]) {
+                                                   int by, int bz, int gx, int gy, double (*rows)[kPairTy],
+                                                   const float* rg = nullptr) {
   if (pair_tile_full(S, bx2, by, bz * ZC, ZC))
-    pair_tile_sweep_body<ZC, true, W_ZERO>(sw, sr, S, J, wout, partial, bx2, by, bz, gx, gy, rows);
+    pair_tile_sweep_body<ZC, true, W_ZERO, R_GLOBAL>(sw, sr, S, J, wout, partial, bx2, by, bz, gx, gy, rows, rg);
   else
-    pair_tile_sweep_body<ZC, false, W_ZERO>(sw, sr, S, J, wout, partial, bx2, by, bz, gx, gy, rows);
+    pair_tile_sweep_body<ZC, false, W_ZERO, R_GLOBAL>(sw, sr, S, J, wout, partial, bx2, by, bz, gx, gy, rows, rg);
 }
 
 // The same with the zero-iterate flag known only at run time (per run in the

@@ -159,7 +159,8 @@ static cudaError_t single_sweep(picard_ctx* c, int in, int rsel, double* partial
   float* R[2] = {c->r, c->r + f32_elems(K)};
   const int out = 1 - in;
   if (c->G.tma && c->G.pairs)
-    return launch_sweep_tma2(K, c->G, &c->tmw2[in], &c->tmr2[rsel], c->w[out], partial, w_zero, c->d_err, c->st);
+    return launch_sweep_tma2(K, c->G, &c->tmw2[in], &c->tmr2[rsel], R[rsel], c->w[out], partial, w_zero, c->d_err,
+                             c->st);
   if (c->G.tma)
     return launch_sweep_tma(K, c->G, &c->tmw[in], &c->tmr[rsel], c->w[out], partial, w_zero, c->d_err, c->st);
   return launch_sweep_f32(K, c->G, c->w[in], c->w[out], R[rsel], partial, w_zero, c->st);
@@ -410,9 +411,10 @@ namespace picard {
 namespace {
 struct SweepShape {
   int ctas, pdl, stages;
-  int res;     // 0: TMA sweep kernel; q + 1: resident sweep with CTA shape q
-  int pairs;   // TMA sweep: 1 the x-pair kernel
-  int fused2;  // x-pair sweeps two per launch
+  int res;      // 0: TMA sweep kernel; q + 1: resident sweep with CTA shape q
+  int pairs;    // TMA sweep: 1 the x-pair kernel
+  int fused2;   // x-pair sweeps two per launch
+  int rglobal;  // x-pair sweep, one CTA per tile: r from global memory
 };
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, SweepShape> g_tuned;
@@ -423,6 +425,7 @@ int apply_shape(picard_ctx* c, const SweepShape& sh) {
   c->G.stages = sh.stages;
   c->G.pairs = sh.pairs;
   c->G.fused2 = sh.fused2;
+  c->G.rglobal = sh.rglobal;
   c->G.res = 0;
   if (sh.res > 0) {
     if (!resident_plan(c->K, c->G, sh.res - 1)) return fail(PICARD_ERR_STATE, "resident sweep shape does not fit");
@@ -449,7 +452,7 @@ int set_resident(picard_ctx* c, int value) {
     return PICARD_OK;
   }
   if (!c->G.tma || !c->w[0]) return fail(PICARD_ERR_STATE, "resident sweeps need open boundaries and the F32_REFINE solver");
-  SweepShape sh{0, 0, 1, value, 0, 0};
+  SweepShape sh{0, 0, 1, value, 0, 0, 0};
   JacobiGeom g = c->G;
   if (!resident_plan(c->K, g, value - 1)) return fail(PICARD_ERR_STATE, "resident sweep shape does not fit the device");
   c->G.res = 0;
@@ -461,6 +464,7 @@ int set_resident(picard_ctx* c, int value) {
   sh.stages = stages;
   sh.pairs = c->G.pairs;
   sh.fused2 = c->G.fused2;
+  sh.rglobal = c->G.rglobal;
   return apply_shape(c, sh);
 }
 
@@ -480,7 +484,7 @@ int tune_sweep(picard_ctx* c, bool fresh) {
   if (const char* v = std::getenv("PICARD_SWEEP_TUNE"); v && v[0] == '0' && !fresh) {
     // no timing: the x-pair kernel, one CTA per tile, PDL (the 32-wide
     // kernel when the grid is at most one tile wide)
-    return apply(SweepShape{0, 1, 1, 0, c->K.nx > 32 ? 1 : 0, 0});
+    return apply(SweepShape{0, 1, 1, 0, c->K.nx > 32 ? 1 : 0, 0, 0});
   }
   if (!fresh) {
     SweepShape cached;
@@ -503,17 +507,18 @@ int tune_sweep(picard_ctx* c, bool fresh) {
     const int occ2 = pairs ? sweep_tma2_occupancy(c->G, 2) : sweep_tma_occupancy(c->G, 2);
     const int tiles = pairs ? sweep_tma2_tiles(c->K, c->G) : c->G.nblocks;
     for (int pdl = 1; pdl >= 0; --pdl) {
-      cand.push_back({0, pdl, 1, 0, pairs, 0});  // one CTA per tile
+      cand.push_back({0, pdl, 1, 0, pairs, 0, 0});  // one CTA per tile
+      if (pairs) cand.push_back({0, pdl, 1, 0, pairs, 0, 1});  // the same, r from global memory
       for (int k = 1; k <= occ2; ++k)
-        if ((long long)k * sms < tiles) cand.push_back({k * sms, pdl, 2, 0, pairs, 0});
-      if ((long long)occ1 * sms < tiles) cand.push_back({occ1 * sms, pdl, 1, 0, pairs, 0});
+        if ((long long)k * sms < tiles) cand.push_back({k * sms, pdl, 2, 0, pairs, 0, 0});
+      if ((long long)occ1 * sms < tiles) cand.push_back({occ1 * sms, pdl, 1, 0, pairs, 0, 0});
     }
   }
   if (c->G.zc <= 8)
-    for (int pdl = 1; pdl >= 0; --pdl) cand.push_back({0, pdl, 1, 0, 1, 1});  // two sweeps per launch
+    for (int pdl = 1; pdl >= 0; --pdl) cand.push_back({0, pdl, 1, 0, 1, 1, 0});  // two sweeps per launch
   for (int q = 0; q < kResidentShapes; ++q) {
     JacobiGeom g = c->G;
-    if (resident_plan(c->K, g, q)) cand.push_back({0, 0, 1, q + 1, 0, 0});
+    if (resident_plan(c->K, g, q)) cand.push_back({0, 0, 1, q + 1, 0, 0, 0});
   }
   constexpr int kReps = 24;
   std::vector<float> best(cand.size(), 1e30f);
@@ -537,8 +542,8 @@ int tune_sweep(picard_ctx* c, bool fresh) {
           if (c->G.fused2)  // sweeps s, s+1
             return launch_sweep2_tma(c->K, c->G, &c->tmw3[in], &c->tmr3[0], c->w[out], c->partials,
                                      c->partials + c->G.nblocks, 0, c->d_err, c->st);
-          return c->G.pairs ? launch_sweep_tma2(c->K, c->G, &c->tmw2[in], &c->tmr2[0], c->w[out], c->partials, 0,
-                                                c->d_err, c->st)
+          return c->G.pairs ? launch_sweep_tma2(c->K, c->G, &c->tmw2[in], &c->tmr2[0], c->r, c->w[out], c->partials,
+                                                0, c->d_err, c->st)
                             : launch_sweep_tma(c->K, c->G, &c->tmw[in], &c->tmr[0], c->w[out], c->partials, 0,
                                                c->d_err, c->st);
         };
@@ -565,9 +570,10 @@ int tune_sweep(picard_ctx* c, bool fresh) {
                      c->K.nz, c->G.zc, cand[q].res - 1, best[q] * 1e3, q == pick ? "  <- picked" : "");
       else
         std::fprintf(stderr,
-                     "picard sweep tune %dx%dx%d zc=%d: pairs=%d fused2=%d ctas=%d pdl=%d stages=%d  %.3f us%s\n",
-                     c->K.nx, c->K.ny, c->K.nz, c->G.zc, cand[q].pairs, cand[q].fused2, cand[q].ctas, cand[q].pdl,
-                     cand[q].stages, best[q] * 1e3, q == pick ? "  <- picked" : "");
+                     "picard sweep tune %dx%dx%d zc=%d: pairs=%d fused2=%d rglobal=%d ctas=%d pdl=%d stages=%d  "
+                     "%.3f us%s\n",
+                     c->K.nx, c->K.ny, c->K.nz, c->G.zc, cand[q].pairs, cand[q].fused2, cand[q].rglobal, cand[q].ctas,
+                     cand[q].pdl, cand[q].stages, best[q] * 1e3, q == pick ? "  <- picked" : "");
     }
   }
   PICARD_TRY(apply(cand[pick]));

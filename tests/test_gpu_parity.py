@@ -244,7 +244,8 @@ def test_jacobi_matches_oracle(mode):
 @pytest.mark.parametrize("dims", [(72, 40, 36), (40, 24, 72)])
 def test_sweep_variant_does_not_change_bits(dims):
     # how the FP32 sweeps run -- the TMA kernel (32-wide tiles, or 64-wide
-    # tiles of x pairs, one or two sweeps per launch) with any persistent grid
+    # tiles of x pairs, one or two sweeps per launch, r staged by TMA or read
+    # from global memory) with any persistent grid
     # size, stage count and programmatic dependent launch, or the
     # register-resident kernel with any CTA shape -- never changes a bit: the same potential and the
     # same sweep count, within 1e-6 of the FP64 oracle.  (72, 40, 36): 3 x 5 x
@@ -271,14 +272,16 @@ def test_sweep_variant_does_not_change_bits(dims):
     assert conv
     variants = ([("tma", -1, 0, 1), ("tma", -1, 1, 1), ("tma", 7, 1, 2), ("tma", 40, 0, 2), ("tma", 64, 1, 1),
                  ("tma", -1, 1, 2), ("pairs", -1, 1, 1), ("pairs", -1, 0, 2), ("pairs", 5, 1, 2),
-                 ("pairs", 30, 0, 1), ("fused", -1, 1, 1), ("fused", -1, 0, 1)]
+                 ("pairs", 30, 0, 1), ("fused", -1, 1, 1), ("fused", -1, 0, 1), ("rglobal", -1, 1, 1),
+                 ("rglobal", -1, 0, 1)]
                 + [("resident", q, 0, 0) for q in range(1, 6)])
     results = []
     for kind, a, b, c_ in variants:
-        if kind in ("tma", "pairs", "fused"):
+        if kind in ("tma", "pairs", "fused", "rglobal"):
             g.set_option(capi.OPT_SWEEP_RESIDENT, 0)
             g.set_option(capi.OPT_SWEEP_PAIRS, 0 if kind == "tma" else 1)
             g.set_option(capi.OPT_SWEEP_FUSED, 1 if kind == "fused" else 0)
+            g.set_option(capi.OPT_SWEEP_R_GLOBAL, 1 if kind == "rglobal" else 0)
             g.set_option(capi.OPT_SWEEP_CTAS, a)
             g.set_option(capi.OPT_SWEEP_PDL, b)
             g.set_option(capi.OPT_SWEEP_STAGES, c_)
