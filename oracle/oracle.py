@@ -219,3 +219,62 @@ class OracleState:
             raise RuntimeError("oracle: capacity exceeded")
         self.last_sweeps = s
         return s
+
+
+# ------------------------------------------------------------------ dumps
+
+def format_e(value: float, w: int = 10, d: int = 4) -> str:
+    """Fortran Ew.d editing with scale factor 0 (Fortran 2008 10.7.2.3.3), as
+    Write.f90 uses it: 0.d1..dd E+ee with the mantissa correctly rounded, the
+    optional leading zero dropped when the sign needs its column, the E
+    dropped for three-digit exponents, gfortran's NaN / Infinity words right
+    justified, and w asterisks when the field is too narrow."""
+    import math
+
+    if math.isnan(value):
+        s = "NaN"
+    elif math.isinf(value):
+        s = "Infinity" if value > 0 else "-Infinity"
+    else:
+        neg = math.copysign(1.0, value) < 0 and value != 0.0
+        if value == 0.0:
+            digits, exp = "0" * d, 0
+        else:
+            m = f"{abs(value):.{d - 1}e}"          # correctly rounded d digits
+            mant, e = m.split("e")
+            digits = mant.replace(".", "")
+            exp = int(e) + 1                       # 0.d1d2.. x 10^exp
+        ex = f"E{'-' if exp < 0 else '+'}{abs(exp):02d}" if abs(exp) <= 99 else f"{'-' if exp < 0 else '+'}{abs(exp):03d}"
+        body = "." + digits + ex
+        s = ("-" if neg else "") + ("0" + body if len(body) + (1 if neg else 0) < w else body)
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+def dump_particles(rp: np.ndarray, ip: np.ndarray, root: str, iteration: int) -> int:
+    """Write.f90:2-31: real_particles(1:7, 1:num_local) with column 7 = the
+    species number, 7E10.4 (one particle per line), to
+    root/particles/particles_IIIII_00000; returns the next file number."""
+    d = os.path.join(root, "particles")
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, f"particles_{iteration:05d}_00000"), "w") as f:
+        for row, s in zip(rp, ip):
+            f.write("".join(format_e(float(v)) for v in row[:6]) + format_e(float(s)) + "\n")
+    return iteration + 1
+
+
+def dump_fields(st: "OracleState", root: str, iteration: int) -> int:
+    """Write.f90:34-523: UE, Ex, Ey, Ez, then N#, X#, Y#, Z# for species
+    1..species, one E10.4 value per line in x-fastest order (ghost nodes
+    included), to root/fields/NAME_IIIII_00000; returns the next file
+    number."""
+    d = os.path.join(root, "fields")
+    os.makedirs(d, exist_ok=True)
+    arrays = [("UE", st.U), ("Ex", st.E[..., 0]), ("Ey", st.E[..., 1]), ("Ez", st.E[..., 2])]
+    S = st.p.species
+    arrays += [(f"N{s + 1}", st.N[..., s]) for s in range(S)]
+    for c, comp in (("X", 0), ("Y", 1), ("Z", 2)):
+        arrays += [(f"{c}{s + 1}", st.F[..., comp, s]) for s in range(S)]
+    for name, a in arrays:
+        with open(os.path.join(d, f"{name}_{iteration:05d}_00000"), "w") as f:
+            f.write("".join(format_e(float(v)) + "\n" for v in a.ravel()))
+    return iteration + 1

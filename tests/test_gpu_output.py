@@ -113,3 +113,95 @@ def test_run_io_is_the_write_step_sequence(tmp_path):
             assert _lines(os.path.join(root, sub, name)) == _lines(os.path.join(broot, sub, name)), name
     a.close()
     b.close()
+
+
+def _fields_of(line: str, width: int = 10):
+    return [line[k:k + width] for k in range(0, len(line), width)]
+
+
+def _value(field: str) -> float:
+    s = field.strip()
+    if "E" not in s:  # three-digit exponent: the E is dropped
+        k = max(s.rfind("+"), s.rfind("-"))
+        s = s[:k] + "E" + s[k:]
+    return float(s)
+
+
+def test_dumps_equal_the_oracles_dumps(tmp_path):
+    # picard_gpu_run_io (F64 layout, FP64 solver) against the oracle's loop
+    # with the same write-step branch (picard.f90:602-627) and the oracle's
+    # own E10.4 dumps (Write.f90:2-31, 34-523): the same files, line for
+    # line.  Positions are bit-exact, so particle lines are identical but
+    # for a velocity on a rounding boundary of its fourth digit.  A field
+    # line may differ only by less than 1e-7 of the field's largest value
+    # (a node where the field is a near cancellation prints its rounding).
+    from oracle import oracle as O
+
+    p = O.derive(small_haser(nx=12, ny=8, nz=6, ppc=2))
+    dt = p.dt
+    steps, fint, pint = 5, 2.0 * dt, 3.0 * dt
+    g = Simulation(p, derive=False, **F64)
+    g.calc_distance()
+    g.particles_initialize()
+    root = str(tmp_path / "gpu")
+    g.run_io(0, steps, root, fields_interval=fint, particles_interval=pint)
+    o = O.OracleState(p)
+    o.calc_distance()
+    o.initialize()
+    oroot = str(tmp_path / "oracle")
+    t, fi, pi = 0.0, 0, 0
+    for it in range(1, steps + 1):
+        t = t + dt
+        o.bc_inflow(it)
+        o.advance_position()
+        o.produce(it)
+        o.bc_outflow()
+        o.transfer()
+        o.gridify()
+        o.bc_potentials()
+        o.calc_epotential()
+        o.calc_efield()
+        o.bc_fields()
+        wf, wp = math.fmod(t, fint) < dt, math.fmod(t, pint) < dt
+        if wf or wp:
+            o.advance_velocity(mode=2, deltat=0.5 * dt)
+            if wp:
+                pi = O.dump_particles(*o.particles(), oroot, pi)
+            if wf:
+                o.gridify_all()
+                fi = O.dump_fields(o, oroot, fi)
+            o.advance_velocity(mode=1, deltat=0.5 * dt)
+        else:
+            o.advance_velocity()
+    assert fi >= 2 and pi >= 1
+    compared = 0
+    for sub in ("fields", "particles"):
+        names = sorted(os.listdir(os.path.join(oroot, sub)))
+        assert sorted(os.listdir(os.path.join(root, sub))) == names
+        for name in names:
+            got = _lines(os.path.join(root, sub, name))
+            want = _lines(os.path.join(oroot, sub, name))
+            assert len(got) == len(want), name
+            differ = [(a, b) for a, b in zip(got, want) if a != b]
+            if sub == "particles":
+                # positions bit-exact; a velocity may sit on a rounding
+                # boundary of its fourth digit: one line, one unit
+                assert len(differ) <= 1, (name, differ[:3])
+                for a, b in differ:
+                    for fa, fb in zip(_fields_of(a), _fields_of(b)):
+                        if fa != fb:
+                            va, vb = _value(fa), _value(fb)
+                            unit = 10.0 ** (math.floor(math.log10(max(abs(vb), 1e-300))) - 3)
+                            assert abs(va - vb) <= 1.01 * unit, (name, fa, fb)
+            else:
+                # the FP64 field agrees with the oracle's to 1e-10 (U) and
+                # 1e-7 (E, a difference of nearly equal potentials) of the
+                # field's scale, so the printed values may differ only where
+                # four digits resolve less than that
+                scale = max(abs(_value(v)) for v in want)
+                for a, b in differ:
+                    assert abs(_value(a) - _value(b)) <= 1e-7 * scale, (name, a, b, scale)
+                assert len(differ) <= max(2, len(want) // 100), (name, len(differ))
+            compared += len(got)
+    assert compared > 1000
+    g.close()

@@ -124,3 +124,12 @@ def test_parameter_and_warning_files(tmp_path):
     for t in capi.warning_texts(mask):
         assert t in text
     assert text.count("****\n") == 2 * bin(mask).count("1")
+
+
+@pytest.mark.parametrize("value,text", E10_4)
+def test_oracle_e10_4(value, text):
+    # the oracle's own restatement of Ew.d, which the dump parity test
+    # formats the oracle's arrays with
+    from oracle import oracle as O
+
+    assert O.format_e(value, 10, 4) == text
