@@ -336,10 +336,11 @@ __global__ void __launch_bounds__(256, 6) advance_velocity_c32_kernel(KParams P,
 // AdvanceVelocity of one step followed by AdvancePosition of the next, in one
 // pass over the particles: the same operations as advance_velocity_c32_kernel
 // (mode 0) then advance_position_c32_kernel, so the same bits, with one read
-// and one write of each particle instead of two.  The E gather is latency
-// bound: 32 registers (8 blocks of 256 per SM, full occupancy) keep the most
-// gathers in flight (4.67 ms instead of 5.24 ms for 268 M particles).
-__global__ void __launch_bounds__(256, 8) push_advance_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, long long n,
+// and one write of each particle instead of two.  With the 64-bit fixed-point
+// advance the kernel needs 64 registers to run without spills: 4 blocks of
+// 256 per SM (E-field + push phase 4.5 ms at 268 M particles; 6.4 ms at 32
+// registers with 160 bytes of spills per thread, 5.1 ms at 40).
+__global__ void __launch_bounds__(256, 4) push_advance_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, long long n,
                                                                   const float4* E, float dtdx, float dtdy,
                                                                   float dtdz) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
