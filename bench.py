@@ -5,7 +5,8 @@ Haser production, outflow, wrap, CIC deposit, open-boundary potential, Jacobi
 solve, E-field, Boris push) over the whole run.  The default workload is the
 at-scale plain configuration: 256x128x128 cells of 1 km, 32 H+ and 32
 electrons per cell (268,435,456 particles), drifting solar-wind Maxwellian,
-Haser source at the centre, FP32 particles (CELL32 layout), Jacobi with FP32
+Haser source at the centre, CELL32 particles (32-bit fixed-point in-cell
+offsets, FP32 velocities), Jacobi with FP32
 sweeps under FP64 anchors, tolerance 1e-6.  Inputs are synthetic (seeded
 Philox, seed = rank); the particle arrays (7.8 GB) are far larger than L2.
 

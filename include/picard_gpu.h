@@ -55,8 +55,9 @@ typedef enum picard_status {
  * F64:    SoA FP64 positions and velocities, the reference's arithmetic.  Cell
  *         indices and the removed/wrapped particle sets match the FP64 oracle
  *         bit for bit.
- * CELL32: packed int32 CIC base-node index + FP32 in-cell offset + FP32
- *         velocity (28 B per particle + 1 B species).  The performance layout. */
+ * CELL32: packed int32 CIC base-node index + 32-bit fixed-point in-cell
+ *         offsets + FP32 velocity (28 B per particle + 1 B species).  The
+ *         performance layout. */
 typedef enum picard_layout { PICARD_LAYOUT_F64 = 0, PICARD_LAYOUT_CELL32 = 1 } picard_layout;
 
 /* Jacobi arithmetic.

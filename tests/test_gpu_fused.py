@@ -28,9 +28,9 @@ pytestmark = pytest.mark.gpu
 C32 = dict(layout=capi.LAYOUT_CELL32, solver=capi.SOLVER_F32_REFINE)
 F64 = dict(layout=capi.LAYOUT_F64, solver=capi.SOLVER_F64)
 
-# FP32 in-cell offsets resolve 2^-24 of a cell; a few steps of FP32 pushes
-# leave positions within 1e-5 cells and velocities within 1e-5 of the
-# largest speed of the FP64 trajectories.
+# Fixed-point in-cell offsets resolve 2^-32 of a cell; a few steps of FP32
+# pushes leave positions well within 1e-5 cells and velocities within 1e-5
+# of the largest speed of the FP64 trajectories.
 POS_CELLS = 1e-5
 VEL_REL = 1e-5
 

@@ -5,7 +5,7 @@ sets, species, particle counts, D) bit-exact; FP64-layout positions bit-exact
 and velocities within 1e-13 relative (libm log/sin differ from CUDA's by an
 ulp); fixed-point deposits within 1e-10 relative L2; potential and field
 within 1e-6 relative L2 of the FP64 oracle (the tolerance for the potential; the
-FP64 solver meets 1e-10).  CELL32 (FP32 particles) is held to tolerances
+FP64 solver meets 1e-10).  CELL32 (fixed-point offsets, FP32 velocities) is held to tolerances
 written beside each check.
 """
 import numpy as np
@@ -138,7 +138,7 @@ def test_outflow_keep_patterns_in_reference_order(layout, pattern, size):
     if layout is F64:
         np.testing.assert_array_equal(rg, ro)
     else:
-        # CELL32 holds positions as a cell and FP32 offsets: same particles in
+        # CELL32 holds positions as a cell and fixed-point offsets: same particles in
         # the same slots, positions to FP32 resolution, velocities as FP32
         d = np.array(list(p.dxyz))
         np.testing.assert_allclose(rg[:, :3], ro[:, :3], rtol=0, atol=1e-6 * d.max())
@@ -381,7 +381,7 @@ def test_one_step_parity_f64_layout():
 def test_one_step_parity_cell32_layout():
     # Start from a developed plasma (20 oracle steps): right after the
     # co-located start C is an almost exact cancellation of the species and the
-    # FP32 in-cell offsets (2^-24 cell) dominate its relative error.
+    # rounding of the particle positions dominates its relative error.
     p, o, g = make(small_plasma(n=10, ppc=4, seed=13), **C32)
     o.calc_distance()
     o.initialize()
@@ -394,7 +394,7 @@ def test_one_step_parity_cell32_layout():
     assert abs(g.num_local - o.num_local) <= 2
     rg, ig = g.particles()
     ro, io = o.particles()
-    # FP32 offsets: cell indices equal except for particles within 1e-5 cells of a face
+    # FP32 velocities: cell indices equal except for particles within 1e-5 cells of a face
     d = np.array(list(p.dxyz))
     if g.num_local == o.num_local:
         rg, ig = sort_particles(rg, ig)
