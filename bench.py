@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--poisson-sweeps", type=int, default=400)
     ap.add_argument("--layout", choices=["cell32", "f64"], default="cell32")
     ap.add_argument("--solver", choices=["refine", "f64"], default="refine")
+    ap.add_argument("--sort-every", type=int, default=0,
+                    help="fused loop: sort the particles by CIC stencil every k iterations (0: never)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-phi", action="store_true", help="skip the FP64 check of the timed run's potential")
     ap.add_argument("--no-served", action="store_true",
@@ -194,6 +196,8 @@ def run_picard(args, rank, world, local_rank):
     W, K = args.warmup, args.steps
 
     sim = Simulation(p, layout=layout, solver=solver)
+    if args.sort_every:
+        sim.set_option(capi.OPT_SORT_EVERY, args.sort_every)
     sim.calc_distance()
     sim.particles_initialize()
     sim.run_fused(0, W)
@@ -288,11 +292,12 @@ def run_picard(args, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 particles, f32 Jacobi sweeps with f64 anchors" if args.layout == "cell32" else "f64",
+            "dtype": ("cell32 particles (32-bit fixed-point offsets, f32 velocities), f32 Jacobi sweeps with f64 "
+                      "anchors") if args.layout == "cell32" else "f64",
             "data": "synthetic (seeded Philox plasma, seed = rank)",
             "config": line_config(desc, world),
             "impl": "picard",
-            "layout": args.layout, "solver": args.solver,
+            "layout": args.layout, "solver": args.solver, "sort_every": args.sort_every,
             "gpu_launches": st["kernel_launches"],
             "jacobi_sweeps_per_step": sweeps_per_step,
             "phase_ms_per_step": {k: round(v / K, 3) for k, v in st["phase_ms"].items()},
@@ -652,7 +657,7 @@ def serving_measure(args, local_rank, requests: int, run_steps: int) -> dict:
         "metric": "particle-steps/s & run p50/p99 latency, served vs plain", "value": max(served_tput, batched_tput),
         "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "impl": "picard",
         "workload": "serving", "vs_baseline": None,
-        "dtype": "f32 particles, f32 Jacobi sweeps with f64 anchors",
+        "dtype": "cell32 particles (32-bit fixed-point offsets, f32 velocities), f32 Jacobi sweeps with f64 anchors",
         "data": "synthetic (seeded Philox plasma, run seeds 0..requests-1)",
         "config": {"workload": f"serving stream: {len(reqs)} runs, Poisson arrivals {args.rate}/s, cubic grids "
                                f"24..128 cells, 8..64 ppc, Haser Q log-uniform [1e25, 1e28] s^-1, "
@@ -862,7 +867,7 @@ def batch_measure(args, local_rank, nruns: int, run_steps: int) -> dict:
     line = {
         "metric": "particle-steps/s, batched vs plain", "value": ps_batch / t_batch, "unit": UNIT, "n_gpus": 1,
         "higher_is_better": True, "impl": "picard", "workload": "batch", "vs_baseline": None,
-        "dtype": "f32 particles, f32 Jacobi sweeps with f64 anchors",
+        "dtype": "cell32 particles (32-bit fixed-point offsets, f32 velocities), f32 Jacobi sweeps with f64 anchors",
         "data": "synthetic (seeded Philox plasma, run seeds 0..runs-1)",
         "config": {"workload": f"batched parameter sweep: {len(runs)} runs, cubic grids 16..96 cells, 8..32 ppc, "
                                f"drift 300..800 km/s, |B| 1..10 nT random direction, {steps} steps each",

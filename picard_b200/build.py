@@ -1,7 +1,8 @@
 """Builds libpicard_gpu.so in-tree for sm_100a with nvcc.
 
 particles_exact.cu is compiled with --fmad=false (the FP64 kernels keep the
-reference's separately rounded multiplies and adds); every other unit uses the
+reference's separately rounded multiplies and adds), and sort.cu too (its F64
+sort key is the deposit's base-node expression); every other unit uses the
 default contraction.  Objects go to picard_b200/_build/, the library to
 picard_b200/lib/libpicard_gpu.so.
 """
@@ -33,6 +34,7 @@ UNITS = {
     "batch.cu": [],
     "output.cu": [],
     "f90.cu": [],
+    "sort.cu": ["--fmad=false"],
 }
 
 

@@ -38,6 +38,8 @@ OPT_SWEEP_PAIRS = 5
 OPT_SWEEP_FUSED = 6
 OPT_WAIT_TEST = 7
 OPT_SWEEP_R_GLOBAL = 8
+OPT_SORT_EVERY = 9
+OPT_DEPOSIT = 10
 
 class PicardStats(C.Structure):
     _fields_ = [
@@ -178,6 +180,7 @@ def lib():
         "picard_gpu_particles_produce": [ctx, C.c_int32],
         "picard_gpu_bc_outflow": [ctx],
         "picard_gpu_particles_transfer": [ctx],
+        "picard_gpu_sort_particles": [ctx],
         "picard_gpu_particles_gridify": [ctx],
         "picard_gpu_particles_gridify_all": [ctx],
         "picard_gpu_bc_potentials": [ctx],

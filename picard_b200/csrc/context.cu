@@ -157,6 +157,14 @@ int dalloc(picard_ctx* c, T*& p, size_t n) {
   return PICARD_OK;
 }
 
+// Frees one allocation of dalloc on the context's stream.
+void release(picard_ctx* c, void* q) {
+  auto it = std::find(c->allocs.begin(), c->allocs.end(), q);
+  if (it == c->allocs.end()) return;
+  c->allocs.erase(it);
+  cudaFreeAsync(q, c->st);
+}
+
 }  // namespace
 
 namespace picard {
@@ -234,6 +242,10 @@ int check_dev_err(picard_ctx* c) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
     return fail(PICARD_ERR_TIMEOUT, "a bounded device wait gave up");
   }
+  if (e == kDevRange) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+    return fail(PICARD_ERR_STATE, "a particle move left its range on the device and was skipped");
+  }
   return PICARD_OK;
 }
 
@@ -282,6 +294,14 @@ int bc_potentials_async(picard_ctx* c) {
   return PICARD_OK;
 }
 
+static cudaError_t launch_outflow_split(picard_ctx* c, long long n, const OutflowSplit* sp) {
+  if (c->layout == PICARD_LAYOUT_F64)
+    return launch_outflow_f64(c->K, c->f64, n, c->out_words, c->blk_counts, c->blk_offsets, c->d_count, 0, c->d_err,
+                              c->st, sp);
+  return launch_outflow_c32(c->K, c->c32, n, c->out_words, c->blk_counts, c->blk_offsets, c->d_count, 0, c->d_err,
+                            c->st, sp);
+}
+
 cudaError_t launch_outflow(picard_ctx* c, int wrap) {
   if (c->layout == PICARD_LAYOUT_F64)
     return launch_outflow_f64(c->K, c->f64, c->num_local, c->out_words, c->blk_counts, c->blk_offsets, c->d_count,
@@ -314,6 +334,10 @@ int count_collect(picard_ctx* c) {
   if (c->h_pinned_i[2] == kDevTimeout) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
     return fail(PICARD_ERR_TIMEOUT, "a bounded device wait gave up");
+  }
+  if (c->h_pinned_i[2] == kDevRange) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+    return fail(PICARD_ERR_STATE, "a particle move left its range on the device and was skipped");
   }
   c->num_local = c->h_pinned_i[0];
   return PICARD_OK;
@@ -386,7 +410,7 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
       return bail(rc);
   }
   const long long nn = s.nodes;
-  if ((rc = dalloc(c, c->d_count, 1)) || (rc = dalloc(c, c->d_err, 1)) ||
+  if ((rc = dalloc(c, c->d_count, 1)) || (rc = dalloc(c, c->d_err, 1)) || (rc = dalloc(c, c->d_info, 4)) ||
       (rc = dalloc(c, c->Nacc, nn * s.species)) || (rc = dalloc(c, c->N, nn * s.species)) ||
       (rc = dalloc(c, c->C, nn)) || (rc = dalloc(c, c->U, nn)) || (rc = dalloc(c, c->E, 3 * nn)) ||
       (rc = dalloc(c, c->D, s.dsize)) || (rc = dalloc(c, c->b, nn)) || (rc = dalloc(c, c->U1, nn)))
@@ -723,11 +747,40 @@ int picard_gpu_particles_produce(picard_ctx* c, int32_t iteration) {
 }
 
 // BCoutflow.f90:5-87, in place and in the reference's order (outflow.cuh)
+//
+// In two stages around a read of the survivor count n': when the window
+// [n', n) is wide (2^16 positions or more) and at least 64 times its
+// survivors -- right after BCinflow has appended every candidate -- its chains
+// are resolved by pointer jumping (outflow.cuh), with scratch of two ints per
+// window position allocated on first use.
 int picard_gpu_bc_outflow(picard_ctx* c) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
-  PICARD_CUDA(launch_outflow(c, 0));
-  PICARD_TRY(check_dev_err(c));
-  return sync_count(c);
+  const long long n = c->num_local;
+  OutflowSplit sp{1, 0, c->d_info, {nullptr, nullptr}};
+  PICARD_CUDA(launch_outflow_split(c, n, &sp));
+  PICARD_CUDA(cudaMemcpyAsync(c->h_pinned_i + 6, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  PICARD_TRY(sync_count(c));
+  c->stats.d2h_bytes += sizeof(int);
+  const long long np = c->num_local, window = n - np, m = c->h_pinned_i[6];
+  sp.stage = 2;
+  sp.np = np;
+  if (window >= (1LL << 16) && window >= 64 * m) {
+    if (c->jump_cap < window) {
+      const long long cap = std::min<long long>(c->capacity, std::max<long long>(window, 2 * c->jump_cap));
+      for (int q = 0; q < 2; ++q) {
+        if (c->jump[q]) {
+          release(c, c->jump[q]);
+          c->jump[q] = nullptr;
+        }
+        PICARD_TRY(dalloc(c, c->jump[q], (size_t)cap));
+      }
+      c->jump_cap = cap;
+    }
+    sp.nxt[0] = c->jump[0];
+    sp.nxt[1] = c->jump[1];
+  }
+  PICARD_CUDA(launch_outflow_split(c, n, &sp));
+  return check_dev_err(c);
 }
 
 // ParticlesTransfer.f90:2-614 (one rank: periodic wrap, ibid. 494-519)
@@ -754,7 +807,9 @@ static int deposit(picard_ctx* c, bool with_flux) {
   if (c->layout == PICARD_LAYOUT_F64)
     PICARD_CUDA(launch_deposit_f64(c->K, c->f64, c->num_local, c->Nacc, Facc, c->st));
   else
-    PICARD_CUDA(launch_deposit_c32(c->K, c->c32, c->num_local, c->Nacc, Facc, c->st));
+    PICARD_CUDA(launch_deposit_c32(c->K, c->c32, c->num_local, c->Nacc, Facc,
+                                   c->deposit_kernel == 2 || (c->deposit_kernel == 0 && c->sort_every > 0),
+                                   c->st));
   PICARD_CUDA(launch_finish_deposit(c->K, c->Nacc, c->N, c->C, c->st));
   if (with_flux) PICARD_CUDA(launch_finish_flux(c->K, Facc, c->F, c->st));
   return PICARD_OK;
@@ -816,6 +871,16 @@ int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
     if (c->G.rglobal) c->G.pairs = 1, c->G.fused2 = 0;
     return PICARD_OK;
   }
+  if (option == PICARD_OPT_SORT_EVERY) {
+    if (value < 0) return fail(PICARD_ERR_BAD_ARG, "SORT_EVERY must be >= 0");
+    c->sort_every = value;
+    return PICARD_OK;
+  }
+  if (option == PICARD_OPT_DEPOSIT) {
+    if (value < 0 || value > 2) return fail(PICARD_ERR_BAD_ARG, "DEPOSIT must be 0, 1 or 2");
+    c->deposit_kernel = value;
+    return PICARD_OK;
+  }
   if (option == PICARD_OPT_WAIT_TEST) {
     if (value != 0 && value != 1) return fail(PICARD_ERR_BAD_ARG, "WAIT_TEST must be 0 or 1");
     c->wait_test = value;
@@ -836,6 +901,8 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
     case PICARD_OPT_SWEEP_RESIDENT: *value = resident_option_value(c); return PICARD_OK;
     case PICARD_OPT_WAIT_TEST: *value = c->wait_test; return PICARD_OK;
     case PICARD_OPT_SWEEP_R_GLOBAL: *value = c->G.rglobal; return PICARD_OK;
+    case PICARD_OPT_SORT_EVERY: *value = c->sort_every; return PICARD_OK;
+    case PICARD_OPT_DEPOSIT: *value = c->deposit_kernel; return PICARD_OK;
   }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");
 }

@@ -8,6 +8,23 @@
 #include "grid.cuh"
 #include "kernels.cuh"
 
+namespace picard {
+// Scratch of the counting sort by stencil (sort.cu), sized for `cap`
+// particles on first use.
+struct SortBuf {
+  long long cap = 0;
+  uint32_t* key[2] = {nullptr, nullptr};  // run keys (radix ping-pong)
+  int* val[2] = {nullptr, nullptr};       // run ids
+  int* run_start = nullptr;               // [runs + 1]
+  int* tile_counts = nullptr;             // heads per 2,048-particle tile
+  int* tile_offsets = nullptr;
+  int* hist = nullptr;                    // [256][tiles of runs]
+  int* hist_off = nullptr;
+  int* info = nullptr;                    // runs, descents, scan totals
+  int* scan_scratch = nullptr;
+};
+}  // namespace picard
+
 struct picard_ctx {
   picard_params prm;
   picard::KParams K;
@@ -21,6 +38,7 @@ struct picard_ctx {
   picard::PartC32 c32 = {};
   int* d_count = nullptr;    // live particle count
   int* d_err = nullptr;
+  int* d_info = nullptr;     // small device results read with a count (BCoutflow window)
   long long num_local = 0;   // host mirror of *d_count
 
   // node arrays (plane-major, see common.cuh)
@@ -55,6 +73,8 @@ struct picard_ctx {
   int* blk_counts = nullptr;     // BCoutflow block counts and offsets
   int* blk_offsets = nullptr;
   uint2* out_words = nullptr;    // BCoutflow keep words (outflow.cuh)
+  int* jump[2] = {nullptr, nullptr};  // BCoutflow pointer jumping (allocated on first use)
+  long long jump_cap = 0;
   int* inflow_counts = nullptr;  // fused BCinflow block counts and offsets
   int* inflow_offsets = nullptr;
   int* cell_counts = nullptr;
@@ -71,6 +91,15 @@ struct picard_ctx {
   long long res_faces_cap = 0;  // floats
 
   int wait_test = 0;  // PICARD_OPT_WAIT_TEST
+  // counting sort by stencil (sort.cu): the second particle buffer and the
+  // scratch are allocated on the first sort
+  int sort_every = 0;      // PICARD_OPT_SORT_EVERY
+  int deposit_kernel = 0;  // PICARD_OPT_DEPOSIT
+  picard::PartF64 f64b = {};
+  picard::PartC32 c32b = {};
+  picard::SortBuf sortbuf;
+  long long sort_geom_keys = 0;
+  long long stats_sorts = 0, stats_sorts_moved = 0;
   // tensor-core BCpotentials (bcpot_tc.cu)
   int bcpot_tensor = 0;
   void* tc_cs = nullptr;
@@ -119,6 +148,9 @@ int tune_sweep(picard_ctx* c, bool fresh);
 // PICARD_OPT_SWEEP_RESIDENT: 0 off, q + 1 resident with CTA shape q.
 int set_resident(picard_ctx* c, int value);
 int resident_option_value(const picard_ctx* c);
+// Stable counting sort of the context's particles by CIC stencil (base node,
+// then species); synchronises once to read the run count.
+int sort_particles(picard_ctx* c);
 }  // namespace picard
 
 #define PICARD_CUDA(expr)                                          \

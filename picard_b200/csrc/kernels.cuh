@@ -61,13 +61,25 @@ cudaError_t launch_advance_position_f64(const KParams& P, PartF64 a, long long n
 cudaError_t launch_transfer_f64(const KParams& P, PartF64 a, long long n, cudaStream_t st);
 // Keep words per 2048-particle BCoutflow block (one per 32 particles).
 constexpr int kOutflowWordsPerBlock = 64;
+// BCoutflow split around a host read of the survivor count (for callers that
+// synchronise anyway): stage 1 marks, scans and writes m, the survivors at or
+// above the new count n', to info[0]; stage 2 fills the holes below n', by
+// pointer jumping over the window [n', n) when nxt[0] and nxt[1] (n - n' ints
+// each) are given, else by following each hole's chain (outflow.cuh).
+struct OutflowSplit {
+  int stage;
+  long long np;  // stage 2: n' (*count after stage 1)
+  int* info;     // stage 1: one int
+  int* nxt[2];   // stage 2: pointer-jumping scratch, or null
+};
 // BCoutflow in place, leaving the particles in the reference's order
 // (outflow.cuh); *count receives the survivors.  wrap != 0 also applies the
 // ParticlesTransfer periodic wrap to them.  words: 64 compact_blocks(n)
 // entries; block_counts / block_offsets as for launch_scan_int over
 // compact_blocks(n) counts.
 cudaError_t launch_outflow_f64(const KParams& P, PartF64 a, long long n, uint2* words, int* block_counts,
-                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st);
+                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st,
+                               const OutflowSplit* split = nullptr);
 cudaError_t launch_advance_velocity_f64(const KParams& P, PartF64 a, long long n, const double* E, double dt,
                                         double deltat, int mode, cudaStream_t st);
 cudaError_t launch_deposit_f64(const KParams& P, PartF64 a, long long n, unsigned long long* Nacc,
@@ -82,11 +94,16 @@ cudaError_t launch_push_advance_c32(const KParams& P, PartC32 a, long long n, co
                                     cudaStream_t st);
 cudaError_t launch_transfer_c32(const KParams& P, PartC32 a, long long n, cudaStream_t st);
 cudaError_t launch_outflow_c32(const KParams& P, PartC32 a, long long n, uint2* words, int* block_counts,
-                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st);
+                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st,
+                               const OutflowSplit* split = nullptr);
 cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
                                         double deltat, int mode, cudaStream_t st);
+// Without flux the shared-memory tiled kernel, its lanes summed per stencil
+// first when stencil != 0 (for particles sorted by stencil); with flux the
+// warp-aggregated kernel with global atomics.  Every variant gives the same N
+// bits.
 cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
-                               unsigned long long* Facc, cudaStream_t st);
+                               unsigned long long* Facc, int stencil, cudaStream_t st);
 cudaError_t launch_energy_particles_c32(const KParams& P, PartC32 a, long long n, ReduceBuf rb, cudaStream_t st);
 cudaError_t launch_c32_to_f64(const KParams& P, PartC32 a, long long n, PartF64 out, cudaStream_t st);
 cudaError_t launch_f64_to_c32(const KParams& P, PartF64 a, long long n, PartC32 out, cudaStream_t st);

@@ -149,18 +149,113 @@ __global__ void __launch_bounds__(kOutflowThreads)
   }
 }
 
+// ------------------------------------------------ the fill by pointer jumping
+//
+// When the window [n', n) is wide and its survivors sparse -- BCoutflow right
+// after BCinflow has appended every inflow candidate, most of which are
+// removed -- a chain steps through the window ~(n - n') / m times (m
+// survivors in the window), each step a dependent pair of loads, and the
+// longest chain sets the time.  The same chains are then resolved in
+// ceil(log2(n - n')) parallel rounds instead: every window position x holds
+// the next position of its chain, x + S(x) (itself for a survivor), and each
+// round replaces it by the next position's entry, so after the rounds every
+// position holds the survivor its chain ends at.  The holes below n' then
+// take the survivor at the end of the chain from q + S(q), exactly as in
+// outflow_fill_kernel.
+
+// m (the survivors in the window, = the holes below n') into info[0].
+__global__ void outflow_window_kernel(const uint2* words, const int* block_offsets, const int* survivors, int* info) {
+  const long long np = *survivors;
+  info[0] = np > 0 ? int(np - kept_through(block_offsets, np - 1, words[(np - 1) >> 5])) : 0;
+}
+
+__global__ void outflow_jump_init_kernel(long long n, const uint2* words, const int* block_offsets,
+                                         const int* survivors, int* nxt) {
+  const long long np = *survivors;
+  for (long long x = np + (long long)blockIdx.x * blockDim.x + threadIdx.x; x < n;
+       x += (long long)gridDim.x * blockDim.x) {
+    const uint2 w = words[x >> 5];
+    if ((w.x >> (x & 31)) & 1u)
+      nxt[x - np] = int(x);
+    else
+      nxt[x - np] = int(x + (np - kept_through(block_offsets, x, w)));  // in [x, n)
+  }
+}
+
+__global__ void outflow_jump_kernel(const int* __restrict__ in, int* __restrict__ out, long long n,
+                                    const int* survivors) {
+  const long long np = *survivors;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n - np;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[in[i] - np];
+}
+
+template <class L>
+__global__ void __launch_bounds__(kOutflowThreads)
+    outflow_fill_jump_kernel(L lay, long long n, const uint2* words, const int* block_offsets, const int* survivors,
+                             const int* term, int* err) {
+  const long long np = *survivors;
+  const long long base = (long long)blockIdx.x * kOutflowTile;
+  if (base >= np) return;
+  for (int q = 0; q < kOutflowItems; ++q) {
+    const long long p = base + (long long)q * kOutflowThreads + threadIdx.x;
+    if (p >= np) break;
+    const uint2 w = words[p >> 5];
+    if ((w.x >> (p & 31)) & 1u) continue;
+    const long long s = p + (np - kept_through(block_offsets, p, w));
+    const long long t = (s >= np && s < n) ? (long long)term[s - np] : -1;
+    if (t >= np && t < n && ((words[t >> 5].x >> (t & 31)) & 1u))
+      lay.move(p, t);
+    else
+      atomicCAS(err, 0, int(kDevRange));
+  }
+}
+
 // n particles of `lay`; *count receives the number of survivors.  words holds
 // compact_blocks(n) * 64 entries, block_counts compact_blocks(n), and
 // block_offsets 2 compact_blocks(n) + 2 + scan_scratch_ints(...) ints.
+// split: the stages of OutflowSplit (kernels.cuh), or null for all at once.
 template <class L>
 cudaError_t launch_outflow_inplace(const L& lay, long long n, uint2* words, int* block_counts, int* block_offsets,
-                                   int* count, int wrap, int* err, cudaStream_t st) {
-  if (n <= 0) return cudaMemsetAsync(count, 0, sizeof(int), st);
+                                   int* count, int wrap, int* err, cudaStream_t st,
+                                   const OutflowSplit* split = nullptr) {
+  if (n <= 0) {
+    if (split && split->stage == 2) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), st);
+    if (e == cudaSuccess && split) e = cudaMemsetAsync(split->info, 0, sizeof(int), st);
+    return e;
+  }
   const int nb = int((n + kOutflowTile - 1) / kOutflowTile);
-  note_launch();
-  outflow_mark_kernel<<<nb, kOutflowThreads, 0, st>>>(lay, n, words, block_counts, wrap);
-  cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, count, block_offsets + nb + 1, st);
-  if (e != cudaSuccess) return e;
+  if (!split || split->stage == 1) {
+    note_launch();
+    outflow_mark_kernel<<<nb, kOutflowThreads, 0, st>>>(lay, n, words, block_counts, wrap);
+    cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, count, block_offsets + nb + 1, st);
+    if (e != cudaSuccess) return e;
+    if (split) {
+      note_launch();
+      outflow_window_kernel<<<1, 1, 0, st>>>(words, block_offsets, count, split->info);
+      return cudaGetLastError();
+    }
+  }
+  if (split && split->nxt[0] && n > split->np) {
+    const long long W = n - split->np;
+    const long long want = (W + 255) / 256;
+    const int g = int(want < 148LL * 16 ? want : 148LL * 16);
+    note_launch();
+    outflow_jump_init_kernel<<<g, 256, 0, st>>>(n, words, block_offsets, count, split->nxt[0]);
+    int* a = split->nxt[0];
+    int* b = split->nxt[1];
+    for (long long hops = 1; hops < W; hops <<= 1) {
+      note_launch();
+      outflow_jump_kernel<<<g, 256, 0, st>>>(a, b, n, count);
+      int* t = a;
+      a = b;
+      b = t;
+    }
+    note_launch();
+    outflow_fill_jump_kernel<<<nb, kOutflowThreads, 0, st>>>(lay, n, words, block_offsets, count, a, err);
+    return cudaGetLastError();
+  }
   note_launch();
   outflow_fill_kernel<<<nb, kOutflowThreads, 0, st>>>(lay, n, words, block_offsets, count, err);
   return cudaGetLastError();

@@ -966,8 +966,9 @@ cudaError_t launch_transfer_f64(const KParams& P, PartF64 a, long long n, cudaSt
 }
 
 cudaError_t launch_outflow_f64(const KParams& P, PartF64 a, long long n, uint2* words, int* block_counts,
-                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st) {
-  return launch_outflow_inplace(OutflowF64{P, a}, n, words, block_counts, block_offsets, count, wrap, err, st);
+                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st,
+                               const OutflowSplit* split) {
+  return launch_outflow_inplace(OutflowF64{P, a}, n, words, block_counts, block_offsets, count, wrap, err, st, split);
 }
 
 cudaError_t launch_advance_velocity_f64(const KParams& P, PartF64 a, long long n, const double* E, double dt,

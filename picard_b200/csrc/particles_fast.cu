@@ -2,10 +2,10 @@
 // the integer scan used by compaction and production.
 //
 // A CELL32 particle is its CIC base node (i, j, k), packed in one uint32, the
-// in-cell fractions f = (x - Lx_min)/dx + 1/2 - i in [0, 1) as FP32, and the
-// velocity as FP32: 28 bytes plus one species byte.  Node i sits at
-// x = Lx_min + (i - 1/2) dx, so the CIC weights are (1 - f, f) directly and
-// the position advance is one FP32 add per axis.
+// in-cell fractions f = (x - Lx_min)/dx + 1/2 - i in [0, 1) as 32-bit fixed
+// point (f 2^32), and the velocity as FP32: 28 bytes plus one species byte.
+// Node i sits at x = Lx_min + (i - 1/2) dx, so the CIC weights are (1 - f, f)
+// directly and the position advance is one integer add per axis.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -138,7 +138,6 @@ __device__ inline void move_axis(int& i, uint32_t& f, float d, int n, int open) 
   } else if (i > n + 1) {  // whole periods down to the first index <= n + 1
     i = int((long long)i - (long long)n * (((long long)i - n - 1 + n - 1) / n));
   }
-  f = t;
 }
 
 // x < min  <=>  i + f < 1/2;  x > max  <=>  i + f > n + 1/2.
@@ -501,6 +500,13 @@ __device__ inline void block_min8(int (&v)[8], int (*red8)[8]) {
   __syncthreads();
 }
 
+// AGG: for particles sorted by stencil (sort.cu).  The lanes of a warp first
+// group by stencil and species (match_any; one or two groups on a sorted
+// array, where the plain kernel's 32 lanes would add to the same 16 words one
+// after another), sum each corner's two halves over the group (redux), and
+// the group's first lane alone adds them to the tile.  The sums are the same
+// integers, so N is the same bits.
+template <bool AGG>
 __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC32 a, long long n,
                                                                unsigned long long* Nacc) {
   extern __shared__ unsigned int dep_tile[];  // [2][kDepTile]: low and high 20-bit halves
@@ -544,18 +550,44 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
       __syncthreads();
 #pragma unroll
       for (int m = 0; m < kPer; ++m) {
+        unsigned grp = 0u;
+        if (AGG) {
+          // groups: runs of equal (stencil, species) over consecutive lanes,
+          // from a comparison with the lane below (a run split by another
+          // key just forms two groups; the sums are the same)
+          const int lane = threadIdx.x & 31;
+          const unsigned am = __ballot_sync(0xffffffffu, act[m]);
+          const unsigned long long key =
+              act[m] ? ((unsigned long long)pack_cell(c[m].i, c[m].j, c[m].k) << 8 | (unsigned)(sp[m] & 0xff))
+                     : ~0ull;
+          const unsigned long long below = __shfl_up_sync(0xffffffffu, key, 1);
+          const unsigned heads = __ballot_sync(0xffffffffu, act[m] && (lane == 0 || below != key));
+          const unsigned upto = 0xffffffffu >> (31 - lane);  // lanes 0..lane
+          const int start = 31 - __clz(heads & upto);
+          const unsigned later = heads & ~upto;
+          const unsigned end_mask = later ? (1u << (__ffs(later) - 1)) - 1u : 0xffffffffu;
+          grp = end_mask & ~((1u << start) - 1u) & am;
+        }
         if (!act[m]) continue;
         long long w[8];
         double F[8];
         cic_fixed_c32(c[m], w, F);
         const int b0 = (((sp[m] - smin) * int(bk) + (c[m].k - kmin)) * int(bj) + (c[m].j - jmin)) * int(bi) +
                        (c[m].i - imin);
+        const bool leader = !AGG || (threadIdx.x & 31) == __ffs(grp) - 1;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const unsigned long long wq = (unsigned long long)w[q];
+          unsigned l = unsigned(wq & 0xFFFFFu), h = unsigned(wq >> 20);
+          if (AGG) {
+            l = __reduce_add_sync(grp, l);
+            h = __reduce_add_sync(grp, h);
+          }
           const int e = b0 + (corner(q, 2) * int(bj) + corner(q, 1)) * int(bi) + corner(q, 0);
-          atomicAdd(lo + e, unsigned(wq & 0xFFFFFu));
-          atomicAdd(hi + e, unsigned(wq >> 20));
+          if (leader) {
+            atomicAdd(lo + e, l);
+            atomicAdd(hi + e, h);
+          }
         }
       }
       __syncthreads();
@@ -677,8 +709,9 @@ cudaError_t launch_transfer_c32(const KParams& P, PartC32 a, long long n, cudaSt
 }
 
 cudaError_t launch_outflow_c32(const KParams& P, PartC32 a, long long n, uint2* words, int* block_counts,
-                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st) {
-  return launch_outflow_inplace(OutflowC32{P, a}, n, words, block_counts, block_offsets, count, wrap, err, st);
+                               int* block_offsets, int* count, int wrap, int* err, cudaStream_t st,
+                               const OutflowSplit* split) {
+  return launch_outflow_inplace(OutflowC32{P, a}, n, words, block_counts, block_offsets, count, wrap, err, st, split);
 }
 
 cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
@@ -701,21 +734,27 @@ cudaError_t launch_push_advance_c32(const KParams& P, PartC32 a, long long n, co
 }
 
 cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
-                               unsigned long long* Facc, cudaStream_t st) {
+                               unsigned long long* Facc, int stencil, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   if (!Facc) {
     const size_t smem = 2 * sizeof(unsigned int) * kDepTile;
     static bool attr = false;
     if (!attr) {
-      cudaError_t e = cudaFuncSetAttribute(deposit_tile_c32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
+      cudaError_t e = cudaFuncSetAttribute(deposit_tile_c32_kernel<false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(deposit_tile_c32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
       if (e != cudaSuccess) return e;
       attr = true;
     }
     long long chunks = (n + kDepChunk - 1) / kDepChunk;
     int grid = int(chunks < 148LL * 3 ? chunks : 148LL * 3);
     note_launch();
-    deposit_tile_c32_kernel<<<grid, 256, smem, st>>>(P, a, n, Nacc);
+    if (stencil)
+      deposit_tile_c32_kernel<true><<<grid, 256, smem, st>>>(P, a, n, Nacc);
+    else
+      deposit_tile_c32_kernel<false><<<grid, 256, smem, st>>>(P, a, n, Nacc);
     return cudaGetLastError();
   }
   note_launch();

@@ -132,6 +132,9 @@ class Simulation:
     def particles_transfer(self):                  # ParticlesTransfer.f90:2
         self._call("picard_gpu_particles_transfer")
 
+    def sort_particles(self):                      # no reference counterpart
+        self._call("picard_gpu_sort_particles")
+
     def particles_gridify(self):                   # ParticlesGridify.f90:1
         self._call("picard_gpu_particles_gridify")
 

@@ -107,6 +107,12 @@ def _keep_pattern(name: str, n: int) -> np.ndarray:
         keep = rng.random(n) > 0.9
     elif name == "random_3":
         keep = rng.random(n) > 0.03
+    elif name == "inflow_tail":
+        # BCoutflow right after BCinflow: the last 40 % (the candidates) almost
+        # all removed, a few leavers in the bulk
+        t = n - (2 * n) // 5
+        keep[t:] = rng.random(n - t) < 0.003
+        keep[:t] = rng.random(t) > 0.003
     return keep
 
 
@@ -119,6 +125,20 @@ def test_outflow_keep_patterns_in_reference_order(layout, pattern, size):
     # face), kept ones stay where ParticlesInitialize put them; the surviving
     # arrays must equal the oracle's in order.  The larger size spans many
     # 2048-particle blocks, so chains cross block boundaries.
+    check_outflow_pattern(layout, pattern, size)
+
+
+@pytest.mark.parametrize("layout", [F64, C32], ids=["f64", "cell32"])
+@pytest.mark.parametrize("pattern", ["inflow_tail", "last_survives", "all_removed", "random_90"])
+def test_outflow_wide_window_in_reference_order(layout, pattern):
+    # 165,888 particles: the first three patterns leave a window [n', n) of
+    # 2^16 positions or more with few survivors, which BCoutflow resolves by
+    # pointer jumping; random_90 (dense survivors) follows the chains.  Both
+    # must leave the oracle's order.
+    check_outflow_pattern(layout, pattern, (24, 6))
+
+
+def check_outflow_pattern(layout, pattern, size):
     p, o, g = make(small_plasma(n=size[0], ppc=size[1], seed=5), **layout)
     assert p.xflow
     o.initialize()
