@@ -160,15 +160,18 @@ PICARD_API int picard_gpu_particles_produce(picard_ctx* ctx, int32_t iteration);
  * reference's loop (each removed particle replaced by the current last one). */
 PICARD_API int picard_gpu_bc_outflow(picard_ctx* ctx);                          /* BCoutflow.f90:5-87           */
 PICARD_API int picard_gpu_particles_transfer(picard_ctx* ctx);                  /* ParticlesTransfer.f90:2-614  */
-/* Stable counting sort of the particles by CIC stencil: by base node (x
- * fastest, then y, z), species within a node, equal keys in their previous
- * order.  No reference counterpart: it takes the place of the MPI particle
- * migration of ParticlesTransfer.f90:48-482 in keeping each rank's particles
- * local.  A permutation: every particle keeps every bit and the deposit
- * gives the same N bits.  The first call allocates a second particle buffer
- * and scratch (up to 53 (F64) or 33 (CELL32) bytes per particle of
- * capacity plus 24 bytes per particle for the runs); an already sorted array
- * is left in place after two passes over the keys.  Synchronises once. */
+/* Stable counting sort of the particles by cell: by the node-centred cell
+ * that holds each particle (x fastest, then y, z), particles of one cell in
+ * their previous order -- the order ParticlesInitialize creates them in,
+ * which the loop's deposit and gather work best on and which cell crossings,
+ * BCoutflow's hole filling and appended particles wear down.  No reference
+ * counterpart: it takes the place of the MPI particle migration of
+ * ParticlesTransfer.f90:48-482 in keeping each domain's particles local.  A
+ * permutation: every particle keeps every bit and the deposit gives the same
+ * N bits.  The first call allocates a second particle buffer and scratch (up
+ * to 53 (F64) or 33 (CELL32) bytes per particle of capacity plus 24 bytes per
+ * particle for the runs); an array already in cell order is left in place
+ * after two passes over the keys.  Synchronises once. */
 PICARD_API int picard_gpu_sort_particles(picard_ctx* ctx);
 PICARD_API int picard_gpu_particles_gridify(picard_ctx* ctx);                  /* ParticlesGridify.f90:1-296   */
 PICARD_API int picard_gpu_particles_gridify_all(picard_ctx* ctx);               /* ParticlesGridifyAll.f90:1-455*/
@@ -297,17 +300,11 @@ typedef enum picard_option {
    * (with one CTA per tile and one stage; otherwise ignored); 0 r box by TMA.
    * Never changes a result bit. */
   PICARD_OPT_SWEEP_R_GLOBAL = 8,
-  /* k > 0: picard_gpu_run_fused sorts the particles by CIC stencil
+  /* k > 0: picard_gpu_run_fused sorts the particles by cell
    * (picard_gpu_sort_particles) in the ParticlesTransfer slot of every
    * iteration divisible by k; 0 (the default): never.  The per-subroutine
    * loops never sort (their particles stay in the reference's order). */
-  PICARD_OPT_SORT_EVERY = 9,
-  /* CELL32 charge deposit: 1 shared-memory tiled kernel (for particles in
-   * cell order), 2 the same with the lanes of a warp summed per stencil
-   * before the shared-memory atomics (for particles sorted by stencil), 0
-   * (the default) 2 when SORT_EVERY > 0, else 1.  Every choice gives the same
-   * N bits. */
-  PICARD_OPT_DEPOSIT = 10
+  PICARD_OPT_SORT_EVERY = 9
 } picard_option;
 /* Reads an option's current value (SWEEP_CTAS: 0 means one CTA per tile). */
 PICARD_API int picard_gpu_get_option(picard_ctx* ctx, int32_t option, int32_t* value);

@@ -39,7 +39,6 @@ OPT_SWEEP_FUSED = 6
 OPT_WAIT_TEST = 7
 OPT_SWEEP_R_GLOBAL = 8
 OPT_SORT_EVERY = 9
-OPT_DEPOSIT = 10
 
 class PicardStats(C.Structure):
     _fields_ = [

@@ -807,9 +807,7 @@ static int deposit(picard_ctx* c, bool with_flux) {
   if (c->layout == PICARD_LAYOUT_F64)
     PICARD_CUDA(launch_deposit_f64(c->K, c->f64, c->num_local, c->Nacc, Facc, c->st));
   else
-    PICARD_CUDA(launch_deposit_c32(c->K, c->c32, c->num_local, c->Nacc, Facc,
-                                   c->deposit_kernel == 2 || (c->deposit_kernel == 0 && c->sort_every > 0),
-                                   c->st));
+    PICARD_CUDA(launch_deposit_c32(c->K, c->c32, c->num_local, c->Nacc, Facc, c->st));
   PICARD_CUDA(launch_finish_deposit(c->K, c->Nacc, c->N, c->C, c->st));
   if (with_flux) PICARD_CUDA(launch_finish_flux(c->K, Facc, c->F, c->st));
   return PICARD_OK;
@@ -876,11 +874,6 @@ int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
     c->sort_every = value;
     return PICARD_OK;
   }
-  if (option == PICARD_OPT_DEPOSIT) {
-    if (value < 0 || value > 2) return fail(PICARD_ERR_BAD_ARG, "DEPOSIT must be 0, 1 or 2");
-    c->deposit_kernel = value;
-    return PICARD_OK;
-  }
   if (option == PICARD_OPT_WAIT_TEST) {
     if (value != 0 && value != 1) return fail(PICARD_ERR_BAD_ARG, "WAIT_TEST must be 0 or 1");
     c->wait_test = value;
@@ -902,7 +895,6 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
     case PICARD_OPT_WAIT_TEST: *value = c->wait_test; return PICARD_OK;
     case PICARD_OPT_SWEEP_R_GLOBAL: *value = c->G.rglobal; return PICARD_OK;
     case PICARD_OPT_SORT_EVERY: *value = c->sort_every; return PICARD_OK;
-    case PICARD_OPT_DEPOSIT: *value = c->deposit_kernel; return PICARD_OK;
   }
   return fail(PICARD_ERR_BAD_ARG, "unknown option");
 }

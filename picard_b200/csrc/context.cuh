@@ -9,7 +9,7 @@
 #include "kernels.cuh"
 
 namespace picard {
-// Scratch of the counting sort by stencil (sort.cu), sized for `cap`
+// Scratch of the counting sort by cell (sort.cu), sized for `cap`
 // particles on first use.
 struct SortBuf {
   long long cap = 0;
@@ -91,10 +91,9 @@ struct picard_ctx {
   long long res_faces_cap = 0;  // floats
 
   int wait_test = 0;  // PICARD_OPT_WAIT_TEST
-  // counting sort by stencil (sort.cu): the second particle buffer and the
+  // counting sort by cell (sort.cu): the second particle buffer and the
   // scratch are allocated on the first sort
   int sort_every = 0;      // PICARD_OPT_SORT_EVERY
-  int deposit_kernel = 0;  // PICARD_OPT_DEPOSIT
   picard::PartF64 f64b = {};
   picard::PartC32 c32b = {};
   picard::SortBuf sortbuf;
@@ -148,8 +147,8 @@ int tune_sweep(picard_ctx* c, bool fresh);
 // PICARD_OPT_SWEEP_RESIDENT: 0 off, q + 1 resident with CTA shape q.
 int set_resident(picard_ctx* c, int value);
 int resident_option_value(const picard_ctx* c);
-// Stable counting sort of the context's particles by CIC stencil (base node,
-// then species); synchronises once to read the run count.
+// Stable counting sort of the context's particles by cell; synchronises once
+// to read the run count.
 int sort_particles(picard_ctx* c);
 }  // namespace picard
 

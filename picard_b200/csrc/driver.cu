@@ -264,7 +264,7 @@ int picard_gpu_run_fused(picard_ctx* c, int32_t iter_start, int32_t iter_end, in
     PICARD_CUDA(launch_inflow_fused(c, it));
     PICARD_TRY(sync_count_public(c));
     // ParticlesTransfer's slot: every sort_every iterations, the particles
-    // sorted by CIC stencil (a permutation; nothing downstream depends on it)
+    // put back in cell order (a permutation; nothing downstream depends on it)
     if (c->sort_every > 0 && it % c->sort_every == 0) PICARD_TRY(sort_particles(c));
     PICARD_CUDA(cudaEventRecord(c->pev[1], c->st));
     PICARD_TRY(picard_gpu_particles_gridify(c));

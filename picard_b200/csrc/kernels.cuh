@@ -98,12 +98,8 @@ cudaError_t launch_outflow_c32(const KParams& P, PartC32 a, long long n, uint2* 
                                const OutflowSplit* split = nullptr);
 cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n, const float4* E, double dt,
                                         double deltat, int mode, cudaStream_t st);
-// Without flux the shared-memory tiled kernel, its lanes summed per stencil
-// first when stencil != 0 (for particles sorted by stencil); with flux the
-// warp-aggregated kernel with global atomics.  Every variant gives the same N
-// bits.
 cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
-                               unsigned long long* Facc, int stencil, cudaStream_t st);
+                               unsigned long long* Facc, cudaStream_t st);
 cudaError_t launch_energy_particles_c32(const KParams& P, PartC32 a, long long n, ReduceBuf rb, cudaStream_t st);
 cudaError_t launch_c32_to_f64(const KParams& P, PartC32 a, long long n, PartF64 out, cudaStream_t st);
 cudaError_t launch_f64_to_c32(const KParams& P, PartF64 a, long long n, PartC32 out, cudaStream_t st);

@@ -500,13 +500,6 @@ __device__ inline void block_min8(int (&v)[8], int (*red8)[8]) {
   __syncthreads();
 }
 
-// AGG: for particles sorted by stencil (sort.cu).  The lanes of a warp first
-// group by stencil and species (match_any; one or two groups on a sorted
-// array, where the plain kernel's 32 lanes would add to the same 16 words one
-// after another), sum each corner's two halves over the group (redux), and
-// the group's first lane alone adds them to the tile.  The sums are the same
-// integers, so N is the same bits.
-template <bool AGG>
 __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC32 a, long long n,
                                                                unsigned long long* Nacc) {
   extern __shared__ unsigned int dep_tile[];  // [2][kDepTile]: low and high 20-bit halves
@@ -550,44 +543,18 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
       __syncthreads();
 #pragma unroll
       for (int m = 0; m < kPer; ++m) {
-        unsigned grp = 0u;
-        if (AGG) {
-          // groups: runs of equal (stencil, species) over consecutive lanes,
-          // from a comparison with the lane below (a run split by another
-          // key just forms two groups; the sums are the same)
-          const int lane = threadIdx.x & 31;
-          const unsigned am = __ballot_sync(0xffffffffu, act[m]);
-          const unsigned long long key =
-              act[m] ? ((unsigned long long)pack_cell(c[m].i, c[m].j, c[m].k) << 8 | (unsigned)(sp[m] & 0xff))
-                     : ~0ull;
-          const unsigned long long below = __shfl_up_sync(0xffffffffu, key, 1);
-          const unsigned heads = __ballot_sync(0xffffffffu, act[m] && (lane == 0 || below != key));
-          const unsigned upto = 0xffffffffu >> (31 - lane);  // lanes 0..lane
-          const int start = 31 - __clz(heads & upto);
-          const unsigned later = heads & ~upto;
-          const unsigned end_mask = later ? (1u << (__ffs(later) - 1)) - 1u : 0xffffffffu;
-          grp = end_mask & ~((1u << start) - 1u) & am;
-        }
         if (!act[m]) continue;
         long long w[8];
         double F[8];
         cic_fixed_c32(c[m], w, F);
         const int b0 = (((sp[m] - smin) * int(bk) + (c[m].k - kmin)) * int(bj) + (c[m].j - jmin)) * int(bi) +
                        (c[m].i - imin);
-        const bool leader = !AGG || (threadIdx.x & 31) == __ffs(grp) - 1;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const unsigned long long wq = (unsigned long long)w[q];
-          unsigned l = unsigned(wq & 0xFFFFFu), h = unsigned(wq >> 20);
-          if (AGG) {
-            l = __reduce_add_sync(grp, l);
-            h = __reduce_add_sync(grp, h);
-          }
           const int e = b0 + (corner(q, 2) * int(bj) + corner(q, 1)) * int(bi) + corner(q, 0);
-          if (leader) {
-            atomicAdd(lo + e, l);
-            atomicAdd(hi + e, h);
-          }
+          atomicAdd(lo + e, unsigned(wq & 0xFFFFFu));
+          atomicAdd(hi + e, unsigned(wq >> 20));
         }
       }
       __syncthreads();
@@ -734,27 +701,21 @@ cudaError_t launch_push_advance_c32(const KParams& P, PartC32 a, long long n, co
 }
 
 cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigned long long* Nacc,
-                               unsigned long long* Facc, int stencil, cudaStream_t st) {
+                               unsigned long long* Facc, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   if (!Facc) {
     const size_t smem = 2 * sizeof(unsigned int) * kDepTile;
     static bool attr = false;
     if (!attr) {
-      cudaError_t e = cudaFuncSetAttribute(deposit_tile_c32_kernel<false>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(deposit_tile_c32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
+      cudaError_t e = cudaFuncSetAttribute(deposit_tile_c32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
       if (e != cudaSuccess) return e;
       attr = true;
     }
     long long chunks = (n + kDepChunk - 1) / kDepChunk;
     int grid = int(chunks < 148LL * 3 ? chunks : 148LL * 3);
     note_launch();
-    if (stencil)
-      deposit_tile_c32_kernel<true><<<grid, 256, smem, st>>>(P, a, n, Nacc);
-    else
-      deposit_tile_c32_kernel<false><<<grid, 256, smem, st>>>(P, a, n, Nacc);
+    deposit_tile_c32_kernel<<<grid, 256, smem, st>>>(P, a, n, Nacc);
     return cudaGetLastError();
   }
   note_launch();

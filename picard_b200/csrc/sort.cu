@@ -1,23 +1,28 @@
-// sort.cu -- stable counting sort of the particles by CIC stencil.
+// sort.cu -- stable counting sort of the particles by cell.
 //
 // On one rank ParticlesTransfer (ParticlesTransfer.f90:488-519) only wraps
 // coordinates across periodic faces; its slot in the loop is where the
-// particles are re-ordered by the node their CIC stencil starts at, species
-// within a node.  The key of a particle is
-//   ((k + 1) (Ny + 3) + j + 1) (Nx + 3) + i + 1) S + s,
-// (i, j, k) its 0-based CIC base node (clamped to [-1, N+1]) and s its
-// 0-based species, so that the 32 lanes of a warp share one stencil and the
-// deposit reduces them in registers before one atomic per node.
+// particles are put back in cell order.  The cell of a particle is the node
+// whose cell [x_c - dx/2, x_c + dx/2) holds it, (i_c, j_c, k_c) with
+// i_c = floor((x - Lx_min)/dx + 1) (0-based node index, clamped to
+// [-1, N+2]), and its key is
+//   ((k_c + 1) (Ny + 4) + j_c + 1) (Nx + 4) + i_c + 1,
+// x fastest: the order in which ParticlesInitialize (ParticlesInitialize.f90:
+// 54-119) creates them.  The tiled deposit and the E-field gather rely on it:
+// a chunk of consecutive particles then covers a small box of nodes.  The
+// loop breaks it slowly -- particles cross cells, BCoutflow fills holes with
+// particles from the end of the array, new particles are appended -- and a
+// sort every few hundred steps restores it.
 //
-// The sort is stable: equal keys keep their order, so the result is a
-// function of the particle arrays alone and every later step is
+// The sort is stable: particles of one cell keep their order, so the result
+// is a function of the particle arrays alone and every later step is
 // deterministic.  It is a permutation: every particle keeps every bit, N is a
 // sum of fixed-point integers (order-independent) and every other phase
 // treats particles one by one, so a sorted run holds the same particle set
 // and the same fields as an unsorted one, bit for bit.
 //
-// Particles move ~10^-3 cells per step, so between sorts the array stays a
-// concatenation of long runs of one key.  The sort works on those runs:
+// Particles move ~10^-3 cells per step, so the array stays a concatenation of
+// long runs of one key.  The sort works on those runs:
 //   1. heads: a particle whose key differs from its predecessor's starts a
 //      run; per 2,048-particle tile, the number of heads (one pass over the
 //      keys);
@@ -25,12 +30,13 @@
 //      run's key and start (a second pass).  If no run's key is below the
 //      previous run's, the array is already sorted and nothing moves;
 //   3. the R runs are sorted by key with a stable LSD radix sort (8 bits per
-//      pass; R is ~1/30 of the particles on a developed plasma);
+//      pass; R is a few per cell on a developed plasma);
 //   4. an exclusive scan of the run lengths in sorted order gives every run's
 //      destination, and one pass copies each particle to the other particle
 //      buffer at its run's destination plus its place in the run.
-// Traffic on a developed plasma: two key passes (5 B per CELL32 particle
-// each), the radix sort of the runs, and one copy (29 B read, 29 B written).
+// Traffic on a developed plasma: two key passes (16 B per CELL32 particle
+// each, the offsets decide the cell), the radix sort of the runs, and one
+// copy (29 B read, 29 B written).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -52,27 +58,25 @@ constexpr int kSortWords = kSortTile / 32;            // ballot words per tile
 
 struct SortKeyGeom {
   int nx, ny, nz;
-  int nx3, ny3;
-  int species;
+  int nx4, ny4;
 };
 
-__device__ __forceinline__ uint32_t stencil_sort_key(const SortKeyGeom& G, int i, int j, int k, int s) {
-  i = min(max(i, -1), G.nx + 1);
-  j = min(max(j, -1), G.ny + 1);
-  k = min(max(k, -1), G.nz + 1);
-  s = min(max(s, 0), G.species - 1);
-  const uint32_t node = (uint32_t(k + 1) * uint32_t(G.ny3) + uint32_t(j + 1)) * uint32_t(G.nx3) + uint32_t(i + 1);
-  return node * uint32_t(G.species) + uint32_t(s);
+__device__ __forceinline__ uint32_t cell_sort_key(const SortKeyGeom& G, int i, int j, int k) {
+  i = min(max(i, -1), G.nx + 2);
+  j = min(max(j, -1), G.ny + 2);
+  k = min(max(k, -1), G.nz + 2);
+  return (uint32_t(k + 1) * uint32_t(G.ny4) + uint32_t(j + 1)) * uint32_t(G.nx4) + uint32_t(i + 1);
 }
 
-// CELL32: the base node is the packed cell word.
+// CELL32: the CIC base node plus one where the in-cell offset is >= 1/2.
 struct SortC32 {
   PartC32 a;
   SortKeyGeom G;
   __device__ uint32_t key(long long p) const {
     int i, j, k;
     unpack_cell(__ldg(a.cell + p), i, j, k);
-    return stencil_sort_key(G, i, j, k, __ldg(a.sp + p));
+    return cell_sort_key(G, i + int(__ldg(a.fx + p) >> 31), j + int(__ldg(a.fy + p) >> 31),
+                         k + int(__ldg(a.fz + p) >> 31));
   }
   __device__ void copy(const SortC32& d, long long to, long long from) const {
     d.a.cell[to] = a.cell[from];
@@ -86,16 +90,16 @@ struct SortC32 {
   }
 };
 
-// F64: the base node of ParticlesGridify.f90:65-67, int((x - Lx_min)/dx + 0.5).
+// F64: floor((x - Lx_min)/dx + 1) per axis.
 struct SortF64 {
   PartF64 a;
   SortKeyGeom G;
   double Lx_min, Ly_min, Lz_min, dx, dy, dz;
   __device__ uint32_t key(long long p) const {
-    const int i = __double2int_rz((__ldg(a.x + p) - Lx_min) / dx + 0.5);
-    const int j = __double2int_rz((__ldg(a.y + p) - Ly_min) / dy + 0.5);
-    const int k = __double2int_rz((__ldg(a.z + p) - Lz_min) / dz + 0.5);
-    return stencil_sort_key(G, i, j, k, __ldg(a.sp + p));
+    const int i = __double2int_rd((__ldg(a.x + p) - Lx_min) / dx + 1.0);
+    const int j = __double2int_rd((__ldg(a.y + p) - Ly_min) / dy + 1.0);
+    const int k = __double2int_rd((__ldg(a.z + p) - Lz_min) / dz + 1.0);
+    return cell_sort_key(G, i, j, k);
   }
   __device__ void copy(const SortF64& d, long long to, long long from) const {
     d.a.x[to] = a.x[from];
@@ -436,11 +440,11 @@ int sort_with(picard_ctx* c, const L& src, const L& dst, bool* moved) {
 int sort_particles(picard_ctx* c) {
   if (c->num_local < 2) return PICARD_OK;
   const picard_params& p = c->prm;
-  const long long keys = (long long)(p.nx + 3) * (p.ny + 3) * (p.nz + 3) * p.species;
-  if (keys > 0xffffffffLL) return fail(PICARD_ERR_BAD_ARG, "grid too large for 32-bit stencil keys");
+  const long long keys = (long long)(p.nx + 4) * (p.ny + 4) * (p.nz + 4);
+  if (keys > 0xffffffffLL) return fail(PICARD_ERR_BAD_ARG, "grid too large for 32-bit cell keys");
   c->sort_geom_keys = keys;
   PICARD_TRY(ensure_sort_buffers(c));
-  const SortKeyGeom G{p.nx, p.ny, p.nz, p.nx + 3, p.ny + 3, p.species};
+  const SortKeyGeom G{p.nx, p.ny, p.nz, p.nx + 4, p.ny + 4};
   bool moved = false;
   if (c->layout == PICARD_LAYOUT_F64) {
     const KParams& K = c->K;

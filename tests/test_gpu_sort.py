@@ -1,13 +1,14 @@
-"""The counting sort by CIC stencil (picard_gpu_sort_particles) and the
-warp-aggregated tiled deposit that takes sorted particles.
+"""The counting sort by cell (picard_gpu_sort_particles).
 
 On one rank ParticlesTransfer.f90:488-519 only wraps coordinates; the sort
-sits in its slot.  Bars: the sort equals numpy's stable argsort of the stencil
-keys (base node x fastest, then y and z, species within a node) bit for bit,
-on shuffled, clustered and already sorted arrays in both layouts; the
-deposit gives the same N bits whatever the kernel and the order; and the
-fused loop with a sort every other step holds exactly the same particles
-(as a set), the same sweep counts and the same N, U and E bits as without.
+sits in its slot and puts the particles back in the order ParticlesInitialize
+creates them (cell by cell, x fastest), which cell crossings, BCoutflow's hole
+filling and appended particles wear down.  Bars: the sort equals numpy's
+stable argsort of the cell keys bit for bit, on shuffled, clustered and
+already sorted arrays in both layouts; a freshly initialised plasma is already
+in that order; the deposit gives the same N bits before and after; and the
+fused loop with a sort every other step holds exactly the same particles (as
+a set), the same sweep counts and the same N, U and E bits as without.
 """
 import numpy as np
 import pytest
@@ -37,20 +38,18 @@ def random_particles(p, n, rng, cells=None):
     return rp, ip
 
 
-def stencil_keys(p, rp, ip):
-    """((k+1)(Ny+3) + j+1)(Nx+3) + i+1) S + s: the 0-based CIC base node
-    (ParticlesGridify.f90:65-67) clamped to [-1, N+1], species 0-based."""
+def cell_keys(p, rp):
+    """((k+1)(Ny+4) + j+1)(Nx+4) + i+1 with (i, j, k) = floor((x - L_min)/d + 1),
+    the node-centred cell holding the particle, clamped to [-1, N+2]."""
     lo = np.array([p.Lx_min, p.Ly_min, p.Lz_min])
-    t = (rp[:, :3] - lo) / np.array(list(p.dxyz)) + 0.5
+    t = (rp[:, :3] - lo) / np.array(list(p.dxyz)) + 1.0
     frac = t - np.floor(t)
-    # no particle within 1e-9 cells of a node plane, so the host's base node
-    # is the device's whatever the rounding of either conversion
+    # no particle within 1e-9 cells of a cell face, so the host's cell is the
+    # device's whatever the rounding of either conversion
     assert np.all(np.minimum(frac, 1.0 - frac) > 1e-9)
-    b = np.floor(t).astype(np.int64)
-    hi = np.array([p.nx, p.ny, p.nz]) + 1
-    b = np.clip(b, -1, hi)
-    node = ((b[:, 2] + 1) * (p.ny + 3) + (b[:, 1] + 1)) * (p.nx + 3) + (b[:, 0] + 1)
-    return node * p.species + (ip.astype(np.int64) - 1)
+    c = np.floor(t).astype(np.int64)
+    c = np.clip(c, -1, np.array([p.nx, p.ny, p.nz]) + 2)
+    return ((c[:, 2] + 1) * (p.ny + 4) + (c[:, 1] + 1)) * (p.nx + 4) + (c[:, 0] + 1)
 
 
 def make(layout, nx=16, ny=12, nz=10, n=20000, seed=1, cells=None, **flows):
@@ -72,7 +71,7 @@ def make(layout, nx=16, ny=12, nz=10, n=20000, seed=1, cells=None, **flows):
 @pytest.mark.parametrize("case", ["shuffled", "clustered", "large_grid"])
 def test_sort_equals_stable_argsort(layout, case):
     # shuffled: one run per particle on a 16x12x10 grid (2 radix passes);
-    # clustered: 20,000 particles in 3^3 cells, ~300 per key (stability);
+    # clustered: 20,000 particles in 3^3 cells, ~700 per key (stability);
     # large_grid: 64x32x32, 3 radix passes over ~120,000 runs.
     if case == "shuffled":
         p, g = make(layout, n=20000, seed=2)
@@ -81,7 +80,7 @@ def test_sort_equals_stable_argsort(layout, case):
     else:
         p, g = make(layout, nx=64, ny=32, nz=32, n=120000, seed=4)
     rp, ip = g.particles()
-    order = np.argsort(stencil_keys(p, rp, ip), kind="stable")
+    order = np.argsort(cell_keys(p, rp), kind="stable")
     g.sort_particles()
     assert g.num_local == len(ip)
     rs, is_ = g.particles()
@@ -95,33 +94,43 @@ def test_sort_equals_stable_argsort(layout, case):
     g.close()
 
 
-@pytest.mark.parametrize("flows", [dict(), dict(yflow=0), dict(xflow=0, zflow=0)])
-def test_stencil_deposit_equals_tiled_deposit(flows):
-    # The same particles deposited by the tiled kernel (OPT_DEPOSIT 1) and its
-    # warp-aggregated form (2), unsorted and sorted: N and C bit for bit.
-    p, g = make("cell32", n=60000, seed=5, **flows)
-    out = []
-    for sort in (False, True):
-        if sort:
-            g.sort_particles()
-        for kernel in (1, 2):
-            g.set_option(capi.OPT_DEPOSIT, kernel)
-            g.particles_gridify()
-            out.append((g.field(capi.FIELD_N), g.field(capi.FIELD_C)))
-    for n_, c_ in out[1:]:
-        np.testing.assert_array_equal(n_, out[0][0])
-        np.testing.assert_array_equal(c_, out[0][1])
-    assert np.abs(out[0][0]).sum() > 0
+@pytest.mark.parametrize("layout", list(LAYOUTS))
+def test_initialised_plasma_is_in_cell_order(layout):
+    # ParticlesInitialize creates the particles cell by cell, x fastest: the
+    # sort finds no run out of order and moves nothing.
+    p = O.derive(small_haser(nx=16, ny=12, nz=10, ppc=4, seed=8))
+    g = Simulation(p, derive=False, **LAYOUTS[layout])
+    g.particles_initialize()
+    rp, ip = g.particles()
+    assert np.all(np.diff(cell_keys(p, rp)) >= 0)
+    g.sort_particles()
+    r2, i2 = g.particles()
+    np.testing.assert_array_equal(i2, ip)
+    np.testing.assert_array_equal(r2, rp)
     g.close()
 
 
-def test_stencil_deposit_matches_oracle():
-    # The warp-aggregated kernel on sorted particles against the FP64 oracle's
-    # ParticlesGridify of the same particles (the bar of the other CELL32
-    # deposits: 1e-10 relative L2).
+@pytest.mark.parametrize("flows", [dict(), dict(yflow=0), dict(xflow=0, zflow=0)])
+def test_deposit_after_sort_is_bit_identical(flows):
+    # The same particles deposited before and after the sort (the tiled
+    # kernel, in random order and in cell order): N and C bit for bit.
+    p, g = make("cell32", n=60000, seed=5, **flows)
+    g.particles_gridify()
+    n0, c0 = g.field(capi.FIELD_N), g.field(capi.FIELD_C)
+    g.sort_particles()
+    g.particles_gridify()
+    np.testing.assert_array_equal(g.field(capi.FIELD_N), n0)
+    np.testing.assert_array_equal(g.field(capi.FIELD_C), c0)
+    assert np.abs(n0).sum() > 0
+    g.close()
+
+
+def test_sorted_deposit_matches_oracle():
+    # The deposit of sorted particles against the FP64 oracle's
+    # ParticlesGridify of the same particles (the bar of the CELL32 deposit:
+    # 1e-10 relative L2).
     p, g = make("cell32", n=40000, seed=6, yflow=0)
     g.sort_particles()
-    g.set_option(capi.OPT_DEPOSIT, 2)
     g.particles_gridify()
     o = O.OracleState(p)
     o.set_particles(*g.particles())
@@ -164,7 +173,5 @@ def test_sort_option_is_checked():
     p, g = make("cell32", n=1000, seed=7)
     with pytest.raises(capi.PicardError):
         g.set_option(capi.OPT_SORT_EVERY, -1)
-    with pytest.raises(capi.PicardError):
-        g.set_option(capi.OPT_DEPOSIT, 3)
-    assert g.get_option(capi.OPT_DEPOSIT) == 0
+    assert g.get_option(capi.OPT_SORT_EVERY) == 0
     g.close()
