@@ -162,16 +162,46 @@ __device__ inline void wrap_c32(const KParams& P, C32& c) {
   if (above(c.i, c.f[0], P.nx)) c.i -= P.nx;
 }
 
+__device__ __forceinline__ void advance_one(const KParams& P, uint32_t& cell, uint32_t& fx, uint32_t& fy, uint32_t& fz,
+                                            float vx, float vy, float vz, float dtdx, float dtdy, float dtdz) {
+  int i, j, k;
+  unpack_cell(cell, i, j, k);
+  move_axis(i, fx, vx * dtdx, P.nx, P.xflow);
+  move_axis(j, fy, vy * dtdy, P.ny, P.yflow);
+  move_axis(k, fz, vz * dtdz, P.nz, P.zflow);
+  cell = pack_cell(i, j, k);
+}
+
+// Four particles per thread and pass with 16-byte loads and stores (the
+// particle arrays are 256-byte aligned): seven loads of 16 bytes in flight per
+// thread instead of seven of 4.  The remainder n % 4 goes one by one.
 __global__ void advance_position_c32_kernel(KParams P, PartC32 a, long long n, float dtdx, float dtdy, float dtdz) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    C32 c = load_pos(a, p);
-    move_axis(c.i, c.f[0], a.vx[p] * dtdx, P.nx, P.xflow);
-    move_axis(c.j, c.f[1], a.vy[p] * dtdy, P.ny, P.yflow);
-    move_axis(c.k, c.f[2], a.vz[p] * dtdz, P.nz, P.zflow);
-    a.cell[p] = pack_cell(c.i, c.j, c.k);
-    a.fx[p] = c.f[0];
-    a.fy[p] = c.f[1];
-    a.fz[p] = c.f[2];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long n4 = n >> 2;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+    uint4 c = reinterpret_cast<const uint4*>(a.cell)[q];
+    uint4 x = reinterpret_cast<const uint4*>(a.fx)[q];
+    uint4 y = reinterpret_cast<const uint4*>(a.fy)[q];
+    uint4 z = reinterpret_cast<const uint4*>(a.fz)[q];
+    const float4 u = reinterpret_cast<const float4*>(a.vx)[q];
+    const float4 v = reinterpret_cast<const float4*>(a.vy)[q];
+    const float4 w = reinterpret_cast<const float4*>(a.vz)[q];
+    advance_one(P, c.x, x.x, y.x, z.x, u.x, v.x, w.x, dtdx, dtdy, dtdz);
+    advance_one(P, c.y, x.y, y.y, z.y, u.y, v.y, w.y, dtdx, dtdy, dtdz);
+    advance_one(P, c.z, x.z, y.z, z.z, u.z, v.z, w.z, dtdx, dtdy, dtdz);
+    advance_one(P, c.w, x.w, y.w, z.w, u.w, v.w, w.w, dtdx, dtdy, dtdz);
+    reinterpret_cast<uint4*>(a.cell)[q] = c;
+    reinterpret_cast<uint4*>(a.fx)[q] = x;
+    reinterpret_cast<uint4*>(a.fy)[q] = y;
+    reinterpret_cast<uint4*>(a.fz)[q] = z;
+  }
+  for (long long p = 4 * n4 + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    uint32_t c = a.cell[p], x = a.fx[p], y = a.fy[p], z = a.fz[p];
+    advance_one(P, c, x, y, z, a.vx[p], a.vy[p], a.vz[p], dtdx, dtdy, dtdz);
+    a.cell[p] = c;
+    a.fx[p] = x;
+    a.fy[p] = y;
+    a.fz[p] = z;
   }
 }
 
@@ -179,17 +209,28 @@ __global__ void advance_position_c32_kernel(KParams P, PartC32 a, long long n, f
 // wrap, so interior cells are decided from the cell word alone, the in-cell
 // offsets are read only for the rest, and a cell word is written only when it
 // changes.
+__device__ __forceinline__ void transfer_one(const KParams& P, const PartC32& a, long long p, uint32_t cell) {
+  const uint32_t cx = cell & kCellMaskX, cy = (cell >> kCellBitsX) & kCellMaskY, cz = cell >> (kCellBitsX + kCellBitsY);
+  if (cx - 2u < uint32_t(P.nx - 1) && cy - 2u < uint32_t(P.ny - 1) && cz - 2u < uint32_t(P.nz - 1)) return;
+  C32 c = load_pos(a, p);
+  wrap_c32(P, c);
+  const uint32_t moved = pack_cell(c.i, c.j, c.k);
+  if (moved != cell) a.cell[p] = moved;
+}
+
+// Cell words four at a time (16-byte loads), the remainder one by one.
 __global__ void transfer_c32_kernel(KParams P, PartC32 a, long long n) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const uint32_t cell = a.cell[p];
-    const uint32_t cx = cell & kCellMaskX, cy = (cell >> kCellBitsX) & kCellMaskY,
-                   cz = cell >> (kCellBitsX + kCellBitsY);
-    if (cx - 2u < uint32_t(P.nx - 1) && cy - 2u < uint32_t(P.ny - 1) && cz - 2u < uint32_t(P.nz - 1)) continue;
-    C32 c = load_pos(a, p);
-    wrap_c32(P, c);
-    const uint32_t moved = pack_cell(c.i, c.j, c.k);
-    if (moved != cell) a.cell[p] = moved;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long n4 = n >> 2;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+    const uint4 c = reinterpret_cast<const uint4*>(a.cell)[q];
+    transfer_one(P, a, 4 * q, c.x);
+    transfer_one(P, a, 4 * q + 1, c.y);
+    transfer_one(P, a, 4 * q + 2, c.z);
+    transfer_one(P, a, 4 * q + 3, c.w);
   }
+  for (long long p = 4 * n4 + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride)
+    transfer_one(P, a, p, a.cell[p]);
 }
 
 // BCoutflow.f90:28-53 and ParticlesTransfer.f90:494-519 on the CELL32

@@ -84,3 +84,34 @@ def test_long_run_energy_log_and_density_moments(oracle_run, name, kw, tol):
         for ax in range(3):
             assert abs(a[1][ax] - b[1][ax]) <= tol["m1"], (name, s, ax, "centre")
             assert abs(a[2][ax] - b[2][ax]) <= tol["m2"] * b[2][ax], (name, s, ax, "spread")
+
+
+def test_long_fused_run_with_sort_keeps_the_moments(oracle_run):
+    # The benchmarked path over the same 100 steps: picard_gpu_run_fused in
+    # CELL32 with the FP32-refine Jacobi, the particles put back in cell order
+    # every 10 steps.  The particle count, the energies after the last step and
+    # the density moments meet the CELL32 bars above.
+    p, elog, mo = oracle_run
+    tol = dict(n=1e-5, uP=1e-6, uE=1e-3, uB=1e-11, m0=1e-9, m1=1e-4, m2=1e-5)
+    g = Simulation(p, derive=False, layout=capi.LAYOUT_CELL32, solver=capi.SOLVER_F32_REFINE)
+    g.set_option(capi.OPT_SORT_EVERY, 10)
+    g.calc_distance()
+    g.particles_initialize()
+    g.run_fused(0, STEPS)
+    n = g.num_local
+    up, ue, ub = (float(v) / p.u0 for v in g.energy())
+    mg = _moments(g.field(capi.FIELD_N))
+    g.close()
+    it, n_o, up_o, ue_o, ub_o = elog[-1]
+    assert it == STEPS
+    print(f"fused + sort, step {it}: particles {n} vs {n_o}, kinetic {up / up_o - 1:.1e}, "
+          f"field {ue / ue_o - 1:.1e}, magnetic {ub / ub_o - 1:.1e}")
+    assert abs(n - n_o) <= tol["n"] * n_o
+    assert abs(up - up_o) <= tol["uP"] * abs(up_o)
+    assert abs(ue - ue_o) <= tol["uE"] * abs(ue_o)
+    assert abs(ub - ub_o) <= tol["uB"] * abs(ub_o)
+    for s, (a, b) in enumerate(zip(mg, mo)):
+        assert abs(a[0] - b[0]) <= tol["m0"] * b[0], (s, "total")
+        for ax in range(3):
+            assert abs(a[1][ax] - b[1][ax]) <= tol["m1"], (s, ax, "centre")
+            assert abs(a[2][ax] - b[2][ax]) <= tol["m2"] * b[2][ax], (s, ax, "spread")
