@@ -297,8 +297,8 @@ typedef enum picard_option {
    * Nothing else uses it. */
   PICARD_OPT_WAIT_TEST = 7,
   /* 1: the x-pair sweep reads r from global memory and stages only the w box
-   * (with one CTA per tile and one stage; otherwise ignored); 0 r box by TMA.
-   * Never changes a result bit. */
+   * (with one CTA per tile and one stage, or two sweeps per launch; otherwise
+   * ignored); 0 r box by TMA.  Never changes a result bit. */
   PICARD_OPT_SWEEP_R_GLOBAL = 8,
   /* k > 0: picard_gpu_run_fused sorts the particles by cell
    * (picard_gpu_sort_particles) in the ParticlesTransfer slot of every

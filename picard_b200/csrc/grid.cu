@@ -671,10 +671,18 @@ __global__ void __launch_bounds__(256, 7) sweep_tma2r_kernel(const __grid_consta
 // sweep_tma2_kernel (per-column FP32 sums in z order, the 32-lane tree, rows
 // in order), so results are bit-identical to two single sweeps.  L2 traffic
 // per sweep drops from ~15 to ~10.6 bytes per node and launches halve.
-template <int ZC>
+//
+// RG: r is read from global memory (8-byte pair loads, only where a pair has
+// a node inside the domain; the value elsewhere is never used), so only the w
+// box is staged: 70.7 KB of shared memory at ZC = 8 instead of 99.5, three
+// CTAs per SM instead of two.  The CTA then has 12 rows of 32 threads, so the
+// 340 x-pair columns of the first sweep's tile-plus-halo take one pass; the
+// second sweep runs on the first 8 rows.  The same arithmetic on the same
+// values: the same bits.
+template <int ZC, bool RG = false>
 struct Sweep2Smem {
   static constexpr int kW0 = (ZC + 4) * 12 * kTma2BoxX;  // w_{s-1}: [ZC+4][12][72]
-  static constexpr int kR = (ZC + 2) * 10 * kTma2BoxX;   // r:       [ZC+2][10][72]
+  static constexpr int kR = RG ? 0 : (ZC + 2) * 10 * kTma2BoxX;  // r: [ZC+2][10][72]
   static constexpr int kW1X = 68;
   static constexpr int kW1 = (ZC + 2) * 10 * kW1X;       // w_s:     [ZC+2][10][68]
   static constexpr int kCS = kTmaTy * kTma2Tile;         // sweep-s column sums [8][64]
@@ -695,13 +703,13 @@ __device__ __forceinline__ double pair_row_tree(float c0, float c1) {
   return v0 + v1;
 }
 
-template <int ZC>
-__global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__ CUtensorMap tw,
-                                                         const __grid_constant__ CUtensorMap tr, Stencil S,
-                                                         JacobiCoefF J, float* __restrict__ wout, double* partialA,
-                                                         double* partialB, int w_zero, int gx2, int gx, int gy,
-                                                         int ntiles, int* err) {
-  using L = Sweep2Smem<ZC>;
+template <int ZC, bool RG>
+__global__ void __launch_bounds__(RG ? 384 : 256, RG ? 3 : 1)
+    sweep2_tma_kernel(const __grid_constant__ CUtensorMap tw, const __grid_constant__ CUtensorMap tr,
+                      const float* __restrict__ rg, Stencil S, JacobiCoefF J, float* __restrict__ wout,
+                      double* partialA, double* partialB, int w_zero, int gx2, int gx, int gy, int ntiles, int* err) {
+  using L = Sweep2Smem<ZC, RG>;
+  constexpr int kThreads2 = RG ? 384 : 256;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float* W0 = reinterpret_cast<float*>(smem_raw);
   float* R = W0 + L::kW0;
@@ -725,7 +733,9 @@ __global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__
   if (t >= ntiles) return;
   const int bx2 = t % gx2, by = (t / gx2) % gy, bz = t / (gx2 * gy);
   const int x0 = bx2 * kTma2Tile, y0 = by * kTmaTy, z0 = bz * ZC;
-  if (tid == 0) {
+  // RG with a zero entering iterate: nothing to stage
+  const bool staged = !RG || !w_zero;
+  if (tid == 0 && staged) {
     uint32_t bytes = (uint32_t)(L::kR * sizeof(float));
     if (!w_zero) bytes += (uint32_t)(L::kW0 * sizeof(float));
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
@@ -735,17 +745,20 @@ __global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__
           ::"r"((uint32_t)__cvta_generic_to_shared(W0)), "l"((unsigned long long)&tw), "r"(x0), "r"(y0 - 1),
           "r"(z0 - 1), "r"(mb)
           : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-        ::"r"((uint32_t)__cvta_generic_to_shared(R)), "l"((unsigned long long)&tr), "r"(x0), "r"(y0), "r"(z0),
-        "r"(mb)
-        : "memory");
+    if (!RG)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+          ::"r"((uint32_t)__cvta_generic_to_shared(R)), "l"((unsigned long long)&tr), "r"(x0), "r"(y0), "r"(z0),
+          "r"(mb)
+          : "memory");
   }
-  const bool ok = __syncthreads_and(mbar_wait(mb, 0, kMbarSpin) ? 1 : 0);
-  if (!ok) {
-    if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
-    mbar_wait(mb, 0, kMbarSpin);
-    return;
+  if (staged) {
+    const bool ok = __syncthreads_and(mbar_wait(mb, 0, kMbarSpin) ? 1 : 0);
+    if (!ok) {
+      if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+      mbar_wait(mb, 0, kMbarSpin);
+      return;
+    }
   }
   const unsigned long long m2 = pk2(-2.0f, -2.0f), ix2 = pk2(J.idx2, J.idx2), iy2 = pk2(J.idy2, J.idy2),
                            iz2 = pk2(J.idz2, J.idz2), naf = pk2(-J.af, -J.af);
@@ -762,7 +775,7 @@ __global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__
   auto u64at = [](const float* base, int idx) { return *reinterpret_cast<const unsigned long long*>(base + idx); };
 
   // ---- sweep s on the tile and its one-node halo: 34 x-pairs x 10 rows, z marching
-  for (int item = tid; item < 34 * 10; item += 256) {
+  for (int item = tid; item < 34 * 10; item += kThreads2) {
     const int p = item % 34, ry = item / 34;
     const int xr = 2 * p - 2, yr = ry - 1;  // first node of the pair, tile-relative
     const int i0 = x0 + 1 + xr, j = y0 + 1 + yr;
@@ -787,9 +800,13 @@ __global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__
         xl = w0s(zr, -1);
         xrr = w0s(zr, 2);
       }
-      const unsigned long long rr = u64at(R, ((zr + 1) * 10 + (yr + 1)) * kTma2BoxX + xr + 4);
-      const unsigned long long res = node_res(wc, xl, xrr, ym, yp, wm, wp, rr);
       const bool kin = k >= 1 && k <= S.nz;
+      unsigned long long rr;
+      if (RG)
+        rr = ((in0 || in1) && kin) ? __ldg(reinterpret_cast<const unsigned long long*>(rg + fidx(S, i0, j, k))) : 0ull;
+      else
+        rr = u64at(R, ((zr + 1) * 10 + (yr + 1)) * kTma2BoxX + xr + 4);
+      const unsigned long long res = node_res(wc, xl, xrr, ym, yp, wm, wp, rr);
       const float2 rf = up2(res);
       const float2 wn = up2(fma2(naf, res, wc));
       const bool a0 = in0 && kin, a1 = in1 && kin;
@@ -806,7 +823,9 @@ __global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__
   }
   __syncthreads();
 
-  // ---- sweep s+1 on the tile from w_s in shared memory
+  // ---- sweep s+1 on the tile from w_s in shared memory (rows ty < 8; whole
+  // warps, so the shuffles below see full warps)
+  if (!RG || ty < kTmaTy) {
   const int i0 = x0 + 2 * tx + 1, j = y0 + ty + 1;
   const bool act0 = i0 <= S.nx && j <= S.ny, act1 = i0 + 1 <= S.nx && j <= S.ny;
   const int kend = min(ZC, S.nz - z0);
@@ -820,7 +839,12 @@ __global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__
   for (int zr = 0; zr < ZC; ++zr) {
     if (zr < kend) {
       const unsigned long long wp = w1(zr + 1, 0);
-      const unsigned long long rr = u64at(R, ((zr + 1) * 10 + (ty + 1)) * kTma2BoxX + 2 * tx + 4);
+      unsigned long long rr;
+      if (RG)
+        rr = (act0 || act1) ? __ldg(reinterpret_cast<const unsigned long long*>(rg + fidx(S, i0, j, z0 + 1 + zr)))
+                            : 0ull;
+      else
+        rr = u64at(R, ((zr + 1) * 10 + (ty + 1)) * kTma2BoxX + 2 * tx + 4);
       const unsigned long long res = node_res(wc, w1s(zr, -1), w1s(zr, 2), w1(zr, -1), w1(zr, 1), wm, wp, rr);
       const float2 rf = up2(res);
       const unsigned long long resm = pk2(act0 ? rf.x : 0.0f, act1 ? rf.y : 0.0f);
@@ -844,6 +868,7 @@ __global__ void __launch_bounds__(256) sweep2_tma_kernel(const __grid_constant__
   if ((tx & 15) == 0) {
     rows[0][tx >> 4][ty] = rowA;
     rows[1][tx >> 4][ty] = rowB;
+  }
   }
   __syncthreads();
   if (tid < 4) {
@@ -1272,14 +1297,15 @@ cudaError_t launch_sweep_tma2(const KParams& P, const JacobiGeom& G, const CUten
   return cudaErrorInvalidValue;
 }
 
-template <int ZC>
+template <int ZC, bool RG>
 static cudaError_t launch_sweep2_zc(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw,
-                                    const CUtensorMap* tr, float* wout, double* partialA, double* partialB,
-                                    int w_zero, int* err, cudaStream_t st) {
-  const size_t smem = Sweep2Smem<ZC>::kBytes;
+                                    const CUtensorMap* tr, const float* r, float* wout, double* partialA,
+                                    double* partialB, int w_zero, int* err, cudaStream_t st) {
+  const size_t smem = Sweep2Smem<ZC, RG>::kBytes;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(sweep2_tma_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(sweep2_tma_kernel<ZC, RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -1287,7 +1313,7 @@ static cudaError_t launch_sweep2_zc(const KParams& P, const JacobiGeom& G, const
   const int ntiles = gx2 * (int)G.grid.y * (int)G.grid.z;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(ntiles);
-  cfg.blockDim = dim3(kTmaTx, kTmaTy);
+  cfg.blockDim = dim3(kTmaTx, RG ? 12 : kTmaTy);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
@@ -1296,16 +1322,21 @@ static cudaError_t launch_sweep2_zc(const KParams& P, const JacobiGeom& G, const
   cfg.attrs = at;
   cfg.numAttrs = 1;
   note_launch();
-  return cudaLaunchKernelEx(&cfg, sweep2_tma_kernel<ZC>, *tw, *tr, make_stencil(P), jacobi_coef_f(P), wout, partialA,
-                            partialB, w_zero, gx2, (int)G.grid.x, (int)G.grid.y, ntiles, err);
+  return cudaLaunchKernelEx(&cfg, sweep2_tma_kernel<ZC, RG>, *tw, *tr, r, make_stencil(P), jacobi_coef_f(P), wout,
+                            partialA, partialB, w_zero, gx2, (int)G.grid.x, (int)G.grid.y, ntiles, err);
 }
 
 cudaError_t launch_sweep2_tma(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
-                              float* wout, double* partialA, double* partialB, int w_zero, int* err,
+                              const float* r, float* wout, double* partialA, double* partialB, int w_zero, int* err,
                               cudaStream_t st) {
+  const bool rg = G.rglobal != 0;
   switch (G.zc) {
-    case 4: return launch_sweep2_zc<4>(P, G, tw, tr, wout, partialA, partialB, w_zero, err, st);
-    case 8: return launch_sweep2_zc<8>(P, G, tw, tr, wout, partialA, partialB, w_zero, err, st);
+    case 4:
+      return rg ? launch_sweep2_zc<4, true>(P, G, tw, tr, r, wout, partialA, partialB, w_zero, err, st)
+                : launch_sweep2_zc<4, false>(P, G, tw, tr, r, wout, partialA, partialB, w_zero, err, st);
+    case 8:
+      return rg ? launch_sweep2_zc<8, true>(P, G, tw, tr, r, wout, partialA, partialB, w_zero, err, st)
+                : launch_sweep2_zc<8, false>(P, G, tw, tr, r, wout, partialA, partialB, w_zero, err, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -29,7 +29,7 @@ struct JacobiGeom {
   int stages = 1;  // shared-memory stages per CTA (2: the next tile is prefetched)
   int pairs = 0;   // 1: the x-pair kernel (64-wide tiles)
   int fused2 = 0;  // 1 (with pairs): two sweeps per launch where a batch allows
-  int rglobal = 0; // 1 (with pairs, one CTA per tile, one stage): r read from global memory
+  int rglobal = 0; // 1 (with pairs, one CTA per tile, one stage, or fused2): r read from global memory
   // register-resident sweeps (jacobi_resident.cu): one cooperative launch per
   // batch of sweeps over CTAs of 32 x res_by x res_nz nodes
   int res = 0;
@@ -58,10 +58,11 @@ cudaError_t launch_sweep_tma2(const KParams& P, const JacobiGeom& G, const CUten
 int sweep_tma2_occupancy(const JacobiGeom& G, int stages);
 // Sweeps s and s+1 in one launch (x pairs, temporal blocking; zc 4 or 8):
 // reads w_{s-1} through tw (boxes 72 x 12 x zc+4) and r through tr (boxes 72 x
-// 10 x zc+2), writes w_{s+1} and the partials of sweep s (partialA) and s+1
-// (partialB); bit-identical to two launch_sweep_tma2 calls.
+// 10 x zc+2) -- or, with G.rglobal, r from global memory at r -- writes
+// w_{s+1} and the partials of sweep s (partialA) and s+1 (partialB);
+// bit-identical to two launch_sweep_tma2 calls.
 cudaError_t launch_sweep2_tma(const KParams& P, const JacobiGeom& G, const CUtensorMap* tw, const CUtensorMap* tr,
-                              float* wout, double* partialA, double* partialB, int w_zero, int* err,
+                              const float* r, float* wout, double* partialA, double* partialB, int w_zero, int* err,
                               cudaStream_t st);
 int sweep_tma2_tiles(const KParams& P, const JacobiGeom& G);
 // CTAs of one SM the TMA sweep kernel of this geometry can hold.

@@ -361,15 +361,17 @@ __device__ inline void boris_c32(const KParams& P, const SpeciesF32& S, int s, i
 
 __global__ void __launch_bounds__(256, 6) advance_velocity_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, long long n,
                                                                       const float4* E, int mode) {
+  // streaming loads and stores for the particles, so that they leave the E
+  // table in L2 (as in push_advance_c32_kernel)
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    C32 c = load_pos(a, p);
+    C32 c = load_pos_cs(a, p);
     float Ep[3];
     gather_c32(P, c, E, Ep);
-    float v[3] = {a.vx[p], a.vy[p], a.vz[p]};
-    boris_c32(P, S, a.sp[p], mode, Ep, v);
-    a.vx[p] = v[0];
-    a.vy[p] = v[1];
-    a.vz[p] = v[2];
+    float v[3] = {__ldcs(a.vx + p), __ldcs(a.vy + p), __ldcs(a.vz + p)};
+    boris_c32(P, S, __ldcs(a.sp + p), mode, Ep, v);
+    __stcs(a.vx + p, v[0]);
+    __stcs(a.vy + p, v[1]);
+    __stcs(a.vz + p, v[2]);
   }
 }
 

@@ -186,7 +186,7 @@ int run_sweeps_single(picard_ctx* c, int count, int rsel, double* partial_base, 
     // sweeps t and t+1 per launch
     for (; t + 1 <= count; t += 2) {
       const int out = 1 - *wcur;
-      PICARD_CUDA(launch_sweep2_tma(K, c->G, &c->tmw3[*wcur], &c->tmr3[rsel], c->w[out],
+      PICARD_CUDA(launch_sweep2_tma(K, c->G, &c->tmw3[*wcur], &c->tmr3[rsel], R[rsel], c->w[out],
                                     partial_base + (size_t)(t - 1) * nb, partial_base + (size_t)t * nb,
                                     t == 1 ? 1 : 0, c->d_err, c->st));
       *wcur = out;
@@ -515,7 +515,8 @@ int tune_sweep(picard_ctx* c, bool fresh) {
     }
   }
   if (c->G.zc <= 8)
-    for (int pdl = 1; pdl >= 0; --pdl) cand.push_back({0, pdl, 1, 0, 1, 1, 0});  // two sweeps per launch
+    for (int pdl = 1; pdl >= 0; --pdl)
+      for (int rg = 0; rg <= 1; ++rg) cand.push_back({0, pdl, 1, 0, 1, 1, rg});  // two sweeps per launch
   for (int q = 0; q < kResidentShapes; ++q) {
     JacobiGeom g = c->G;
     if (resident_plan(c->K, g, q)) cand.push_back({0, 0, 1, q + 1, 0, 0, 0});
@@ -540,7 +541,7 @@ int tune_sweep(picard_ctx* c, bool fresh) {
         auto one = [&](int s) {
           const int in = (s - 1) % 2, out = 1 - in;
           if (c->G.fused2)  // sweeps s, s+1
-            return launch_sweep2_tma(c->K, c->G, &c->tmw3[in], &c->tmr3[0], c->w[out], c->partials,
+            return launch_sweep2_tma(c->K, c->G, &c->tmw3[in], &c->tmr3[0], c->r, c->w[out], c->partials,
                                      c->partials + c->G.nblocks, 0, c->d_err, c->st);
           return c->G.pairs ? launch_sweep_tma2(c->K, c->G, &c->tmw2[in], &c->tmr2[0], c->r, c->w[out], c->partials,
                                                 0, c->d_err, c->st)

@@ -293,15 +293,15 @@ def test_sweep_variant_does_not_change_bits(dims):
     variants = ([("tma", -1, 0, 1), ("tma", -1, 1, 1), ("tma", 7, 1, 2), ("tma", 40, 0, 2), ("tma", 64, 1, 1),
                  ("tma", -1, 1, 2), ("pairs", -1, 1, 1), ("pairs", -1, 0, 2), ("pairs", 5, 1, 2),
                  ("pairs", 30, 0, 1), ("fused", -1, 1, 1), ("fused", -1, 0, 1), ("rglobal", -1, 1, 1),
-                 ("rglobal", -1, 0, 1)]
+                 ("rglobal", -1, 0, 1), ("fused_rglobal", -1, 1, 1), ("fused_rglobal", -1, 0, 1)]
                 + [("resident", q, 0, 0) for q in range(1, 6)])
     results = []
     for kind, a, b, c_ in variants:
-        if kind in ("tma", "pairs", "fused", "rglobal"):
+        if kind in ("tma", "pairs", "fused", "rglobal", "fused_rglobal"):
             g.set_option(capi.OPT_SWEEP_RESIDENT, 0)
             g.set_option(capi.OPT_SWEEP_PAIRS, 0 if kind == "tma" else 1)
-            g.set_option(capi.OPT_SWEEP_FUSED, 1 if kind == "fused" else 0)
-            g.set_option(capi.OPT_SWEEP_R_GLOBAL, 1 if kind == "rglobal" else 0)
+            g.set_option(capi.OPT_SWEEP_FUSED, 1 if kind.startswith("fused") else 0)
+            g.set_option(capi.OPT_SWEEP_R_GLOBAL, 1 if kind.endswith("rglobal") else 0)
             g.set_option(capi.OPT_SWEEP_CTAS, a)
             g.set_option(capi.OPT_SWEEP_PDL, b)
             g.set_option(capi.OPT_SWEEP_STAGES, c_)
