@@ -364,7 +364,7 @@ int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver,
   b += 8.0 * (double)s.cells;                // produce counts + offsets
   b += 8.0 * (double)s.nb_compact * (3 + kOutflowWordsPerBlock);  // BCoutflow scratch
   b += 8.0 * (double)s.nb_inflow * 2;        // fused BCinflow scan
-  b += 8.0 * 1025.0 * s.nb_jacobi;           // sweep partials
+  b += 8.0 * (kMaxSweepsPerRound + 1.0) * s.nb_jacobi;  // sweep partials
   if (layout == PICARD_LAYOUT_CELL32) {      // tensor-core BCpotentials scratch
     long long cs = 0, pe = 0;
     bcpot_tc_scratch(make_kparams(*p), &cs, &pe);

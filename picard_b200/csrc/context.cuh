@@ -9,6 +9,11 @@
 #include "kernels.cuh"
 
 namespace picard {
+// Longest round of FP32 sweeps between two FP64 anchors (solve_f32.cuh): the
+// host reads a round's residual norms in one copy, so fewer, longer rounds mean
+// fewer host round trips and anchor passes per solve.
+constexpr int kMaxSweepsPerRound = 4096;
+
 // Scratch of the counting sort by cell (sort.cu), sized for `cap`
 // particles on first use.
 struct SortBuf {
@@ -65,7 +70,7 @@ struct picard_ctx {
   double* partials = nullptr;  // [m_max + 1][nblocks]
   double* r2 = nullptr;        // [m_max + 1]
   picard::JacobiGeom G;
-  int m_max = 1024;
+  int m_max = picard::kMaxSweepsPerRound;
   double last_residual = 0.0, last_bnorm = 0.0;
   long long last_sweeps = 0;
 

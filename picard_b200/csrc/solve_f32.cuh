@@ -40,7 +40,7 @@ struct F32Solve {
 };
 
 // CalcEpotential's set-up and wrap-up around the solve loop.
-constexpr int kPinnedB2 = 1024 + 8;  // slot of ||b||^2 in ctx->h_pinned (past the r2 copies)
+constexpr int kPinnedB2 = kMaxSweepsPerRound + 8;  // slot of ||b||^2 in ctx->h_pinned (past the r2 copies)
 struct EpotSetup {
   double bnorm = 0.0, tol = 0.0, sigma = 1.0;
   long long smax = 0;
