@@ -133,7 +133,12 @@ PICARD_API int picard_gpu_destroy(picard_ctx* ctx);
 PICARD_API int picard_gpu_synchronize(picard_ctx* ctx);
 PICARD_API const char* picard_gpu_last_error(void);
 /* Device bytes held by a context created with these arguments (for admission
- * by memory budget); nothing is allocated. */
+ * by memory budget); nothing is allocated.  Not counted: buffers a context
+ * allocates on first use -- the flux accumulators of GridifyAll (48 B per
+ * node and species), the second particle buffer and scratch of
+ * picard_gpu_sort_particles, and the pointer-jumping scratch of
+ * picard_gpu_bc_outflow (8 B per removed particle, up to 8 B per particle of
+ * capacity). */
 PICARD_API int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver, uint64_t* bytes);
 
 /* Particles in the reference layout: real_particles(8, n) column-major
