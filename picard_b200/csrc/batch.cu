@@ -11,10 +11,12 @@
 // run table (tensor maps, stencil, coefficients, output, tile range) rides in
 // the kernel parameters -- instead of one launch per run.  Anchors, reductions
 // and the stop tests stay per run, asynchronous to the ticks; runs that
-// converge drop out.  The sweep kernels are the x-pair TMA sweep and, on
-// request, the 32-wide one, with the same per-node arithmetic and per-tile
-// partials as the single-run kernels, so every run's result is bit-identical
-// to the same run advanced alone with picard_gpu_run_fused.
+// converge drop out.  One launch per tick covers every run: each CTA takes
+// the tile body of its run's class -- the x-pair TMA sweep, or the 32-wide one
+// for runs whose x extent would leave half of a 64-wide tile empty -- with the
+// same per-node arithmetic and per-tile partials as the single-run kernels,
+// so every run's result is bit-identical to the same run advanced alone with
+// picard_gpu_run_fused.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -56,6 +58,7 @@ struct alignas(64) BatchRun {
   float* wout;
   double* partial;
   int gx2, gx, gy, tiles, tile_base, w_zero;
+  int zc, w32;  // the run's tile depth and width (sweep_batch_any_kernel)
 };
 
 struct BatchArgs {
@@ -233,6 +236,150 @@ __global__ void __launch_bounds__(256) sweep_batch32_kernel(const __grid_constan
                    R.w_zero, bx, by, bz);
 }
 
+// Bounded wait for a CTA's TMA boxes; false (after recording kDevTimeout and
+// letting the copies land, also bounded) when they did not arrive.
+__device__ inline bool batch_wait_boxes(uint32_t mb, int tid, int* err) {
+  bool done = false;
+  for (long long it = 0; it < (1LL << 24); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(mb), "r"(0u)
+        : "memory");
+    if (ok) {
+      done = true;
+      break;
+    }
+  }
+  if (__syncthreads_and(done ? 1 : 0)) return true;
+  if (tid == 0) atomicCAS(err, 0, int(kDevTimeout));
+  for (long long it = 0; it < (1LL << 24); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(mb), "r"(0u)
+        : "memory");
+    if (ok) break;
+  }
+  return false;
+}
+
+// Issue one tile's w and r boxes (w only when the entering iterate is not zero).
+__device__ inline void batch_issue_boxes(const BatchRun& R, uint32_t mb, float* sw, float* sr, uint32_t wbytes,
+                                         uint32_t rbytes, int x0, int y0, int z0) {
+  uint32_t bytes = rbytes;
+  if (!R.w_zero) bytes += wbytes;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+  if (!R.w_zero)
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"((uint32_t)__cvta_generic_to_shared(sw)), "l"((unsigned long long)&R.tw), "r"(x0), "r"(y0), "r"(z0),
+        "r"(mb)
+        : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"((uint32_t)__cvta_generic_to_shared(sr)), "l"((unsigned long long)&R.tr), "r"(x0 + 4), "r"(y0 + 1),
+      "r"(z0 + 1), "r"(mb)
+      : "memory");
+}
+
+// Tile lt of run R with the x-pair body (64 x 8 x ZC).
+template <int ZC>
+__device__ inline void batch_pair_tile(const BatchRun& R, int lt, float* smem, uint32_t mb, int tid, int* err,
+                                       double (*rows)[8]) {
+  constexpr int kW = (ZC + 2) * 10 * 72, kR = ZC * 8 * 64;
+  float* sw = smem;
+  float* sr = smem + kW;
+  const int bx2 = lt % R.gx2, by = (lt / R.gx2) % R.gy, bz = lt / (R.gx2 * R.gy);
+  if (tid == 0) batch_issue_boxes(R, mb, sw, sr, kW * 4u, kR * 4u, bx2 * 64, by * 8, bz * ZC);
+  if (!batch_wait_boxes(mb, tid, err)) return;
+  pair_tile_sweep<ZC>(sw, sr, R.S, R.J, R.wout, R.partial, R.w_zero, bx2, by, bz, R.gx, R.gy, rows);
+}
+
+// Tile lt of run R with the 32-wide body (32 x 8 x ZC).
+template <int ZC>
+__device__ inline void batch_w32_tile(const BatchRun& R, int lt, float* smem, uint32_t mb, int tid, int* err) {
+  constexpr int kW = (ZC + 2) * (kT32Ty + 2) * kT32BoxX, kR = ZC * kT32Ty * kT32Tx;
+  float* sw = smem;
+  float* sr = smem + kW;
+  const int bx = lt % R.gx, by = (lt / R.gx) % R.gy, bz = lt / (R.gx * R.gy);
+  if (tid == 0) batch_issue_boxes(R, mb, sw, sr, kW * 4u, kR * 4u, bx * kT32Tx, by * kT32Ty, bz * ZC);
+  if (!batch_wait_boxes(mb, tid, err)) return;
+  tile32_sweep<ZC>(sw, sr, R.S, R.J, R.wout, R.partial + (bx + (long long)R.gx * (by + (long long)R.gy * bz)),
+                   R.w_zero, bx, by, bz);
+}
+
+// One tick over runs of every class -- tile depth 4 or 8, x-pair or 32-wide
+// tiles -- in ONE launch: CTA t finds its run and takes the body of that run's
+// class, so a tick pays one dependent-launch floor instead of one per class.
+// Each run's tiles, arithmetic and partials are those of its class's own
+// kernel: the same bits.  Dynamic shared memory is the largest class's in the
+// launch.
+__global__ void __launch_bounds__(256, 8) sweep_batch_any_kernel(const __grid_constant__ BatchArgs A) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* smem = reinterpret_cast<float*>(smem_raw);
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ double rows[2][8];
+  const int tid = threadIdx.x + 32 * threadIdx.y;
+  const int t = blockIdx.x;
+  const int r = batch_run_of(A, t);
+  const BatchRun& R = A.run[r];
+  const int lt = t - R.tile_base;
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  if (R.w32) {
+    if (R.zc == 8)
+      batch_w32_tile<8>(R, lt, smem, mb, tid, A.err);
+    else
+      batch_w32_tile<4>(R, lt, smem, mb, tid, A.err);
+  } else {
+    if (R.zc == 8)
+      batch_pair_tile<8>(R, lt, smem, mb, tid, A.err, rows);
+    else
+      batch_pair_tile<4>(R, lt, smem, mb, tid, A.err, rows);
+  }
+}
+
+// Shared memory of one tile of a class.
+inline size_t batch_class_smem(int zc, bool w32) {
+  return w32 ? sizeof(float) * ((size_t)(zc + 2) * 10 * 40 + (size_t)zc * 8 * 32)
+             : sizeof(float) * ((size_t)(zc + 2) * 10 * 72 + (size_t)zc * 8 * 64);
+}
+
+cudaError_t launch_batch_any(const BatchArgs& A, size_t smem, int pdl, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(sweep_batch_any_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)batch_class_smem(8, false));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(A.total_tiles);
+  cfg.blockDim = dim3(32, 8);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, sweep_batch_any_kernel, A);
+}
+
 template <int ZC>
 cudaError_t launch_batch32_zc(const BatchArgs& A, int pdl, cudaStream_t st) {
   constexpr size_t smem = sizeof(float) * ((size_t)(ZC + 2) * 10 * 40 + (size_t)ZC * 8 * 32);
@@ -301,8 +448,58 @@ struct RunSolve {
 // its predecessor there); the first tick of a solve phase follows event waits
 // on the runs' streams, which PDL would not cover, so it is a plain launch.
 int launch_tick(std::vector<RunSolve*>& runs, int* err, cudaStream_t st, bool pdl, std::vector<RunSolve*>& ended,
-                long long* launches) {
+                long long* launches, int unified) {
   bool first = !pdl;
+  // unified 1: one launch per tile depth (the x-pair and 32-wide runs of that
+  // depth together); 2: one launch for every class
+  for (int zgroup = 0; unified && zgroup < (unified == 2 ? 1 : 2); ++zgroup) {
+    BatchArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.err = err;
+    size_t smem = 0;
+    auto flush = [&]() -> int {
+      if (A.nruns == 0) return PICARD_OK;
+      PICARD_CUDA(launch_batch_any(A, smem, first ? 0 : 1, st));
+      first = false;
+      ++*launches;
+      g_batch_ctas += A.total_tiles;
+      std::memset(&A, 0, sizeof(A));
+      A.err = err;
+      smem = 0;
+      return PICARD_OK;
+    };
+    for (RunSolve* rs : runs) {
+      if (rs->done || !rs->batched || rs->phase != 1) continue;
+      if (unified == 1 && rs->c->G.zc != (zgroup ? 8 : 4)) continue;
+      picard_ctx* c = rs->c;
+      const bool w32 = rs->w32;
+      const int t = rs->p + 1;                  // sweep t of the round
+      const int in = rs->S.wcur, out = 1 - in;  // never write the buffer being read
+      BatchRun& R = A.run[A.nruns];
+      R.tw = w32 ? c->tmw[in] : c->tmw2[in];
+      R.tr = w32 ? c->tmr[rs->S.rcur] : c->tmr2[rs->S.rcur];
+      R.S = make_stencil(c->K);
+      R.J = jacobi_coef_f(c->K);
+      R.wout = c->w[out];
+      rs->S.wcur = out;
+      R.partial = c->partials + (size_t)(t - 1) * c->G.nblocks;
+      R.gx2 = (c->K.nx + 63) / 64;
+      R.gx = (int)c->G.grid.x;
+      R.gy = (int)c->G.grid.y;
+      R.tiles = (w32 ? R.gx : R.gx2) * (int)c->G.grid.y * (int)c->G.grid.z;
+      R.tile_base = A.total_tiles;
+      R.w_zero = t == 1 ? 1 : 0;
+      R.zc = c->G.zc;
+      R.w32 = w32 ? 1 : 0;
+      smem = std::max(smem, batch_class_smem(c->G.zc, w32));
+      A.total_tiles += R.tiles;
+      rs->p = t;
+      if (t == rs->S.m_eff) ended.push_back(rs);
+      if (++A.nruns == kBatchRuns) PICARD_TRY(flush());
+    }
+    PICARD_TRY(flush());
+  }
+  if (unified) return PICARD_OK;
   for (int cls = 0; cls < 4; ++cls) {
     const int zc = cls & 1 ? 8 : 4;
     const bool w32 = cls >= 2;
@@ -403,12 +600,19 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
   std::vector<RunSolve*> rp(n);
   for (int r = 0; r < n; ++r) rp[r] = &solves[r];
 
-  // PICARD_BATCH_W32=1: 32-wide tiles for runs whose x extent leaves half of a
-  // 64-wide tile empty.  Off by default: the sweep's cost follows the bytes a
-  // tile moves through L2, not the lanes it keeps busy, and the extra launch
-  // class per tick cancels the lanes saved (measured on the 64-run set).
+  // PICARD_BATCH_W32 (default 1): 32-wide tiles for runs whose x extent
+  // leaves half of a 64-wide tile empty; 0 x-pair tiles for every run.
   const char* w32v = std::getenv("PICARD_BATCH_W32");
-  const bool tile_w32 = w32v && *w32v == '1';
+  const bool tile_w32 = !(w32v && *w32v == '0');
+  // PICARD_BATCH_UNIFIED: 2 (the default) one launch per tick for every tile
+  // class (sweep_batch_any_kernel); 1 one launch per tick and tile depth; 0 one
+  // launch per tick and tile class (sweep_batch_kernel, sweep_batch32_kernel).
+  // Measured on the 64-run set (64 runs of 16..96^3, 20 steps): Jacobi 10.84 s
+  // (2, 32-wide tiles on), 11.04 s (1), 11.33 s (0, x-pair tiles only), 11.82 s
+  // (0 with 32-wide tiles: their extra launch class per tick costs more than
+  // the lanes they save).
+  const char* univ = std::getenv("PICARD_BATCH_UNIFIED");
+  const int tick_unified = univ && *univ ? std::atoi(univ) : 2;
   // PICARD_BATCH_SET_MB: working-set budget of the runs that sweep together
   const char* setv = std::getenv("PICARD_BATCH_SET_MB");
   const double tick_set_bytes = setv && *setv ? std::atof(setv) * 1e6 : kTickSetBytes;
@@ -555,7 +759,7 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
             ++retired;
           }
           ended.clear();
-          PICARD_TRY(launch_tick(rp, berr, bst, !first_tick, ended, &launches));
+          PICARD_TRY(launch_tick(rp, berr, bst, !first_tick, ended, &launches, tick_unified));
           ++ticks;
           first_tick = false;
           PICARD_CUDA(cudaEventRecord(tick_ev[issued % kTicksAhead], bst));

@@ -40,9 +40,11 @@ def _start(p):
     return g
 
 
-@pytest.mark.parametrize("w32", ["0", "1"])
-def test_batch_equals_each_run_alone(w32, monkeypatch):
+@pytest.mark.parametrize("w32,unified", [("0", "1"), ("1", "1"), ("1", "2"), ("0", "0"), ("1", "0")])
+def test_batch_equals_each_run_alone(w32, unified, monkeypatch):
     monkeypatch.setenv("PICARD_BATCH_W32", w32)  # 32-wide tiles for the 24^3 and 16^3 runs when "1"
+    # one launch per tick and tile depth ("1"), per tick ("2") or per tile class ("0")
+    monkeypatch.setenv("PICARD_BATCH_UNIFIED", unified)
     steps = 4
     params = _runs()
     alone = []
