@@ -65,7 +65,7 @@ def parse_args():
     ap.add_argument("--poisson-dims", type=str, default=None, help="poisson workload: nx,ny,nz (default n^3)")
     ap.add_argument("--poisson-sweeps", type=int, default=400)
     ap.add_argument("--layout", choices=["cell32", "f64"], default="cell32")
-    ap.add_argument("--solver", choices=["refine", "f64"], default="refine")
+    ap.add_argument("--solver", choices=["refine", "f64", "spectral"], default="refine")
     ap.add_argument("--sort-every", type=int, default=0,
                     help="fused loop: sort the particles by CIC stencil every k iterations (0: never)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -178,6 +178,9 @@ def combine_ranks(ms: float, work: float, dist=None, device: str = "cpu"):
 
 # ---------------------------------------------------------------- GPU arm
 
+SOLVERS = {"f64": 0, "refine": 1, "spectral": 2}  # picard_solver (include/picard_gpu.h)
+
+
 def run_picard(args, rank, world, local_rank):
     import torch
 
@@ -189,7 +192,7 @@ def run_picard(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
     layout = capi.LAYOUT_CELL32 if args.layout == "cell32" else capi.LAYOUT_F64
-    solver = capi.SOLVER_F32_REFINE if args.solver == "refine" else capi.SOLVER_F64
+    solver = SOLVERS[args.solver]
     p, desc = workload(args.workload, seed=rank, ppc=args.ppc)
     if args.ppc is not None:
         desc = dict(desc, ppc_total=2 * args.ppc, workload=desc["workload"] + f" (ppc override {args.ppc})")

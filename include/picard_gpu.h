@@ -65,8 +65,19 @@ typedef enum picard_layout { PICARD_LAYOUT_F64 = 0, PICARD_LAYOUT_CELL32 = 1 } p
  * F32_REFINE: the iterate is held as an FP64 anchor plus an FP32 increment; the
  *             FP32 sweeps advance the increment and an FP64 pass folds it into
  *             the anchor every few sweeps.  Same iterate sequence and stopping
- *             rule as the FP64 sweeps (12 B per node per sweep). */
-typedef enum picard_solver { PICARD_SOLVER_F64 = 0, PICARD_SOLVER_F32_REFINE = 1 } picard_solver;
+ *             rule as the FP64 sweeps (12 B per node per sweep).
+ * SPECTRAL:   the same iterate in closed form: the sweep operator is diagonal
+ *             in the product of per-axis sine (open) or Fourier (periodic)
+ *             bases, so the residual norm of every iterate is a Parseval sum
+ *             and the iterate of the stopping sweep is one forward transform of
+ *             the initial residual, a per-mode factor and one inverse
+ *             transform, all in FP64.  Same stopping sweep and iterate as the
+ *             FP64 sweeps, to rounding; independent of the sweep count. */
+typedef enum picard_solver {
+  PICARD_SOLVER_F64 = 0,
+  PICARD_SOLVER_F32_REFINE = 1,
+  PICARD_SOLVER_SPECTRAL = 2
+} picard_solver;
 
 /* Fields that can be copied in the reference's layouts (picard.f90:95-113). */
 typedef enum picard_field {
@@ -255,6 +266,9 @@ typedef struct picard_stats {
    * solve, E-field + velocity push */
   double phase_ms[5];
   int64_t last_sweeps;     /* Jacobi iterations of the most recent solve     */
+  int64_t spectral_transforms; /* SOLVER_SPECTRAL: 3-axis transforms run     */
+  double spectral_transform_ms; /* their device time (with the initial residual
+                                 * and the per-mode scaling)                   */
 } picard_stats;
 
 PICARD_API int picard_gpu_get_stats(picard_ctx* ctx, picard_stats* out);

@@ -35,6 +35,7 @@ UNITS = {
     "output.cu": [],
     "f90.cu": [],
     "sort.cu": ["--fmad=false"],
+    "spectral.cu": [],
 }
 
 

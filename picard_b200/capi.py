@@ -27,6 +27,7 @@ LAYOUT_F64 = 0
 LAYOUT_CELL32 = 1
 SOLVER_F64 = 0
 SOLVER_F32_REFINE = 1
+SOLVER_SPECTRAL = 2
 
 FIELD_U, FIELD_E, FIELD_N, FIELD_C, FIELD_F, FIELD_D = range(6)
 OPT_BCPOT_TENSOR = 0
@@ -57,6 +58,8 @@ class PicardStats(C.Structure):
         ("d2h_bytes", C.c_int64),
         ("phase_ms", C.c_double * 5),
         ("last_sweeps", C.c_int64),
+        ("spectral_transforms", C.c_int64),
+        ("spectral_transform_ms", C.c_double),
     ]
 
     PHASES = ("particles", "deposit", "bc_potentials", "jacobi", "field_push")

@@ -204,7 +204,8 @@ int validate(const picard_params* p, int layout, int solver) {
   if (p->species < 2 || p->species > 8) return fail(PICARD_ERR_BAD_ARG, "species must be in 2..8");
   if (p->max_per_proc < 1) return fail(PICARD_ERR_BAD_ARG, "max_per_proc must be positive");
   if (layout != PICARD_LAYOUT_F64 && layout != PICARD_LAYOUT_CELL32) return fail(PICARD_ERR_BAD_ARG, "unknown layout");
-  if (solver != PICARD_SOLVER_F64 && solver != PICARD_SOLVER_F32_REFINE) return fail(PICARD_ERR_BAD_ARG, "unknown solver");
+  if (solver != PICARD_SOLVER_F64 && solver != PICARD_SOLVER_F32_REFINE && solver != PICARD_SOLVER_SPECTRAL)
+    return fail(PICARD_ERR_BAD_ARG, "unknown solver");
   if (layout == PICARD_LAYOUT_CELL32 &&
       (p->nx + 2 > (int)kCellMaskX || p->ny + 2 > (int)kCellMaskY || p->nz + 2 > (int)kCellMaskZ))
     return fail(PICARD_ERR_BAD_ARG, "CELL32 layout holds at most 2045 x 2045 x 1021 cells");
@@ -359,6 +360,7 @@ int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver,
   b += (double)s.nodes * (8.0 * s.species /*Nacc*/ + 8.0 * s.species /*N*/ + 8 * 3 /*C,U,b*/ + 24 /*E*/ + 8 /*U1*/);
   if (layout == PICARD_LAYOUT_CELL32) b += 16.0 * s.nodes;
   if (solver == PICARD_SOLVER_F64) b += 8.0 * s.nodes;
+  else if (solver == PICARD_SOLVER_SPECTRAL) b += (double)spectral_bytes(make_kparams(*p));
   else b += 16.0 * (double)f32_elems(make_kparams(*p));
   b += 8.0 * (double)s.dsize;
   b += 8.0 * (double)s.cells;                // produce counts + offsets
@@ -418,6 +420,8 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
   if (layout == PICARD_LAYOUT_CELL32 && (rc = dalloc(c, c->E32, nn))) return bail(rc);
   if (solver == PICARD_SOLVER_F64) {
     if ((rc = dalloc(c, c->Usnap, nn))) return bail(rc);
+  } else if (solver == PICARD_SOLVER_SPECTRAL) {
+    if ((rc = spectral_alloc(c))) return bail(rc);
   } else {
     const long long fe = f32_elems(c->K);
     if ((rc = dalloc(c, c->w[0], fe)) || (rc = dalloc(c, c->w[1], fe)) || (rc = dalloc(c, c->r, 2 * fe))) return bail(rc);

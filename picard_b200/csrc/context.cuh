@@ -28,6 +28,18 @@ struct SortBuf {
   int* info = nullptr;                    // runs, descents, scan totals
   int* scan_scratch = nullptr;
 };
+// Closed-form Jacobi solve (spectral.cu): per-axis orthonormal bases of the
+// sweep operator and the compact FP64 interior arrays the transforms use.
+struct SpectralPlan {
+  double* Q[3] = {nullptr, nullptr, nullptr};   // [n_d][n_d], row = mode
+  double* QT[3] = {nullptr, nullptr, nullptr};  // transposes
+  double* om[3] = {nullptr, nullptr, nullptr};  // a_d (2 - sigma_d) per mode
+  double* T[2] = {nullptr, nullptr};            // nx*ny*nz each
+  double* partial = nullptr;                    // [norm_blocks][32]
+  double* sums = nullptr;                       // [32]
+  int norm_blocks = 0;
+  long long evals = 0;                          // Parseval evaluations (launch pairs)
+};
 }  // namespace picard
 
 struct picard_ctx {
@@ -70,6 +82,7 @@ struct picard_ctx {
   double* partials = nullptr;  // [m_max + 1][nblocks]
   double* r2 = nullptr;        // [m_max + 1]
   picard::JacobiGeom G;
+  picard::SpectralPlan spec;  // SOLVER_SPECTRAL
   int m_max = picard::kMaxSweepsPerRound;
   double last_residual = 0.0, last_bnorm = 0.0;
   long long last_sweeps = 0;
@@ -155,6 +168,12 @@ int resident_option_value(const picard_ctx* c);
 // Stable counting sort of the context's particles by cell; synchronises once
 // to read the run count.
 int sort_particles(picard_ctx* c);
+// SOLVER_SPECTRAL (spectral.cu): device buffers of the closed-form solve,
+// their size in bytes, and the solve itself (the iterate of the reference's
+// stopping sweep, or of sweep smax when no iterate passes).
+int spectral_alloc(picard_ctx* c);
+long long spectral_bytes(const KParams& K);
+int solve_spectral(picard_ctx* c, double tol, long long smax, int maxit, long long* sweeps, bool* converged);
 }  // namespace picard
 
 #define PICARD_CUDA(expr)                                          \

@@ -387,6 +387,8 @@ extern "C" int picard_gpu_calc_epotential(picard_ctx* c, double maxerr, int32_t 
     sweeps = 0;
   } else if (c->solver == PICARD_SOLVER_F64) {
     PICARD_TRY(solve_f64(c, e.tol, e.smax, maxit, &sweeps, &converged));
+  } else if (c->solver == PICARD_SOLVER_SPECTRAL) {
+    PICARD_TRY(solve_spectral(c, e.tol, e.smax, maxit, &sweeps, &converged));
   } else {
     PICARD_TRY(solve_f32(c, e.tol, e.smax, maxit, e.sigma, &sweeps, &converged));
   }
