@@ -179,6 +179,13 @@ def combine_ranks(ms: float, work: float, dist=None, device: str = "cpu"):
 # ---------------------------------------------------------------- GPU arm
 
 SOLVERS = {"f64": 0, "refine": 1, "spectral": 2}  # picard_solver (include/picard_gpu.h)
+SOLVER_WORDS = {"f64": "f64 Jacobi sweeps", "refine": "f32 Jacobi sweeps with f64 anchors",
+                "spectral": "f64 closed-form Jacobi iterate (sine-basis transforms)"}
+
+
+def dtype_of(args) -> str:
+    parts = "cell32 particles (32-bit fixed-point offsets, f32 velocities)" if args.layout == "cell32" else "f64 particles"
+    return f"{parts}, {SOLVER_WORDS[args.solver]}"
 
 
 def run_picard(args, rank, world, local_rank):
@@ -295,8 +302,7 @@ def run_picard(args, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": ("cell32 particles (32-bit fixed-point offsets, f32 velocities), f32 Jacobi sweeps with f64 "
-                      "anchors") if args.layout == "cell32" else "f64",
+            "dtype": dtype_of(args),
             "data": "synthetic (seeded Philox plasma, seed = rank)",
             "config": line_config(desc, world),
             "impl": "picard",
@@ -583,7 +589,7 @@ def serving_measure(args, local_rank, requests: int, run_steps: int) -> dict:
         if run_steps != steps:
             p = P._size_capacity(p, run_steps, max(1, int(p.ppc[1])))
         reqs.append((t, capi.params_derive(p), run_steps))
-    layout, solver = capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE
+    layout, solver = capi.LAYOUT_CELL32, SOLVERS[args.solver]
 
     # warm-up, untimed: load the kernels, and run the sweep launch tuner once per
     # grid shape (cached for the process) so that neither arm pays for tuning
@@ -660,7 +666,7 @@ def serving_measure(args, local_rank, requests: int, run_steps: int) -> dict:
         "metric": "particle-steps/s & run p50/p99 latency, served vs plain", "value": max(served_tput, batched_tput),
         "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "impl": "picard",
         "workload": "serving", "vs_baseline": None,
-        "dtype": "cell32 particles (32-bit fixed-point offsets, f32 velocities), f32 Jacobi sweeps with f64 anchors",
+        "dtype": dtype_of(args),
         "data": "synthetic (seeded Philox plasma, run seeds 0..requests-1)",
         "config": {"workload": f"serving stream: {len(reqs)} runs, Poisson arrivals {args.rate}/s, cubic grids "
                                f"24..128 cells, 8..64 ppc, Haser Q log-uniform [1e25, 1e28] s^-1, "
@@ -798,7 +804,7 @@ def batch_measure(args, local_rank, nruns: int, run_steps: int) -> dict:
             p = P._size_capacity(p, run_steps, max(1, int(p.ppc[1])))
         runs.append(capi.params_derive(p))
     steps = run_steps
-    layout, solver = capi.LAYOUT_CELL32, capi.SOLVER_F32_REFINE
+    layout, solver = capi.LAYOUT_CELL32, SOLVERS[args.solver]
     # warm-up, untimed: kernels loaded, and the sweep launch tuner run once per
     # grid shape (its choices are cached for the process), so that neither
     # arm pays for tuning
@@ -870,7 +876,7 @@ def batch_measure(args, local_rank, nruns: int, run_steps: int) -> dict:
     line = {
         "metric": "particle-steps/s, batched vs plain", "value": ps_batch / t_batch, "unit": UNIT, "n_gpus": 1,
         "higher_is_better": True, "impl": "picard", "workload": "batch", "vs_baseline": None,
-        "dtype": "cell32 particles (32-bit fixed-point offsets, f32 velocities), f32 Jacobi sweeps with f64 anchors",
+        "dtype": dtype_of(args),
         "data": "synthetic (seeded Philox plasma, run seeds 0..runs-1)",
         "config": {"workload": f"batched parameter sweep: {len(runs)} runs, cubic grids 16..96 cells, 8..32 ppc, "
                                f"drift 300..800 km/s, |B| 1..10 nT random direction, {steps} steps each",

@@ -431,6 +431,8 @@ struct RunSolve {
   picard_ctx* c = nullptr;
   EpotSetup e;
   F32Solve S;
+  SpecSolve Q;           // SOLVER_SPECTRAL: the closed-form solve
+  bool spectral = false;
   bool batched = false;  // the batched loop drives this run's solve
   bool active = false;   // in the set of runs that sweep together
   bool w32 = false;      // 32-wide tiles (tile32.cuh) instead of 64-wide x pairs
@@ -682,7 +684,12 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
         rs.sweeps = 0;
         rs.converged = true;
         if (rs.done) continue;
-        if (c->solver == PICARD_SOLVER_F32_REFINE && c->G.tma && c->G.zc <= 8) {
+        if (c->solver == PICARD_SOLVER_SPECTRAL) {
+          // closed form: queued now, its Parseval evaluations collected for
+          // every such run together below
+          rs.spectral = true;
+          PICARD_TRY(spec_begin(rs.Q, c, rs.e.tol, rs.e.smax, rs.e.maxit));
+        } else if (c->solver == PICARD_SOLVER_F32_REFINE && c->G.tma && c->G.zc <= 8) {
           rs.batched = true;
           // 32-wide tiles when 64-wide ones would leave a 32-column half empty
           rs.w32 = tile_w32 && ((c->K.nx + 31) / 32) % 2 == 1;
@@ -792,9 +799,27 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
           if (sweeping == 0) break;  // one at a time while blocking: replan at once
         }
       }
+      // closed-form solves: one host round trip per evaluation for all runs
+      for (bool pending = true; pending;) {
+        pending = false;
+        for (int r = 0; r < n; ++r) {
+          RunSolve& rs = solves[r];
+          if (!rs.spectral || rs.done) continue;
+          PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
+          if (rs.Q.done) {
+            spec_account(rs.Q);
+            rs.done = true;
+            rs.sweeps = rs.Q.d;
+            rs.converged = rs.Q.converged;
+            continue;
+          }
+          PICARD_TRY(spec_collect(rs.Q));
+          pending = true;
+        }
+      }
       for (int r = 0; r < n; ++r) {
         RunSolve& rs = solves[r];
-        if (!rs.batched && !rs.e.trivial) continue;  // solved on its own above
+        if (!rs.batched && !rs.spectral && !rs.e.trivial) continue;  // solved on its own above
         int32_t sw = 0;
         int q = epot_finish(ctxs[r], rs.e, rs.sweeps, rs.converged, &sw);
         if (q == PICARD_ERR_NOT_CONVERGED) nc = true;

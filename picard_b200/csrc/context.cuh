@@ -174,6 +174,26 @@ int sort_particles(picard_ctx* c);
 int spectral_alloc(picard_ctx* c);
 long long spectral_bytes(const KParams& K);
 int solve_spectral(picard_ctx* c, double tol, long long smax, int maxit, long long* sweeps, bool* converged);
+// The same solve as a resumable state machine, so that a batch of runs can
+// take its host round trips together: spec_begin queues the initial residual,
+// the forward transform and the first Parseval evaluation; after the run's
+// stream has been synchronised, spec_collect reads the evaluation and queues
+// the next one, or the scaling, inverse transform and update of U (then
+// done is set; spec_account books the device time once the stream has passed
+// that work).
+struct SpecSolve {
+  picard_ctx* c = nullptr;
+  double tol2 = 0.0, r2_hit = 0.0;
+  long long smax = 0, dmax = 0, lo = 0, hi = 0;
+  long long d0 = 0, step = 0, d = 0;  // pending evaluation; the accepted sweep count
+  int count = 0;
+  bool doubling = false, final_eval = false, done = false, converged = true;
+};
+int spec_begin(SpecSolve& Q, picard_ctx* c, double tol, long long smax, int maxit);
+int spec_collect(SpecSolve& Q);
+int spec_finish_issue(SpecSolve& Q);
+int spec_apply_issue(SpecSolve& Q);
+void spec_account(SpecSolve& Q);
 }  // namespace picard
 
 #define PICARD_CUDA(expr)                                          \

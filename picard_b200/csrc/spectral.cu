@@ -317,8 +317,9 @@ cudaError_t transform(picard_ctx* c, bool forward) {
   return gemm<false>(S.T[1], nx, 0, S.Q[0], nx, 0, S.T[0], nx, 0, ny * nz, nx, nx, 1, c->st);
 }
 
-// Evaluates f at count (<= kSpecPoints) sweep counts; results in c->h_pinned[0..count).
-int eval_norms(picard_ctx* c, long long d0, long long step, int count, bool doubling) {
+// Queues the evaluation of f at count (<= kSpecPoints) sweep counts and the
+// copy of the sums to c->h_pinned[0..count); the caller waits on the stream.
+int issue_norms(picard_ctx* c, long long d0, long long step, int count, bool doubling) {
   SpectralPlan& S = c->spec;
   note_launch();
   spec_norms_kernel<<<S.norm_blocks, kSpecThreads, 0, c->st>>>(S.T[1], c->K.nx, c->K.ny, c->K.nz, S.om[0], S.om[1],
@@ -328,7 +329,6 @@ int eval_norms(picard_ctx* c, long long d0, long long step, int count, bool doub
   spec_sum_kernel<<<1, 32, 0, c->st>>>(S.partial, S.norm_blocks, S.sums);
   PICARD_CUDA(cudaGetLastError());
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, S.sums, sizeof(double) * count, cudaMemcpyDeviceToHost, c->st));
-  PICARD_CUDA(cudaStreamSynchronize(c->st));
   c->stats.d2h_bytes += (int64_t)sizeof(double) * count;
   S.evals += 1;
   return PICARD_OK;
@@ -379,11 +379,25 @@ long long spectral_bytes(const KParams& K) {
                 K.ny + K.nz + (long long)stream_blocks(n) * kSpecPoints + kSpecPoints);
 }
 
-int solve_spectral(picard_ctx* c, double tol, long long smax, int maxit, long long* sweeps, bool* converged) {
+// The stopping-sweep search: the first d in [1, dmax] with f(d) <= tol^2
+// (checked at the top of sweep d + 1 <= maxit).  Invariant: f(lo) > tol^2
+// (lo = 0: no sweep yet), and f(hi) <= tol^2 when hi <= dmax (hi = dmax + 1:
+// no passing d known).  The first evaluation doubles d from 1 up to the
+// first power of two >= dmax; later ones take evenly spaced candidates of
+// (lo, hi).
+
+int spec_begin(SpecSolve& Q, picard_ctx* c, double tol, long long smax, int maxit) {
   SpectralPlan& S = c->spec;
   const KParams& K = c->K;
   const long long n = (long long)K.nx * K.ny * K.nz;
   const JacobiCoef J = jacobi_coef(K);
+  Q = SpecSolve();
+  Q.c = c;
+  Q.tol2 = tol * tol;
+  Q.smax = smax;
+  Q.dmax = (long long)maxit - 1;
+  Q.lo = 0;
+  Q.hi = Q.dmax + 1;
   PICARD_CUDA(cudaEventRecord(c->ev[0], c->st));
   note_launch();
   spec_r0_kernel<<<stream_blocks(n), kSpecThreads, 0, c->st>>>(K, 1.0 / J.dx2, 1.0 / J.dy2, 1.0 / J.dz2, c->U, c->b,
@@ -391,75 +405,114 @@ int solve_spectral(picard_ctx* c, double tol, long long smax, int maxit, long lo
   PICARD_CUDA(cudaGetLastError());
   PICARD_CUDA(transform(c, true));
   PICARD_CUDA(cudaEventRecord(c->ev[1], c->st));
-
-  // the first d in [1, dmax] with f(d) <= tol^2 (checked at the top of sweep
-  // d + 1 <= maxit).  Invariant: f(lo) > tol^2 (lo = 0: no sweep yet), and
-  // f(hi) <= tol^2 when hi <= dmax (hi = dmax + 1: no passing d known).
-  const double tol2 = tol * tol;
-  const long long dmax = (long long)maxit - 1;
-  long long lo = 0, hi = dmax + 1;
-  double r2_hit = 0.0;
-  if (dmax >= 1) {
-    // doubling pass: d = 1, 2, 4, ... up to the first power of two >= dmax
+  if (Q.dmax >= 1) {
     int cnt = 1;
-    while (cnt < kSpecPoints && (1LL << (cnt - 1)) < dmax) ++cnt;
-    PICARD_TRY(eval_norms(c, 1, 0, cnt, true));
-    for (int t = 0; t < cnt; ++t) {
+    while (cnt < kSpecPoints && (1LL << (cnt - 1)) < Q.dmax) ++cnt;
+    Q.d0 = 1;
+    Q.step = 0;
+    Q.count = cnt;
+    Q.doubling = true;
+    return issue_norms(c, 1, 0, cnt, true);
+  }
+  return spec_finish_issue(Q);
+}
+
+int spec_collect(SpecSolve& Q) {
+  picard_ctx* c = Q.c;
+  if (Q.final_eval) {  // f(smax) of a solve without a hit
+    c->last_residual = std::sqrt(c->h_pinned[0]);
+    Q.final_eval = false;
+    return spec_apply_issue(Q);
+  }
+  if (Q.doubling) {
+    for (int t = 0; t < Q.count; ++t) {
       const long long d = 1LL << t;
-      if (d > dmax) break;
-      if (c->h_pinned[t] <= tol2) {
-        hi = d;
-        r2_hit = c->h_pinned[t];
+      if (d > Q.dmax) break;
+      if (c->h_pinned[t] <= Q.tol2) {
+        Q.hi = d;
+        Q.r2_hit = c->h_pinned[t];
         break;
       }
-      lo = d;
+      Q.lo = d;
     }
-    // uniform passes over the candidates lo + 1 .. hi - 1
-    while (hi - lo > 1) {
-      const long long span = hi - 1 - lo;
-      const long long step = (span + kSpecPoints - 1) / kSpecPoints;
-      const int count = int(span / step);
-      PICARD_TRY(eval_norms(c, lo + step, step, count, false));
-      long long nlo = lo + step * count;
-      for (int t = 0; t < count; ++t) {
-        if (c->h_pinned[t] <= tol2) {
-          hi = lo + step * (t + 1);
-          r2_hit = c->h_pinned[t];
-          nlo = lo + step * t;
-          break;
-        }
-      }
-      lo = nlo;
-    }
-  }
-  const long long hit = hi <= dmax ? hi : -1;
-  long long d = hit;
-  if (hit >= 1) {
-    *converged = true;
-    c->last_residual = std::sqrt(r2_hit);
+    Q.doubling = false;
   } else {
-    d = smax;
-    *converged = false;
-    PICARD_TRY(eval_norms(c, d, 1, 1, false));
-    c->last_residual = std::sqrt(c->h_pinned[0]);
+    long long nlo = Q.d0 + Q.step * (Q.count - 1);
+    for (int t = 0; t < Q.count; ++t) {
+      if (c->h_pinned[t] <= Q.tol2) {
+        Q.hi = Q.d0 + Q.step * t;
+        Q.r2_hit = c->h_pinned[t];
+        nlo = Q.hi - Q.step;
+        break;
+      }
+    }
+    Q.lo = nlo;
   }
+  if (Q.hi - Q.lo > 1) {
+    const long long span = Q.hi - 1 - Q.lo;  // candidates lo + 1 .. hi - 1
+    Q.step = (span + kSpecPoints - 1) / kSpecPoints;
+    Q.count = int(span / Q.step);
+    Q.d0 = Q.lo + Q.step;
+    return issue_norms(c, Q.d0, Q.step, Q.count, false);
+  }
+  return spec_finish_issue(Q);
+}
+
+int spec_finish_issue(SpecSolve& Q) {
+  picard_ctx* c = Q.c;
+  if (Q.hi <= Q.dmax) {
+    Q.d = Q.hi;
+    Q.converged = true;
+    c->last_residual = std::sqrt(Q.r2_hit);
+    return spec_apply_issue(Q);
+  }
+  Q.d = Q.smax;
+  Q.converged = false;
+  Q.final_eval = true;
+  return issue_norms(c, Q.smax, 1, 1, false);
+}
+
+int spec_apply_issue(SpecSolve& Q) {
+  picard_ctx* c = Q.c;
+  SpectralPlan& S = c->spec;
+  const KParams& K = c->K;
+  const long long n = (long long)K.nx * K.ny * K.nz;
+  const JacobiCoef J = jacobi_coef(K);
   PICARD_CUDA(cudaEventRecord(c->ev[2], c->st));
   note_launch();
   spec_scale_kernel<<<stream_blocks(n), kSpecThreads, 0, c->st>>>(S.T[1], K.nx, K.ny, K.nz, S.om[0], S.om[1],
-                                                                   S.om[2], d, J.af);
+                                                                   S.om[2], Q.d, J.af);
   PICARD_CUDA(cudaGetLastError());
   PICARD_CUDA(transform(c, false));
   note_launch();
   spec_apply_kernel<<<stream_blocks(n), kSpecThreads, 0, c->st>>>(K, S.T[0], c->U);
   PICARD_CUDA(cudaGetLastError());
   PICARD_CUDA(cudaEventRecord(c->ev[3], c->st));
-  PICARD_CUDA(cudaEventSynchronize(c->ev[3]));
+  Q.done = true;
+  return PICARD_OK;
+}
+
+// Device time of a finished solve (after its stream has passed ev[3]).
+void spec_account(SpecSolve& Q) {
+  picard_ctx* c = Q.c;
   float f0 = 0.f, f1 = 0.f;
   cudaEventElapsedTime(&f0, c->ev[0], c->ev[1]);
   cudaEventElapsedTime(&f1, c->ev[2], c->ev[3]);
   c->stats.spectral_transforms += 2;
   c->stats.spectral_transform_ms += f0 + f1;
-  *sweeps = d;
+}
+
+int solve_spectral(picard_ctx* c, double tol, long long smax, int maxit, long long* sweeps, bool* converged) {
+  SpecSolve Q;
+  PICARD_TRY(spec_begin(Q, c, tol, smax, maxit));
+  for (;;) {
+    PICARD_CUDA(cudaStreamSynchronize(c->st));
+    if (Q.done) break;
+    PICARD_TRY(spec_collect(Q));
+  }
+  spec_account(Q);
+  *sweeps = Q.d;
+  *converged = Q.converged;
   return PICARD_OK;
 }
 

@@ -33,8 +33,8 @@ def _runs():
     return out
 
 
-def _start(p):
-    g = Simulation(p, derive=False, layout=capi.LAYOUT_CELL32, solver=capi.SOLVER_F32_REFINE)
+def _start(p, solver=capi.SOLVER_F32_REFINE):
+    g = Simulation(p, derive=False, layout=capi.LAYOUT_CELL32, solver=solver)
     g.calc_distance()
     g.particles_initialize()
     return g
@@ -105,5 +105,32 @@ def test_staggered_steps_equal_each_run_alone():
         assert g.num_local == n, k
         np.testing.assert_array_equal(g.field(capi.FIELD_U), U, err_msg=f"run {k}")
         np.testing.assert_array_equal(g.field(capi.FIELD_N), N, err_msg=f"run {k}")
+    for g in sims:
+        g.close()
+
+
+def test_batch_with_closed_form_solves_equals_each_run_alone():
+    """Runs with SOLVER_SPECTRAL in a batch (their Parseval evaluations
+    collected for all of them together), mixed with FP32-sweep runs ticked
+    together: every run bit for bit where it ends alone."""
+    steps = 3
+    params = _runs()
+    solvers = [capi.SOLVER_SPECTRAL, capi.SOLVER_F32_REFINE, capi.SOLVER_SPECTRAL, capi.SOLVER_SPECTRAL]
+    alone = []
+    for p, sv in zip(params, solvers):
+        g = _start(p, sv)
+        sw = g.run_fused(0, steps)
+        alone.append((sw, g.num_local, g.field(capi.FIELD_U), g.field(capi.FIELD_N), g.particles()))
+        g.close()
+    sims = [_start(p, sv) for p, sv in zip(params, solvers)]
+    sweeps = batch_run_fused(sims, 0, steps)
+    for k, g in enumerate(sims):
+        sw, n, U, N, (rp, ip) = alone[k]
+        assert sweeps[k] == sw, k
+        assert g.num_local == n, k
+        np.testing.assert_array_equal(g.field(capi.FIELD_U), U, err_msg=f"run {k}")
+        np.testing.assert_array_equal(g.field(capi.FIELD_N), N, err_msg=f"run {k}")
+        rg, ig = g.particles()
+        np.testing.assert_array_equal(rg, rp, err_msg=f"run {k}")
     for g in sims:
         g.close()
