@@ -279,10 +279,18 @@ PICARD_API int picard_gpu_get_stream(picard_ctx* ctx, void** stream);
 
 /* ---------------------------------------------------------------- options */
 
+typedef enum picard_bcpot_method {
+  PICARD_BCPOT_DIRECT = 0,
+  PICARD_BCPOT_TENSOR = 1,
+  PICARD_BCPOT_FFT = 2
+} picard_bcpot_method;
+
 typedef enum picard_option {
-  /* 1: BCpotentials on the tensor cores (three-way BF16 split, FP32
-   * accumulation folded into FP64 every 512 K-values; the default of the
-   * CELL32 layout).  0: FP64 direct sum (the default of the F64 layout). */
+  /* BCpotentials method (picard_bcpot_method).  0: FP64 direct sum (the
+   * default of the F64 layout).  1: tensor cores (three-way BF16 split, FP32
+   * accumulation folded into FP64 every 512 K-values).  2: FP64 FFT
+   * convolution over each face's tangential axes (the default of the CELL32
+   * layout where every open face is at most 512 x 1024 cells, else 1). */
   PICARD_OPT_BCPOT_TENSOR = 0,
   /* Launch shape of the TMA Jacobi sweep (open boundaries with the F32_REFINE
    * solver).  It never changes a result bit.  SWEEP_CTAS: > 0 persistent grid

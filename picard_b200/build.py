@@ -36,6 +36,7 @@ UNITS = {
     "f90.cu": [],
     "sort.cu": ["--fmad=false"],
     "spectral.cu": [],
+    "bcpot_fft.cu": [],
 }
 
 

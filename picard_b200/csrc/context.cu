@@ -279,7 +279,8 @@ int sync_count_public(picard_ctx* c) {
 int check_dev_err_public(picard_ctx* c) { return check_dev_err(c); }
 
 int bc_potentials_async(picard_ctx* c) {
-  if (c->bcpot_tensor) {
+  if (c->bcpot_tensor == PICARD_BCPOT_FFT) return bc_potentials_fft(c);
+  if (c->bcpot_tensor == PICARD_BCPOT_TENSOR) {
     if (!c->tc_cs) {
       long long cs = 0, pe = 0;
       bcpot_tc_scratch(c->K, &cs, &pe);
@@ -367,10 +368,15 @@ int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver,
   b += 8.0 * (double)s.nb_compact * (3 + kOutflowWordsPerBlock);  // BCoutflow scratch
   b += 8.0 * (double)s.nb_inflow * 2;        // fused BCinflow scan
   b += 8.0 * (kMaxSweepsPerRound + 1.0) * s.nb_jacobi;  // sweep partials
-  if (layout == PICARD_LAYOUT_CELL32) {      // tensor-core BCpotentials scratch
-    long long cs = 0, pe = 0;
-    bcpot_tc_scratch(make_kparams(*p), &cs, &pe);
-    b += 2.0 * (double)cs + 8.0 * (double)pe;
+  if (layout == PICARD_LAYOUT_CELL32) {      // BCpotentials scratch of the layout's default method
+    const KParams K = make_kparams(*p);
+    if (bcpot_fft_supported(K)) {
+      b += (double)bcpot_fft_bytes(K);
+    } else {
+      long long cs = 0, pe = 0;
+      bcpot_tc_scratch(K, &cs, &pe);
+      b += 2.0 * (double)cs + 8.0 * (double)pe;
+    }
   }
   *bytes = (uint64_t)b;
   return PICARD_OK;
@@ -387,7 +393,9 @@ int picard_gpu_create(const picard_params* p, int32_t layout, int32_t solver, pi
   c->capacity = p->max_per_proc;
   c->inflow = make_inflow_table(*p);
   c->G = jacobi_geom(c->K);
-  c->bcpot_tensor = layout == PICARD_LAYOUT_CELL32 ? 1 : 0;
+  c->bcpot_tensor = layout != PICARD_LAYOUT_CELL32 ? PICARD_BCPOT_DIRECT
+                    : bcpot_fft_supported(c->K)   ? PICARD_BCPOT_FFT
+                                                  : PICARD_BCPOT_TENSOR;
   int rc = PICARD_OK;
   auto bail = [&](int code) {
     picard_gpu_destroy(c);
@@ -482,6 +490,7 @@ int picard_gpu_destroy(picard_ctx* c) {
     for (void* q : c->allocs) cudaFreeAsync(q, c->st);
     cudaStreamSynchronize(c->st);
   }
+  bcpot_fft_free(c);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   if (c->h_pinned_i) cudaFreeHost(c->h_pinned_i);
   for (int e = 0; e < 4; ++e)
@@ -670,6 +679,7 @@ int picard_gpu_set_field(picard_ctx* c, int32_t which, const double* in) {
     for (long long g = 0; g < n; ++g) h[(size_t)pl * n + g] = in[ref_index(which, c->prm.species, pl, g)];
   PICARD_CUDA(cudaMemcpyAsync(dev, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->st));
   c->stats.h2d_bytes += (int64_t)(sizeof(double) * h.size());
+  if (which == PICARD_FIELD_D) bcpot_fft_invalidate(c);
   if (which == PICARD_FIELD_E && c->E32) {
     std::vector<float4> e32(n);
     for (long long g = 0; g < n; ++g)
@@ -687,6 +697,7 @@ int picard_gpu_set_field(picard_ctx* c, int32_t which, const double* in) {
 int picard_gpu_calc_distance(picard_ctx* c) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
   PICARD_CUDA(launch_calc_distance(c->K, c->D, c->st));
+  bcpot_fft_invalidate(c);
   return PICARD_OK;
 }
 
@@ -832,7 +843,11 @@ int picard_gpu_particles_gridify_all(picard_ctx* c) {
 int picard_gpu_set_option(picard_ctx* c, int32_t option, int32_t value) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
   if (option == PICARD_OPT_BCPOT_TENSOR) {
-    c->bcpot_tensor = value != 0;
+    if (value < PICARD_BCPOT_DIRECT || value > PICARD_BCPOT_FFT)
+      return fail(PICARD_ERR_BAD_ARG, "BCPOT_TENSOR must be 0 (direct), 1 (tensor cores) or 2 (FFT)");
+    if (value == PICARD_BCPOT_FFT && !bcpot_fft_supported(c->K))
+      return fail(PICARD_ERR_BAD_ARG, "FFT BCpotentials: a face is longer than its shared-memory FFT");
+    c->bcpot_tensor = value;
     return PICARD_OK;
   }
   if (option == PICARD_OPT_SWEEP_CTAS) {
@@ -907,7 +922,7 @@ int picard_gpu_get_option(picard_ctx* c, int32_t option, int32_t* value) {
 int picard_gpu_bc_potentials(picard_ctx* c) {
   if (!c) return fail(PICARD_ERR_BAD_ARG, "ctx is NULL");
   PICARD_TRY(bc_potentials_async(c));
-  return c->bcpot_tensor ? check_dev_err_timeout(c) : PICARD_OK;
+  return c->bcpot_tensor == PICARD_BCPOT_TENSOR ? check_dev_err_timeout(c) : PICARD_OK;
 }
 
 // CalcEfield.f90:3-232

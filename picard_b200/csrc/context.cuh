@@ -28,6 +28,9 @@ struct SortBuf {
   int* info = nullptr;                    // runs, descents, scan totals
   int* scan_scratch = nullptr;
 };
+// FFT BCpotentials (bcpot_fft.cu): slice transforms of D and stage buffers.
+struct BcFft;
+
 // Closed-form Jacobi solve (spectral.cu): per-axis orthonormal bases of the
 // sweep operator and the compact FP64 interior arrays the transforms use.
 struct SpectralPlan {
@@ -117,8 +120,10 @@ struct picard_ctx {
   picard::SortBuf sortbuf;
   long long sort_geom_keys = 0;
   long long stats_sorts = 0, stats_sorts_moved = 0;
-  // tensor-core BCpotentials (bcpot_tc.cu)
+  // BCpotentials method (PICARD_OPT_BCPOT_TENSOR): 0 FP64 direct sum, 1 tensor
+  // cores (bcpot_tc.cu), 2 FP64 FFT convolution (bcpot_fft.cu)
   int bcpot_tensor = 0;
+  picard::BcFft* bcfft = nullptr;
   void* tc_cs = nullptr;
   double* tc_partial = nullptr;
 
@@ -172,6 +177,15 @@ int sort_particles(picard_ctx* c);
 // their size in bytes, and the solve itself (the iterate of the reference's
 // stopping sweep, or of sweep smax when no iterate passes).
 int spectral_alloc(picard_ctx* c);
+// FFT BCpotentials (bcpot_fft.cu): device bytes of its scratch, whether every
+// open face fits its shared-memory FFTs (tangential lengths up to 512 and
+// 1024 cells), the launch sequence (U zeroed, the face values written; the
+// slice transforms of D are computed first when D changed), and upkeep.
+long long bcpot_fft_bytes(const KParams& K);
+int bcpot_fft_supported(const KParams& K);
+int bc_potentials_fft(picard_ctx* c);
+void bcpot_fft_invalidate(picard_ctx* c);
+void bcpot_fft_free(picard_ctx* c);
 long long spectral_bytes(const KParams& K);
 int solve_spectral(picard_ctx* c, double tol, long long smax, int maxit, long long* sweeps, bool* converged);
 // The same solve as a resumable state machine, so that a batch of runs can
