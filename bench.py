@@ -6,9 +6,11 @@ solve, E-field, Boris push) over the whole run.  The default workload is the
 at-scale plain configuration: 256x128x128 cells of 1 km, 32 H+ and 32
 electrons per cell (268,435,456 particles), drifting solar-wind Maxwellian,
 Haser source at the centre, CELL32 particles (32-bit fixed-point in-cell
-offsets, FP32 velocities), Jacobi with FP32
-sweeps under FP64 anchors, tolerance 1e-6.  Inputs are synthetic (seeded
-Philox, seed = rank); the particle arrays (7.8 GB) are far larger than L2.
+offsets, FP32 velocities), BCpotentials as FP64 FFT convolutions, and the
+Jacobi iterate of the reference's stopping sweep (tolerance 1e-6) in closed
+form (--solver spectral; --solver refine runs the FP32 sweeps under FP64
+anchors instead).  Inputs are synthetic (seeded Philox, seed = rank); the
+particle arrays (7.8 GB) are far larger than L2.
 
 Arms:
   --impl picard     the sm_100a kernels through the C ABI (default)
@@ -65,11 +67,13 @@ def parse_args():
     ap.add_argument("--poisson-dims", type=str, default=None, help="poisson workload: nx,ny,nz (default n^3)")
     ap.add_argument("--poisson-sweeps", type=int, default=400)
     ap.add_argument("--layout", choices=["cell32", "f64"], default="cell32")
-    ap.add_argument("--solver", choices=["refine", "f64", "spectral"], default="refine")
+    ap.add_argument("--solver", choices=["refine", "f64", "spectral"], default="spectral")
     ap.add_argument("--sort-every", type=int, default=0,
                     help="fused loop: sort the particles by CIC stencil every k iterations (0: never)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-phi", action="store_true", help="skip the FP64 check of the timed run's potential")
+    ap.add_argument("--no-sweep", action="store_true",
+                    help="skip the FP32 sweep solve of the timed run's charge (the jacobi_sweep block)")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the served and batched blocks of the default (N=1) line")
     ap.add_argument("--served-requests", type=int, default=16, help="default line: runs in the serving stream")
@@ -232,12 +236,15 @@ def run_picard(args, rank, world, local_rank):
     st = sim.stats()
     particle_steps = st["particle_steps"]
     sweeps_per_step = st["sweeps"] / max(st["solves"], 1)
-    # dominant kernel: the Jacobi sweep; algorithmic bytes per launch
-    cells = p.nx * p.ny * p.nz
-    bytes_per_node = 12 if solver == capi.SOLVER_F32_REFINE else 24
-    sweep_avg_ms = st["sweep_ms"] / max(st["sweep_launches"], 1)
-    alg_bytes = bytes_per_node * cells
-    achieved = alg_bytes / (sweep_avg_ms * 1e-3) / 1e9 if sweep_avg_ms > 0 else 0.0
+    # dominant kernel: the CIC deposit (ParticlesGridify), timed on its own
+    # right after the timed region on the run's final particles, K launches
+    # of the entry point (deposit kernel + fixed-point finish) on the
+    # library's stream; algorithmic bytes = the particle stream it reads
+    dep_ms = deposit_launch_ms(sim, ext, K, torch)
+    n_dep = sim.num_local
+    alg_bytes = DEPOSIT_BYTES_PER_PARTICLE * n_dep
+    achieved = alg_bytes / (dep_ms * 1e-3) / 1e9
+    sweep = sweep_roofline(sim, p, torch) if not args.no_sweep else None
     num_final = sim.num_local
     phi = None
     if not args.no_phi:
@@ -245,7 +252,6 @@ def run_picard(args, rank, world, local_rank):
     sim.close()
     del sim
     torch.cuda.synchronize()
-    l2_gbs = l2_copy_gbs(torch)
 
     # end to end through the reference-facing entry points (picard_gpu_run:
     # the per-subroutine call sequence of picard.f90), from the host-side
@@ -312,19 +318,21 @@ def run_picard(args, rank, world, local_rank):
             "phase_ms_per_step": {k: round(v / K, 3) for k, v in st["phase_ms"].items()},
             "particles_final": num_final,
             "roofline": {"bound": "hbm",
-                         "kernel": ("sweep_tma2_kernel" if p.xflow and p.yflow and p.zflow else "sweep_f32_kernel")
-                         if solver else "sweep_f64_kernel",
+                         "kernel": "deposit_tile_c32_kernel" if args.layout == "cell32" else "deposit_f64_kernel",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "alg_bytes_per_launch": alg_bytes, "launch_ms": sweep_avg_ms,
-                         "traffic": SWEEP_DRAM_BYTES.get((p.nx, p.ny, p.nz, solver)),
-                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of "
-                                           "the sweep kernel on this grid (caches flushed by the replay; in the "
-                                           "live loop the 52 MB working set stays in L2)",
-                         "note": "the sweep's working set is L2-resident, so achieved algorithmic bytes can "
-                                 "exceed the HBM copy rate (frac > 1); l2_frac is the same achieved rate over a "
-                                 "device copy whose buffers stay in L2, measured in this run",
-                         "l2_copy_gbs": l2_gbs, "l2_frac": achieved / l2_gbs if l2_gbs else None},
+                         "alg_bytes_per_launch": alg_bytes, "launch_ms": dep_ms,
+                         "alg_bytes_rule": f"{DEPOSIT_BYTES_PER_PARTICLE} B per particle read (cell word, three "
+                                           "32-bit offsets, species) x the live particles",
+                         "traffic": (DEPOSIT_DRAM_BYTES_PER_PARTICLE * n_dep
+                                     if DEPOSIT_DRAM_BYTES_PER_PARTICLE and args.layout == "cell32" else None),
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per particle of one ncu "
+                                           "capture of the deposit at 256x128x128 x 8 ppc, scaled by the particles",
+                         "note": "launch_ms is the ParticlesGridify entry point (deposit kernel and the "
+                                 "fixed-point finish) timed with CUDA events on the library stream, K launches on "
+                                 "the timed run's final particles; the step's other phases are in "
+                                 "phase_ms_per_step"},
+            "jacobi_sweep": sweep,
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -337,6 +345,70 @@ def run_picard(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
+
+
+# CELL32 ParticlesGridify reads the cell word, the three 32-bit offsets and
+# the species of every particle.
+DEPOSIT_BYTES_PER_PARTICLE = 17
+# DRAM bytes per particle of one deposit launch (dram__bytes_read.sum +
+# dram__bytes_write.sum over the particles), from an ncu capture at
+# 256x128x128 with 4 + 4 ppc; None until captured.
+DEPOSIT_DRAM_BYTES_PER_PARTICLE = None
+
+
+def deposit_launch_ms(sim, ext, reps: int, torch) -> float:
+    """Device time of one ParticlesGridify call on the run's particles: reps
+    calls between CUDA events on the library's stream, after one untimed call."""
+    sim.particles_gridify()
+    sim.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(max(1, reps)):
+        sim.particles_gridify()
+    e1.record(ext)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / max(1, reps)
+
+
+def sweep_roofline(sim, p, torch) -> dict:
+    """The FP32 Jacobi sweep kernel on the timed run's grid: one solve of the
+    run's last charge density with the F32_REFINE solver (the sweeps the
+    closed form replaces), its sweep launches timed with CUDA events on the
+    library's stream; 12 B per interior node per sweep against the measured
+    HBM copy rate and a device copy whose buffers stay in L2 (the 52 MB
+    working set is L2-resident)."""
+    from picard_b200 import capi
+    from picard_b200.simulation import Simulation
+
+    C = sim.field(capi.FIELD_C)
+    st = sim.stats()
+    q = p.copy()
+    q.max_per_proc = 1024
+    ref = Simulation(q, layout=capi.LAYOUT_CELL32, solver=capi.SOLVER_F32_REFINE)
+    ref.calc_distance()
+    ref.set_field(capi.FIELD_C, C)
+    ref.bc_potentials()
+    ref.reset_stats()
+    sweeps = ref.calc_epotential()
+    ref.synchronize()
+    s2 = ref.stats()
+    ref.close()
+    launch_ms = s2["sweep_ms"] / max(s2["sweep_launches"], 1)
+    alg = 12 * p.nx * p.ny * p.nz
+    achieved = alg / (launch_ms * 1e-3) / 1e9
+    peak, kind = measured_peaks()
+    l2 = l2_copy_gbs(torch)
+    spec_ms = st["spectral_transform_ms"] / max(st["spectral_transforms"] / 2, 1)
+    return {"kernel": "sweep_tma2_kernel" if p.xflow and p.yflow and p.zflow else "sweep_f32_kernel",
+            "bound": "l2", "sweeps": sweeps, "launch_ms": launch_ms, "alg_bytes_per_launch": alg,
+            "achieved": achieved, "unit": "GB/s", "frac_of_hbm_copy": achieved / peak, "peak_kind": kind,
+            "l2_copy_gbs": l2, "l2_frac": achieved / l2 if l2 else None,
+            "traffic": SWEEP_DRAM_BYTES.get((p.nx, p.ny, p.nz, 1)),
+            "solve_ms_sweeps": s2["sweep_ms"] + s2["anchor_ms"],
+            "solve_ms_closed_form_transforms": spec_ms,
+            "note": "the FP32 sweep solve of the timed run's last charge density; the timed loop takes the same "
+                    "iterate in closed form (two FP64 transforms + a few Parseval evaluations)"}
 
 
 def phi_check(sim, p, desc) -> dict:
@@ -370,8 +442,8 @@ def phi_check(sim, p, desc) -> dict:
     rel = float(np.linalg.norm(d.ravel()) / np.linalg.norm(U64.ravel()))
     return {"rel_l2": rel, "max_rel": float(np.abs(d).max() / np.abs(U64).max()), "bar": 1e-6, "ok": rel <= 1e-6,
             "sweeps_fp64": sweeps64, "sweeps_timed_run_last_solve": sweeps_run, "fp64_solve_s": round(t64, 3),
-            "what": "U after the last timed iteration (tensor-core BCpotentials, FP32 sweeps with FP64 anchors) vs "
-                    "FP64 BCpotentials + FP64 Jacobi (SOLVER_F64) from the same C"}
+            "what": "U after the last timed iteration (the run's BCpotentials method and solver) vs FP64 direct-sum "
+                    "BCpotentials + FP64 Jacobi sweeps (SOLVER_F64) from the same C"}
 
 
 def l2_copy_gbs(torch) -> float:
@@ -955,7 +1027,7 @@ def run_deposit(args, local_rank):
     torch.cuda.set_device(local_rank)
     ppc = args.ppc or 32
     sim = Simulation(P.config_plain_scale(seed=0, ppc_ion=ppc), layout=capi.LAYOUT_CELL32,
-                     solver=capi.SOLVER_F32_REFINE)
+                     solver=capi.SOLVER_SPECTRAL)
     sim.calc_distance()
     sim.particles_initialize()
     sim.run_fused(0, 2)

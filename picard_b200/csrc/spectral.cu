@@ -165,13 +165,28 @@ __global__ void __launch_bounds__(kSpecThreads) spec_norms_kernel(const double* 
     const double w = r * r;
     const double g = 1.0 - (omx[mx] + omy[my] + omz[mz]);
     const double g2 = g * g;
-    double x = ipow(g2, d0);
-    const double h = doubling ? 0.0 : ipow(g2, step);
+    const double x = ipow(g2, d0);
+    if (doubling) {
+      double y = x;  // d0 * 2^t: a chain of squarings
 #pragma unroll
-    for (int t = 0; t < kSpecPoints; ++t) {
-      if (t < count) {
-        acc[t] = fma(w, x, acc[t]);
-        x = doubling ? x * x : x * h;
+      for (int t = 0; t < kSpecPoints; ++t) {
+        if (t < count) acc[t] = fma(w, y, acc[t]);
+        y *= y;
+      }
+    } else {
+      // x h^t with h^t from the binary digits of t: 32 short independent
+      // chains instead of one chain of 32 dependent products
+      double hp[5];
+      hp[0] = ipow(g2, step);
+#pragma unroll
+      for (int b = 1; b < 5; ++b) hp[b] = hp[b - 1] * hp[b - 1];
+#pragma unroll
+      for (int t = 0; t < kSpecPoints; ++t) {
+        double y = x;
+#pragma unroll
+        for (int b = 0; b < 5; ++b)
+          if (t & (1 << b)) y *= hp[b];
+        if (t < count) acc[t] = fma(w, y, acc[t]);
       }
     }
   }
@@ -191,12 +206,14 @@ __global__ void __launch_bounds__(kSpecThreads) spec_norms_kernel(const double* 
   }
 }
 
+// out[t] = sum_b partial[b][t]: warp t, lanes striding over the blocks, then
+// a fixed shuffle tree (deterministic for a fixed block count).
 __global__ void spec_sum_kernel(const double* __restrict__ partial, int nb, double* __restrict__ out) {
-  const int t = threadIdx.x;
-  if (t >= kSpecPoints) return;
+  const int t = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double s = 0.0;
-  for (int b = 0; b < nb; ++b) s += partial[(long long)b * kSpecPoints + t];
-  out[t] = s;
+  for (int b = lane; b < nb; b += 32) s += partial[(long long)b * kSpecPoints + t];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[t] = s;
 }
 
 // rh -> -af (1 - g^d)/(1 - g) rh in place.  For g > 0 the factor is
@@ -326,7 +343,7 @@ int issue_norms(picard_ctx* c, long long d0, long long step, int count, bool dou
                                                                 S.om[2], d0, step, count, doubling ? 1 : 0,
                                                                 S.partial);
   note_launch();
-  spec_sum_kernel<<<1, 32, 0, c->st>>>(S.partial, S.norm_blocks, S.sums);
+  spec_sum_kernel<<<1, 32 * kSpecPoints, 0, c->st>>>(S.partial, S.norm_blocks, S.sums);
   PICARD_CUDA(cudaGetLastError());
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, S.sums, sizeof(double) * count, cudaMemcpyDeviceToHost, c->st));
   c->stats.d2h_bytes += (int64_t)sizeof(double) * count;
