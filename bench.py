@@ -778,7 +778,10 @@ def run_precision(args, local_rank):
                 sweeps, the same number of sweeps from the same FP64 boundary
                 potential;
       end to end: tensor-core boundary + FP32/FP64 Jacobi against FP64 boundary
-                + FP64 Jacobi.
+                + FP64 Jacobi;
+      and the FP64 methods of the default path: the FFT boundary against the
+      direct sum, the closed-form iterate of the same sweep count against the
+      FP64 sweeps, and FFT boundary + closed form end to end.
     Errors are relative L2 over the nodes compared, and the largest pointwise
     error relative to the largest |U|."""
     import numpy as np
@@ -821,8 +824,13 @@ def run_precision(args, local_rank):
     g64.set_option(capi.OPT_BCPOT_TENSOR, 1)
     out["bcpot_tensor_ms"] = timed(g64.bc_potentials, s64)
     Ubtc = g64.field(capi.FIELD_U)
+    g64.set_option(capi.OPT_BCPOT_TENSOR, 2)
+    g64.bc_potentials()  # the first call after CalcDistance also transforms the slices of D
+    out["bcpot_fft_ms"] = timed(g64.bc_potentials, s64)
+    Ubfft = g64.field(capi.FIELD_U)
     face = Ub64 != 0.0
     out["boundary"] = rel(Ubtc, Ub64, face)
+    out["boundary_fft"] = rel(Ubfft, Ub64, face)
     out["face_nodes"] = int(face.sum())
     # FP64 Jacobi from the FP64 boundary potential
     g64.set_field(capi.FIELD_U, Ub64)
@@ -841,6 +849,16 @@ def run_precision(args, local_rank):
     Ue2e = g32.field(capi.FIELD_U)
     out["end_to_end"] = rel(Ue2e, U64)
     g32.close()
+    gsp = Simulation(p, layout=capi.LAYOUT_F64, solver=capi.SOLVER_SPECTRAL)
+    ssp = torch.cuda.ExternalStream(gsp.stream_handle)
+    gsp.set_field(capi.FIELD_C, C)
+    gsp.set_field(capi.FIELD_U, Ub64)
+    out["jacobi_closed_form_ms"] = timed(lambda: gsp.calc_epotential(maxerr=1e-300, maxit=maxit), ssp)
+    out["jacobi_closed_form"] = rel(gsp.field(capi.FIELD_U), U64)
+    gsp.set_field(capi.FIELD_U, Ubfft)
+    gsp.calc_epotential(maxerr=1e-300, maxit=maxit)
+    out["end_to_end_fft_closed_form"] = rel(gsp.field(capi.FIELD_U), U64)
+    gsp.close()
     print(json.dumps(out), flush=True)
 
 
