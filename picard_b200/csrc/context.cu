@@ -313,11 +313,21 @@ cudaError_t launch_outflow(picard_ctx* c, int wrap) {
 }
 
 cudaError_t launch_inflow_fused(picard_ctx* c, int iteration) {
+  const long long cand = (long long)c->inflow.cells * c->inflow.per_cell;
+  if (cand > 0 && !c->inflow_stage.x) {
+    const long long slots = inflow_stage_slots(cand);
+    double* x = nullptr;
+    int8_t* sp = nullptr;
+    if (dalloc(c, x, (size_t)(6 * slots)) != PICARD_OK || dalloc(c, sp, (size_t)slots) != PICARD_OK)
+      return cudaErrorMemoryAllocation;
+    c->inflow_stage.x = x;
+    c->inflow_stage.sp = sp;
+  }
   if (c->layout == PICARD_LAYOUT_F64)
     return launch_inflow_fused_f64(c->K, c->inflow, iteration, c->f64, c->d_count, c->capacity, c->inflow_counts,
-                                   c->inflow_offsets, c->d_err, c->st);
+                                   c->inflow_offsets, c->d_err, c->inflow_stage, c->st);
   return launch_inflow_fused_c32(c->K, c->inflow, iteration, c->c32, c->d_count, c->capacity, c->inflow_counts,
-                                 c->inflow_offsets, c->d_err, c->st);
+                                 c->inflow_offsets, c->d_err, c->inflow_stage, c->st);
 }
 
 int count_issue(picard_ctx* c) {
@@ -367,6 +377,11 @@ int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver,
   b += 8.0 * (double)s.cells;                // produce counts + offsets
   b += 8.0 * (double)s.nb_compact * (3 + kOutflowWordsPerBlock);  // BCoutflow scratch
   b += 8.0 * (double)s.nb_inflow * 2;        // fused BCinflow scan
+  {
+    const InflowTable T = make_inflow_table(*p);  // fused BCinflow survivors' staging area
+    const long long cand = (long long)T.cells * T.per_cell;
+    if (cand > 0) b += 49.0 * (double)inflow_stage_slots(cand);
+  }
   b += 8.0 * (kMaxSweepsPerRound + 1.0) * s.nb_jacobi;  // sweep partials
   if (layout == PICARD_LAYOUT_CELL32) {      // BCpotentials scratch of the layout's default method
     const KParams K = make_kparams(*p);

@@ -98,6 +98,7 @@ struct picard_ctx {
   long long jump_cap = 0;
   int* inflow_counts = nullptr;  // fused BCinflow block counts and offsets
   int* inflow_offsets = nullptr;
+  picard::InflowStage inflow_stage;  // fused BCinflow survivors (allocated on first use)
   int* cell_counts = nullptr;
   int* cell_offsets = nullptr;
   double* red_partial = nullptr;

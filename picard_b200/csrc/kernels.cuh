@@ -42,13 +42,21 @@ cudaError_t launch_inflow_c32(const KParams& P, const InflowTable& T, int iterat
 // Fused inflow (fast path): candidates are generated, advanced by dt and kept
 // only if BCoutflow would keep them; survivors are appended at *count in
 // candidate order.  block_counts holds inflow_blocks(candidates) ints,
-// block_offsets that many + 2 + scan_scratch_ints(that many).
+// block_offsets that many + 2 + scan_scratch_ints(that many).  With a
+// staging area (inflow_stage_slots(candidates) slots: six doubles in planes
+// of that stride and a species byte) every candidate is generated once;
+// without one (x == nullptr) twice, counted and then emitted.
+struct InflowStage {
+  double* x = nullptr;
+  int8_t* sp = nullptr;
+};
+long long inflow_stage_slots(long long candidates);
 cudaError_t launch_inflow_fused_c32(const KParams& P, const InflowTable& T, int iteration, PartC32 out, int* count,
                                     long long capacity, int* block_counts, int* block_offsets, int* err,
-                                    cudaStream_t st);
+                                    const InflowStage& stage, cudaStream_t st);
 cudaError_t launch_inflow_fused_f64(const KParams& P, const InflowTable& T, int iteration, PartF64 out, int* count,
                                     long long capacity, int* block_counts, int* block_offsets, int* err,
-                                    cudaStream_t st);
+                                    const InflowStage& stage, cudaStream_t st);
 int inflow_blocks(long long candidates);
 // ParticlesProduce: per-cell counts, then emission at offsets[].
 cudaError_t launch_produce_count(const KParams& P, int iteration, int* counts, cudaStream_t st);

@@ -523,6 +523,51 @@ __global__ void __launch_bounds__(kThreads) inflow_emit_kernel(KParams P, Inflow
   }
 }
 
+// The fused inflow in one generation: every block generates its candidates
+// once and writes its survivors, in candidate order, to its own stretch of a
+// staging area (FP64 position and velocity, species); after the scan of the
+// block counts, the place pass stores them at *count + the block's offset +
+// their rank -- the same slots and values as count + emit.
+__global__ void __launch_bounds__(kThreads) inflow_stage_kernel(KParams P, InflowTable T, int iteration,
+                                                                long long total, int* block_counts, double* stage,
+                                                                int8_t* stage_sp, long long stride) {
+  __shared__ int warp_sums[32];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double x[3], v[3];
+  int sp = 0;
+  const bool keep = t < total && inflow_candidate(P, T, iteration, t, x, v, sp);
+  int sum;
+  const int rank = block_exclusive_scan(keep ? 1 : 0, warp_sums, sum);
+  if (keep) {
+    const long long q = (long long)blockIdx.x * blockDim.x + rank;
+    stage[q] = x[0];
+    stage[q + stride] = x[1];
+    stage[q + 2 * stride] = x[2];
+    stage[q + 3 * stride] = v[0];
+    stage[q + 4 * stride] = v[1];
+    stage[q + 5 * stride] = v[2];
+    stage_sp[q] = int8_t(sp);
+  }
+  if (threadIdx.x == 0) block_counts[blockIdx.x] = sum;
+}
+
+template <class Store>
+__global__ void __launch_bounds__(kThreads) inflow_place_kernel(const int* block_counts, const int* offsets,
+                                                                const int* count, long long capacity, int* err,
+                                                                const double* stage, const int8_t* stage_sp,
+                                                                long long stride, Store store) {
+  const int r = threadIdx.x;
+  if (r >= block_counts[blockIdx.x]) return;
+  const long long q = (long long)blockIdx.x * blockDim.x + r;
+  const double x[3] = {stage[q], stage[q + stride], stage[q + 2 * stride]};
+  const double v[3] = {stage[q + 3 * stride], stage[q + 4 * stride], stage[q + 5 * stride]};
+  const long long slot = (long long)*count + offsets[blockIdx.x] + r;
+  if (slot < capacity)
+    store(slot, x, v, int(stage_sp[q]));
+  else
+    atomicCAS(err, 0, int(kDevCapacity));
+}
+
 // CIC weights of ParticlesGridify.f90:70-88 (F1..F8 before the 1/dV).
 struct Cic64 {
   int i, j, k;  // 0-based base node
@@ -896,13 +941,28 @@ __global__ void add_count_kernel(int* count, const int* add, long long capacity)
 
 template <class Store>
 static cudaError_t inflow_fused(const KParams& P, const InflowTable& T, int iteration, Store store, int* count,
-                                long long capacity, int* block_counts, int* block_offsets, int* err, cudaStream_t st) {
+                                long long capacity, int* block_counts, int* block_offsets, int* err,
+                                const InflowStage& S, cudaStream_t st) {
   const long long total = T.cells * T.per_cell;
   if (total == 0) return cudaSuccess;
   const int nb = inflow_blocks(total);
+  cudaError_t e;
+  if (S.x) {
+    const long long stride = (long long)nb * kThreads;
+    note_launch();
+    inflow_stage_kernel<<<nb, kThreads, 0, st>>>(P, T, iteration, total, block_counts, S.x, S.sp, stride);
+    e = launch_scan_int(block_counts, block_offsets, nb, block_offsets + nb, block_offsets + nb + 1, st);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    inflow_place_kernel<<<nb, kThreads, 0, st>>>(block_counts, block_offsets, count, capacity, err, S.x, S.sp, stride,
+                                                 store);
+    note_launch();
+    add_count_kernel<<<1, 1, 0, st>>>(count, block_offsets + nb, capacity);
+    return cudaGetLastError();
+  }
   note_launch();
   inflow_count_kernel<<<nb, kThreads, 0, st>>>(P, T, iteration, total, block_counts);
-  cudaError_t e = launch_scan_int(block_counts, block_offsets, nb, block_offsets + nb, block_offsets + nb + 1, st);
+  e = launch_scan_int(block_counts, block_offsets, nb, block_offsets + nb, block_offsets + nb + 1, st);
   if (e != cudaSuccess) return e;
   note_launch();
   inflow_emit_kernel<<<nb, kThreads, 0, st>>>(P, T, iteration, total, block_offsets, count, capacity, err, store);
@@ -913,15 +973,18 @@ static cudaError_t inflow_fused(const KParams& P, const InflowTable& T, int iter
 
 cudaError_t launch_inflow_fused_c32(const KParams& P, const InflowTable& T, int iteration, PartC32 out, int* count,
                                     long long capacity, int* block_counts, int* block_offsets, int* err,
-                                    cudaStream_t st) {
-  return inflow_fused(P, T, iteration, StoreC32{P, out}, count, capacity, block_counts, block_offsets, err, st);
+                                    const InflowStage& stage, cudaStream_t st) {
+  return inflow_fused(P, T, iteration, StoreC32{P, out}, count, capacity, block_counts, block_offsets, err, stage,
+                      st);
 }
 
 cudaError_t launch_inflow_fused_f64(const KParams& P, const InflowTable& T, int iteration, PartF64 out, int* count,
                                     long long capacity, int* block_counts, int* block_offsets, int* err,
-                                    cudaStream_t st) {
-  return inflow_fused(P, T, iteration, StoreF64{out}, count, capacity, block_counts, block_offsets, err, st);
+                                    const InflowStage& stage, cudaStream_t st) {
+  return inflow_fused(P, T, iteration, StoreF64{out}, count, capacity, block_counts, block_offsets, err, stage, st);
 }
+
+long long inflow_stage_slots(long long candidates) { return (long long)inflow_blocks(candidates) * kThreads; }
 
 cudaError_t launch_produce_emit_f64(const KParams& P, int iteration, const int* offsets, PartF64 out, int* count,
                                     long long capacity, int* err, cudaStream_t st) {
