@@ -17,8 +17,8 @@
 // plane (rows along P keep LP/2+1 outputs, then columns along Q), the
 // contraction over planes against the precomputed slice transforms (the
 // constant (2 tau eps0)^-1 / (LP LQ) folded in), and one inverse FFT per face.
-// FP64 throughout: radix-2 Stockham FFTs in shared memory with twiddles
-// computed on the host.  The slice transforms depend only on D and are
+// FP64 throughout: radix-4 Stockham FFTs (one radix-2 stage for odd powers
+// of two) in shared memory with twiddles computed on the host.  The slice transforms depend only on D and are
 // computed on the first call after D changes.
 #include <cuda_runtime.h>
 
@@ -40,27 +40,57 @@ __device__ inline double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// B sequences of length L (a power of two) in x (x[b*L + i]); radix-2
-// Stockham stages ping-pong between x and y.  Returns the buffer holding the
-// transform (natural order).  tw[t] = exp(-2 pi i t / L), t < L/2; inv uses the
-// conjugates (no scaling).
+// B sequences of length L (a power of two) in x (x[b*L + i]); Stockham
+// stages ping-pong between x and y: one radix-2 stage when log2 L is odd, then
+// radix-4 stages.  Returns the buffer holding the transform (natural order).
+// tw[t] = exp(-2 pi i t / L), t < L; inv uses the conjugates (no scaling).
 __device__ double2* fft_batch(double2* x, double2* y, int L, int logL, int B, const double2* __restrict__ tw,
                               bool inv) {
-  const int half = L >> 1;
-  for (int s = 0; s < logL; ++s) {
-    const int Ns = 1 << s;
-    const int tws = logL - 1 - s;  // twiddle index = (j mod Ns) * L/(2 Ns)
+  int s = 0;  // log2 of the sub-transform length Ns done so far
+  if (logL & 1) {
+    const int half = L >> 1;
     for (int e = threadIdx.x; e < B * half; e += blockDim.x) {
       const int b = e >> (logL - 1), j = e & (half - 1);
       const double2* xb = x + (b << logL);
       double2* yb = y + (b << logL);
+      const double2 v0 = xb[j], v1 = xb[j + half];
+      yb[2 * j] = make_double2(v0.x + v1.x, v0.y + v1.y);
+      yb[2 * j + 1] = make_double2(v0.x - v1.x, v0.y - v1.y);
+    }
+    __syncthreads();
+    double2* t = x;
+    x = y;
+    y = t;
+    s = 1;
+  }
+  const int quarter = L >> 2;
+  for (; s < logL; s += 2) {
+    const int Ns = 1 << s;
+    const int tws = logL - 2 - s;  // twiddle index of factor r = r (j mod Ns) L / (4 Ns)
+    for (int e = threadIdx.x; e < B * quarter; e += blockDim.x) {
+      const int b = e >> (logL - 2), j = e & (quarter - 1);
+      const double2* xb = x + (b << logL);
+      double2* yb = y + (b << logL);
+      const int k = j & (Ns - 1);
+      double2 w1 = tw[k << tws], w2 = tw[(2 * k) << tws], w3 = tw[(3 * k) << tws];
+      if (inv) {
+        w1.y = -w1.y;
+        w2.y = -w2.y;
+        w3.y = -w3.y;
+      }
       const double2 v0 = xb[j];
-      double2 w = tw[(j & (Ns - 1)) << tws];
-      if (inv) w.y = -w.y;
-      const double2 v1 = cmul(xb[j + half], w);
-      const int idx = ((j & ~(Ns - 1)) << 1) + (j & (Ns - 1));
-      yb[idx] = make_double2(v0.x + v1.x, v0.y + v1.y);
-      yb[idx + Ns] = make_double2(v0.x - v1.x, v0.y - v1.y);
+      const double2 v1 = cmul(xb[j + quarter], w1);
+      const double2 v2 = cmul(xb[j + 2 * quarter], w2);
+      const double2 v3 = cmul(xb[j + 3 * quarter], w3);
+      const double2 a0 = make_double2(v0.x + v2.x, v0.y + v2.y), a1 = make_double2(v0.x - v2.x, v0.y - v2.y);
+      const double2 a2 = make_double2(v1.x + v3.x, v1.y + v3.y);
+      const double2 d = make_double2(v1.x - v3.x, v1.y - v3.y);
+      const double2 a3 = inv ? make_double2(-d.y, d.x) : make_double2(d.y, -d.x);  // (v1 - v3) * (+-i)
+      const int idx = ((j & ~(Ns - 1)) << 2) + k;
+      yb[idx] = make_double2(a0.x + a2.x, a0.y + a2.y);
+      yb[idx + Ns] = make_double2(a1.x + a3.x, a1.y + a3.y);
+      yb[idx + 2 * Ns] = make_double2(a0.x - a2.x, a0.y - a2.y);
+      yb[idx + 3 * Ns] = make_double2(a1.x - a3.x, a1.y - a3.y);
     }
     __syncthreads();
     double2* t = x;
@@ -339,7 +369,7 @@ long long bcpot_fft_bytes(const KParams& K) {
     w = std::max(w, std::max((long long)F.nA * F.nQ, (long long)F.LQ) * F.HP * 16);
     s = std::max(s, (long long)F.G * 2 * F.HP * F.LQ * 16);
     v = std::max(v, 2LL * F.nQ * F.HP * 16);
-    tw += (long long)(F.LP + F.LQ) * 8;
+    tw += (long long)(F.LP + F.LQ) * 16;
   }
   return dh + w + s + v + tw;
 }
@@ -362,10 +392,9 @@ struct AxisPlan {
 
 void twiddles(int L, std::vector<double2>& t) {
   const double pi = 3.14159265358979323846264338327950288;
-  t.assign(std::max(1, L / 2), make_double2(1.0, 0.0));
-  for (int k = 0; k < L / 2; ++k) {
-    // exp(-2 pi i k / L), the angle reduced to the first octant's symmetries
-    // by computing sin and cos of the same small argument
+  t.assign(std::max(1, L), make_double2(1.0, 0.0));
+  for (int k = 0; k < L; ++k) {
+    // exp(-2 pi i k / L) from the FP64 cosine and sine of the angle
     const double ang = 2.0 * pi * (double)k / (double)L;
     t[k] = make_double2(std::cos(ang), -std::sin(ang));
   }

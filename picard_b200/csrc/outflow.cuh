@@ -21,8 +21,10 @@
 // every hole below n' follows its chain and copies the particle it reaches.
 //
 // A layout L provides
-//   bool keep_wrap(long long p, int wrap)  -- the BCoutflow test of particle
-//        p; when wrap != 0 also wraps a survivor across periodic faces;
+//   Key load_key(long long p)  -- what the test reads first (issued for all of
+//        a thread's items before any is tested, so the loads overlap);
+//   bool keep_wrap(long long p, Key key, int wrap)  -- the BCoutflow test of
+//        particle p; when wrap != 0 also wraps a survivor across periodic faces;
 //   void move(long long dst, long long src).
 #pragma once
 
@@ -46,10 +48,16 @@ __global__ void __launch_bounds__(kOutflowThreads)
   __shared__ unsigned bits[kOutflowWords];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long base = (long long)blockIdx.x * kOutflowTile;
+  typename L::Key key[kOutflowItems];
 #pragma unroll
   for (int q = 0; q < kOutflowItems; ++q) {
     const long long p = base + (long long)q * kOutflowThreads + threadIdx.x;
-    const bool keep = p < n && lay.keep_wrap(p, wrap);
+    if (p < n) key[q] = lay.load_key(p);
+  }
+#pragma unroll
+  for (int q = 0; q < kOutflowItems; ++q) {
+    const long long p = base + (long long)q * kOutflowThreads + threadIdx.x;
+    const bool keep = p < n && lay.keep_wrap(p, key[q], wrap);
     const unsigned m = __ballot_sync(0xffffffffu, keep);
     if (lane == 0) bits[q * (kOutflowThreads / 32) + warp] = m;
   }
@@ -91,6 +99,8 @@ __global__ void __launch_bounds__(kOutflowThreads)
   const long long np = *survivors;
   const long long base = (long long)blockIdx.x * kOutflowTile;
   if (base >= np) return;
+  // a tile whose particles all survive has no hole
+  if (blockIdx.x + 1 < gridDim.x && block_offsets[blockIdx.x + 1] - block_offsets[blockIdx.x] == kOutflowTile) return;
   for (int q = 0; q < kOutflowItems; ++q) {
     const long long p = base + (long long)q * kOutflowThreads + threadIdx.x;
     if (p >= np) break;

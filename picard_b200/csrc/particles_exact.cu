@@ -462,8 +462,10 @@ __device__ inline int block_exclusive_scan(int v, int* smem_warp, int& total) {
 struct OutflowF64 {
   KParams P;
   PartF64 a;
-  __device__ bool keep_wrap(long long p, int wrap) const {
-    const double x = a.x[p], y = a.y[p], z = a.z[p];
+  using Key = double3;
+  __device__ Key load_key(long long p) const { return make_double3(a.x[p], a.y[p], a.z[p]); }
+  __device__ bool keep_wrap(long long p, double3 key, int wrap) const {
+    const double x = key.x, y = key.y, z = key.z;
     if (!outflow_keep(P, x, y, z)) return false;
     if (wrap) {
       double wx = x, wy = y, wz = z;
