@@ -1148,6 +1148,12 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    # every arm creates and releases contexts: let the stream-ordered pool keep
+    # freed memory for reuse (as the serving loop does for its budget), so that
+    # no arm maps memory afresh for each run
+    from picard_b200 import capi
+
+    capi.pool_keep(local_rank, int(args.budget_gb * 1e9))
     if args.workload == "poisson":
         run_poisson(args, local_rank)
         return

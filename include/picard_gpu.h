@@ -151,6 +151,13 @@ PICARD_API const char* picard_gpu_last_error(void);
  * picard_gpu_bc_outflow (8 B per removed particle, up to 8 B per particle of
  * capacity). */
 PICARD_API int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver, uint64_t* bytes);
+/* Context memory comes from the device's stream-ordered pool.  By default the
+ * pool hands freed memory back to the driver at the next synchronisation, so
+ * a process that creates and releases many contexts (parameter sweeps, the
+ * serving loop) maps memory again for every one.  This keeps up to `bytes` of
+ * freed memory in the pool of `device` for reuse (the serving loop sets its
+ * budget).  No counterpart in the reference (its arrays are static). */
+PICARD_API int picard_gpu_pool_keep(int32_t device, uint64_t bytes);
 
 /* Particles in the reference layout: real_particles(8, n) column-major
  * (x, y, z, vx, vy, vz, tmp, tmp) and int_particles(n) holding the 1-based

@@ -170,6 +170,7 @@ def lib():
         "picard_gpu_destroy": [ctx],
         "picard_gpu_synchronize": [ctx],
         "picard_gpu_footprint": [P, C.c_int32, C.c_int32, C.POINTER(C.c_uint64)],
+        "picard_gpu_pool_keep": [C.c_int32, C.c_uint64],
         "picard_gpu_set_particles": [ctx, dp, ip, C.c_int32],
         "picard_gpu_get_particles": [ctx, dp, ip, C.c_int32, ip],
         "picard_gpu_get_num_local": [ctx, ip],
@@ -259,6 +260,11 @@ def footprint(p: PicardParams, layout: int, solver: int) -> int:
     b = C.c_uint64(0)
     check(lib().picard_gpu_footprint(C.byref(p), layout, solver, C.byref(b)), "picard_gpu_footprint")
     return int(b.value)
+
+
+def pool_keep(device: int, nbytes: int) -> None:
+    """Keep up to nbytes of freed context memory in the device's pool."""
+    check(lib().picard_gpu_pool_keep(device, nbytes), "picard_gpu_pool_keep")
 
 
 def format_e(value: float, w: int = 10, d: int = 4) -> str:

@@ -362,6 +362,13 @@ extern "C" {
 
 const char* picard_gpu_last_error(void) { return g_last_error.c_str(); }
 
+int picard_gpu_pool_keep(int32_t device, uint64_t bytes) {
+  cudaMemPool_t pool;
+  PICARD_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  PICARD_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &bytes));
+  return PICARD_OK;
+}
+
 int picard_gpu_footprint(const picard_params* p, int32_t layout, int32_t solver, uint64_t* bytes) {
   PICARD_TRY(validate(p, layout, solver));
   if (!bytes) return fail(PICARD_ERR_BAD_ARG, "bytes is NULL");
