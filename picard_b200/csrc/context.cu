@@ -32,6 +32,9 @@ int fail(int code, const std::string& msg) {
 
 int check_cuda(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return PICARD_OK;
+  // reported here: clear the runtime's last-error slot so that a later,
+  // unrelated launch check does not report it again (sticky errors stay)
+  (void)cudaGetLastError();
   return fail(PICARD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
@@ -363,6 +366,9 @@ extern "C" {
 const char* picard_gpu_last_error(void) { return g_last_error.c_str(); }
 
 int picard_gpu_pool_keep(int32_t device, uint64_t bytes) {
+  int count = 0;
+  PICARD_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(PICARD_ERR_BAD_ARG, "no such device");
   cudaMemPool_t pool;
   PICARD_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
   PICARD_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &bytes));

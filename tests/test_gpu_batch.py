@@ -134,3 +134,20 @@ def test_batch_with_closed_form_solves_equals_each_run_alone():
         np.testing.assert_array_equal(rg, rp, err_msg=f"run {k}")
     for g in sims:
         g.close()
+
+
+def test_pool_keep_then_contexts_come_and_go():
+    """picard_gpu_pool_keep: freed context memory stays in the device's pool;
+    contexts created and released afterwards run as before."""
+    capi.pool_keep(0, 1 << 30)
+    p = _runs()[2]
+    out = []
+    for _ in range(2):
+        g = _start(p, capi.SOLVER_SPECTRAL)
+        g.run_fused(0, 2)
+        out.append(g.field(capi.FIELD_U))
+        g.close()
+    np.testing.assert_array_equal(out[0], out[1])
+    with pytest.raises(capi.PicardError) as e:
+        capi.pool_keep(1 << 20, 0)  # no such device
+    assert e.value.code == capi.ERR_BAD_ARG
