@@ -447,14 +447,14 @@ int bcpot_fft_alloc(picard_ctx* c) {
     twiddles(F.LP, t);
     PICARD_TRY(dev_alloc(c, &p, sizeof(double2) * t.size()));
     A.twP = static_cast<double2*>(p);
+    // no wait: an asynchronous copy from pageable memory returns once the host
+    // data is staged, so the vector may be refilled
     PICARD_CUDA(cudaMemcpyAsync(A.twP, t.data(), sizeof(double2) * t.size(), cudaMemcpyHostToDevice, c->st));
-    PICARD_CUDA(cudaStreamSynchronize(c->st));
     c->stats.h2d_bytes += (int64_t)(sizeof(double2) * t.size());
     twiddles(F.LQ, t);
     PICARD_TRY(dev_alloc(c, &p, sizeof(double2) * t.size()));
     A.twQ = static_cast<double2*>(p);
     PICARD_CUDA(cudaMemcpyAsync(A.twQ, t.data(), sizeof(double2) * t.size(), cudaMemcpyHostToDevice, c->st));
-    PICARD_CUDA(cudaStreamSynchronize(c->st));
     c->stats.h2d_bytes += (int64_t)(sizeof(double2) * t.size());
     w = std::max(w, (long long)F.nA * F.nQ * F.HP);
     w = std::max(w, (long long)F.LQ * F.HP);  // at least one kernel slice

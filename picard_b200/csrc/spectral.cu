@@ -374,7 +374,8 @@ int spectral_alloc(picard_ctx* c) {
     PICARD_CUDA(cudaMemcpyAsync(S.Q[d], Q.data(), sizeof(double) * Q.size(), cudaMemcpyHostToDevice, c->st));
     PICARD_CUDA(cudaMemcpyAsync(S.QT[d], QT.data(), sizeof(double) * QT.size(), cudaMemcpyHostToDevice, c->st));
     PICARD_CUDA(cudaMemcpyAsync(S.om[d], om.data(), sizeof(double) * om.size(), cudaMemcpyHostToDevice, c->st));
-    PICARD_CUDA(cudaStreamSynchronize(c->st));  // the host vectors go out of scope
+    // no wait: an asynchronous copy from pageable memory returns once the host
+    // data is staged, so the vectors may go out of scope
     c->stats.h2d_bytes += (int64_t)sizeof(double) * (Q.size() + QT.size() + om.size());
   }
   void* p = nullptr;
