@@ -664,13 +664,11 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
       }
       for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));
       lap(1);
-      // ---- ParticlesGridify, BCpotentials, b and ||b||
-      for (int r = 0; r < n; ++r) {
-        picard_ctx* c = ctxs[r];
-        PICARD_TRY(picard_gpu_particles_gridify(c));
-        PICARD_TRY(bc_potentials_async(c));
-        PICARD_TRY(epot_rhs_issue(c));
-      }
+      // ---- ParticlesGridify, BCpotentials (FFT runs: one launch per stage
+      // for all of them), b and ||b||
+      for (int r = 0; r < n; ++r) PICARD_TRY(picard_gpu_particles_gridify(ctxs[r]));
+      PICARD_TRY(bc_potentials_batch(ctxs, n, bst, rev.data(), bev));
+      for (int r = 0; r < n; ++r) PICARD_TRY(epot_rhs_issue(ctxs[r]));
       // ---- CalcEpotential: lockstep rounds over the runs
       for (int r = 0; r < n; ++r) PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
       lap(2);

@@ -125,15 +125,15 @@ __device__ inline int circ_off(int t, int L, int n, bool& ok) {
 // [a0, a0+B1), q = blockIdx.y < nQ, from C; mode 1: the kernel rows (s, tQ)
 // of slices s0 + a (a < count), tQ = blockIdx.y < LQ, from D.  Output
 // W[(a * rowsQ + q) * HP + kP], kP < HP.
-__global__ void __launch_bounds__(kFftThreads) bcfft_rows_kernel(FaceGeom F, int mode, const double* __restrict__ src,
-                                                                 int s0, int count, const double2* __restrict__ tw,
-                                                                 double2* __restrict__ W) {
+__device__ __forceinline__ void bcfft_rows_body(const FaceGeom& F, int mode, const double* __restrict__ src, int s0,
+                                                int count, const double2* __restrict__ tw, double2* __restrict__ W,
+                                                int bx, int by) {
   extern __shared__ double2 smem[];
   const int B = F.B1;
   double2* x = smem;
   double2* y = smem + B * F.LP;
-  const int a0 = blockIdx.x * B;
-  const int q = blockIdx.y;
+  const int a0 = bx * B;
+  const int q = by;
   const int rowsQ = mode == 0 ? F.nQ : F.LQ;
   const int na = mode == 0 ? F.nA : count;
   const bool afast = F.sA == 1 && mode == 0;
@@ -177,24 +177,23 @@ __global__ void __launch_bounds__(kFftThreads) bcfft_rows_kernel(FaceGeom F, int
 // group's partial to S[(g * 2 + f) * HP * LQ + kP * LQ + kQ].
 // mode 1 (kernel transforms): slices a < count of W, real part times scale
 // to Dh[(s0 + a) * HP * LQ + kP * LQ + kQ].
-__global__ void __launch_bounds__(kFftThreads) bcfft_cols_kernel(FaceGeom F, int mode, const double2* __restrict__ W,
-                                                                 int s0, int count, double scale,
-                                                                 const double2* __restrict__ tw,
-                                                                 double* __restrict__ Dh, double2* __restrict__ S) {
+__device__ __forceinline__ void bcfft_cols_body(const FaceGeom& F, int mode, const double2* __restrict__ W, int s0,
+                                                int count, double scale, const double2* __restrict__ tw,
+                                                double* __restrict__ Dh, double2* __restrict__ S, int bx, int by) {
   extern __shared__ double2 smem[];
   const int B = F.B2;
   double2* x = smem;
   double2* y = smem + B * F.LQ;
-  const int k0 = blockIdx.x * B;
+  const int k0 = bx * B;
   const int rowsQ = mode == 0 ? F.nQ : F.LQ;
   const long long plane = (long long)F.HP * F.LQ;
   int a_lo, a_hi;
   if (mode == 0) {
     const int per = (F.nA + F.G - 1) / F.G;
-    a_lo = blockIdx.y * per;
+    a_lo = by * per;
     a_hi = min(F.nA, a_lo + per);
   } else {
-    a_lo = blockIdx.y;
+    a_lo = by;
     a_hi = min(count, a_lo + 1);
   }
   double2 acc0[kColElems / kFftThreads], acc1[kColElems / kFftThreads];
@@ -237,22 +236,22 @@ __global__ void __launch_bounds__(kFftThreads) bcfft_cols_kernel(FaceGeom F, int
     const int b = e >> F.logQ, kq = e & (F.LQ - 1);
     const int k = k0 + b;
     if (k >= F.HP) continue;
-    S[((long long)blockIdx.y * 2 + 0) * plane + (long long)k * F.LQ + kq] = acc0[u];
-    S[((long long)blockIdx.y * 2 + 1) * plane + (long long)k * F.LQ + kq] = acc1[u];
+    S[((long long)by * 2 + 0) * plane + (long long)k * F.LQ + kq] = acc0[u];
+    S[((long long)by * 2 + 1) * plane + (long long)k * F.LQ + kq] = acc1[u];
   }
 }
 
 // Stage 3a: sum of the group partials (fixed order) and the inverse FFT along
 // Q of columns kP in [k0, k0+B2) of face f = blockIdx.y; V[(f*nQ + q)*HP + kP]
 // for q < nQ.
-__global__ void __launch_bounds__(kFftThreads) bcfft_invq_kernel(FaceGeom F, const double2* __restrict__ S,
-                                                                 const double2* __restrict__ tw,
-                                                                 double2* __restrict__ V) {
+__device__ __forceinline__ void bcfft_invq_body(const FaceGeom& F, const double2* __restrict__ S,
+                                                const double2* __restrict__ tw, double2* __restrict__ V, int bx,
+                                                int by) {
   extern __shared__ double2 smem[];
   const int B = F.B2;
   double2* x = smem;
   double2* y = smem + B * F.LQ;
-  const int k0 = blockIdx.x * B, f = blockIdx.y;
+  const int k0 = bx * B, f = by;
   const long long plane = (long long)F.HP * F.LQ;
   for (int e = threadIdx.x; e < B * F.LQ; e += blockDim.x) {
     const int b = e >> F.logQ, kq = e & (F.LQ - 1);
@@ -278,14 +277,14 @@ __global__ void __launch_bounds__(kFftThreads) bcfft_invq_kernel(FaceGeom F, con
 // Stage 3b: inverse real FFT along P of rows q in [q0, q0+B1) of face f =
 // blockIdx.y (the spectrum's upper half from Hermitian symmetry); the real
 // parts p < nP are the face potential.
-__global__ void __launch_bounds__(kFftThreads) bcfft_invp_kernel(FaceGeom F, const double2* __restrict__ V,
-                                                                 const double2* __restrict__ tw,
-                                                                 double* __restrict__ U) {
+__device__ __forceinline__ void bcfft_invp_body(const FaceGeom& F, const double2* __restrict__ V,
+                                                const double2* __restrict__ tw, double* __restrict__ U, int bx,
+                                                int by) {
   extern __shared__ double2 smem[];
   const int B = F.B1;
   double2* x = smem;
   double2* y = smem + B * F.LP;
-  const int q0 = blockIdx.x * B, f = blockIdx.y;
+  const int q0 = bx * B, f = by;
   for (int e = threadIdx.x; e < B * F.LP; e += blockDim.x) {
     const int b = e >> F.logP, k = e & (F.LP - 1);
     const int q = q0 + b;
@@ -308,6 +307,70 @@ __global__ void __launch_bounds__(kFftThreads) bcfft_invp_kernel(FaceGeom F, con
     const int q = q0 + b;
     if (q < F.nQ) U[face + (long long)p * F.sP + (long long)q * F.sQ] = X[(b << F.logP) + p].x;
   }
+}
+
+__global__ void __launch_bounds__(kFftThreads) bcfft_rows_kernel(FaceGeom F, int mode, const double* __restrict__ src,
+                                                                 int s0, int count, const double2* __restrict__ tw,
+                                                                 double2* __restrict__ W) {
+  bcfft_rows_body(F, mode, src, s0, count, tw, W, blockIdx.x, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(kFftThreads) bcfft_cols_kernel(FaceGeom F, int mode, const double2* __restrict__ W,
+                                                                 int s0, int count, double scale,
+                                                                 const double2* __restrict__ tw,
+                                                                 double* __restrict__ Dh, double2* __restrict__ S) {
+  bcfft_cols_body(F, mode, W, s0, count, scale, tw, Dh, S, blockIdx.x, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(kFftThreads) bcfft_invq_kernel(FaceGeom F, const double2* __restrict__ S,
+                                                                 const double2* __restrict__ tw,
+                                                                 double2* __restrict__ V) {
+  bcfft_invq_body(F, S, tw, V, blockIdx.x, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(kFftThreads) bcfft_invp_kernel(FaceGeom F, const double2* __restrict__ V,
+                                                                 const double2* __restrict__ tw,
+                                                                 double* __restrict__ U) {
+  bcfft_invp_body(F, V, tw, U, blockIdx.x, blockIdx.y);
+}
+
+// One face pair of one run in a batched launch: its geometry and buffers,
+// and per stage (rows, columns + contraction, inverse along Q, inverse along
+// P) the first block of its blocks in the launch and its blocks along x.
+struct FftJob {
+  FaceGeom F;
+  const double* C;
+  double2* W;
+  const double2* twP;
+  const double2* twQ;
+  double* Dh;
+  double2* S;
+  double2* V;
+  double* U;
+  long long start[4];
+  int bx[4];
+};
+
+// One stage for every face pair of every run of a batch in one launch: block
+// b belongs to the job with the largest start <= b (binary search), and runs
+// that job's block (local % bx, local / bx) of the stage.
+__global__ void __launch_bounds__(kFftThreads) bcfft_batch_kernel(const FftJob* __restrict__ jobs, int njobs,
+                                                                  int stage) {
+  const long long b = blockIdx.x;
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].start[stage] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const FftJob& J = jobs[lo];
+  const FaceGeom F = J.F;
+  const long long local = b - J.start[stage];
+  const int bx = int(local % J.bx[stage]), by = int(local / J.bx[stage]);
+  if (stage == 0) bcfft_rows_body(F, 0, J.C, 0, F.nA, J.twP, J.W, bx, by);
+  else if (stage == 1) bcfft_cols_body(F, 0, J.W, 0, 0, 0.0, J.twQ, J.Dh, J.S, bx, by);
+  else if (stage == 2) bcfft_invq_body(F, J.S, J.twQ, J.V, bx, by);
+  else bcfft_invp_body(F, J.V, J.twP, J.U, bx, by);
 }
 
 int pow2_at_least(int v) {
@@ -366,9 +429,9 @@ long long bcpot_fft_bytes(const KParams& K) {
     if (!flows[a]) continue;
     FaceGeom F = face_geom(K, a);
     dh += (long long)F.nA * F.HP * F.LQ * 8;
-    w = std::max(w, std::max((long long)F.nA * F.nQ, (long long)F.LQ) * F.HP * 16);
-    s = std::max(s, (long long)F.G * 2 * F.HP * F.LQ * 16);
-    v = std::max(v, 2LL * F.nQ * F.HP * 16);
+    w += std::max((long long)F.nA * F.nQ, (long long)F.LQ) * F.HP * 16;
+    s += (long long)F.G * 2 * F.HP * F.LQ * 16;
+    v += 2LL * F.nQ * F.HP * 16;
     tw += (long long)(F.LP + F.LQ) * 16;
   }
   return dh + w + s + v + tw;
@@ -383,11 +446,17 @@ int bcpot_fft_supported(const KParams& K) {
 
 namespace {
 
+// One face pair's plan and buffers: its own stage buffers, so that the face
+// pairs of a run can go through a batched stage at the same time.
 struct AxisPlan {
   FaceGeom F;
   double* Dh = nullptr;
   double2* twP = nullptr;
   double2* twQ = nullptr;
+  double2* W = nullptr;  // row transforms
+  long long w_elems = 0;
+  double2* S = nullptr;  // the contraction's group partials
+  double2* V = nullptr;  // face spectra after the inverse along Q
 };
 
 void twiddles(int L, std::vector<double2>& t) {
@@ -407,10 +476,6 @@ size_t smem_cols(const FaceGeom& F) { return sizeof(double2) * 2 * (size_t)F.B2 
 
 struct BcFft {
   AxisPlan ax[3];
-  double2* W = nullptr;
-  long long w_elems = 0;
-  double2* S = nullptr;
-  double2* V = nullptr;
   bool ready = false;  // slice transforms of the current D
 };
 
@@ -422,6 +487,7 @@ static int set_smem_limits() {
   PICARD_CUDA(cudaFuncSetAttribute(bcfft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   PICARD_CUDA(cudaFuncSetAttribute(bcfft_invq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   PICARD_CUDA(cudaFuncSetAttribute(bcfft_invp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  PICARD_CUDA(cudaFuncSetAttribute(bcfft_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   done = true;
   return PICARD_OK;
 }
@@ -434,7 +500,6 @@ int bcpot_fft_alloc(picard_ctx* c) {
   c->bcfft = B;
   const KParams& K = c->K;
   const int flows[3] = {K.xflow, K.yflow, K.zflow};
-  long long w = 0, s = 0, v = 0;
   for (int a = 0; a < 3; ++a) {
     if (!flows[a]) continue;
     AxisPlan& A = B->ax[a];
@@ -456,19 +521,16 @@ int bcpot_fft_alloc(picard_ctx* c) {
     A.twQ = static_cast<double2*>(p);
     PICARD_CUDA(cudaMemcpyAsync(A.twQ, t.data(), sizeof(double2) * t.size(), cudaMemcpyHostToDevice, c->st));
     c->stats.h2d_bytes += (int64_t)(sizeof(double2) * t.size());
-    w = std::max(w, (long long)F.nA * F.nQ * F.HP);
-    w = std::max(w, (long long)F.LQ * F.HP);  // at least one kernel slice
-    s = std::max(s, (long long)F.G * 2 * F.HP * F.LQ);
-    v = std::max(v, 2LL * F.nQ * F.HP);
+    // at least one kernel slice's rows, for the slice transforms
+    const long long w = std::max((long long)F.nA * F.nQ, (long long)F.LQ) * F.HP;
+    PICARD_TRY(dev_alloc(c, &p, sizeof(double2) * (size_t)w));
+    A.W = static_cast<double2*>(p);
+    A.w_elems = w;
+    PICARD_TRY(dev_alloc(c, &p, sizeof(double2) * (size_t)F.G * 2 * F.HP * F.LQ));
+    A.S = static_cast<double2*>(p);
+    PICARD_TRY(dev_alloc(c, &p, sizeof(double2) * 2 * (size_t)F.nQ * F.HP));
+    A.V = static_cast<double2*>(p);
   }
-  void* p = nullptr;
-  PICARD_TRY(dev_alloc(c, &p, sizeof(double2) * (size_t)w));
-  B->W = static_cast<double2*>(p);
-  B->w_elems = w;
-  PICARD_TRY(dev_alloc(c, &p, sizeof(double2) * (size_t)s));
-  B->S = static_cast<double2*>(p);
-  PICARD_TRY(dev_alloc(c, &p, sizeof(double2) * (size_t)v));
-  B->V = static_cast<double2*>(p);
   return PICARD_OK;
 }
 
@@ -491,17 +553,17 @@ static int prepare(picard_ctx* c) {
     if (!A.Dh) continue;
     const FaceGeom& F = A.F;
     const double scale = K0 / ((double)F.LP * (double)F.LQ);
-    const int chunk = int(std::max<long long>(1, B->w_elems / ((long long)F.LQ * F.HP)));
+    const int chunk = int(std::max<long long>(1, A.w_elems / ((long long)F.LQ * F.HP)));
     for (int s0 = 0; s0 < F.nA; s0 += chunk) {
       const int cnt = std::min(chunk, F.nA - s0);
       dim3 g1((cnt + F.B1 - 1) / F.B1, F.LQ);
       note_launch();
       // slice index a <-> normal offset s0 + a + 1 (the D table at offset a + 1 along A)
-      bcfft_rows_kernel<<<g1, kFftThreads, smem_rows(F), c->st>>>(F, 1, c->D + F.dA, s0, cnt, A.twP, B->W);
+      bcfft_rows_kernel<<<g1, kFftThreads, smem_rows(F), c->st>>>(F, 1, c->D + F.dA, s0, cnt, A.twP, A.W);
       PICARD_CUDA(cudaGetLastError());
       dim3 g2((F.HP + F.B2 - 1) / F.B2, cnt);
       note_launch();
-      bcfft_cols_kernel<<<g2, kFftThreads, smem_cols(F), c->st>>>(F, 1, B->W, s0, cnt, scale, A.twQ, A.Dh, nullptr);
+      bcfft_cols_kernel<<<g2, kFftThreads, smem_cols(F), c->st>>>(F, 1, A.W, s0, cnt, scale, A.twQ, A.Dh, nullptr);
       PICARD_CUDA(cudaGetLastError());
     }
   }
@@ -520,21 +582,87 @@ int bc_potentials_fft(picard_ctx* c) {
     const FaceGeom& F = A.F;
     dim3 g1((F.nA + F.B1 - 1) / F.B1, F.nQ);
     note_launch();
-    bcfft_rows_kernel<<<g1, kFftThreads, smem_rows(F), c->st>>>(F, 0, c->C, 0, F.nA, A.twP, B->W);
+    bcfft_rows_kernel<<<g1, kFftThreads, smem_rows(F), c->st>>>(F, 0, c->C, 0, F.nA, A.twP, A.W);
     PICARD_CUDA(cudaGetLastError());
     dim3 g2((F.HP + F.B2 - 1) / F.B2, F.G);
     note_launch();
-    bcfft_cols_kernel<<<g2, kFftThreads, smem_cols(F), c->st>>>(F, 0, B->W, 0, 0, 0.0, A.twQ, A.Dh, B->S);
+    bcfft_cols_kernel<<<g2, kFftThreads, smem_cols(F), c->st>>>(F, 0, A.W, 0, 0, 0.0, A.twQ, A.Dh, A.S);
     PICARD_CUDA(cudaGetLastError());
     dim3 g3((F.HP + F.B2 - 1) / F.B2, 2);
     note_launch();
-    bcfft_invq_kernel<<<g3, kFftThreads, smem_cols(F), c->st>>>(F, B->S, A.twQ, B->V);
+    bcfft_invq_kernel<<<g3, kFftThreads, smem_cols(F), c->st>>>(F, A.S, A.twQ, A.V);
     PICARD_CUDA(cudaGetLastError());
     dim3 g4((F.nQ + F.B1 - 1) / F.B1, 2);
     note_launch();
-    bcfft_invp_kernel<<<g4, kFftThreads, smem_rows(F), c->st>>>(F, B->V, A.twP, c->U);
+    bcfft_invp_kernel<<<g4, kFftThreads, smem_rows(F), c->st>>>(F, A.V, A.twP, c->U);
     PICARD_CUDA(cudaGetLastError());
   }
+  return PICARD_OK;
+}
+
+// BCpotentials of many runs: the FFT runs' face pairs advance stage by stage,
+// each stage one launch over all of them on the batch stream (after every
+// such run's U is zeroed and its slice transforms exist, on its own stream);
+// the other runs take their own method on their own streams.
+int bc_potentials_batch(picard_ctx** ctxs, int n, cudaStream_t bst, cudaEvent_t* rev, cudaEvent_t bev) {
+  std::vector<FftJob> jobs;
+  std::vector<int> fft_runs;
+  long long total[4] = {0, 0, 0, 0};
+  size_t smem[4] = {0, 0, 0, 0};
+  for (int r = 0; r < n; ++r) {
+    picard_ctx* c = ctxs[r];
+    if (c->bcpot_tensor != PICARD_BCPOT_FFT) {
+      PICARD_TRY(bc_potentials_async(c));
+      continue;
+    }
+    PICARD_TRY(bcpot_fft_alloc(c));
+    BcFft* B = c->bcfft;
+    if (!B->ready) PICARD_TRY(prepare(c));
+    PICARD_CUDA(cudaMemsetAsync(c->U, 0, sizeof(double) * c->K.nodes, c->st));  // BCpotentials.f90:36
+    PICARD_CUDA(cudaEventRecord(rev[r], c->st));
+    PICARD_CUDA(cudaStreamWaitEvent(bst, rev[r], 0));
+    fft_runs.push_back(r);
+    for (int a = 0; a < 3; ++a) {
+      AxisPlan& A = B->ax[a];
+      if (!A.Dh) continue;
+      FftJob J;
+      J.F = A.F;
+      J.C = c->C;
+      J.W = A.W;
+      J.twP = A.twP;
+      J.twQ = A.twQ;
+      J.Dh = A.Dh;
+      J.S = A.S;
+      J.V = A.V;
+      J.U = c->U;
+      const FaceGeom& F = A.F;
+      const int bxs[4] = {(F.nA + F.B1 - 1) / F.B1, (F.HP + F.B2 - 1) / F.B2, (F.HP + F.B2 - 1) / F.B2,
+                          (F.nQ + F.B1 - 1) / F.B1};
+      const int bys[4] = {F.nQ, F.G, 2, 2};
+      const size_t sm[4] = {smem_rows(F), smem_cols(F), smem_cols(F), smem_rows(F)};
+      for (int t = 0; t < 4; ++t) {
+        J.start[t] = total[t];
+        J.bx[t] = bxs[t];
+        total[t] += (long long)bxs[t] * bys[t];
+        smem[t] = std::max(smem[t], sm[t]);
+      }
+      jobs.push_back(J);
+    }
+  }
+  if (jobs.empty()) return PICARD_OK;
+  // the job table lives on the batch stream until its last launch
+  void* dj = nullptr;
+  PICARD_CUDA(cudaMallocAsync(&dj, sizeof(FftJob) * jobs.size(), bst));
+  PICARD_CUDA(cudaMemcpyAsync(dj, jobs.data(), sizeof(FftJob) * jobs.size(), cudaMemcpyHostToDevice, bst));
+  for (int t = 0; t < 4; ++t) {
+    note_launch();
+    bcfft_batch_kernel<<<(unsigned)total[t], kFftThreads, smem[t], bst>>>(static_cast<const FftJob*>(dj),
+                                                                            (int)jobs.size(), t);
+    PICARD_CUDA(cudaGetLastError());
+  }
+  PICARD_CUDA(cudaFreeAsync(dj, bst));
+  PICARD_CUDA(cudaEventRecord(bev, bst));
+  for (int r : fft_runs) PICARD_CUDA(cudaStreamWaitEvent(ctxs[r]->st, bev, 0));
   return PICARD_OK;
 }
 

@@ -185,6 +185,11 @@ int spectral_alloc(picard_ctx* c);
 long long bcpot_fft_bytes(const KParams& K);
 int bcpot_fft_supported(const KParams& K);
 int bc_potentials_fft(picard_ctx* c);
+// BCpotentials of a batch of runs: the runs with the FFT method go through one
+// launch per stage for all of them on bst (rev[r]: an event per run; bev: one
+// event), the others through their own method on their own streams.  Each
+// run's stream is ordered after its BCpotentials; nothing waits on the host.
+int bc_potentials_batch(picard_ctx** ctxs, int n, cudaStream_t bst, cudaEvent_t* rev, cudaEvent_t bev);
 void bcpot_fft_invalidate(picard_ctx* c);
 void bcpot_fft_free(picard_ctx* c);
 long long spectral_bytes(const KParams& K);
