@@ -84,16 +84,22 @@ def test_fused_cell32_matches_oracle(steps):
     g.close()
 
 
-def test_push_advance_equals_velocity_then_position():
-    # run_fused(20, 24) fuses the push of steps 21..23 with the position
+@pytest.mark.parametrize("flows", [(1, 1, 1), (1, 0, 1), (0, 1, 0)])
+@pytest.mark.parametrize("solver", [capi.SOLVER_F32_REFINE, capi.SOLVER_SPECTRAL])
+def test_push_advance_equals_velocity_then_position(flows, solver):
+    # run_fused(10, 14) fuses the push of steps 11..13 with the position
     # advance of the next step; four one-step calls run the same steps with
     # advance_velocity_c32_kernel and advance_position_c32_kernel apart.
     # Everything else is the same sequence, so the runs agree bit for bit:
-    # particles in the same slots, the same sweeps, N and U.
-    p = O.derive(small_haser(nx=16, ny=12, nz=10, ppc=4, seed=5))
+    # particles in the same slots, the same sweeps, N and U -- with both
+    # solvers, and with periodic axes (the wrap of ParticlesTransfer).
+    xf, yf, zf = flows
+    q = small_haser(nx=16, ny=12, nz=10, ppc=4, seed=5)
+    q.xflow, q.yflow, q.zflow = xf, yf, zf
+    p = O.derive(q)
     o = developed(p, steps=10)
-    a = Simulation(p, derive=False, **C32)
-    b = Simulation(p, derive=False, **C32)
+    a = Simulation(p, derive=False, layout=capi.LAYOUT_CELL32, solver=solver)
+    b = Simulation(p, derive=False, layout=capi.LAYOUT_CELL32, solver=solver)
     for s in (a, b):
         s.calc_distance()
         s.set_particles(*o.particles())
