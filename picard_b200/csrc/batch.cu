@@ -20,8 +20,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -49,6 +54,86 @@ constexpr int kTicksAhead = 6;  // batched sweep launches queued ahead of the de
 // the other runs wait, and join as runs of the set converge.
 constexpr double kTickSetBytes = 80e6;
 long long g_batch_ctas = 0;  // CTAs launched by batched sweeps (PICARD_BATCH_LOG)
+
+// Host threads that issue the runs' per-run work in parallel (launches on the
+// runs' own streams, waits on them), so that one host thread's launch rate and
+// round trips do not bound a batch of many small runs.  run(n, fn) calls fn(r)
+// for every r < n, run r on worker r % threads, and returns when all are done
+// with the status of the lowest-numbered failing run (its message re-raised on
+// the calling thread).  Each run's work stays in its own stream order, so the
+// results do not depend on the thread count.
+class RunPool {
+ public:
+  RunPool(int threads, int device) : T_(threads), device_(device) {
+    for (int w = 1; w < T_; ++w) th_.emplace_back([this, w]() { worker(w); });
+  }
+  ~RunPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (std::thread& t : th_) t.join();
+  }
+  int run(int n, const std::function<int(int)>& fn) {
+    rc_.assign(n, PICARD_OK);
+    msg_.assign(n, std::string());
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      fn_ = &fn;
+      n_ = n;
+      pending_ = T_ - 1;
+      ++gen_;
+    }
+    cv_.notify_all();
+    slice(0);  // the calling thread is worker 0
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      done_cv_.wait(lk, [&]() { return pending_ == 0; });
+    }
+    for (int r = 0; r < n; ++r)
+      if (rc_[r] != PICARD_OK) return fail(rc_[r], msg_[r]);
+    return PICARD_OK;
+  }
+
+ private:
+  void slice(int w) {
+    for (int r = w; r < n_; r += T_) {
+      const int q = (*fn_)(r);
+      if (q != PICARD_OK) {
+        rc_[r] = q;
+        msg_[r] = picard_gpu_last_error();
+      }
+    }
+  }
+  void worker(int w) {
+    cudaSetDevice(device_);
+    long long seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&]() { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      slice(w);
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (--pending_ == 0) done_cv_.notify_one();
+      }
+    }
+  }
+  const int T_, device_;
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<int(int)>* fn_ = nullptr;
+  int n_ = 0, pending_ = 0;
+  long long gen_ = 0;
+  bool stop_ = false;
+  std::vector<int> rc_;
+  std::vector<std::string> msg_;
+};
 
 struct alignas(64) BatchRun {
   CUtensorMap tw;  // w of the sweep's input iterate (boxes 72 x 10 x zc+2; 32-wide tiles 40 x 10 x zc+2)
@@ -597,7 +682,12 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
     return rc;
   }
   berr = ctxs[0]->d_err;
-  bool nc = false;
+  std::atomic<bool> nc{false};
+  // PICARD_BATCH_THREADS: host threads issuing the per-run work (default
+  // min(runs, 8); 1: the calling thread alone)
+  const char* thv = std::getenv("PICARD_BATCH_THREADS");
+  const int threads = std::max(1, std::min(n, thv && *thv ? std::atoi(thv) : 8));
+  RunPool pool(threads, dev);
   std::vector<RunSolve> solves(n);
   std::vector<RunSolve*> rp(n);
   for (int r = 0; r < n; ++r) rp[r] = &solves[r];
@@ -635,7 +725,7 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
     for (int32_t step = 1; step <= nsteps; ++step) {
       tick = now();
       // ---- AdvancePosition, ParticlesProduce (device count) for every run
-      for (int r = 0; r < n; ++r) {
+      PICARD_TRY(pool.run(n, [&](int r) -> int {
         picard_ctx* c = ctxs[r];
         const KParams& K = c->K;
         const int cells = c->prm.nx * c->prm.ny * c->prm.nz;
@@ -651,28 +741,32 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
           PICARD_CUDA(launch_produce_emit_c32(K, it, c->cell_offsets, c->c32, c->d_count,
                                               c->capacity, c->d_err, c->st));
         PICARD_TRY(count_issue(c));
-      }
-      for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));
+        return count_collect(c);
+      }));
       lap(0);
       // ---- BCoutflow + ParticlesTransfer (in place), BCinflow (fused)
-      for (int r = 0; r < n; ++r) {
+      PICARD_TRY(pool.run(n, [&](int r) -> int {
         picard_ctx* c = ctxs[r];
         const int32_t it = it0[r] + step;
         PICARD_CUDA(launch_outflow(c, 1));
         PICARD_CUDA(launch_inflow_fused(c, it));
         PICARD_TRY(count_issue(c));
-      }
-      for (int r = 0; r < n; ++r) PICARD_TRY(count_collect(ctxs[r]));
+        return count_collect(c);
+      }));
       lap(1);
       // ---- ParticlesGridify, BCpotentials (FFT runs: one launch per stage
       // for all of them), b and ||b||
-      for (int r = 0; r < n; ++r) PICARD_TRY(picard_gpu_particles_gridify(ctxs[r]));
+      PICARD_TRY(pool.run(n, [&](int r) -> int { return picard_gpu_particles_gridify(ctxs[r]); }));
       PICARD_TRY(bc_potentials_batch(ctxs, n, bst, rev.data(), bev));
-      for (int r = 0; r < n; ++r) PICARD_TRY(epot_rhs_issue(ctxs[r]));
-      // ---- CalcEpotential: lockstep rounds over the runs
-      for (int r = 0; r < n; ++r) PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
+      PICARD_TRY(pool.run(n, [&](int r) -> int {
+        PICARD_TRY(epot_rhs_issue(ctxs[r]));
+        PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
+        return PICARD_OK;
+      }));
       lap(2);
-      for (int r = 0; r < n; ++r) {
+      // ---- CalcEpotential: closed-form solves and solves of their own
+      // issued per run in parallel; FP32 runs in lockstep ticks below
+      PICARD_TRY(pool.run(n, [&](int r) -> int {
         picard_ctx* c = ctxs[r];
         RunSolve& rs = solves[r];
         rs = RunSolve();
@@ -681,7 +775,7 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
         rs.done = rs.e.trivial;
         rs.sweeps = 0;
         rs.converged = true;
-        if (rs.done) continue;
+        if (rs.done) return PICARD_OK;
         if (c->solver == PICARD_SOLVER_SPECTRAL) {
           // closed form: queued now, its Parseval evaluations collected for
           // every such run together below
@@ -703,7 +797,8 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
           rs.batched = false;
           rs.e.trivial = false;
         }
-      }
+        return PICARD_OK;
+      }));
       // Rounds are asynchronous across runs: every tick advances each run in
       // the middle of a round by one sweep; a run whose round ends gets its
       // anchor, reduction and stop test on its own stream while the ticks go
@@ -797,42 +892,48 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
           if (sweeping == 0) break;  // one at a time while blocking: replan at once
         }
       }
-      // closed-form solves: one host round trip per evaluation for all runs
-      for (bool pending = true; pending;) {
-        pending = false;
-        for (int r = 0; r < n; ++r) {
-          RunSolve& rs = solves[r];
-          if (!rs.spectral || rs.done) continue;
-          PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
-          if (rs.Q.done) {
-            spec_account(rs.Q);
-            rs.done = true;
-            rs.sweeps = rs.Q.d;
-            rs.converged = rs.Q.converged;
-            continue;
+      // closed-form solves: each worker takes its runs' Parseval evaluations
+      // in turn, one host round trip per evaluation for all of them
+      PICARD_TRY(pool.run(threads, [&](int w) -> int {
+        for (bool pending = true; pending;) {
+          pending = false;
+          for (int r = w; r < n; r += threads) {
+            RunSolve& rs = solves[r];
+            if (!rs.spectral || rs.done) continue;
+            PICARD_CUDA(cudaStreamSynchronize(ctxs[r]->st));
+            if (rs.Q.done) {
+              spec_account(rs.Q);
+              rs.done = true;
+              rs.sweeps = rs.Q.d;
+              rs.converged = rs.Q.converged;
+              continue;
+            }
+            PICARD_TRY(spec_collect(rs.Q));
+            pending = true;
           }
-          PICARD_TRY(spec_collect(rs.Q));
-          pending = true;
         }
-      }
-      for (int r = 0; r < n; ++r) {
+        return PICARD_OK;
+      }));
+      PICARD_TRY(pool.run(n, [&](int r) -> int {
         RunSolve& rs = solves[r];
-        if (!rs.batched && !rs.spectral && !rs.e.trivial) continue;  // solved on its own above
+        if (!rs.batched && !rs.spectral && !rs.e.trivial) return PICARD_OK;  // solved on its own above
         int32_t sw = 0;
         int q = epot_finish(ctxs[r], rs.e, rs.sweeps, rs.converged, &sw);
         if (q == PICARD_ERR_NOT_CONVERGED) nc = true;
         else if (q != PICARD_OK) return q;
         if (sweeps_total) sweeps_total[r] += sw;
-      }
+        return PICARD_OK;
+      }));
       lap(3);
       // ---- CalcEfield + BCfields, AdvanceVelocity
-      for (int r = 0; r < n; ++r) {
+      PICARD_TRY(pool.run(n, [&](int r) -> int {
         picard_ctx* c = ctxs[r];
         PICARD_TRY(picard_gpu_calc_efield(c));
         PICARD_TRY(picard_gpu_advance_velocity(c, c->prm.dt));
         c->stats.steps += 1;
         c->stats.particle_steps += c->num_local;
-      }
+        return PICARD_OK;
+      }));
       lap(4);
     }
     for (int r = 0; r < n; ++r) {
