@@ -25,6 +25,7 @@
 #include <condition_variable>
 #include <cstdio>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <cstdlib>
@@ -134,6 +135,30 @@ class RunPool {
   std::vector<int> rc_;
   std::vector<std::string> msg_;
 };
+
+// Pools kept between batched calls (the continuous-batching server calls the
+// batched step once per iteration): a call takes a pool of its device and
+// thread count from the cache, or makes one, and puts it back when done.
+std::mutex g_pool_mu;
+std::vector<std::pair<std::pair<int, int>, std::unique_ptr<RunPool>>> g_pools;
+
+std::unique_ptr<RunPool> take_pool(int device, int threads) {
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (auto it = g_pools.begin(); it != g_pools.end(); ++it)
+      if (it->first == std::make_pair(device, threads)) {
+        std::unique_ptr<RunPool> p = std::move(it->second);
+        g_pools.erase(it);
+        return p;
+      }
+  }
+  return std::unique_ptr<RunPool>(new RunPool(threads, device));
+}
+
+void give_pool(int device, int threads, std::unique_ptr<RunPool> p) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  g_pools.emplace_back(std::make_pair(device, threads), std::move(p));
+}
 
 struct alignas(64) BatchRun {
   CUtensorMap tw;  // w of the sweep's input iterate (boxes 72 x 10 x zc+2; 32-wide tiles 40 x 10 x zc+2)
@@ -687,7 +712,13 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
   // min(runs, 8); 1: the calling thread alone)
   const char* thv = std::getenv("PICARD_BATCH_THREADS");
   const int threads = std::max(1, std::min(n, thv && *thv ? std::atoi(thv) : 8));
-  RunPool pool(threads, dev);
+  std::unique_ptr<RunPool> pool_owner = take_pool(dev, threads);
+  RunPool& pool = *pool_owner;
+  struct PoolReturn {
+    int dev, threads;
+    std::unique_ptr<RunPool>& p;
+    ~PoolReturn() { give_pool(dev, threads, std::move(p)); }
+  } pool_return{dev, threads, pool_owner};
   std::vector<RunSolve> solves(n);
   std::vector<RunSolve*> rp(n);
   for (int r = 0; r < n; ++r) rp[r] = &solves[r];
@@ -729,7 +760,8 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
         picard_ctx* c = ctxs[r];
         const KParams& K = c->K;
         const int cells = c->prm.nx * c->prm.ny * c->prm.nz;
-        PICARD_TRY(picard_gpu_advance_position(c, c->prm.dt));
+        // CELL32 runs after their first step: the previous step's push advanced them
+        if (step == 1 || c->layout != PICARD_LAYOUT_CELL32) PICARD_TRY(picard_gpu_advance_position(c, c->prm.dt));
         const int32_t it = it0[r] + step;
         PICARD_CUDA(launch_produce_count(K, it, c->cell_counts, c->st));
         PICARD_CUDA(launch_scan_int(c->cell_counts, c->cell_offsets, cells, c->cell_offsets + cells,
@@ -925,11 +957,15 @@ int batch_run_impl(picard_ctx** ctxs, int32_t n, const int32_t* it0, int32_t nst
         return PICARD_OK;
       }));
       lap(3);
-      // ---- CalcEfield + BCfields, AdvanceVelocity
+      // ---- CalcEfield + BCfields, AdvanceVelocity (CELL32, when another step
+      // follows: fused with that step's AdvancePosition, as the single-run loop)
       PICARD_TRY(pool.run(n, [&](int r) -> int {
         picard_ctx* c = ctxs[r];
         PICARD_TRY(picard_gpu_calc_efield(c));
-        PICARD_TRY(picard_gpu_advance_velocity(c, c->prm.dt));
+        if (step < nsteps && c->layout == PICARD_LAYOUT_CELL32)
+          PICARD_CUDA(launch_push_advance_c32(c->K, c->c32, c->num_local, c->E32, c->prm.dt, c->st));
+        else
+          PICARD_TRY(picard_gpu_advance_velocity(c, c->prm.dt));
         c->stats.steps += 1;
         c->stats.particle_steps += c->num_local;
         return PICARD_OK;

@@ -40,6 +40,7 @@ struct SpectralPlan {
   double* T[2] = {nullptr, nullptr};            // nx*ny*nz each
   double* partial = nullptr;                    // [norm_blocks][32]
   double* sums = nullptr;                       // [32]
+  unsigned int* counter = nullptr;              // blocks done in an evaluation (re-armed by the last)
   int norm_blocks = 0;
   long long evals = 0;                          // Parseval evaluations (launch pairs)
 };
@@ -203,7 +204,7 @@ int solve_spectral(picard_ctx* c, double tol, long long smax, int maxit, long lo
 // that work).
 struct SpecSolve {
   picard_ctx* c = nullptr;
-  double tol2 = 0.0, r2_hit = 0.0;
+  double tol2 = 0.0, r2_hit = 0.0, f1 = 0.0;  // f1: ||r_1||^2 from the doubling pass
   long long smax = 0, dmax = 0, lo = 0, hi = 0;
   long long d0 = 0, step = 0, d = 0;  // pending evaluation; the accepted sweep count
   int count = 0;

@@ -148,23 +148,28 @@ __device__ inline double ipow(double x, long long e) {
 
 // Parseval sums f(d_t) = sum_m g_m^(2 d_t) rh_m^2 at the sweep counts
 // d_t = d0 + t*step (doubling == 0) or d_t = d0 * 2^t (doubling == 1), for
-// t < count; per-block partials in a fixed order.
+// t < count.  Modes with g^2 <= g2_skip add nothing (the caller bounds what
+// they could add far below the stop test's resolution).  Per-block partials
+// in a fixed order; the last block to finish sums them (in block order) into
+// out[t] and re-arms the counter.
 __global__ void __launch_bounds__(kSpecThreads) spec_norms_kernel(const double* __restrict__ Rh, int nx, int ny,
                                                                   int nz, const double* __restrict__ omx,
                                                                   const double* __restrict__ omy,
                                                                   const double* __restrict__ omz, long long d0,
                                                                   long long step, int count, int doubling,
-                                                                  double* __restrict__ partial) {
+                                                                  double g2_skip, double* __restrict__ partial,
+                                                                  unsigned int* counter, double* __restrict__ out) {
   double acc[kSpecPoints];
 #pragma unroll
   for (int t = 0; t < kSpecPoints; ++t) acc[t] = 0.0;
   const long long n = (long long)nx * ny * nz;
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const int mx = int(q % nx), my = int((q / nx) % ny), mz = int(q / ((long long)nx * ny));
-    const double r = Rh[q];
-    const double w = r * r;
     const double g = 1.0 - (omx[mx] + omy[my] + omz[mz]);
     const double g2 = g * g;
+    if (g2 <= g2_skip) continue;
+    const double r = Rh[q];
+    const double w = r * r;
     const double x = ipow(g2, d0);
     if (doubling) {
       double y = x;  // d0 * 2^t: a chain of squarings
@@ -191,6 +196,7 @@ __global__ void __launch_bounds__(kSpecThreads) spec_norms_kernel(const double* 
     }
   }
   __shared__ double sh[kSpecThreads / 32][kSpecPoints];
+  __shared__ bool last;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int t = 0; t < kSpecPoints; ++t) {
@@ -204,16 +210,20 @@ __global__ void __launch_bounds__(kSpecThreads) spec_norms_kernel(const double* 
     for (int w2 = 0; w2 < kSpecThreads / 32; ++w2) s += sh[w2][threadIdx.x];
     partial[(long long)blockIdx.x * kSpecPoints + threadIdx.x] = s;
   }
-}
-
-// out[t] = sum_b partial[b][t]: warp t, lanes striding over the blocks, then
-// a fixed shuffle tree (deterministic for a fixed block count).
-__global__ void spec_sum_kernel(const double* __restrict__ partial, int nb, double* __restrict__ out) {
-  const int t = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double s = 0.0;
-  for (int b = lane; b < nb; b += 32) s += partial[(long long)b * kSpecPoints + t];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) out[t] = s;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // the last block: out[t] = sum_b partial[b][t], warp w taking points w, w + 8, ...
+  for (int t = wid; t < kSpecPoints; t += kSpecThreads / 32) {
+    double s = 0.0;
+    for (int b2 = lane; b2 < (int)gridDim.x; b2 += 32) s += __ldcg(partial + (long long)b2 * kSpecPoints + t);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[t] = s;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
 }
 
 // rh -> -af (1 - g^d)/(1 - g) rh in place.  For g > 0 the factor is
@@ -336,14 +346,12 @@ cudaError_t transform(picard_ctx* c, bool forward) {
 
 // Queues the evaluation of f at count (<= kSpecPoints) sweep counts and the
 // copy of the sums to c->h_pinned[0..count); the caller waits on the stream.
-int issue_norms(picard_ctx* c, long long d0, long long step, int count, bool doubling) {
+int issue_norms(picard_ctx* c, long long d0, long long step, int count, bool doubling, double g2_skip) {
   SpectralPlan& S = c->spec;
   note_launch();
   spec_norms_kernel<<<S.norm_blocks, kSpecThreads, 0, c->st>>>(S.T[1], c->K.nx, c->K.ny, c->K.nz, S.om[0], S.om[1],
-                                                                S.om[2], d0, step, count, doubling ? 1 : 0,
-                                                                S.partial);
-  note_launch();
-  spec_sum_kernel<<<1, 32 * kSpecPoints, 0, c->st>>>(S.partial, S.norm_blocks, S.sums);
+                                                                S.om[2], d0, step, count, doubling ? 1 : 0, g2_skip,
+                                                                S.partial, S.counter, S.sums);
   PICARD_CUDA(cudaGetLastError());
   PICARD_CUDA(cudaMemcpyAsync(c->h_pinned, S.sums, sizeof(double) * count, cudaMemcpyDeviceToHost, c->st));
   c->stats.d2h_bytes += (int64_t)sizeof(double) * count;
@@ -388,6 +396,8 @@ int spectral_alloc(picard_ctx* c) {
   S.partial = static_cast<double*>(p);
   PICARD_TRY(dev_alloc(c, &p, sizeof(double) * kSpecPoints));
   S.sums = static_cast<double*>(p);
+  PICARD_TRY(dev_alloc(c, &p, sizeof(unsigned int)));  // zeroed
+  S.counter = static_cast<unsigned int*>(p);
   return PICARD_OK;
 }
 
@@ -403,6 +413,17 @@ long long spectral_bytes(const KParams& K) {
 // no passing d known).  The first evaluation doubles d from 1 up to the
 // first power of two >= dmax; later ones take evenly spaced candidates of
 // (lo, hi).
+
+// Modes whose g^2 is at most the returned value add at most 2^-60 tol^2 to
+// any f(d) the uniform passes evaluate (d > lo): sum over those modes of
+// w g^(2d) <= g2_max^(d-1) f(1).  None is skipped while lo < 2 or f(1) is
+// unknown.
+static double skip_threshold(const SpecSolve& Q) {
+  if (Q.lo < 2 || !(Q.f1 > 0.0) || !(Q.tol2 > 0.0)) return -1.0;
+  const double ratio = Q.tol2 * 0x1p-60 / Q.f1;
+  if (!(ratio < 1.0)) return -1.0;
+  return std::exp(std::log(ratio) / double(Q.lo - 1));
+}
 
 int spec_begin(SpecSolve& Q, picard_ctx* c, double tol, long long smax, int maxit) {
   SpectralPlan& S = c->spec;
@@ -430,7 +451,7 @@ int spec_begin(SpecSolve& Q, picard_ctx* c, double tol, long long smax, int maxi
     Q.step = 0;
     Q.count = cnt;
     Q.doubling = true;
-    return issue_norms(c, 1, 0, cnt, true);
+    return issue_norms(c, 1, 0, cnt, true, -1.0);
   }
   return spec_finish_issue(Q);
 }
@@ -443,6 +464,7 @@ int spec_collect(SpecSolve& Q) {
     return spec_apply_issue(Q);
   }
   if (Q.doubling) {
+    Q.f1 = c->h_pinned[0];  // f(1)
     for (int t = 0; t < Q.count; ++t) {
       const long long d = 1LL << t;
       if (d > Q.dmax) break;
@@ -471,7 +493,7 @@ int spec_collect(SpecSolve& Q) {
     Q.step = (span + kSpecPoints - 1) / kSpecPoints;
     Q.count = int(span / Q.step);
     Q.d0 = Q.lo + Q.step;
-    return issue_norms(c, Q.d0, Q.step, Q.count, false);
+    return issue_norms(c, Q.d0, Q.step, Q.count, false, skip_threshold(Q));
   }
   return spec_finish_issue(Q);
 }
@@ -487,7 +509,7 @@ int spec_finish_issue(SpecSolve& Q) {
   Q.d = Q.smax;
   Q.converged = false;
   Q.final_eval = true;
-  return issue_norms(c, Q.smax, 1, 1, false);
+  return issue_norms(c, Q.smax, 1, 1, false, -1.0);
 }
 
 int spec_apply_issue(SpecSolve& Q) {
