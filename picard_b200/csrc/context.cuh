@@ -34,8 +34,15 @@ struct BcFft;
 // Closed-form Jacobi solve (spectral.cu): per-axis orthonormal bases of the
 // sweep operator and the compact FP64 interior arrays the transforms use.
 struct SpectralPlan {
-  double* Q[3] = {nullptr, nullptr, nullptr};   // [n_d][n_d], row = mode
+  double* Q[3] = {nullptr, nullptr, nullptr};   // periodic axes: [n_d][n_d], row = mode
   double* QT[3] = {nullptr, nullptr, nullptr};  // transposes
+  // open axes: the sine basis folded by its even/odd symmetry (spectral.cu
+  // folded_basis), modes in the order [even | odd]
+  int folded[3] = {0, 0, 0};
+  double* Qe[3] = {nullptr, nullptr, nullptr};
+  double* QeT[3] = {nullptr, nullptr, nullptr};
+  double* QoR[3] = {nullptr, nullptr, nullptr};
+  double* QoRT[3] = {nullptr, nullptr, nullptr};
   double* om[3] = {nullptr, nullptr, nullptr};  // a_d (2 - sigma_d) per mode
   double* T[2] = {nullptr, nullptr};            // nx*ny*nz each
   double* partial = nullptr;                    // [norm_blocks][32]

@@ -260,6 +260,26 @@ __global__ void spec_apply_kernel(KParams P, const double* __restrict__ D, doubl
   }
 }
 
+// In-place fold along one axis of an (O, n, I) array (element (o, i, t) at
+// (o n + i) I + t): for i < n/2, x[i] <- x[i] + x[n-1-i] and x[n-1-i] <-
+// x[i] - x[n-1-i] (the middle of an odd n unchanged); unfold is the same
+// butterfly after the inverse products (E + O, E - O).
+__global__ void spec_fold_kernel(double* __restrict__ x, long long O, int n, long long I) {
+  const int h = n / 2;
+  const long long pairs = O * h * I;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < pairs;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long t = q % I;
+    const long long r = q / I;
+    const int i = int(r % h);
+    const long long o = r / h;
+    double* row = x + o * n * I + t;
+    const double a = row[(long long)i * I], b = row[(long long)(n - 1 - i) * I];
+    row[(long long)i * I] = a + b;
+    row[(long long)(n - 1 - i) * I] = a - b;
+  }
+}
+
 int stream_blocks(long long n) {
   long long b = (n + kSpecThreads - 1) / kSpecThreads;
   return int(std::max<long long>(1, std::min<long long>(b, 148LL * 8)));
@@ -267,6 +287,41 @@ int stream_blocks(long long n) {
 
 // One axis basis: Q (n x n, row = mode), its transpose, and a_d (2 - sigma)
 // per mode.
+void axis_basis(int n, bool periodic, double a, std::vector<double>& Q, std::vector<double>& QT,
+                std::vector<double>& om);
+
+// The sine basis folded by its symmetry Q[m][n-1-i] = (-1)^m Q[m][i]: with
+// hs = ceil(n/2), h = floor(n/2), the even modes 2k come from the folded sums
+// x[i] + x[n-1-i] (i < h) and the middle x[h] through Qe (hs x hs), the odd
+// modes 2k+1 from the differences x[i] - x[n-1-i], held at position n-1-i,
+// through QoR[k][j] = Q[2k+1][h-1-j] (h x h).  Modes are kept in the order
+// [even | odd]; om follows that order.
+void folded_basis(int n, double a, std::vector<double>& Qe, std::vector<double>& QeT, std::vector<double>& QoR,
+                  std::vector<double>& QoRT, std::vector<double>& om) {
+  std::vector<double> Q, QT, om0;
+  axis_basis(n, false, a, Q, QT, om0);
+  const int h = n / 2, hs = n - h;
+  Qe.assign((size_t)hs * hs, 0.0);
+  QeT.assign((size_t)hs * hs, 0.0);
+  QoR.assign((size_t)std::max(h, 1) * std::max(h, 1), 0.0);
+  QoRT.assign(QoR.size(), 0.0);
+  om.assign(n, 0.0);
+  for (int k = 0; k < hs; ++k) {
+    for (int i = 0; i < hs; ++i) {
+      Qe[(size_t)k * hs + i] = Q[(size_t)(2 * k) * n + i];
+      QeT[(size_t)i * hs + k] = Q[(size_t)(2 * k) * n + i];
+    }
+    om[k] = om0[2 * k];
+  }
+  for (int k = 0; k < h; ++k) {
+    for (int j = 0; j < h; ++j) {
+      QoR[(size_t)k * h + j] = Q[(size_t)(2 * k + 1) * n + (h - 1 - j)];
+      QoRT[(size_t)j * h + k] = QoR[(size_t)k * h + j];
+    }
+    om[hs + k] = om0[2 * k + 1];
+  }
+}
+
 void axis_basis(int n, bool periodic, double a, std::vector<double>& Q, std::vector<double>& QT,
                 std::vector<double>& om) {
   const double pi = 3.14159265358979323846264338327950288;
@@ -320,28 +375,78 @@ cudaError_t gemm(const double* A, int lda, long long sa, const double* B, int ld
   return cudaGetLastError();
 }
 
-// Forward: out = Qz Qy Qx in (three passes, in -> tmp -> in -> out ping-pong
-// over T[0], T[1]); result in T[1].  Inverse: Qx^T Qy^T Qz^T; result in T[0].
-cudaError_t transform(picard_ctx* c, bool forward) {
+cudaError_t fold(picard_ctx* c, double* x, long long O, int n, long long I) {
+  if (n < 2) return cudaSuccess;
+  note_launch();
+  spec_fold_kernel<<<stream_blocks(O * (n / 2) * I), kSpecThreads, 0, c->st>>>(x, O, n, I);
+  return cudaGetLastError();
+}
+
+// One axis pass from `in` to `out`.  Axis d of length n has outer extent O
+// and inner extent I (x: O = ny nz, I = 1; y: O = nz, I = nx; z: O = 1, I =
+// nx ny).  Dense axes (periodic): out = Q in (forward) or Q^T in (inverse)
+// along the axis.  Folded axes (open): forward folds `in` in place and applies
+// Qe and QoR to its two halves; inverse applies Qe^T and QoR^T to the two
+// halves of `in` and unfolds `out` in place.
+cudaError_t axis_pass(picard_ctx* c, int d, bool forward, double* in, double* out) {
   SpectralPlan& S = c->spec;
   const int nx = c->K.nx, ny = c->K.ny, nz = c->K.nz;
+  const int n = d == 0 ? nx : d == 1 ? ny : nz;
+  const long long O = d == 0 ? (long long)ny * nz : d == 1 ? nz : 1;
+  const long long I = d == 0 ? 1 : d == 1 ? nx : (long long)nx * ny;
   const long long plane = (long long)nx * ny;
   cudaError_t e;
-  if (forward) {
-    // x: T1[r][m] = sum_i T0[r][i] Qx[m][i]   (B K-contiguous: B(k=i, n=m) = Qx[m*nx + i])
-    if ((e = gemm<true>(S.T[0], nx, 0, S.Q[0], nx, 0, S.T[1], nx, 0, ny * nz, nx, nx, 1, c->st))) return e;
-    // y: T0[k][m][i] = sum_j Qy[m][j] T1[k][j][i]
-    if ((e = gemm<false>(S.Q[1], ny, 0, S.T[1], nx, plane, S.T[0], nx, plane, ny, nx, ny, nz, c->st))) return e;
-    // z: T1[m][.] = sum_k Qz[m][k] T0[k][.]
-    return gemm<false>(S.Q[2], nz, 0, S.T[0], (int)plane, 0, S.T[1], (int)plane, 0, nz, (int)plane, nz, 1, c->st);
+  if (!S.folded[d]) {
+    if (d == 0) {
+      // x: out[r][m] = sum_i in[r][i] Q[m][i] (B K-contiguous), or sum_m in[r][m] Q[m][i]
+      return forward ? gemm<true>(in, nx, 0, S.Q[0], nx, 0, out, nx, 0, ny * nz, nx, nx, 1, c->st)
+                     : gemm<false>(in, nx, 0, S.Q[0], nx, 0, out, nx, 0, ny * nz, nx, nx, 1, c->st);
+    }
+    const double* M = forward ? S.Q[d] : S.QT[d];
+    if (d == 1) return gemm<false>(M, ny, 0, in, nx, plane, out, nx, plane, ny, nx, ny, nz, c->st);
+    return gemm<false>(M, nz, 0, in, (int)plane, 0, out, (int)plane, 0, nz, (int)plane, nz, 1, c->st);
   }
-  // z: T0[k][.] = sum_m QzT[k][m] T1[m][.]
-  if ((e = gemm<false>(S.QT[2], nz, 0, S.T[1], (int)plane, 0, S.T[0], (int)plane, 0, nz, (int)plane, nz, 1, c->st)))
-    return e;
-  // y: T1[k][j][i] = sum_m QyT[j][m] T0[k][m][i]
-  if ((e = gemm<false>(S.QT[1], ny, 0, S.T[0], nx, plane, S.T[1], nx, plane, ny, nx, ny, nz, c->st))) return e;
-  // x: T0[r][i] = sum_m T1[r][m] Qx[m][i]   (B N-contiguous: B(k=m, n=i) = Qx[m*nx + i])
-  return gemm<false>(S.T[1], nx, 0, S.Q[0], nx, 0, S.T[0], nx, 0, ny * nz, nx, nx, 1, c->st);
+  const int h = n / 2, hs = n - h;
+  if (forward && (e = fold(c, in, O, n, I))) return e;
+  const double* Me = forward ? S.Qe[d] : S.QeT[d];
+  const double* Mo = forward ? S.QoR[d] : S.QoRT[d];
+  if (d == 0) {
+    if (forward) {
+      if ((e = gemm<true>(in, nx, 0, Me, hs, 0, out, nx, 0, ny * nz, hs, hs, 1, c->st))) return e;
+      if (h > 0 && (e = gemm<true>(in + hs, nx, 0, Mo, h, 0, out + hs, nx, 0, ny * nz, h, h, 1, c->st))) return e;
+    } else {
+      if ((e = gemm<false>(in, nx, 0, S.Qe[0], hs, 0, out, nx, 0, ny * nz, hs, hs, 1, c->st))) return e;
+      if (h > 0 && (e = gemm<false>(in + hs, nx, 0, S.QoR[0], h, 0, out + hs, nx, 0, ny * nz, h, h, 1, c->st)))
+        return e;
+    }
+  } else if (d == 1) {
+    if ((e = gemm<false>(Me, hs, 0, in, nx, plane, out, nx, plane, hs, nx, hs, nz, c->st))) return e;
+    if (h > 0 && (e = gemm<false>(Mo, h, 0, in + (long long)hs * nx, nx, plane, out + (long long)hs * nx, nx, plane, h,
+                                  nx, h, nz, c->st)))
+      return e;
+  } else {
+    if ((e = gemm<false>(Me, hs, 0, in, (int)plane, 0, out, (int)plane, 0, hs, (int)plane, hs, 1, c->st))) return e;
+    if (h > 0 && (e = gemm<false>(Mo, h, 0, in + (long long)hs * plane, (int)plane, 0, out + (long long)hs * plane,
+                                  (int)plane, 0, h, (int)plane, h, 1, c->st)))
+      return e;
+  }
+  if (!forward) return fold(c, out, O, n, I);
+  return cudaSuccess;
+}
+
+// Forward: Qz Qy Qx of T[0] into T[1] (x, y, z passes ping-ponging T[0] and
+// T[1]); inverse: Qx^T Qy^T Qz^T of T[1] into T[0].
+cudaError_t transform(picard_ctx* c, bool forward) {
+  SpectralPlan& S = c->spec;
+  cudaError_t e;
+  if (forward) {
+    if ((e = axis_pass(c, 0, true, S.T[0], S.T[1]))) return e;
+    if ((e = axis_pass(c, 1, true, S.T[1], S.T[0]))) return e;
+    return axis_pass(c, 2, true, S.T[0], S.T[1]);
+  }
+  if ((e = axis_pass(c, 2, false, S.T[1], S.T[0]))) return e;
+  if ((e = axis_pass(c, 1, false, S.T[0], S.T[1]))) return e;
+  return axis_pass(c, 0, false, S.T[1], S.T[0]);
 }
 
 // Queues the evaluation of f at count (<= kSpecPoints) sweep counts and the
@@ -370,9 +475,26 @@ int spectral_alloc(picard_ctx* c) {
   const int len[3] = {K.nx, K.ny, K.nz};
   const bool per[3] = {!K.xflow, !K.yflow, !K.zflow};
   for (int d = 0; d < 3; ++d) {
+    void* p = nullptr;
+    if (!per[d]) {
+      std::vector<double> Qe, QeT, QoR, QoRT, om;
+      folded_basis(len[d], a[d], Qe, QeT, QoR, QoRT, om);
+      double** dst[5] = {&S.Qe[d], &S.QeT[d], &S.QoR[d], &S.QoRT[d], &S.om[d]};
+      const std::vector<double>* srcv[5] = {&Qe, &QeT, &QoR, &QoRT, &om};
+      for (int t = 0; t < 5; ++t) {
+        PICARD_TRY(dev_alloc(c, &p, sizeof(double) * srcv[t]->size()));
+        *dst[t] = static_cast<double*>(p);
+        // no wait: an asynchronous copy from pageable memory returns once the
+        // host data is staged, so the vectors may go out of scope
+        PICARD_CUDA(cudaMemcpyAsync(*dst[t], srcv[t]->data(), sizeof(double) * srcv[t]->size(),
+                                    cudaMemcpyHostToDevice, c->st));
+        c->stats.h2d_bytes += (int64_t)(sizeof(double) * srcv[t]->size());
+      }
+      S.folded[d] = 1;
+      continue;
+    }
     std::vector<double> Q, QT, om;
     axis_basis(len[d], per[d], a[d], Q, QT, om);
-    void* p = nullptr;
     PICARD_TRY(dev_alloc(c, &p, sizeof(double) * Q.size()));
     S.Q[d] = static_cast<double*>(p);
     PICARD_TRY(dev_alloc(c, &p, sizeof(double) * QT.size()));

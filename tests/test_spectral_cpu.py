@@ -144,3 +144,35 @@ def test_closed_form_with_periodic_axes_equals_wrapped_sweeps(periodic):
     ref = jacobi_loop(p, U0, Cg, d, periodic)
     assert d > 10
     assert rel_l2(U, ref) < 1e-12
+
+
+def folded(n):
+    """Qe, QoR of the folded sine basis: even modes from x[i] + x[n-1-i] (and
+    the middle of an odd n), odd modes from x[i] - x[n-1-i] held at n-1-i."""
+    Q, _ = axis_basis(n, False)
+    h = n // 2
+    hs = n - h
+    Qe = Q[0::2, :hs]
+    QoR = Q[1::2, :h][:, ::-1]
+    return Q, Qe, QoR, h, hs
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 8, 9, 128, 257])
+def test_folded_sine_basis_equals_the_dense_one(n):
+    # the in-place butterfly, the two half products and the inverse butterfly
+    # reproduce y = Q x and x = Q^T y with modes in the order [even | odd]
+    rng = np.random.default_rng(n)
+    x = rng.normal(size=n)
+    Q, Qe, QoR, h, hs = folded(n)
+    f = x.copy()
+    for i in range(h):
+        a, b = f[i], f[n - 1 - i]
+        f[i], f[n - 1 - i] = a + b, a - b
+    y = np.concatenate([Qe @ f[:hs], QoR @ f[hs:]])
+    dense = Q @ x
+    np.testing.assert_allclose(y, np.concatenate([dense[0::2], dense[1::2]]), rtol=0, atol=1e-13 * np.abs(x).sum())
+    g = np.concatenate([Qe.T @ y[:hs], QoR.T @ y[hs:]])
+    for i in range(h):
+        e, o = g[i], g[n - 1 - i]
+        g[i], g[n - 1 - i] = e + o, e - o
+    np.testing.assert_allclose(g, x, rtol=0, atol=1e-12 * np.abs(x).max())
