@@ -589,63 +589,44 @@ __global__ void deposit_c32_kernel(KParams P, PartC32 a, long long n, unsigned l
   }
 }
 
-// ParticlesGridify.f90:65-123, shared-memory tiled.  Particles are stored in
-// cell order (initialisation and every append go cell by cell; compaction
-// keeps the order) and move a small fraction of a cell per step, so a chunk
-// of kDepChunk consecutive particles touches a small box of nodes.  Each CTA
-// takes the bounding box of its chunk's CIC stencils (base node + 1 on every
-// axis, by species), accumulates the fixed-point weights there with 32-bit
-// shared-memory atomics -- weights lie in [0, 2^40], split into 20-bit halves
-// so neither half-sum can overflow over a chunk -- and adds every touched node
-// to global memory once, with the ghost folds applied.  A chunk whose box does
-// not fit the tile falls back to one global atomic per particle corner.
+// ParticlesGridify.f90:65-123, shared-memory tiled, one tile per warp.
+// Particles are stored in cell order (initialisation and every append go cell
+// by cell; compaction keeps the order) and move a small fraction of a cell per
+// step, so a warp's kDepWarpChunk consecutive particles (one or two cells
+// at 64 per cell) touch a small box of nodes.  Each warp takes the bounding
+// box of its particles' CIC stencils (base node + 1 on every axis, by
+// species) with warp reductions, accumulates the fixed-point weights in its
+// own slice of shared memory with 32-bit atomics -- weights lie in [0, 2^40],
+// split into 20-bit halves so neither half-sum can overflow -- and adds every
+// touched node to global memory once, with the ghost folds applied.  A warp
+// whose box does not fit its slice (a row or plane boundary, or a particle
+// far from the rest after BCoutflow filled a hole) falls back to one global
+// atomic per particle corner.  Warps synchronise only with themselves: no
+// block barrier holds a warp's loads behind another warp's atomics.
 // Integer sums are exact and order-independent: N is bit-identical to the
 // warp-aggregated kernel's.
-constexpr int kDepChunk = 1024;          // particles per CTA iteration (4 per thread)
-constexpr int kDepTile = 8192;           // tile entries (two u32 halves each: 64 KB)
+constexpr int kDepPer = 2;                       // particles per lane
+constexpr int kDepWarpChunk = 32 * kDepPer;      // particles per warp iteration
+constexpr int kDepWarpTile = 512;                // tile entries per warp (two u32 halves each: 4 KB)
+constexpr int kDepWarps = 8;                     // warps per CTA
 
-// Block-wide minima of 8 values at once (maxima enter negated): warp minima
-// into red8[warp][8], a barrier, every thread reads the 8 warps', and a
-// barrier so that red8 can be written again (two barriers instead of three
-// per value).
-__device__ inline void block_min8(int (&v)[8], int (*red8)[8]) {
-#pragma unroll
-  for (int q = 0; q < 8; ++q)
-    for (int o = 16; o > 0; o >>= 1) v[q] = min(v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l < 8) {
-    int x = v[0];
-#pragma unroll
-    for (int q = 1; q < 8; ++q)
-      if (l == q) x = v[q];
-    red8[w][l] = x;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    int m = red8[0][q];
-    for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) m = min(m, red8[ww][q]);
-    v[q] = m;
-  }
-  __syncthreads();
-}
-
-__global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC32 a, long long n,
-                                                               unsigned long long* Nacc) {
-  extern __shared__ unsigned int dep_tile[];  // [2][kDepTile]: low and high 20-bit halves
-  __shared__ int red8[8][8];
-  unsigned int* lo = dep_tile;
-  unsigned int* hi = dep_tile + kDepTile;
-  constexpr int kPer = kDepChunk / 256;
-  for (long long base = (long long)blockIdx.x * kDepChunk; base < n; base += (long long)gridDim.x * kDepChunk) {
-    C32 c[kPer];
-    int sp[kPer];
-    bool act[kPer];
+__global__ void __launch_bounds__(256, 4) deposit_tile_c32_kernel(KParams P, PartC32 a, long long n,
+                                                                  unsigned long long* Nacc) {
+  extern __shared__ unsigned int dep_tile[];  // per warp: [2][kDepWarpTile] low and high 20-bit halves
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned int* lo = dep_tile + warp * 2 * kDepWarpTile;
+  unsigned int* hi = lo + kDepWarpTile;
+  const long long warps = (long long)gridDim.x * kDepWarps;
+  for (long long base = ((long long)blockIdx.x * kDepWarps + warp) * kDepWarpChunk; base < n;
+       base += warps * kDepWarpChunk) {
+    C32 c[kDepPer];
+    int sp[kDepPer];
+    bool act[kDepPer];
     int imin = INT_MAX, imax = INT_MIN, jmin = INT_MAX, jmax = INT_MIN, kmin = INT_MAX, kmax = INT_MIN;
     int smin = INT_MAX, smax = INT_MIN;
 #pragma unroll
-    for (int m = 0; m < kPer; ++m) {
-      const long long p = base + threadIdx.x + 256 * m;
+    for (int m = 0; m < kDepPer; ++m) {
+      const long long p = base + lane + 32 * m;
       act[m] = p < n;
       if (act[m]) {
         c[m] = load_pos_cs(a, p);
@@ -656,23 +637,20 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
         smin = min(smin, sp[m]), smax = max(smax, sp[m]);
       }
     }
-    {
-      // the bounding box of the chunk (INT_MIN maxima of idle threads negate
-      // to INT_MAX + 1: clamp them first)
-      int v[8] = {imin, -max(imax, -INT_MAX), jmin, -max(jmax, -INT_MAX),
-                  kmin, -max(kmax, -INT_MAX), smin, -max(smax, -INT_MAX)};
-      block_min8(v, red8);
-      imin = v[0], imax = -v[1], jmin = v[2], jmax = -v[3], kmin = v[4], kmax = -v[5], smin = v[6], smax = -v[7];
-    }
+    // the warp's bounding box (lane 0 always holds a particle: base < n)
+    imin = __reduce_min_sync(0xffffffffu, imin), imax = __reduce_max_sync(0xffffffffu, imax);
+    jmin = __reduce_min_sync(0xffffffffu, jmin), jmax = __reduce_max_sync(0xffffffffu, jmax);
+    kmin = __reduce_min_sync(0xffffffffu, kmin), kmax = __reduce_max_sync(0xffffffffu, kmax);
+    smin = __reduce_min_sync(0xffffffffu, smin), smax = __reduce_max_sync(0xffffffffu, smax);
     const long long bi = (long long)imax - imin + 2, bj = (long long)jmax - jmin + 2, bk = (long long)kmax - kmin + 2,
                     bs = (long long)smax - smin + 1;
     const long long vol = bi * bj * bk * bs;
-    if (vol <= kDepTile) {
+    if (vol <= kDepWarpTile) {
       const int vi = int(vol);
-      for (int e = threadIdx.x; e < vi; e += 256) lo[e] = 0u, hi[e] = 0u;
-      __syncthreads();
+      for (int e = lane; e < vi; e += 32) lo[e] = 0u, hi[e] = 0u;
+      __syncwarp();
 #pragma unroll
-      for (int m = 0; m < kPer; ++m) {
+      for (int m = 0; m < kDepPer; ++m) {
         if (!act[m]) continue;
         long long w[8];
         double F[8];
@@ -687,8 +665,8 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
           atomicAdd(hi + e, unsigned(wq >> 20));
         }
       }
-      __syncthreads();
-      for (int e = threadIdx.x; e < vi; e += 256) {
+      __syncwarp();
+      for (int e = lane; e < vi; e += 32) {
         const unsigned l = lo[e], h = hi[e];
         if ((l | h) == 0u) continue;
         int r = e;
@@ -703,10 +681,10 @@ __global__ void __launch_bounds__(256) deposit_tile_c32_kernel(KParams P, PartC3
         const unsigned long long v = ((unsigned long long)h << 20) + (unsigned long long)l;
         atomicAdd(Nacc + (long long)ss * P.nodes + node_index(P, i, j, k), v);
       }
-      __syncthreads();
+      __syncwarp();
     } else {
 #pragma unroll
-      for (int m = 0; m < kPer; ++m) {
+      for (int m = 0; m < kDepPer; ++m) {
         if (!act[m]) continue;
         long long w[8];
         double F[8];
@@ -834,7 +812,7 @@ cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigne
                                unsigned long long* Facc, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   if (!Facc) {
-    const size_t smem = 2 * sizeof(unsigned int) * kDepTile;
+    const size_t smem = size_t(kDepWarps) * 2 * sizeof(unsigned int) * kDepWarpTile;
     static bool attr = false;
     if (!attr) {
       cudaError_t e = cudaFuncSetAttribute(deposit_tile_c32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -842,8 +820,15 @@ cudaError_t launch_deposit_c32(const KParams& P, PartC32 a, long long n, unsigne
       if (e != cudaSuccess) return e;
       attr = true;
     }
-    long long chunks = (n + kDepChunk - 1) / kDepChunk;
-    int grid = int(chunks < 148LL * 3 ? chunks : 148LL * 3);
+    static int per_sm = 0;
+    if (!per_sm) {
+      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, deposit_tile_c32_kernel, 256, smem);
+      if (e != cudaSuccess) return e;
+      if (per_sm < 1) per_sm = 1;
+    }
+    const long long chunks = (n + kDepWarps * kDepWarpChunk - 1) / (kDepWarps * kDepWarpChunk),
+                    full = 148LL * per_sm;
+    const int grid = int(chunks < full ? chunks : full);
     note_launch();
     deposit_tile_c32_kernel<<<grid, 256, smem, st>>>(P, a, n, Nacc);
     return cudaGetLastError();
