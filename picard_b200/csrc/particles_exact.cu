@@ -205,14 +205,20 @@ struct StoreC32 {
 
 // Guard cell number g of the enumeration -> 1-based (ii, jj, kk) and the
 // lower-edge coordinates of the cell (BCinflow.f90:56-61, 127-132, ...).
-__device__ inline void inflow_cell(const KParams& P, const InflowTable& T, long long g, int& ii, int& jj, int& kk,
+// Candidate indices of one BCinflow call are decoded in 32-bit arithmetic.
+constexpr long long kMaxInflowCandidates = 0xFFFFFFFFLL;
+
+// Guard cell g of the inflow enumeration; the launchers keep every candidate
+// index (and so g) below 2^32, so the decode divides in 32 bits.
+__device__ inline void inflow_cell(const KParams& P, const InflowTable& T, uint32_t g, int& ii, int& jj, int& kk,
                                    double& x0, double& y0, double& z0) {
   int f = 0;
-  while (f < T.nfaces - 1 && g >= T.f[f + 1].first) ++f;
+  while (f < T.nfaces - 1 && (long long)g >= T.f[f + 1].first) ++f;
   const InflowFace& F = T.f[f];
-  long long l = g - F.first;
-  int o = F.o_lo + int(l / F.i_n);
-  int in = F.i_lo + int(l % F.i_n);
+  const uint32_t l = g - uint32_t(F.first), inner = uint32_t(F.i_n);
+  const uint32_t lo = l / inner;
+  int o = F.o_lo + int(lo);
+  int in = F.i_lo + int(l - lo * inner);
   if (F.axis == 0) {  // outer kk, inner jj
     ii = F.fixed;
     kk = o;
@@ -242,8 +248,8 @@ template <class Store>
 __global__ void inflow_kernel(KParams P, InflowTable T, int iteration, long long start, long long total, Store store) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= total) return;
-  long long g = t / T.per_cell;
-  int local = int(t - g * T.per_cell);
+  const uint32_t tu = uint32_t(t), pc = uint32_t(T.per_cell), g = tu / pc;
+  const int local = int(tu - g * pc);
   int ii, jj, kk;
   double x0, y0, z0;
   inflow_cell(P, T, g, ii, jj, kk, x0, y0, z0);
@@ -283,8 +289,8 @@ __device__ inline void transfer_wrap(const KParams& P, double& x, double& y, dou
 // tested and wrapped; true = it survives.
 __device__ inline bool inflow_candidate(const KParams& P, const InflowTable& T, int iteration, long long t,
                                         double x[3], double v[3], int& sp) {
-  long long g = t / T.per_cell;
-  int local = int(t - g * T.per_cell);
+  const uint32_t tu = uint32_t(t), pc = uint32_t(T.per_cell), g = tu / pc;
+  const int local = int(tu - g * pc);
   int ii, jj, kk;
   double x0, y0, z0;
   inflow_cell(P, T, g, ii, jj, kk, x0, y0, z0);
@@ -915,6 +921,7 @@ cudaError_t launch_inflow_f64(const KParams& P, const InflowTable& T, int iterat
                               cudaStream_t st) {
   long long total = T.cells * T.per_cell;
   if (total == 0) return cudaSuccess;
+  if (total > kMaxInflowCandidates) return cudaErrorInvalidValue;
   note_launch();
   inflow_kernel<<<grid_for(total), kThreads, 0, st>>>(P, T, iteration, start, total, StoreF64{out});
   return cudaGetLastError();
@@ -924,6 +931,7 @@ cudaError_t launch_inflow_c32(const KParams& P, const InflowTable& T, int iterat
                               cudaStream_t st) {
   long long total = T.cells * T.per_cell;
   if (total == 0) return cudaSuccess;
+  if (total > kMaxInflowCandidates) return cudaErrorInvalidValue;
   note_launch();
   inflow_kernel<<<grid_for(total), kThreads, 0, st>>>(P, T, iteration, start, total, StoreC32{P, out});
   return cudaGetLastError();
@@ -947,6 +955,7 @@ static cudaError_t inflow_fused(const KParams& P, const InflowTable& T, int iter
                                 const InflowStage& S, cudaStream_t st) {
   const long long total = T.cells * T.per_cell;
   if (total == 0) return cudaSuccess;
+  if (total > kMaxInflowCandidates) return cudaErrorInvalidValue;
   const int nb = inflow_blocks(total);
   cudaError_t e;
   if (S.x) {

@@ -290,7 +290,8 @@ __device__ inline void gather_c32(const KParams& P, const C32& c, const float4* 
   for (int dk = 0; dk < 2; ++dk)
 #pragma unroll
     for (int dj = 0; dj < 2; ++dj) {
-      long long row = (long long)P.nxp * ((long long)jj[dj] + (long long)P.nyp * kk[dk]);
+      // node indices fit 32 bits: the packed cell word bounds nxp*nyp*nzp below 2^32
+      const uint32_t row = uint32_t(P.nxp) * (uint32_t(jj[dj]) + uint32_t(P.nyp) * uint32_t(kk[dk]));
       float4 e0 = __ldg(E + row + ii[0]);
       float4 e1 = __ldg(E + row + ii[1]);
       float w = wy[dj] * wz[dk];
@@ -360,73 +361,68 @@ __device__ inline void boris_c32(const KParams& P, const SpeciesF32& S, int s, i
   }
 }
 
-__global__ void __launch_bounds__(256, 4) advance_velocity_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, long long n,
+__device__ __forceinline__ void advance_velocity_one(const KParams& P, const SpeciesF32& S, const float4* E,
+                                                     int mode, uint32_t cell, uint32_t fx, uint32_t fy, uint32_t fz,
+                                                     float& vx, float& vy, float& vz, int sp) {
+  C32 c;
+  unpack_cell(cell, c.i, c.j, c.k);
+  c.f[0] = fx;
+  c.f[1] = fy;
+  c.f[2] = fz;
+  float Ep[3];
+  gather_c32(P, c, E, Ep);
+  float v[3] = {vx, vy, vz};
+  boris_c32(P, S, sp, mode, Ep, v);
+  vx = v[0];
+  vy = v[1];
+  vz = v[2];
+}
+
+// Streaming loads and stores for the particles, so that they leave the E
+// table in L2 (as in push_advance_c32_kernel); thread q takes particles
+// 4q .. 4q + 3 with 16-byte accesses, the tail of a count that is not a
+// multiple of 4 one by one.
+__global__ void __launch_bounds__(256, 3) advance_velocity_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, long long n,
                                                                       const float4* E, int mode) {
-  // streaming loads and stores for the particles, so that they leave the E
-  // table in L2 (as in push_advance_c32_kernel); thread q takes particles 2q
-  // and 2q + 1 with 8-byte accesses (the tail particle of an odd count alone)
-  const long long npair = n >> 1;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < npair + (n & 1);
-       q += (long long)gridDim.x * blockDim.x) {
-    const int m = q < npair ? 2 : 1;
-    const long long p0 = q < npair ? 2 * q : n - 1;
-    uint32_t cell[2], f[3][2];
-    float v[3][2];
-    int sp[2];
-    if (m == 2) {
-      const uint2 c2 = __ldcs(reinterpret_cast<const uint2*>(a.cell) + q);
-      const uint2 x2 = __ldcs(reinterpret_cast<const uint2*>(a.fx) + q);
-      const uint2 y2 = __ldcs(reinterpret_cast<const uint2*>(a.fy) + q);
-      const uint2 z2 = __ldcs(reinterpret_cast<const uint2*>(a.fz) + q);
-      const float2 u2 = __ldcs(reinterpret_cast<const float2*>(a.vx) + q);
-      const float2 w2 = __ldcs(reinterpret_cast<const float2*>(a.vy) + q);
-      const float2 t2 = __ldcs(reinterpret_cast<const float2*>(a.vz) + q);
-      const char2 s2 = __ldcs(reinterpret_cast<const char2*>(a.sp) + q);
-      cell[0] = c2.x, cell[1] = c2.y, f[0][0] = x2.x, f[0][1] = x2.y, f[1][0] = y2.x, f[1][1] = y2.y;
-      f[2][0] = z2.x, f[2][1] = z2.y, v[0][0] = u2.x, v[0][1] = u2.y, v[1][0] = w2.x, v[1][1] = w2.y;
-      v[2][0] = t2.x, v[2][1] = t2.y, sp[0] = s2.x, sp[1] = s2.y;
-    } else {
-      cell[0] = __ldcs(a.cell + p0), f[0][0] = __ldcs(a.fx + p0), f[1][0] = __ldcs(a.fy + p0);
-      f[2][0] = __ldcs(a.fz + p0), v[0][0] = __ldcs(a.vx + p0), v[1][0] = __ldcs(a.vy + p0);
-      v[2][0] = __ldcs(a.vz + p0), sp[0] = __ldcs(a.sp + p0);
-    }
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      if (u >= m) break;
-      C32 c;
-      unpack_cell(cell[u], c.i, c.j, c.k);
-      c.f[0] = f[0][u];
-      c.f[1] = f[1][u];
-      c.f[2] = f[2][u];
-      float Ep[3];
-      gather_c32(P, c, E, Ep);
-      float vv[3] = {v[0][u], v[1][u], v[2][u]};
-      boris_c32(P, S, sp[u], mode, Ep, vv);
-      v[0][u] = vv[0];
-      v[1][u] = vv[1];
-      v[2][u] = vv[2];
-    }
-    if (m == 2) {
-      __stcs(reinterpret_cast<float2*>(a.vx) + q, make_float2(v[0][0], v[0][1]));
-      __stcs(reinterpret_cast<float2*>(a.vy) + q, make_float2(v[1][0], v[1][1]));
-      __stcs(reinterpret_cast<float2*>(a.vz) + q, make_float2(v[2][0], v[2][1]));
-    } else {
-      __stcs(a.vx + p0, v[0][0]);
-      __stcs(a.vy + p0, v[1][0]);
-      __stcs(a.vz + p0, v[2][0]);
-    }
+  const long long nquad = n >> 2;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nquad; q += stride) {
+    const uint4 cell = __ldcs(reinterpret_cast<const uint4*>(a.cell) + q);
+    const uint4 fx = __ldcs(reinterpret_cast<const uint4*>(a.fx) + q);
+    const uint4 fy = __ldcs(reinterpret_cast<const uint4*>(a.fy) + q);
+    const uint4 fz = __ldcs(reinterpret_cast<const uint4*>(a.fz) + q);
+    float4 vx = __ldcs(reinterpret_cast<const float4*>(a.vx) + q);
+    float4 vy = __ldcs(reinterpret_cast<const float4*>(a.vy) + q);
+    float4 vz = __ldcs(reinterpret_cast<const float4*>(a.vz) + q);
+    const char4 sp = __ldcs(reinterpret_cast<const char4*>(a.sp) + q);
+    advance_velocity_one(P, S, E, mode, cell.x, fx.x, fy.x, fz.x, vx.x, vy.x, vz.x, sp.x);
+    advance_velocity_one(P, S, E, mode, cell.y, fx.y, fy.y, fz.y, vx.y, vy.y, vz.y, sp.y);
+    advance_velocity_one(P, S, E, mode, cell.z, fx.z, fy.z, fz.z, vx.z, vy.z, vz.z, sp.z);
+    advance_velocity_one(P, S, E, mode, cell.w, fx.w, fy.w, fz.w, vx.w, vy.w, vz.w, sp.w);
+    __stcs(reinterpret_cast<float4*>(a.vx) + q, vx);
+    __stcs(reinterpret_cast<float4*>(a.vy) + q, vy);
+    __stcs(reinterpret_cast<float4*>(a.vz) + q, vz);
+  }
+  for (long long p = 4 * nquad + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    float vx = __ldcs(a.vx + p), vy = __ldcs(a.vy + p), vz = __ldcs(a.vz + p);
+    advance_velocity_one(P, S, E, mode, __ldcs(a.cell + p), __ldcs(a.fx + p), __ldcs(a.fy + p), __ldcs(a.fz + p), vx,
+                         vy, vz, __ldcs(a.sp + p));
+    __stcs(a.vx + p, vx);
+    __stcs(a.vy + p, vy);
+    __stcs(a.vz + p, vz);
   }
 }
 
 // AdvanceVelocity of one step followed by AdvancePosition of the next, in one
 // pass over the particles: the same operations as advance_velocity_c32_kernel
 // (mode 0) then advance_position_c32_kernel, so the same bits, with one read
-// and one write of each particle instead of two.  Thread q takes particles 2q
-// and 2q + 1 with 8-byte loads and stores, so twice the particle bytes are in
-// flight per thread before the E gathers that depend on them: 80 registers, 3
-// blocks of 256 per SM, and the E-field + push phase takes 3.6 ms at 268 M
-// particles against 4.6 ms for one particle per thread (64 registers, 4
-// blocks per SM; 6.4 ms at 32 registers with spills, 5.1 ms at 40).
+// and one write of each particle instead of two.  Thread q takes particles
+// 4q .. 4q + 3 with 16-byte loads and stores, so four particles' bytes are in
+// flight per thread before the E gathers that depend on them: 80 registers
+// (no spills), 3 blocks of 256 per SM, and the E-field + push phase takes
+// 3.05 ms at 268 M particles, against 3.56 ms for particle pairs (8-byte
+// accesses, 80 registers), 3.40 ms for quads at 126 registers (2 blocks per
+// SM) and 4.6 ms for one particle per thread (64 registers, 4 blocks per SM).
 __device__ __forceinline__ void push_advance_one(const KParams& P, const SpeciesF32& S, const float4* E, float dtdx,
                                                  float dtdy, float dtdz, uint32_t& cell, uint32_t& fx, uint32_t& fy,
                                                  uint32_t& fz, float& vx, float& vy, float& vz, int sp) {
@@ -454,40 +450,40 @@ __device__ __forceinline__ void push_advance_one(const KParams& P, const Species
 __global__ void __launch_bounds__(256, 3) push_advance_c32_kernel(KParams P, SpeciesF32 S, PartC32 a, long long n,
                                                                    const float4* E, float dtdx, float dtdy,
                                                                    float dtdz) {
-  const long long npair = n >> 1;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < npair + (n & 1);
-       q += (long long)gridDim.x * blockDim.x) {
-    if (q < npair) {
-      uint2 cell = __ldcs(reinterpret_cast<const uint2*>(a.cell) + q);
-      uint2 fx = __ldcs(reinterpret_cast<const uint2*>(a.fx) + q);
-      uint2 fy = __ldcs(reinterpret_cast<const uint2*>(a.fy) + q);
-      uint2 fz = __ldcs(reinterpret_cast<const uint2*>(a.fz) + q);
-      float2 vx = __ldcs(reinterpret_cast<const float2*>(a.vx) + q);
-      float2 vy = __ldcs(reinterpret_cast<const float2*>(a.vy) + q);
-      float2 vz = __ldcs(reinterpret_cast<const float2*>(a.vz) + q);
-      const char2 sp = __ldcs(reinterpret_cast<const char2*>(a.sp) + q);
-      push_advance_one(P, S, E, dtdx, dtdy, dtdz, cell.x, fx.x, fy.x, fz.x, vx.x, vy.x, vz.x, sp.x);
-      push_advance_one(P, S, E, dtdx, dtdy, dtdz, cell.y, fx.y, fy.y, fz.y, vx.y, vy.y, vz.y, sp.y);
-      __stcs(reinterpret_cast<float2*>(a.vx) + q, vx);
-      __stcs(reinterpret_cast<float2*>(a.vy) + q, vy);
-      __stcs(reinterpret_cast<float2*>(a.vz) + q, vz);
-      __stcs(reinterpret_cast<uint2*>(a.cell) + q, cell);
-      __stcs(reinterpret_cast<uint2*>(a.fx) + q, fx);
-      __stcs(reinterpret_cast<uint2*>(a.fy) + q, fy);
-      __stcs(reinterpret_cast<uint2*>(a.fz) + q, fz);
-    } else {
-      const long long p = n - 1;
-      uint32_t cell = __ldcs(a.cell + p), fx = __ldcs(a.fx + p), fy = __ldcs(a.fy + p), fz = __ldcs(a.fz + p);
-      float vx = __ldcs(a.vx + p), vy = __ldcs(a.vy + p), vz = __ldcs(a.vz + p);
-      push_advance_one(P, S, E, dtdx, dtdy, dtdz, cell, fx, fy, fz, vx, vy, vz, __ldcs(a.sp + p));
-      __stcs(a.vx + p, vx);
-      __stcs(a.vy + p, vy);
-      __stcs(a.vz + p, vz);
-      __stcs(a.cell + p, cell);
-      __stcs(a.fx + p, fx);
-      __stcs(a.fy + p, fy);
-      __stcs(a.fz + p, fz);
-    }
+  const long long nquad = n >> 2;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nquad; q += stride) {
+    uint4 cell = __ldcs(reinterpret_cast<const uint4*>(a.cell) + q);
+    uint4 fx = __ldcs(reinterpret_cast<const uint4*>(a.fx) + q);
+    uint4 fy = __ldcs(reinterpret_cast<const uint4*>(a.fy) + q);
+    uint4 fz = __ldcs(reinterpret_cast<const uint4*>(a.fz) + q);
+    float4 vx = __ldcs(reinterpret_cast<const float4*>(a.vx) + q);
+    float4 vy = __ldcs(reinterpret_cast<const float4*>(a.vy) + q);
+    float4 vz = __ldcs(reinterpret_cast<const float4*>(a.vz) + q);
+    const char4 sp = __ldcs(reinterpret_cast<const char4*>(a.sp) + q);
+    push_advance_one(P, S, E, dtdx, dtdy, dtdz, cell.x, fx.x, fy.x, fz.x, vx.x, vy.x, vz.x, sp.x);
+    push_advance_one(P, S, E, dtdx, dtdy, dtdz, cell.y, fx.y, fy.y, fz.y, vx.y, vy.y, vz.y, sp.y);
+    push_advance_one(P, S, E, dtdx, dtdy, dtdz, cell.z, fx.z, fy.z, fz.z, vx.z, vy.z, vz.z, sp.z);
+    push_advance_one(P, S, E, dtdx, dtdy, dtdz, cell.w, fx.w, fy.w, fz.w, vx.w, vy.w, vz.w, sp.w);
+    __stcs(reinterpret_cast<float4*>(a.vx) + q, vx);
+    __stcs(reinterpret_cast<float4*>(a.vy) + q, vy);
+    __stcs(reinterpret_cast<float4*>(a.vz) + q, vz);
+    __stcs(reinterpret_cast<uint4*>(a.cell) + q, cell);
+    __stcs(reinterpret_cast<uint4*>(a.fx) + q, fx);
+    __stcs(reinterpret_cast<uint4*>(a.fy) + q, fy);
+    __stcs(reinterpret_cast<uint4*>(a.fz) + q, fz);
+  }
+  for (long long p = 4 * nquad + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    uint32_t cell = __ldcs(a.cell + p), fx = __ldcs(a.fx + p), fy = __ldcs(a.fy + p), fz = __ldcs(a.fz + p);
+    float vx = __ldcs(a.vx + p), vy = __ldcs(a.vy + p), vz = __ldcs(a.vz + p);
+    push_advance_one(P, S, E, dtdx, dtdy, dtdz, cell, fx, fy, fz, vx, vy, vz, __ldcs(a.sp + p));
+    __stcs(a.vx + p, vx);
+    __stcs(a.vy + p, vy);
+    __stcs(a.vz + p, vz);
+    __stcs(a.cell + p, cell);
+    __stcs(a.fx + p, fx);
+    __stcs(a.fy + p, fy);
+    __stcs(a.fz + p, fz);
   }
 }
 
@@ -794,7 +790,7 @@ cudaError_t launch_advance_velocity_c32(const KParams& P, PartC32 a, long long n
   if (n <= 0) return cudaSuccess;
   SpeciesF32 S = species_f32(P, dt, deltat, mode);
   note_launch();
-  advance_velocity_c32_kernel<<<persistent_grid((n + 1) / 2), kThreads, 0, st>>>(P, S, a, n, E, mode);
+  advance_velocity_c32_kernel<<<persistent_grid((n + 3) / 4), kThreads, 0, st>>>(P, S, a, n, E, mode);
   return cudaGetLastError();
 }
 
@@ -803,7 +799,7 @@ cudaError_t launch_push_advance_c32(const KParams& P, PartC32 a, long long n, co
   if (n <= 0) return cudaSuccess;
   SpeciesF32 S = species_f32(P, dt, 0.0, 0);
   note_launch();
-  push_advance_c32_kernel<<<persistent_grid((n + 1) / 2), kThreads, 0, st>>>(P, S, a, n, E, float(dt / P.dx),
+  push_advance_c32_kernel<<<persistent_grid((n + 3) / 4), kThreads, 0, st>>>(P, S, a, n, E, float(dt / P.dx),
                                                                             float(dt / P.dy), float(dt / P.dz));
   return cudaGetLastError();
 }
