@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--poisson-n", type=int, default=256)
     ap.add_argument("--poisson-dims", type=str, default=None, help="poisson workload: nx,ny,nz (default n^3)")
     ap.add_argument("--poisson-sweeps", type=int, default=400)
+    ap.add_argument("--deposit-dims", type=str, default=None,
+                    help="deposit workload: nx,ny,nz (default 256,128,128)")
     ap.add_argument("--layout", choices=["cell32", "f64"], default="cell32")
     ap.add_argument("--solver", choices=["refine", "f64", "spectral"], default="spectral")
     ap.add_argument("--sort-every", type=int, default=0,
@@ -1037,8 +1039,9 @@ def run_bcpot(args, local_rank):
 
 
 def run_deposit(args, local_rank):
-    """CELL32 ParticlesGridify alone on the at-scale grid with --ppc ions per
-    cell (default 32), after two fused steps; device time per call."""
+    """CELL32 ParticlesGridify alone on the at-scale grid (or --deposit-dims)
+    with --ppc ions per cell (default 32), after two fused steps; device time
+    per call."""
     import torch
 
     from picard_b200 import capi
@@ -1047,7 +1050,8 @@ def run_deposit(args, local_rank):
 
     torch.cuda.set_device(local_rank)
     ppc = args.ppc or 32
-    sim = Simulation(P.config_plain_scale(seed=0, ppc_ion=ppc), layout=capi.LAYOUT_CELL32,
+    nx, ny, nz = (int(v) for v in (args.deposit_dims or "256,128,128").split(","))
+    sim = Simulation(P.config_plain_scale(seed=0, nx=nx, ny=ny, nz=nz, ppc_ion=ppc), layout=capi.LAYOUT_CELL32,
                      solver=capi.SOLVER_SPECTRAL)
     sim.calc_distance()
     sim.particles_initialize()
@@ -1065,7 +1069,7 @@ def run_deposit(args, local_rank):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / reps
     n = sim.num_local
-    print(json.dumps({"workload": f"deposit 256x128x128, {ppc}+{ppc} ppc", "particles": n, "gridify_ms": ms,
+    print(json.dumps({"workload": f"deposit {nx}x{ny}x{nz}, {ppc}+{ppc} ppc", "particles": n, "gridify_ms": ms,
                       "read_gbs": 17.0 * n / (ms * 1e-3) / 1e9}), flush=True)
     sim.close()
 
