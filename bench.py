@@ -328,9 +328,9 @@ def run_picard(args, rank, world, local_rank):
                                            "32-bit offsets, species) x the live particles",
                          "traffic": (DEPOSIT_DRAM_BYTES_PER_PARTICLE * n_dep
                                      if DEPOSIT_DRAM_BYTES_PER_PARTICLE and args.layout == "cell32" else None),
-                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per particle (20.25 B) of "
-                                           "one ncu capture of the deposit at 256x128x128 x 8 ppc, scaled by the "
-                                           "particles (an upper bound at 64 ppc)",
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per particle (17.49 B) of "
+                                           "one ncu capture of the deposit at 128x64x64 x 64 ppc (the default "
+                                           "workload's density), scaled by the particles",
                          "note": "launch_ms is the ParticlesGridify entry point (deposit kernel and the "
                                  "fixed-point finish) timed with CUDA events on the library stream, K launches on "
                                  "the timed run's final particles; the step's other phases are in "
@@ -354,11 +354,11 @@ def run_picard(args, rank, world, local_rank):
 # the species of every particle.
 DEPOSIT_BYTES_PER_PARTICLE = 17
 # DRAM bytes per particle of one deposit launch (dram__bytes_read.sum +
-# dram__bytes_write.sum over the particles): 644.2 + 35.4 MB over 33,554,889
-# particles in an ncu capture at 256x128x128 with 4 + 4 ppc.  The node-array
-# share of it shrinks per particle at 32 + 32 ppc, so the scaled figure is an
-# upper bound there.
-DEPOSIT_DRAM_BYTES_PER_PARTICLE = 20.25
+# dram__bytes_write.sum over the particles): 581.7 + 5.1 MB over 33,556,485
+# particles in an ncu capture at 128x64x64 with 32 + 32 ppc, the density of
+# the default workload (the node arrays' share per particle depends on the
+# density, not on the grid).
+DEPOSIT_DRAM_BYTES_PER_PARTICLE = 17.49
 
 
 def deposit_launch_ms(sim, ext, reps: int, torch) -> float:
