@@ -115,7 +115,8 @@ struct Site {
       philox4x32_10(w, k0, k1);
       blk = bk;
     }
-    uint32_t w0 = w[2 * (n & 1)], w1 = w[2 * (n & 1) + 1];
+    // selects, not an index: a draw number known only at run time keeps w in registers
+    const uint32_t w0 = (n & 1) ? w[2] : w[0], w1 = (n & 1) ? w[3] : w[1];
     return ((double)(w0 >> 5) * 67108864.0 + (double)(w1 >> 6)) * (1.0 / 9007199254740992.0);
   }
 };

@@ -76,15 +76,14 @@ __device__ void gen_member(const KParams& P, uint32_t tag, uint32_t it, uint32_t
   x[0] = x0 + P.dx * ion.u(0);
   x[1] = y0 + P.dy * ion.u(1);
   x[2] = z0 + P.dz * ion.u(2);
-  if (m == 0) {
-    gaussian_from(ion, 3, v, P.v0[s0], P.kelvin[s0], P.mass[s0]);
-    half_rotate(v, P.ve, P.tB[s0]);
-    sp = s0;
-    return;
-  }
-  Site mem(P.seed, a, (uint32_t(ss) << 24) | (uint32_t(pp) << 8) | uint32_t(m), it, tag);
-  int t = m <= P.epp[s0] ? 0 : 1;  // 0 = electron, 1 = proton
-  gaussian_from(mem, 0, v, P.v0[s0], P.kelvin[t], P.mass[t]);
+  // The ion draws its velocity from its own site after the position (from
+  // u(3)); an electron or proton from a site of its own (from u(0)).  One
+  // code path for both, so that a warp holding ions and their members runs
+  // the Gaussian draws and the rotation once, not once per kind.
+  const bool is_ion = m == 0;
+  const int t = is_ion ? s0 : (m <= P.epp[s0] ? 0 : 1);  // member: 0 = electron, 1 = proton
+  Site src = is_ion ? ion : Site(P.seed, a, (uint32_t(ss) << 24) | (uint32_t(pp) << 8) | uint32_t(m), it, tag);
+  gaussian_from(src, is_ion ? 3u : 0u, v, P.v0[s0], P.kelvin[t], P.mass[t]);
   half_rotate(v, P.ve, P.tB[t]);
   sp = t;
 }
